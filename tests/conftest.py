@@ -1,0 +1,21 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libfmmb.so")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    """The CPU checker (restatement + reference build), compiled on demand."""
+    from oracle import pyoracle
+    if not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")):
+        pyoracle.build()
+    return pyoracle
