@@ -1,0 +1,145 @@
+/*
+ * fmmb.h -- C ABI of libfmmb.so, a B200-native fast multipole matvec for the
+ * Laplace kernels of exafmm/old_fmm_bem.
+ *
+ * The reference exposes its FMM as `void fmm(int mi, int mj, int neq)`
+ * (fmm/fmm.cxx:29) over global, pre-sorted particle arrays, with the GPU work
+ * behind the batch ABI p2pgpu_/p2mgpu_/m2lgpu_/l2pgpu_ (libgpu/gpufmm.cu:57,
+ * 200, 336, 481).  This ABI replaces both with a handle: a plan owns the tree,
+ * the translation operators and all device buffers; fmmb_set_geometry builds
+ * the octree on the GPU; fmmb_evaluate runs P2P, P2M, M2M, M2L, L2L and L2P on
+ * the GPU.  Kernel numbering follows the reference's `neq` (fmm/fmm.cxx:47-65).
+ *
+ * Conventions
+ *  - Arrays are structure-of-arrays float32, like the reference's xi/yi/zi...
+ *    (include/arrays.h:5-12).  Pointers may be host or device memory; host
+ *    inputs are copied to the device and host outputs copied back inside the
+ *    call (cudaPointerGetAttributes decides).
+ *  - Every call returns FMMB_OK (0) or a negative error code; the message of
+ *    the last error on the calling thread is fmmb_last_error().  Nothing
+ *    aborts the process (the reference exits through CUDA_SAFE_CALL).
+ *  - A plan is used by one host thread at a time; different plans are
+ *    independent.  Work is queued on the plan's stream (fmmb_set_stream).
+ */
+#ifndef FMMB_H
+#define FMMB_H
+
+#if defined(__GNUC__)
+#define FMMB_API __attribute__((visibility("default")))
+#else
+#define FMMB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FMMB_OK 0
+#define FMMB_ERR_ARG (-1)       /* invalid argument or configuration */
+#define FMMB_ERR_CUDA (-2)      /* a CUDA call failed */
+#define FMMB_ERR_STATE (-3)     /* call out of order (e.g. evaluate before geometry) */
+#define FMMB_ERR_CAPACITY (-4)  /* a size exceeds what the plan supports */
+#define FMMB_ERR_NOMEM (-5)     /* device allocation failed */
+
+/* Kernels, numbered like the reference's neq (fmm/fmm.cxx:47-65). */
+#define FMMB_LAPLACE_G 0    /* potential sum q/(4 pi r) and its gradient */
+#define FMMB_LAPLACE_GNI 1  /* target-normal derivative: sum q (r.n_i)/(4 pi r^3) */
+#define FMMB_LAPLACE_GNJ 2  /* source-normal (double layer): sum q (r.n_j)/(4 pi r^3) */
+
+/* Precision of the evaluation. */
+#define FMMB_FP64 0   /* every phase in FP64 on the CUDA cores */
+#define FMMB_MIXED 1  /* FP32 P2P with compensated sums, M2L as TF32x3 tensor-core GEMMs */
+
+/* Arithmetic semantics. */
+#define FMMB_SEM_REFERENCE 0 /* the reference's conventions: eps=1e-6f added to r^2 and to
+                                expansion radii, single-precision pi, fac/anm/sr tables
+                                rounded to float, self pairs included */
+#define FMMB_SEM_ACCURATE 1  /* exact angles and constants; eps2 as given; exclude_self honoured */
+
+typedef struct {
+  int kernel;       /* FMMB_LAPLACE_* */
+  int p;            /* expansion order, 1..20 (the reference's mp = p+1) */
+  int lmax;         /* octree depth of the leaves, 2..10 */
+  int precision;    /* FMMB_FP64 or FMMB_MIXED */
+  int semantics;    /* FMMB_SEM_REFERENCE or FMMB_SEM_ACCURATE */
+  double eps2;      /* P2P softening added to r^2 (FMMB_SEM_ACCURATE only) */
+  int exclude_self; /* skip pairs at zero distance (FMMB_SEM_ACCURATE only) */
+  int nrhs;         /* right-hand sides per evaluate, >= 1 */
+} fmmb_config;
+
+typedef struct fmmb_plan fmmb_plan;
+
+/* Fills cfg with defaults: Laplace G, p=8, lmax=3, FP64, reference semantics, nrhs=1. */
+FMMB_API int fmmb_config_init(fmmb_config* cfg);
+
+/* Replaces the reference's compile-time setup (include/constants.h:11-35,
+ * fmm/alloc.cxx:32-84, kernel/precalc.cxx:10-213): validates cfg, selects the
+ * current CUDA device, builds the rotation/translation operators. */
+FMMB_API int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** plan);
+FMMB_API int fmmb_plan_destroy(fmmb_plan* plan);
+
+/* Work of this plan is queued on `stream` (a cudaStream_t; NULL = the plan's own). */
+FMMB_API int fmmb_set_stream(fmmb_plan* plan, void* stream);
+
+/* Builds the octree on the GPU (replaces fmm/boxn.cxx, sort/csort.cxx,
+ * sort/sorti.cxx, sort/sortj.cxx, fmm/boxdata{i,j}.cxx, fmm/boxm2m{i,j}.cxx,
+ * fmm/ijbox.cxx).  Targets (tx,ty,tz) with normals (tnx..; used by
+ * FMMB_LAPLACE_GNI, may be NULL otherwise); sources (sx,sy,sz) with normals
+ * (snx..; used by FMMB_LAPLACE_GNJ).  bbox = {xmin, ymin, zmin, rd} is the
+ * root cube, like the reference's xmin/ymin/zmin/rd globals; NULL computes a
+ * cube enclosing all points.  Points are given in caller order: the
+ * permutation into Morton order is internal. */
+FMMB_API int fmmb_set_geometry(fmmb_plan* plan, int ni, const float* tx, const float* ty, const float* tz,
+                      const float* tnx, const float* tny, const float* tnz, int nj,
+                      const float* sx, const float* sy, const float* sz, const float* snx,
+                      const float* sny, const float* snz, const float* bbox);
+
+/* One FMM matvec (replaces fmm(mi, mj, neq), fmm/fmm.cxx:29-152).
+ * q: nrhs x nj charges (caller order).  pot: nrhs x ni potentials (overwritten,
+ * unlike the reference's += into vi).  grad: nrhs x 3 x ni gradient for
+ * FMMB_LAPLACE_G, may be NULL; ignored for the other kernels. */
+FMMB_API int fmmb_evaluate(fmmb_plan* plan, const float* q, float* pot, float* grad);
+/* Same with FP64 outputs. */
+FMMB_API int fmmb_evaluate_f64(fmmb_plan* plan, const float* q, double* pot, double* grad);
+
+/* Direct O(ni*nj) sum on the GPU with the plan's kernel and semantics
+ * (replaces G_dir/Gni_dir/Gnj_dir, kernel/G_dir.cxx:6-30,
+ * kernel/Gni_dir.cxx:6-21, kernel/Gnj_dir.cxx:6-21), FP64 arithmetic.  Uses
+ * the geometry and the first right-hand side of q; targets [i0, i1). */
+FMMB_API int fmmb_direct_f64(fmmb_plan* plan, const float* q, int i0, int i1, double* pot, double* grad);
+
+/* ---- inspection (tests, tooling) ---- */
+
+/* Tree of the current geometry.  kind: 0 target permutation (sorted position
+ * -> caller index, like the reference's nbi), 1 source permutation (nbj),
+ * 2 target box keys of all levels lmax..2 concatenated (nfi), 3 source box
+ * keys (nfj), 4/5 boxes per level [lmax+1], 6/7 leaf ranges (first, last)
+ * pairs (ndi/ndj), 8 interaction lists as a stream
+ * [lev, mode, nbox_i, nbox_j, counts..., entries...] per list in the order
+ * fmm() builds them (mode 0 near field at lmax, 1 level 2, 2 levels 3..lmax).
+ * fmmb_get_tree_size returns the element count (or an error). */
+FMMB_API long fmmb_get_tree_size(fmmb_plan* plan, int kind);
+FMMB_API int fmmb_get_tree(fmmb_plan* plan, int kind, int* out);
+
+/* Expansions after the last evaluate (first right-hand side), in the
+ * reference's unscaled normalisation: which 0 = multipoles of all source boxes,
+ * 1 = locals of all target boxes, levels lmax..2 concatenated; per box
+ * (p+1)(p+2)/2 complex coefficients (n, m>=0 at n(n+1)/2+m) as (re, im). */
+FMMB_API long fmmb_get_expansion_size(fmmb_plan* plan, int which);
+FMMB_API int fmmb_get_expansions(fmmb_plan* plan, int which, double* out);
+
+/* Device time in ms of the phases of the last evaluate:
+ * [0] P2P, [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] whole evaluate. */
+FMMB_API int fmmb_get_timings(fmmb_plan* plan, float* ms7);
+
+/* Counts of the current geometry: [0] ni, [1] nj, [2] target leaves,
+ * [3] source leaves, [4] P2P pairs (sum over near-field leaf pairs of
+ * ni*nj), [5] M2L box pairs, [6] lmax. */
+FMMB_API int fmmb_get_stats(fmmb_plan* plan, long long* out7);
+
+FMMB_API const char* fmmb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMMB_H */

@@ -1,0 +1,250 @@
+"""old_fmm_bem_b200 -- B200-native FMM matvec behind the reference's fmm() interface.
+
+The product is the C-ABI library ``lib/libfmmb.so`` (declared in
+``include/fmmb.h``).  This module is the thin host-side binding over it:
+
+* :class:`Plan` -- one configured FMM (kernel, order, depth, precision,
+  semantics) with a geometry; ``evaluate`` is one matvec.
+* :func:`fmm` / :func:`G_dir` / :func:`Gni_dir` / :func:`Gnj_dir` -- the
+  reference's entry points (fmm/fmm.cxx:29, kernel/G_dir.cxx:6,
+  kernel/Gni_dir.cxx:6, kernel/Gnj_dir.cxx:6) with the particle arrays passed
+  explicitly instead of through globals.
+
+Arrays may be numpy arrays (host) or torch CUDA tensors (device); the library
+decides from the pointer.  There is no CPU fallback: without the built library
+and a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Plan", "FMMError", "fmm", "G_dir", "Gni_dir", "Gnj_dir", "lib_path", "load",
+           "LAPLACE_G", "LAPLACE_GNI", "LAPLACE_GNJ", "FP64", "MIXED", "SEM_REFERENCE", "SEM_ACCURATE"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LAPLACE_G, LAPLACE_GNI, LAPLACE_GNJ = 0, 1, 2
+FP64, MIXED = 0, 1
+SEM_REFERENCE, SEM_ACCURATE = 0, 1
+EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_set_stream", "fmmb_set_geometry",
+           "fmmb_evaluate", "fmmb_evaluate_f64", "fmmb_direct_f64", "fmmb_get_tree_size", "fmmb_get_tree",
+           "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
+           "fmmb_last_error"]
+
+
+def lib_path() -> str:
+    return os.path.join(HERE, "lib", "libfmmb.so")
+
+
+class FMMError(RuntimeError):
+    pass
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("p", ctypes.c_int), ("lmax", ctypes.c_int), ("precision", ctypes.c_int),
+                ("semantics", ctypes.c_int), ("eps2", ctypes.c_double), ("exclude_self", ctypes.c_int),
+                ("nrhs", ctypes.c_int)]
+
+
+_LIB = None
+_vp = ctypes.c_void_p
+
+
+def load():
+    """Loads libfmmb.so (raises when it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = lib_path()
+    if not os.path.exists(path):
+        raise FMMError(f"{path} not built: run `python -m old_fmm_bem_b200.build`")
+    lib = ctypes.CDLL(path)
+    lib.fmmb_config_init.argtypes = [ctypes.POINTER(_Config)]
+    lib.fmmb_plan_create.argtypes = [ctypes.POINTER(_Config), ctypes.POINTER(_vp)]
+    lib.fmmb_plan_destroy.argtypes = [_vp]
+    lib.fmmb_set_stream.argtypes = [_vp, _vp]
+    lib.fmmb_set_geometry.argtypes = [_vp, ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + [_vp] * 6 + [_vp]
+    lib.fmmb_evaluate.argtypes = [_vp, _vp, _vp, _vp]
+    lib.fmmb_evaluate_f64.argtypes = [_vp, _vp, _vp, _vp]
+    lib.fmmb_direct_f64.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_get_tree_size.argtypes = [_vp, ctypes.c_int]
+    lib.fmmb_get_tree_size.restype = ctypes.c_long
+    lib.fmmb_get_tree.argtypes = [_vp, ctypes.c_int, _vp]
+    lib.fmmb_get_expansion_size.argtypes = [_vp, ctypes.c_int]
+    lib.fmmb_get_expansion_size.restype = ctypes.c_long
+    lib.fmmb_get_expansions.argtypes = [_vp, ctypes.c_int, _vp]
+    lib.fmmb_get_timings.argtypes = [_vp, _vp]
+    lib.fmmb_get_stats.argtypes = [_vp, _vp]
+    lib.fmmb_last_error.restype = ctypes.c_char_p
+    _LIB = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        msg = load().fmmb_last_error().decode(errors="replace")
+        raise FMMError(f"fmmb error {rc}: {msg}")
+
+
+def _ptr(a, dtype):
+    """Pointer of a numpy array (host) or torch tensor (device or host), after
+    checking dtype and contiguity.  None stays None."""
+    if a is None:
+        return None, None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        import torch
+        want = {np.float32: torch.float32, np.float64: torch.float64, np.int32: torch.int32}[dtype]
+        if a.dtype != want or not a.is_contiguous():
+            raise FMMError(f"expected a contiguous {want} tensor")
+        return a.data_ptr(), a
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data, arr
+
+
+class Plan:
+    """One FMM configuration bound to a geometry (include/fmmb.h)."""
+
+    def __init__(self, kernel=LAPLACE_G, p=8, lmax=3, precision=FP64, semantics=SEM_REFERENCE, eps2=0.0,
+                 exclude_self=False, nrhs=1):
+        lib = load()
+        cfg = _Config()
+        lib.fmmb_config_init(ctypes.byref(cfg))
+        cfg.kernel, cfg.p, cfg.lmax, cfg.precision = kernel, p, lmax, precision
+        cfg.semantics, cfg.eps2, cfg.exclude_self, cfg.nrhs = semantics, eps2, int(exclude_self), nrhs
+        h = _vp()
+        _check(lib.fmmb_plan_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.kernel, self.p, self.lmax, self.precision, self.semantics, self.nrhs = kernel, p, lmax, precision, semantics, nrhs
+        self.ni = self.nj = 0
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().fmmb_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream):
+        """Queue the plan's work on a cudaStream_t (int handle or torch stream)."""
+        h = getattr(stream, "cuda_stream", stream)
+        _check(load().fmmb_set_stream(self._h, ctypes.c_void_p(h)))
+
+    def set_geometry(self, targets, sources, target_normals=None, source_normals=None, bbox=None):
+        """targets/sources: (3, n) float32 (numpy or torch); bbox = (xmin, ymin, zmin, rd)."""
+        t = [_ptr(targets[k], np.float32) for k in range(3)]
+        s = [_ptr(sources[k], np.float32) for k in range(3)]
+        tn = [_ptr(target_normals[k], np.float32) for k in range(3)] if target_normals is not None else [(None, None)] * 3
+        sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
+        bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
+        ni, nj = len(targets[0]), len(sources[0])
+        _check(load().fmmb_set_geometry(self._h, ni, t[0][0], t[1][0], t[2][0], tn[0][0], tn[1][0], tn[2][0], nj,
+                                        s[0][0], s[1][0], s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0]))
+        self.ni, self.nj = ni, nj
+        return self
+
+    def evaluate(self, q, pot=None, grad=None, f64=False):
+        """One matvec.  q: (nrhs*nj,) charges.  Returns (pot, grad) -- grad only
+        for LAPLACE_G.  Outputs are numpy unless torch CUDA tensors are given."""
+        dt = np.float64 if f64 else np.float32
+        qp, qk = _ptr(q, np.float32)
+        ni = self.ni * self.nrhs
+        if pot is None:
+            pot = np.zeros(ni, dt)
+        if grad is None and self.kernel == LAPLACE_G:
+            grad = np.zeros(3 * ni, dt)
+        pp, pk = _ptr(pot, dt)
+        gp, gk = _ptr(grad, dt) if self.kernel == LAPLACE_G else (None, None)
+        fn = load().fmmb_evaluate_f64 if f64 else load().fmmb_evaluate
+        _check(fn(self._h, qp, pp, gp))
+        return pk, gk
+
+    def direct(self, q, i0=0, i1=None):
+        """FP64 direct sum on the GPU for targets [i0, i1) (caller order)."""
+        i1 = self.ni if i1 is None else i1
+        qp, qk = _ptr(q, np.float32)
+        pot = np.zeros(i1 - i0)
+        grad = np.zeros(3 * (i1 - i0))
+        _check(load().fmmb_direct_f64(self._h, qp, i0, i1, pot.ctypes.data,
+                                      grad.ctypes.data if self.kernel == LAPLACE_G else None))
+        return pot, (grad.reshape(3, -1) if self.kernel == LAPLACE_G else None)
+
+    def tree(self, kind):
+        lib = load()
+        n = lib.fmmb_get_tree_size(self._h, kind)
+        if n < 0:
+            _check(int(n))
+        out = np.zeros(max(n, 1), np.int32)
+        _check(lib.fmmb_get_tree(self._h, kind, out.ctypes.data))
+        return out[:n]
+
+    def expansions(self, which):
+        lib = load()
+        n = lib.fmmb_get_expansion_size(self._h, which)
+        if n < 0:
+            _check(int(n))
+        out = np.zeros(n)
+        _check(lib.fmmb_get_expansions(self._h, which, out.ctypes.data))
+        return out.reshape(-1, 2) @ np.array([1.0, 1j])
+
+    def timings(self):
+        ms = np.zeros(7, np.float32)
+        _check(load().fmmb_get_timings(self._h, ms.ctypes.data))
+        return dict(zip(["p2p", "p2m", "m2m", "m2l_l2l", "l2l", "l2p", "total"], ms.tolist()))
+
+    def stats(self):
+        o = np.zeros(7, np.int64)
+        _check(load().fmmb_get_stats(self._h, o.ctypes.data))
+        return dict(zip(["ni", "nj", "leaves_i", "leaves_j", "p2p_pairs", "m2l_pairs", "lmax"], o.tolist()))
+
+
+def fmm(xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, gxj, gyj, gzj, vj, neq, *, lmax, xmin, ymin, zmin, rd, p=8,
+        precision=FP64, semantics=SEM_REFERENCE):
+    """The reference's fmm(mi, mj, neq) (fmm/fmm.cxx:29-152) with explicit arrays.
+
+    neq 0: returns (vi, gxi, gyi, gzi) -- potential and gradient of Laplace G;
+    neq 1: returns vi for Gni (gxi.. are the target normals);
+    neq 2: returns vi for Gnj (gxj.. are the source normals).
+    Arrays in caller order (no sorti/sortj needed)."""
+    with Plan(kernel=neq, p=p, lmax=lmax, precision=precision, semantics=semantics) as pl:
+        pl.set_geometry((xi, yi, zi), (xj, yj, zj), (gxi, gyi, gzi) if neq == 1 else None,
+                        (gxj, gyj, gzj) if neq == 2 else None, bbox=(xmin, ymin, zmin, rd))
+        pot, grad = pl.evaluate(vj)
+        if neq == 0:
+            g = grad.reshape(3, -1)
+            return pot, g[0], g[1], g[2]
+        return pot
+
+
+def _direct(neq, xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, gxj, gyj, gzj, vj, semantics=SEM_REFERENCE):
+    with Plan(kernel=neq, semantics=semantics, lmax=2) as pl:
+        pl.set_geometry((xi, yi, zi), (xj, yj, zj), (gxi, gyi, gzi) if neq == 1 else None,
+                        (gxj, gyj, gzj) if neq == 2 else None)
+        return pl.direct(vj)
+
+
+def G_dir(xi, yi, zi, xj, yj, zj, vj, semantics=SEM_REFERENCE):
+    """kernel/G_dir.cxx:6-30: potential and gradient by direct summation (FP64)."""
+    return _direct(LAPLACE_G, xi, yi, zi, None, None, None, xj, yj, zj, None, None, None, vj, semantics)
+
+
+def Gni_dir(xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, vj, semantics=SEM_REFERENCE):
+    """kernel/Gni_dir.cxx:6-21 (target normals gxi..)."""
+    return _direct(LAPLACE_GNI, xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, None, None, None, vj, semantics)[0]
+
+
+def Gnj_dir(xi, yi, zi, xj, yj, zj, gxj, gyj, gzj, vj, semantics=SEM_REFERENCE):
+    """kernel/Gnj_dir.cxx:6-21 (source normals gxj..)."""
+    return _direct(LAPLACE_GNJ, xi, yi, zi, None, None, None, xj, yj, zj, gxj, gyj, gzj, vj, semantics)[0]

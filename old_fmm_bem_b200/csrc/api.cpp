@@ -1,0 +1,555 @@
+// C ABI of libfmmb (include/fmmb.h): plan lifetime, geometry, evaluation.
+//
+// The evaluation is the reference's seven-step driver (fmm/fmm.cxx:29-152)
+// recast for one GPU: the near field (P2P) runs on a side stream while the far
+// field runs P2M -> M2M (lmax-1..2) -> M2L at level 2 -> for each level
+// 3..lmax: L2L then M2L -> L2P on the main stream; the two halves meet in the
+// final scatter to caller order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "kernels.h"
+
+namespace fmmb {
+
+thread_local std::string g_last_error;
+void set_error(const std::string& m) { g_last_error = m; }
+
+namespace {
+
+const double kPiF = (double)(float)M_PI;
+const double kEpsF = (double)1e-6f;
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename F>
+int guarded(F f) {
+  try {
+    f();
+    return FMMB_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return FMMB_ERR_ARG;
+  }
+}
+
+Sem make_sem(const fmmb_plan* pl) {
+  Sem s;
+  s.eps2 = pl->eps2;
+  s.coef = pl->coef;
+  s.rho_eps = pl->rho_eps;
+  s.ang_eps = pl->ang_eps;
+  s.pi_ang = pl->pi_ang;
+  s.ref = pl->ref ? 1 : 0;
+  s.excl_self = (!pl->ref && pl->cfg.exclude_self) ? 1 : 0;
+  return s;
+}
+
+// Copies a host or device float array of n elements to a device pointer
+// (staging when needed).  Returns the device pointer to use.
+const float* to_device(const float* src, size_t n, DevBuf<float>& stage, cudaStream_t s) {
+  if (!src) return nullptr;
+  if (is_device_ptr(src)) return src;
+  stage.alloc(n);
+  FMMB_CUDA(cudaMemcpyAsync(stage.get(), src, n * sizeof(float), cudaMemcpyHostToDevice, s));
+  return stage.get();
+}
+
+void upload(DevBuf<double>& d, const std::vector<double>& h, cudaStream_t s) {
+  d.alloc(h.size());
+  FMMB_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+void upload_static_ops(fmmb_plan* pl) {
+  const Operators& o = pl->ops;
+  cudaStream_t s = pl->st.main;
+  upload(pl->d_fac, o.fac, s);
+  upload(pl->d_m2m, o.m2m, s);
+  upload(pl->d_l2l, o.l2l, s);
+  pl->d_slot_rel.alloc(o.slot_rel.size());
+  FMMB_CUDA(cudaMemcpyAsync(pl->d_slot_rel.get(), o.slot_rel.data(), o.slot_rel.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  pl->d_rel_to_op.alloc(o.rel_to_op.size());
+  FMMB_CUDA(cudaMemcpyAsync(pl->d_rel_to_op.get(), o.rel_to_op.data(), o.rel_to_op.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace fmmb
+
+using namespace fmmb;
+
+extern "C" {
+
+const char* fmmb_last_error(void) { return g_last_error.c_str(); }
+
+int fmmb_config_init(fmmb_config* cfg) {
+  if (!cfg) return FMMB_ERR_ARG;
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->kernel = FMMB_LAPLACE_G;
+  cfg->p = 8;
+  cfg->lmax = 3;
+  cfg->precision = FMMB_FP64;
+  cfg->semantics = FMMB_SEM_REFERENCE;
+  cfg->eps2 = 0.0;
+  cfg->exclude_self = 0;
+  cfg->nrhs = 1;
+  return FMMB_OK;
+}
+
+int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
+  return guarded([&] {
+    FMMB_REQUIRE(cfg && out, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(cfg->kernel == FMMB_LAPLACE_G || cfg->kernel == FMMB_LAPLACE_GNI || cfg->kernel == FMMB_LAPLACE_GNJ,
+                 FMMB_ERR_ARG, "unknown kernel");
+    FMMB_REQUIRE(cfg->p >= 1 && cfg->p <= 20, FMMB_ERR_ARG, "p must be in 1..20");
+    FMMB_REQUIRE(cfg->lmax >= 2 && cfg->lmax <= 10, FMMB_ERR_ARG, "lmax must be in 2..10");
+    FMMB_REQUIRE(cfg->precision == FMMB_FP64 || cfg->precision == FMMB_MIXED, FMMB_ERR_ARG, "unknown precision");
+    FMMB_REQUIRE(cfg->semantics == FMMB_SEM_REFERENCE || cfg->semantics == FMMB_SEM_ACCURATE, FMMB_ERR_ARG,
+                 "unknown semantics");
+    FMMB_REQUIRE(cfg->nrhs >= 1 && cfg->nrhs <= 4096, FMMB_ERR_ARG, "nrhs must be in 1..4096");
+    FMMB_REQUIRE(cfg->eps2 >= 0 && std::isfinite(cfg->eps2), FMMB_ERR_ARG, "eps2 must be finite and >= 0");
+    int ndev = 0;
+    FMMB_CUDA(cudaGetDeviceCount(&ndev));
+    FMMB_REQUIRE(ndev > 0, FMMB_ERR_CUDA, "no CUDA device");
+    auto* pl = new fmmb_plan();
+    try {
+      pl->cfg = *cfg;
+      pl->p = cfg->p;
+      pl->K = (cfg->p + 1) * (cfg->p + 1);
+      pl->P = (cfg->p + 1) * (cfg->p + 2) / 2;
+      pl->ref = cfg->semantics == FMMB_SEM_REFERENCE;
+      pl->eps2 = pl->ref ? kEpsF : cfg->eps2;
+      pl->coef = pl->ref ? 0.25 / kPiF : 0.25 / M_PI;
+      pl->rho_eps = pl->ref ? kEpsF : 0.0;
+      pl->ang_eps = pl->ref ? kEpsF : 0.0;
+      pl->pi_ang = pl->ref ? kPiF : M_PI;
+      FMMB_CUDA(cudaGetDevice(&pl->device));
+      FMMB_CUDA(cudaStreamCreateWithFlags(&pl->st.main, cudaStreamNonBlocking));
+      FMMB_CUDA(cudaStreamCreateWithFlags(&pl->st.side, cudaStreamNonBlocking));
+      FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.fork, cudaEventDisableTiming));
+      FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.join, cudaEventDisableTiming));
+      for (auto& e : pl->ev) FMMB_CUDA(cudaEventCreate(&e));
+      build_static_operators(pl->ops, pl->p, pl->ref);
+      upload_static_ops(pl);
+      if (!pl->ref) {  // geometry-independent M2L set
+        build_m2l_operators(pl->ops, 2, 1.0f);
+        upload(pl->d_m2l, pl->ops.m2l, pl->st.main);
+      }
+    } catch (...) {
+      fmmb_plan_destroy(pl);
+      throw;
+    }
+    *out = pl;
+  });
+}
+
+int fmmb_plan_destroy(fmmb_plan* pl) {
+  if (!pl) return FMMB_OK;
+  cudaDeviceSynchronize();
+  if (pl->own_stream && pl->st.main) cudaStreamDestroy(pl->st.main);
+  if (pl->st.side) cudaStreamDestroy(pl->st.side);
+  if (pl->st.fork) cudaEventDestroy(pl->st.fork);
+  if (pl->st.join) cudaEventDestroy(pl->st.join);
+  for (auto& e : pl->ev)
+    if (e) cudaEventDestroy(e);
+  delete pl;
+  return FMMB_OK;
+}
+
+int fmmb_set_stream(fmmb_plan* pl, void* stream) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
+    if (!stream) return;
+    if (pl->own_stream && pl->st.main) FMMB_CUDA(cudaStreamDestroy(pl->st.main));
+    pl->st.main = (cudaStream_t)stream;
+    pl->own_stream = false;
+  });
+}
+
+int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
+                      const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
+                      const float* snx, const float* sny, const float* snz, const float* bbox) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
+    FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
+    FMMB_REQUIRE(tx && ty && tz && sx && sy && sz, FMMB_ERR_ARG, "null coordinates");
+    FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNI || (tnx && tny && tnz), FMMB_ERR_ARG, "Gni needs target normals");
+    FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNJ || (snx && sny && snz), FMMB_ERR_ARG, "Gnj needs source normals");
+    FMMB_REQUIRE((long long)ni * pl->cfg.nrhs < (1LL << 31) && (long long)nj * pl->cfg.nrhs < (1LL << 31),
+                 FMMB_ERR_CAPACITY, "n * nrhs must stay below 2^31");
+    float bb[4];
+    if (bbox) {
+      if (is_device_ptr(bbox)) FMMB_CUDA(cudaMemcpy(bb, bbox, sizeof(bb), cudaMemcpyDeviceToHost));
+      else std::memcpy(bb, bbox, sizeof(bb));
+      FMMB_REQUIRE(bb[3] > 0 && std::isfinite(bb[3]), FMMB_ERR_ARG, "bbox side must be positive");
+    }
+    cudaStream_t s = pl->st.main;
+    pl->have_geometry = false;
+    pl->have_expansions = false;
+    DevBuf<float> st[12];
+    const float* d[12] = {to_device(tx, ni, st[0], s),  to_device(ty, ni, st[1], s),  to_device(tz, ni, st[2], s),
+                          to_device(tnx, ni, st[3], s), to_device(tny, ni, st[4], s), to_device(tnz, ni, st[5], s),
+                          to_device(sx, nj, st[6], s),  to_device(sy, nj, st[7], s),  to_device(sz, nj, st[8], s),
+                          to_device(snx, nj, st[9], s), to_device(sny, nj, st[10], s), to_device(snz, nj, st[11], s)};
+    build_tree(pl, ni, d[0], d[1], d[2], d[3], d[4], d[5], nj, d[6], d[7], d[8], d[9], d[10], d[11], bbox ? bb : nullptr);
+    // reference semantics: the M2L distance carries an absolute eps, so the
+    // operator set depends on the level sizes (rebuilt when they change)
+    if (pl->ref && (pl->ops.m2l_lmax != pl->lmax || pl->ops.m2l_rd != pl->bbox[3])) {
+      build_m2l_operators(pl->ops, pl->lmax, pl->bbox[3]);
+      upload(pl->d_m2l, pl->ops.m2l, s);
+    }
+    // M2L tiles: per level, target boxes grouped by octant, m2l_tile_size() per tile
+    std::vector<int> keys(pl->tot_i);
+    FMMB_CUDA(cudaMemcpy(keys.data(), pl->key_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
+    const int TS = m2l_tile_size();
+    pl->tile_n.assign(pl->lmax + 1, 0);
+    pl->tile_boxes.clear();
+    pl->tile_oct.clear();
+    for (int lev = 0; lev <= pl->lmax; lev++) {
+      pl->tile_boxes.emplace_back(new DevBuf<int>());
+      pl->tile_oct.emplace_back(new DevBuf<int>());
+    }
+    for (int lev = 2; lev <= pl->lmax; lev++) {
+      std::vector<int> tb, to;
+      for (int oct = 0; oct < 8; oct++) {
+        std::vector<int> bx;
+        for (int b = 0; b < pl->nbox_i[lev]; b++)
+          if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
+        for (size_t k = 0; k < bx.size(); k += TS) {
+          for (int t = 0; t < TS; t++) tb.push_back(k + t < bx.size() ? bx[k + t] : -1);
+          to.push_back(oct);
+        }
+      }
+      pl->tile_n[lev] = (int)to.size();
+      pl->tile_boxes[lev]->alloc(tb.size());
+      pl->tile_oct[lev]->alloc(to.size());
+      if (!tb.empty()) {
+        FMMB_CUDA(cudaMemcpy(pl->tile_boxes[lev]->get(), tb.data(), tb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        FMMB_CUDA(cudaMemcpy(pl->tile_oct[lev]->get(), to.data(), to.size() * sizeof(int), cudaMemcpyHostToDevice));
+      }
+    }
+    // inverse target permutation (caller -> sorted) for the direct sum
+    {
+      std::vector<int> perm(ni), inv(ni);
+      FMMB_CUDA(cudaMemcpy(perm.data(), pl->perm_i.get(), ni * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < ni; i++) inv[perm[i]] = i;
+      pl->inv_i.alloc(ni);
+      FMMB_CUDA(cudaMemcpy(pl->inv_i.get(), inv.data(), ni * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    // evaluation buffers
+    const int nr = pl->cfg.nrhs;
+    pl->qs.alloc((size_t)nj * nr);
+    pl->M.alloc((size_t)pl->tot_j * pl->K);
+    pl->L.alloc((size_t)pl->tot_i * pl->K);
+    pl->pot_s.alloc((size_t)ni * 2);          // near, far
+    pl->grad_s.alloc((size_t)ni * 6);         // near xyz, far xyz
+    FMMB_CUDA(cudaMemsetAsync(pl->grad_s.get(), 0, (size_t)ni * 6 * sizeof(double), s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    pl->have_geometry = true;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Runs one right-hand side: qs (sorted, device) -> near/far sorted outputs.
+void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
+  const int K = pl->K, p = pl->p, lmax = pl->lmax, ker = pl->cfg.kernel;
+  const Sem s = make_sem(pl);
+  cudaStream_t m = pl->st.main, side = pl->st.side;
+  double* pot_near = pl->pot_s.get();
+  double* pot_far = pl->pot_s.get() + pl->ni;
+  double* g_near = want_grad ? pl->grad_s.get() : nullptr;
+  double* g_far = want_grad ? pl->grad_s.get() + 3 * (size_t)pl->ni : nullptr;
+  // near field on the side stream
+  FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
+  FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
+  FMMB_CUDA(cudaEventRecord(pl->ev[0], side));
+  const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
+  if (pl->cfg.precision == FMMB_MIXED)
+    launch_p2p_mixed(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
+                     pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+  else
+    launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
+                   pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+  FMMB_CUDA(cudaEventRecord(pl->ev[1], side));
+  FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+
+  // far field on the main stream
+  FMMB_CUDA(cudaEventRecord(pl->ev[2], m));
+  const double rb_leaf = (double)(pl->bbox[3] / (float)(1 << lmax));
+  launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(), qs,
+             pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+  FMMB_CUDA(cudaEventRecord(pl->ev[3], m));
+  for (int lev = lmax - 1; lev >= 2; lev--)
+    launch_m2m(pl->nbox_j[lev], K, pl->child_start_j.get() + pl->off_j[lev], pl->child_count_j.get() + pl->off_j[lev],
+               pl->key_j.get() + pl->off_j[lev + 1], pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->d_m2m.get(),
+               pl->M.get() + (size_t)pl->off_j[lev] * K, m);
+  FMMB_CUDA(cudaEventRecord(pl->ev[4], m));
+  const size_t opsz = (size_t)316 * K * K;
+  for (int lev = 2; lev <= lmax; lev++) {
+    double* Ll = pl->L.get() + (size_t)pl->off_i[lev] * K;
+    if (lev == 2) FMMB_CUDA(cudaMemsetAsync(Ll, 0, (size_t)pl->nbox_i[2] * K * sizeof(double), m));
+    else
+      launch_l2l(pl->nbox_i[lev], K, pl->parent_i.get() + pl->off_i[lev], pl->key_i.get() + pl->off_i[lev],
+                 pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->d_l2l.get(), Ll, m);
+    const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
+    launch_m2l_f64(pl->tile_n[lev], K, pl->tile_boxes[lev]->get(), pl->tile_oct[lev]->get(), pl->m2l_list.get(), pl->d_slot_rel.get(),
+                   pl->d_rel_to_op.get(), pl->d_m2l.get() + set * opsz, pl->M.get() + (size_t)pl->off_j[lev] * K,
+                   pl->L.get(), m);
+  }
+  FMMB_CUDA(cudaEventRecord(pl->ev[5], m));
+  launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
+             pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
+  FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
+  FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));
+}
+
+template <typename T>
+int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && q && pot, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+    cudaStream_t m = pl->st.main;
+    const int ni = pl->ni, nj = pl->nj, nr = pl->cfg.nrhs;
+    const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
+    FMMB_CUDA(cudaEventRecord(pl->ev[7], m));
+    const float* qd = to_device(q, (size_t)nj * nr, pl->stage_f, m);
+    launch_gather_charges(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
+    const bool pot_dev = is_device_ptr(pot);
+    const bool grad_dev = want_grad && is_device_ptr(grad);
+    // device destinations (staged through the plan when the caller gave host memory)
+    T* pd = pot_dev ? pot : nullptr;
+    T* gd = grad_dev ? grad : nullptr;
+    size_t need = 0;
+    if (!pot_dev) need += (size_t)ni * nr;
+    if (want_grad && !grad_dev) need += (size_t)3 * ni * nr;
+    if (need) {
+      pl->stage_out.alloc(need * sizeof(T));
+      char* base = (char*)pl->stage_out.get();
+      if (!pot_dev) {
+        pd = (T*)base;
+        base += (size_t)ni * nr * sizeof(T);
+      }
+      if (want_grad && !grad_dev) gd = (T*)base;
+    }
+    for (int r = 0; r < nr; r++) {
+      run_one(pl, pl->qs.get() + (size_t)r * nj, want_grad);
+      const double* pn = pl->pot_s.get();
+      const double* gn = pl->grad_s.get();
+      if (sizeof(T) == 4)
+        launch_finalize_f32(ni, pl->perm_i.get(), pn, pn + ni, want_grad ? gn : nullptr, want_grad ? gn + 3 * (size_t)ni : nullptr,
+                            (float*)(pd + (size_t)r * ni), want_grad ? (float*)(gd + (size_t)3 * r * ni) : nullptr, m);
+      else
+        launch_finalize_f64(ni, pl->perm_i.get(), pn, pn + ni, want_grad ? gn : nullptr, want_grad ? gn + 3 * (size_t)ni : nullptr,
+                            (double*)(pd + (size_t)r * ni), want_grad ? (double*)(gd + (size_t)3 * r * ni) : nullptr, m);
+    }
+    if (!pot_dev) FMMB_CUDA(cudaMemcpyAsync(pot, pd, (size_t)ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
+    if (want_grad && !grad_dev) FMMB_CUDA(cudaMemcpyAsync(grad, gd, (size_t)3 * ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
+    if (!pot_dev || (want_grad && !grad_dev) || !is_device_ptr(q)) FMMB_CUDA(cudaStreamSynchronize(m));
+    pl->have_expansions = true;
+    pl->timings_valid = true;
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmmb_evaluate(fmmb_plan* pl, const float* q, float* pot, float* grad) { return evaluate_impl<float>(pl, q, pot, grad); }
+int fmmb_evaluate_f64(fmmb_plan* pl, const float* q, double* pot, double* grad) {
+  return evaluate_impl<double>(pl, q, pot, grad);
+}
+
+int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, double* grad) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && q && pot, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+    FMMB_REQUIRE(0 <= i0 && i0 <= i1 && i1 <= pl->ni, FMMB_ERR_ARG, "target range out of bounds");
+    cudaStream_t m = pl->st.main;
+    const int nj = pl->nj, cnt = i1 - i0;
+    const float* qd = to_device(q, nj, pl->stage_f, m);
+    launch_gather_charges(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
+    const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
+    DevBuf<double> out;
+    out.alloc((size_t)cnt * 4 + 1);
+    launch_direct_f64(pl->cfg.kernel, i0, i1, pl->inv_i.get(), pl->tpos.get(), pl->tnrm.get(), nj, pl->spos.get(),
+                      pl->snrm.get(), pl->qs.get(), make_sem(pl), out.get(), want_grad ? out.get() + cnt : nullptr, m);
+    FMMB_CUDA(cudaMemcpyAsync(pot, out.get(), cnt * sizeof(double), is_device_ptr(pot) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, m));
+    if (want_grad)
+      FMMB_CUDA(cudaMemcpyAsync(grad, out.get() + cnt, 3 * (size_t)cnt * sizeof(double),
+                                is_device_ptr(grad) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, m));
+    FMMB_CUDA(cudaStreamSynchronize(m));
+  });
+}
+
+}  // extern "C"
+
+namespace {
+int tree_record(fmmb_plan* pl, int k, std::vector<int>& v) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "no geometry");
+    FMMB_REQUIRE(k >= 0 && k <= 8, FMMB_ERR_ARG, "unknown tree record");
+    const int lmax = pl->lmax;
+    v.clear();
+    auto d2h = [&](const int* src, size_t n) {
+      std::vector<int> h(n);
+      if (n) FMMB_CUDA(cudaMemcpy(h.data(), src, n * sizeof(int), cudaMemcpyDeviceToHost));
+      return h;
+    };
+    if (k == 0) v = d2h(pl->perm_i.get(), pl->ni);
+    else if (k == 1) v = d2h(pl->perm_j.get(), pl->nj);
+    else if (k == 2) v = d2h(pl->key_i.get(), pl->tot_i);
+    else if (k == 3) v = d2h(pl->key_j.get(), pl->tot_j);
+    else if (k == 4 || k == 5) {
+      v.assign(lmax + 1, 0);
+      for (int l = 2; l <= lmax; l++) v[l] = (k == 4 ? pl->nbox_i : pl->nbox_j)[l];
+    } else if (k == 6 || k == 7) {
+      const int nl = (k == 6 ? pl->nbox_i : pl->nbox_j)[lmax];
+      std::vector<int2> lf(nl);
+      FMMB_CUDA(cudaMemcpy(lf.data(), (k == 6 ? pl->leaf_i : pl->leaf_j).get(), nl * sizeof(int2), cudaMemcpyDeviceToHost));
+      for (auto& x : lf) {
+        v.push_back(x.x);
+        v.push_back(x.x + x.y - 1);
+      }
+    } else {
+      // lists in the order fmm() builds them: near field at lmax, level 2, levels 3..lmax
+      const int nli = pl->nbox_i[lmax];
+      std::vector<int> near = d2h(pl->p2p_list.get(), (size_t)nli * kP2PSlots);
+      std::vector<int> far = d2h(pl->m2l_list.get(), (size_t)pl->tot_i * kM2LSlots);
+      auto emit = [&](int lev, int mode, int nbi, int nbj, const std::vector<std::vector<int>>& L) {
+        v.push_back(lev);
+        v.push_back(mode);
+        v.push_back(nbi);
+        v.push_back(nbj);
+        for (auto& l : L) v.push_back((int)l.size());
+        for (auto& l : L) v.insert(v.end(), l.begin(), l.end());
+      };
+      std::vector<std::vector<int>> L(nli);
+      for (int b = 0; b < nli; b++)
+        for (int s = 0; s < kP2PSlots; s++)
+          if (near[(size_t)b * kP2PSlots + s] >= 0) L[b].push_back(near[(size_t)b * kP2PSlots + s]);
+      emit(lmax, 0, nli, pl->nbox_j[lmax], L);
+      for (int lev = 2; lev <= lmax; lev++) {
+        std::vector<std::vector<int>> F(pl->nbox_i[lev]);
+        for (int b = 0; b < pl->nbox_i[lev]; b++) {
+          const size_t g = (size_t)(pl->off_i[lev] + b) * kM2LSlots;
+          for (int s = 0; s < kM2LSlots; s++)
+            if (far[g + s] >= 0) F[b].push_back(far[g + s]);
+          // level 2 visits every source box in index order (fmm/ijbox.cxx:62-72)
+          if (lev == 2) std::sort(F[b].begin(), F[b].end());
+        }
+        emit(lev, lev == 2 ? 1 : 2, pl->nbox_i[lev], pl->nbox_j[lev], F);
+      }
+    }
+  });
+}
+}  // namespace
+
+extern "C" {
+
+long fmmb_get_tree_size(fmmb_plan* pl, int kind) {
+  std::vector<int> v;
+  const int rc = tree_record(pl, kind, v);
+  return rc != FMMB_OK ? rc : (long)v.size();
+}
+
+int fmmb_get_tree(fmmb_plan* pl, int kind, int* out) {
+  std::vector<int> v;
+  const int rc = tree_record(pl, kind, v);
+  if (rc == FMMB_OK && out && !v.empty()) std::memcpy(out, v.data(), v.size() * sizeof(int));
+  return rc;
+}
+
+long fmmb_get_expansion_size(fmmb_plan* pl, int which) {
+  if (!pl || !pl->have_geometry || (which != 0 && which != 1)) return FMMB_ERR_ARG;
+  return (long)(which == 0 ? pl->tot_j : pl->tot_i) * pl->P * 2;
+}
+
+int fmmb_get_expansions(fmmb_plan* pl, int which, double* out) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && out && (which == 0 || which == 1), FMMB_ERR_ARG, "bad argument");
+    FMMB_REQUIRE(pl->have_expansions, FMMB_ERR_STATE, "no evaluate yet");
+    FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
+    const int tot = which == 0 ? pl->tot_j : pl->tot_i;
+    const int K = pl->K, p = pl->p, P = pl->P;
+    std::vector<double> h((size_t)tot * K);
+    FMMB_CUDA(cudaMemcpy(h.data(), (which == 0 ? pl->M : pl->L).get(), h.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const std::vector<int>& off = which == 0 ? pl->off_j : pl->off_i;
+    for (int lev = pl->lmax; lev >= 2; lev--) {
+      const double rb = (double)(pl->bbox[3] / (float)(1 << lev));
+      const int nb = (which == 0 ? pl->nbox_j : pl->nbox_i)[lev];
+      for (int b = 0; b < nb; b++) {
+        const double* v = &h[(size_t)(off[lev] + b) * K];
+        double* o = out + (size_t)(off[lev] + b) * P * 2;
+        for (int n = 0; n <= p; n++) {
+          // undo the scaling: M_n = M^_n rb^n, L_n = L^_n / rb^(n+1)
+          const double sc = which == 0 ? std::pow(rb, n) : std::pow(rb, -(n + 1));
+          o[2 * isym(n, 0)] = v[n * n] * sc;
+          o[2 * isym(n, 0) + 1] = 0.0;
+          for (int mm = 1; mm <= n; mm++) {
+            o[2 * isym(n, mm)] = v[n * n + 2 * mm - 1] * sc;
+            o[2 * isym(n, mm) + 1] = v[n * n + 2 * mm] * sc;
+          }
+        }
+      }
+    }
+  });
+}
+
+int fmmb_get_timings(fmmb_plan* pl, float* ms) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && ms, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->timings_valid, FMMB_ERR_STATE, "no evaluate yet");
+    FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
+    FMMB_CUDA(cudaStreamSynchronize(pl->st.side));
+    auto el = [&](int a, int b) {
+      float t = 0;
+      FMMB_CUDA(cudaEventElapsedTime(&t, pl->ev[a], pl->ev[b]));
+      return t;
+    };
+    ms[0] = el(0, 1);
+    ms[1] = el(2, 3);
+    ms[2] = el(3, 4);
+    ms[3] = el(4, 5);  // M2L and L2L interleaved per level
+    ms[4] = 0.0f;
+    ms[5] = el(5, 6);
+    ms[6] = el(7, 6);
+  });
+}
+
+int fmmb_get_stats(fmmb_plan* pl, long long* o) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && o, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "no geometry");
+    o[0] = pl->ni;
+    o[1] = pl->nj;
+    o[2] = pl->nbox_i[pl->lmax];
+    o[3] = pl->nbox_j[pl->lmax];
+    o[4] = pl->p2p_pairs;
+    o[5] = pl->m2l_pairs;
+    o[6] = pl->lmax;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,162 @@
+// Internal declarations of libfmmb (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fmmb.h"
+
+namespace fmmb {
+
+// ---- error handling: every entry point returns a status, nothing aborts ----
+void set_error(const std::string& msg);
+struct Error {
+  int code;
+  std::string msg;
+};
+#define FMMB_CUDA(call)                                                                      \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ::fmmb::Error{FMMB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+#define FMMB_CHECK_LAUNCH() FMMB_CUDA(cudaGetLastError())
+#define FMMB_REQUIRE(cond, code, msg) \
+  do {                                \
+    if (!(cond)) throw ::fmmb::Error{code, msg}; \
+  } while (0)
+
+// Owning device buffer (allocated at plan/geometry time only).
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && ptr) return;
+    release();
+    size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      throw Error{FMMB_ERR_NOMEM, std::string("cudaMalloc ") + std::to_string(bytes) + " B: " + cudaGetErrorString(e)};
+    }
+    n = count;
+  }
+  T* get() const { return ptr; }
+};
+
+inline int isym(int n, int m) { return n * (n + 1) / 2 + m; }
+inline int ifull(int n, int m) { return n * n + n + m; }
+
+// Number of M2L slots per target box: children of the parent's 27 neighbours
+// that are not adjacent (fmm/ijbox.cxx:74-109).
+constexpr int kM2LSlots = 189;
+constexpr int kP2PSlots = 27;
+constexpr int kRelCodes = 343;  // (dx+3)*49 + (dy+3)*7 + (dz+3)
+
+// Host-side operator tables (operators.cpp).
+struct Operators {
+  int p = 0, K = 0;
+  bool ref = true;
+  std::vector<double> fac;   // ifull(n,m), n <= p (P2M/L2P normalisation)
+  // Scaled, real-packed operators, K x K row-major (out row, in col).
+  std::vector<double> m2m;   // [8][K][K]   child octant -> parent
+  std::vector<double> l2l;   // [8][K][K]   parent -> child octant
+  std::vector<double> m2l;   // [nsets][316][K][K]
+  int m2l_sets = 0;          // 1 (accurate) or one per level 2..lmax (reference)
+  int m2l_lmax = 0;
+  float m2l_rd = 0;
+  std::vector<int> rel_to_op;  // [343] -> operator slot (0..315) or -1
+  std::vector<int> op_rel;     // [316] rel code of each operator slot
+  std::vector<int> slot_rel;   // [8][189] rel code of each M2L slot per octant
+  // Wigner rotation tables per relative position (forward, inverse)
+  std::vector<std::vector<std::vector<std::complex<double>>>> Wf, Wb;
+};
+// fac, M2M, L2L, slot maps and rotation tables (independent of the geometry)
+void build_static_operators(Operators& ops, int p, bool ref_semantics);
+// M2L sets: one in accurate semantics; one per level 2..lmax in reference
+// semantics, where the distance carries an absolute eps (needs the root size).
+void build_m2l_operators(Operators& ops, int lmax, float rd);
+
+struct Stream2 {
+  cudaStream_t main = nullptr, side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+}  // namespace fmmb
+
+struct fmmb_plan {
+  fmmb_config cfg{};
+  int p = 0, K = 0, P = 0;
+  int device = 0;
+  fmmb::Stream2 st;
+  bool own_stream = true;
+  cudaEvent_t ev[8] = {};
+
+  // host copies of the configuration-dependent constants
+  double eps2 = 0, coef = 0, rho_eps = 0, ang_eps = 0, pi_ang = 0;
+  bool ref = true;
+  fmmb::Operators ops;
+
+  // ---- geometry (set_geometry) ----
+  bool have_geometry = false;
+  bool have_expansions = false;
+  int ni = 0, nj = 0, lmax = 0;
+  float bbox[4] = {0, 0, 0, 1};
+  std::vector<int> nbox_i, nbox_j;  // boxes per level [lmax+1]
+  std::vector<int> off_i, off_j;    // offsets of each level in all-level arrays (lmax first)
+  int tot_i = 0, tot_j = 0;
+  long long p2p_pairs = 0, m2l_pairs = 0;
+
+  // sorted particles
+  fmmb::DevBuf<int> perm_i, perm_j;          // sorted position -> caller index
+  fmmb::DevBuf<float4> tpos, tnrm;           // targets (x,y,z,0), normals
+  fmmb::DevBuf<float4> spos, snrm;           // sources
+  // boxes (all levels concatenated, lmax first)
+  fmmb::DevBuf<int> key_i, key_j;            // Morton keys at their level
+  fmmb::DevBuf<int> parent_i, parent_j;      // index (within level l-1) of the parent, -1 at level 2
+  fmmb::DevBuf<int2> leaf_i, leaf_j;         // leaf (first, count) in sorted order
+  fmmb::DevBuf<int> p2p_list;                // [nleaf_i][27] source leaf or -1
+  fmmb::DevBuf<int> m2l_list;                // [tot_i][189] source box (within level) or -1
+  fmmb::DevBuf<int> child_start_j;           // for M2M: per source box at level l (<lmax): first child index, count
+  fmmb::DevBuf<int> child_count_j;
+
+  // operators on the device
+  fmmb::DevBuf<double> d_fac, d_m2m, d_l2l, d_m2l;
+  fmmb::DevBuf<int> d_slot_rel, d_rel_to_op;
+  fmmb::DevBuf<float> d_m2l_tf32;            // [sets][316][2][Kp][Kp] hi/lo (mixed)
+
+  // evaluation buffers
+  fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
+  fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
+  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][Kp] tf32 hi/lo (mixed)
+  fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
+  fmmb::DevBuf<float> stage_f;               // host<->device staging
+  fmmb::DevBuf<double> stage_d;
+  fmmb::DevBuf<int> inv_i;                   // caller index -> sorted target position
+  fmmb::DevBuf<char> stage_out;              // device staging of host outputs
+  bool timings_valid = false;
+  // M2L tiles per level: target boxes of one octant, padded with -1
+  std::vector<int> tile_n;
+  std::vector<std::unique_ptr<fmmb::DevBuf<int>>> tile_boxes, tile_oct;
+};
+
+namespace fmmb {
+void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
+                const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
+                const float* snx, const float* sny, const float* snz, const float* bbox_in);
+}

@@ -1,0 +1,48 @@
+// Kernel launchers shared by the API layer (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fmmb {
+
+// Arithmetic conventions of a plan (reference or accurate semantics).
+struct Sem {
+  double eps2;     // P2P softening added to r^2
+  double coef;     // 1/(4 pi)
+  double rho_eps;  // added to expansion radii (reference: 1e-6)
+  double ang_eps;  // azimuth branch threshold (reference: 1e-6)
+  double pi_ang;   // pi in azimuth branches
+  int ref;         // reference semantics
+  int excl_self;   // skip zero-distance pairs
+};
+
+__host__ __device__ __forceinline__ int ifull_d(int n, int m) { return n * n + n + m; }
+
+void launch_gather_charges(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
+void launch_p2p_f64(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
+                    const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot,
+                    double* grad, int ni, cudaStream_t st);
+void launch_p2p_mixed(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
+                      const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s,
+                      double* pot, double* grad, int ni, cudaStream_t st);
+void launch_p2m(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos, const float4* snrm,
+                const float* qs, const double* fac, const Sem& s, const float* bbox, double rb, double* M, cudaStream_t st);
+void launch_m2m(int nparent, int K, const int* child_start, const int* child_count, const int* child_keys, const double* Mc,
+                const double* ops, double* Mp, cudaStream_t st);
+void launch_l2l(int nchild, int K, const int* parent, const int* keys, const double* Lp, const double* ops, double* Lc,
+                cudaStream_t st);
+int m2l_tile_size();
+void launch_m2l_f64(int ntile, int K, const int* tile_boxes, const int* tile_oct, const int* list, const int* slot_rel,
+                    const int* rel_to_op, const double* ops, const double* M, double* L, cudaStream_t st);
+void launch_l2p(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos, const float4* tnrm,
+                const double* fac, const Sem& s, const float* bbox, double rb, const double* L, double* pot, double* grad,
+                int ni, cudaStream_t st);
+void launch_finalize_f32(int n, const int* perm, const double* pn, const double* pf, const double* gn, const double* gf,
+                         float* pot, float* grad, cudaStream_t st);
+void launch_finalize_f64(int n, const int* perm, const double* pn, const double* pf, const double* gn, const double* gf,
+                         double* pot, double* grad, cudaStream_t st);
+void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float4* tpos, const float4* tnrm, int nj,
+                       const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot, double* grad,
+                       cudaStream_t st);
+
+}  // namespace fmmb

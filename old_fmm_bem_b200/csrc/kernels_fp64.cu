@@ -1,0 +1,620 @@
+// FP64 evaluation kernels: the plain-FP64 form of every FMM phase, and the
+// P2M/M2M/L2L/L2P phases of the mixed-precision form (they are a few percent
+// of the work, so they stay FP64 there too).
+//
+// Expansions are real-packed and scaled by the box size (operators.cpp).  P2M
+// and L2P follow the reference's spherical formulation -- the same radius,
+// angles, Legendre recurrences and Cartesian gradient conversion
+// (kernel/multipole.cxx:7-35, kernel/multipoled.cxx:7-34,
+// kernel/G_p2m.cxx:19-55, kernel/Gn_p2m.cxx:19-63, kernel/G_l2p.cxx:19-76,
+// kernel/Gn_l2p.cxx:19-68) -- so that reference semantics can be reproduced
+// to rounding.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "kernels.h"
+
+namespace fmmb {
+
+namespace {
+
+inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
+
+__device__ __forceinline__ double azimuth(double x, double y, const Sem& s) {
+  if (!s.ref) return (x == 0.0 && y == 0.0) ? 0.0 : atan2(y, x);
+  if (fabs(x) + fabs(y) < s.ang_eps) return 0.0;
+  if (fabs(x) < s.ang_eps) return y / fabs(y) * s.pi_ang * 0.5;
+  if (x > 0) return atan(y / x);
+  return atan(y / x) + s.pi_ang;
+}
+
+// ---------------------------------------------------------------- charges
+__global__ void gather_charges(int n, int nrhs, const int* perm, const float* q, float* qs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int o = perm[i];
+  for (int r = 0; r < nrhs; r++) qs[(size_t)r * n + i] = q[(size_t)r * n + o];
+}
+
+// ---------------------------------------------------------------- P2P (FP64)
+// kernel/G_p2p.cxx:12-37, Gni_p2p.cxx:12-28, Gnj_p2p.cxx:12-28: one block per
+// target leaf, its 27 neighbour slots staged through shared memory.
+constexpr int kP2PThreads = 128;
+
+template <int KER>
+__global__ void __launch_bounds__(kP2PThreads) p2p_f64(const int2* __restrict__ leaf_i, const int2* __restrict__ leaf_j,
+                                                       const int* __restrict__ list, const float4* __restrict__ tpos,
+                                                       const float4* __restrict__ tnrm, const float4* __restrict__ spos,
+                                                       const float4* __restrict__ snrm, const float* __restrict__ qs,
+                                                       Sem s, double* __restrict__ pot, double* __restrict__ grad,
+                                                       int ni) {
+  __shared__ float4 sp[kP2PThreads];
+  __shared__ float4 sn[kP2PThreads];
+  __shared__ float sq[kP2PThreads];
+  const int b = blockIdx.x;
+  const int2 li = leaf_i[b];
+  for (int t0 = 0; t0 < li.y; t0 += kP2PThreads) {
+    const int i = li.x + t0 + threadIdx.x;
+    const bool act = (t0 + threadIdx.x) < li.y;
+    float4 xi = act ? tpos[i] : make_float4(0, 0, 0, 0);
+    float4 ni4 = (KER == FMMB_LAPLACE_GNI && act) ? tnrm[i] : make_float4(0, 0, 0, 0);
+    double p = 0, fx = 0, fy = 0, fz = 0;
+    for (int slot = 0; slot < kP2PSlots; slot++) {
+      const int jl = list[(size_t)b * kP2PSlots + slot];
+      if (jl < 0) continue;
+      const int2 lj = leaf_j[jl];
+      for (int j0 = 0; j0 < lj.y; j0 += kP2PThreads) {
+        const int nld = min(kP2PThreads, lj.y - j0);
+        __syncthreads();
+        if (threadIdx.x < nld) {
+          const int j = lj.x + j0 + threadIdx.x;
+          sp[threadIdx.x] = spos[j];
+          sq[threadIdx.x] = qs[j];
+          if (KER == FMMB_LAPLACE_GNJ) sn[threadIdx.x] = snrm[j];
+        }
+        __syncthreads();
+        for (int jj = 0; jj < nld; jj++) {
+          const float4 xj = sp[jj];
+          double dx, dy, dz;
+          if (s.ref) {  // float differences, as the reference (kernel/G_p2p.cxx:21-23)
+            dx = (double)__fsub_rn(xi.x, xj.x);
+            dy = (double)__fsub_rn(xi.y, xj.y);
+            dz = (double)__fsub_rn(xi.z, xj.z);
+          } else {
+            dx = (double)xi.x - (double)xj.x;
+            dy = (double)xi.y - (double)xj.y;
+            dz = (double)xi.z - (double)xj.z;
+          }
+          if (s.excl_self && dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
+          const double r2 = dx * dx + dy * dy + dz * dz + s.eps2;
+          const double rinv = 1.0 / sqrt(r2);
+          const double qr = s.coef * (double)sq[jj] * rinv;
+          if (KER == FMMB_LAPLACE_G) {
+            const double qr3 = qr * rinv * rinv;
+            p += qr;
+            fx -= dx * qr3;
+            fy -= dy * qr3;
+            fz -= dz * qr3;
+          } else if (KER == FMMB_LAPLACE_GNI) {
+            p += (dx * (double)ni4.x + dy * (double)ni4.y + dz * (double)ni4.z) * qr * rinv * rinv;
+          } else {
+            const float4 nj = sn[jj];
+            p += (dx * (double)nj.x + dy * (double)nj.y + dz * (double)nj.z) * qr * rinv * rinv;
+          }
+        }
+      }
+    }
+    if (act) {
+      pot[i] = p;
+      if (KER == FMMB_LAPLACE_G && grad) {
+        grad[i] = fx;
+        grad[ni + i] = fy;
+        grad[2 * ni + i] = fz;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- P2M
+// One block per source leaf: 4 groups of 32 lanes, lane m owns the order-m
+// coefficients; groups take every 4th point and are summed at the end.
+template <int KER>
+__global__ void __launch_bounds__(128) p2m_f64(int p, int K, const int* __restrict__ keys, const int2* __restrict__ leaf,
+                                               const float4* __restrict__ spos, const float4* __restrict__ snrm,
+                                               const float* __restrict__ qs, const double* __restrict__ fac, Sem s,
+                                               float xmin, float ymin, float zmin, double rb, double* __restrict__ M) {
+  extern __shared__ double acc[];  // [4][K]
+  const int g = threadIdx.x >> 5, m = threadIdx.x & 31;
+  for (int k = threadIdx.x; k < 4 * K; k += blockDim.x) acc[k] = 0.0;
+  __syncthreads();
+  const int b = blockIdx.x;
+  int cx, cy, cz;
+  {
+    const int key = keys[b];
+    cx = cy = cz = 0;
+    for (int i = 0; i < 10; i++) {
+      cy |= ((key >> (3 * i)) & 1) << i;
+      cx |= ((key >> (3 * i + 1)) & 1) << i;
+      cz |= ((key >> (3 * i + 2)) & 1) << i;
+    }
+  }
+  const double xc = (double)xmin + (cx + 0.5) * rb, yc = (double)ymin + (cy + 0.5) * rb, zc = (double)zmin + (cz + 0.5) * rb;
+  const int2 lf = leaf[b];
+  double* my = acc + g * K;
+  if (m <= p) {
+    for (int jj = g; jj < lf.y; jj += 4) {
+      const int j = lf.x + jj;
+      const float4 xs = spos[j];
+      const double x = (double)xs.x - xc, y = (double)xs.y - yc, z = (double)xs.z - zc;
+      const double rh = sqrt(x * x + y * y + z * z) + s.rho_eps;
+      const double al = rh == 0.0 ? 0.0 : acos(z / rh);
+      const double be = azimuth(x, y, s);
+      const double rs = rh / rb;  // radius in units of the leaf size
+      const double xx = cos(al), s2 = sqrt((1 - xx) * (1 + xx));
+      double pmm = 1.0;
+      for (int i = 0; i < m; i++) pmm = -pmm * (2 * i + 1) * s2;
+      double sb, cb;
+      sincos(m * be, &sb, &cb);
+      double rm1 = 1.0;  // rs^(m-1) for m >= 1
+      for (int i = 1; i < m; i++) rm1 *= rs;
+      const double rm = (m == 0) ? 1.0 : rm1 * rs;
+      if (KER != FMMB_LAPLACE_GNJ) {
+        // M^_n^m += q r^n fac P_n^m(cos al) e^{-i m be}
+        const double q = (double)qs[j];
+        double pv = pmm, p1 = pmm, p2 = 0.0;
+        double rn = rm;
+        for (int n = m; n <= p; n++) {
+          if (n > m) {
+            const double pn = (n == m + 1) ? xx * (2 * m + 1) * p1 : (xx * (2 * n - 1) * p1 - (n - 1 + m) * p2) / (n - m);
+            p2 = p1;
+            p1 = pn;
+            pv = pn;
+          }
+          const double bnm = rn * fac[ifull_d(n, m)] * pv;
+          if (m == 0) {
+            my[n * n] += q * bnm;
+          } else {
+            my[n * n + 2 * m - 1] += q * bnm * cb;
+            my[n * n + 2 * m] -= q * bnm * sb;
+          }
+          rn *= rs;
+        }
+      } else {
+        // dipole: sum (q n) . grad R(x - c), in scaled form (1/rb) x the
+        // reference's expression with the scaled radius (kernel/Gn_p2m.cxx:42-57)
+        const float4 nv = snrm[j];
+        const float qf = qs[j];
+        const double qx = (double)(qf * nv.x), qy = (double)(qf * nv.y), qz = (double)(qf * nv.z);
+        const double sa = sin(al), ca = cos(al), sbe = sin(be), cbe = cos(be);
+        const double yy = sa;
+        double p_n = pmm, p_np1 = xx * (2 * m + 1) * pmm;  // P_m^m, P_{m+1}^m
+        double rn = rm, rn1 = (m == 0) ? 0.0 : rm1;        // rs^n, rs^(n-1)
+        for (int n = m; n <= p; n++) {
+          const double f = fac[ifull_d(n, m)];
+          const double bnm = f * p_n;
+          const double bth = (n == m) ? f * (p_np1 - (m + 1) * xx * p_n) / yy
+                                      : f * ((n - m + 1) * p_np1 - (n + 1) * xx * p_n) / yy;
+          // e = e^{-i m be} = (cb, -sb)
+          const double brh_re = n * rn1 * bnm * cb, brh_im = -n * rn1 * bnm * sb;
+          const double bal_re = rn * bth * cb, bal_im = -rn * bth * sb;
+          // bbe = -m rn bnm e i = -m rn bnm (sb, cb)
+          const double bbe_re = -m * rn * bnm * sb, bbe_im = -m * rn * bnm * cb;
+          const double c1x = sa * cbe, c2x = ca * cbe / rs, c3x = sbe / rs / sa;
+          const double c1y = sa * sbe, c2y = ca * sbe / rs, c3y = cbe / rs / sa;
+          const double c1z = ca, c2z = sa / rs;
+          const double bx_re = c1x * brh_re + c2x * bal_re - c3x * bbe_re;
+          const double bx_im = c1x * brh_im + c2x * bal_im - c3x * bbe_im;
+          const double by_re = c1y * brh_re + c2y * bal_re + c3y * bbe_re;
+          const double by_im = c1y * brh_im + c2y * bal_im + c3y * bbe_im;
+          const double bz_re = c1z * brh_re - c2z * bal_re;
+          const double bz_im = c1z * brh_im - c2z * bal_im;
+          const double vre = (qx * bx_re + qy * by_re + qz * bz_re) / rb;
+          const double vim = (qx * bx_im + qy * by_im + qz * bz_im) / rb;
+          if (m == 0) {
+            my[n * n] += vre;
+          } else {
+            my[n * n + 2 * m - 1] += vre;
+            my[n * n + 2 * m] += vim;
+          }
+          // advance the Legendre recurrence (kernel/multipoled.cxx:23-30)
+          const double pn2 = (xx * (2 * (n + 1) + 1) * p_np1 - (n + 1 + m) * p_n) / (n + 1 - m + 1);
+          p_n = p_np1;
+          p_np1 = pn2;
+          rn1 = rn;
+          rn *= rs;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += blockDim.x) M[(size_t)b * K + k] = acc[k] + acc[K + k] + acc[2 * K + k] + acc[3 * K + k];
+}
+
+// ---------------------------------------------------------------- M2M / L2L
+// Dense K x K operator per child octant (operators.cpp).
+__global__ void __launch_bounds__(128) m2m_f64(int K, const int* __restrict__ child_start, const int* __restrict__ child_count,
+                                               const int* __restrict__ child_keys, const double* __restrict__ Mc,
+                                               const double* __restrict__ ops, double* __restrict__ Mp) {
+  extern __shared__ double v[];
+  const int b = blockIdx.x;
+  const int c0 = child_start[b], nc = child_count[b];
+  double acc[4] = {0, 0, 0, 0};
+  for (int c = c0; c < c0 + nc; c++) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) v[k] = Mc[(size_t)c * K + k];
+    __syncthreads();
+    const double* T = ops + (size_t)(child_keys[c] & 7) * K * K;
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      const int row = threadIdx.x + r * 128;
+      if (row < K) {
+        double a = 0;
+        for (int k = 0; k < K; k++) a += T[(size_t)row * K + k] * v[k];
+        acc[r] += a;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int row = threadIdx.x + r * 128;
+    if (row < K) Mp[(size_t)b * K + row] = acc[r];
+  }
+}
+
+__global__ void __launch_bounds__(128) l2l_f64(int K, const int* __restrict__ parent, const int* __restrict__ keys,
+                                               const double* __restrict__ Lp, const double* __restrict__ ops,
+                                               double* __restrict__ Lc) {
+  extern __shared__ double v[];
+  const int b = blockIdx.x;
+  const int pb = parent[b];
+  for (int k = threadIdx.x; k < K; k += blockDim.x) v[k] = Lp[(size_t)pb * K + k];
+  __syncthreads();
+  const double* T = ops + (size_t)(keys[b] & 7) * K * K;
+  for (int row = threadIdx.x; row < K; row += blockDim.x) {
+    double a = 0;
+    for (int k = 0; k < K; k++) a += T[(size_t)row * K + k] * v[k];
+    Lc[(size_t)b * K + row] = a;  // the reference assigns (kernel/l2l.cxx:75-77)
+  }
+}
+
+// ---------------------------------------------------------------- M2L (FP64)
+// Target-stationary: each block owns a tile of target boxes of one octant at
+// one level (so they share one slot -> operator map), keeps their locals in
+// registers and walks the 189 slots; per slot the operator is streamed
+// through shared memory in column panels and applied to the gathered source
+// multipoles of the tile (a batched K x K x tile DGEMM).
+constexpr int kM2LTile = 32;   // target boxes per block
+constexpr int kM2LPanel = 16;  // operator columns per shared-memory panel
+constexpr int kM2LThreads = 256;
+
+__global__ void __launch_bounds__(kM2LThreads) m2l_f64(int K, int ntile, const int* __restrict__ tile_boxes,
+                                                       const int* __restrict__ tile_oct, const int* __restrict__ list,
+                                                       const int* __restrict__ slot_rel, const int* __restrict__ rel_to_op,
+                                                       const double* __restrict__ ops, const double* __restrict__ M,
+                                                       double* __restrict__ L) {
+  // rows of the output handled by this thread: row = ty + 16*r, boxes bx + 16*c
+  constexpr int RPT = 8;  // up to 128 rows (K <= 121 fits; larger K loops over row blocks)
+  __shared__ double sT[kM2LPanel][128 + 1];
+  __shared__ double sB[kM2LPanel][kM2LTile + 1];
+  __shared__ int sSrc[kM2LTile];
+  __shared__ int sBox[kM2LTile];
+  const int tile = blockIdx.x;
+  const int oct = tile_oct[tile];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads
+  if (threadIdx.x < kM2LTile) sBox[threadIdx.x] = tile_boxes[tile * kM2LTile + threadIdx.x];
+  __syncthreads();
+  for (int rb0 = 0; rb0 < K; rb0 += 128) {
+    double acc[RPT][2];
+#pragma unroll
+    for (int r = 0; r < RPT; r++) acc[r][0] = acc[r][1] = 0.0;
+    for (int slot = 0; slot < kM2LSlots; slot++) {
+      __syncthreads();
+      if (threadIdx.x < kM2LTile) {
+        const int box = sBox[threadIdx.x];
+        sSrc[threadIdx.x] = box >= 0 ? list[(size_t)box * kM2LSlots + slot] : -1;
+      }
+      __syncthreads();
+      int any = 0;
+      for (int t = 0; t < kM2LTile; t++) any |= (sSrc[t] >= 0);
+      if (!any) continue;
+      const double* T = ops + (size_t)rel_to_op[slot_rel[oct * kM2LSlots + slot]] * K * K;
+      for (int k0 = 0; k0 < K; k0 += kM2LPanel) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < kM2LPanel * 128; e += kM2LThreads) {
+          const int row = e / kM2LPanel, kk = e % kM2LPanel;
+          const int gr = rb0 + row, gk = k0 + kk;
+          sT[kk][row] = (gr < K && gk < K) ? T[(size_t)gr * K + gk] : 0.0;
+        }
+        for (int e = threadIdx.x; e < kM2LPanel * kM2LTile; e += kM2LThreads) {
+          const int t = e / kM2LPanel, kk = e % kM2LPanel;
+          const int src = sSrc[t], gk = k0 + kk;
+          sB[kk][t] = (src >= 0 && gk < K) ? M[(size_t)src * K + gk] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < kM2LPanel; kk++) {
+          const double b0 = sB[kk][tx], b1 = sB[kk][tx + 16];
+#pragma unroll
+          for (int r = 0; r < RPT; r++) {
+            const double a = sT[kk][ty + 16 * r];
+            acc[r][0] += a * b0;
+            acc[r][1] += a * b1;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < RPT; r++) {
+      const int row = rb0 + ty + 16 * r;
+      if (row < K) {
+        const int b0 = sBox[tx], b1 = sBox[tx + 16];
+        if (b0 >= 0) L[(size_t)b0 * K + row] += acc[r][0];
+        if (b1 >= 0) L[(size_t)b1 * K + row] += acc[r][1];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- L2P
+constexpr int kL2PThreads = 64;
+
+template <int KER>
+__global__ void __launch_bounds__(kL2PThreads) l2p_f64(int p, int K, const int* __restrict__ keys, const int2* __restrict__ leaf,
+                                                       const float4* __restrict__ tpos, const float4* __restrict__ tnrm,
+                                                       const double* __restrict__ fac, Sem s, float xmin, float ymin,
+                                                       float zmin, double rb, const double* __restrict__ L,
+                                                       double* __restrict__ pot, double* __restrict__ grad, int ni) {
+  extern __shared__ double sl[];
+  const int b = blockIdx.x;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) sl[k] = L[(size_t)b * K + k];
+  __syncthreads();
+  int cx = 0, cy = 0, cz = 0;
+  {
+    const int key = keys[b];
+    for (int i = 0; i < 10; i++) {
+      cy |= ((key >> (3 * i)) & 1) << i;
+      cx |= ((key >> (3 * i + 1)) & 1) << i;
+      cz |= ((key >> (3 * i + 2)) & 1) << i;
+    }
+  }
+  const double xc = (double)xmin + (cx + 0.5) * rb, yc = (double)ymin + (cy + 0.5) * rb, zc = (double)zmin + (cz + 0.5) * rb;
+  const int2 lf = leaf[b];
+  for (int ii = threadIdx.x; ii < lf.y; ii += blockDim.x) {
+    const int i = lf.x + ii;
+    const float4 xt = tpos[i];
+    const double x = (double)xt.x - xc, y = (double)xt.y - yc, z = (double)xt.z - zc;
+    const double r = sqrt(x * x + y * y + z * z) + s.rho_eps;
+    const double th = r == 0.0 ? 0.0 : acos(z / r);
+    const double ph = azimuth(x, y, s);
+    const double rs = r / rb;
+    const double xx = cos(th), yy = sin(th), s2 = sqrt((1 - xx) * (1 + xx));
+    double g = 0, gr = 0, gth = 0, gph = 0;
+    double pmm = 1.0, fact = 1.0, rm = 1.0, rm1 = 0.0;  // P_m^m, (2m+1), rs^m, rs^(m-1)
+    for (int m = 0; m <= p; m++) {
+      double sm, cm;
+      sincos(m * ph, &sm, &cm);
+      double p_n = pmm, p_np1 = xx * (2 * m + 1) * pmm;
+      double rn = rm, rn1 = rm1;
+      for (int n = m; n <= p; n++) {
+        const double f = fac[ifull_d(n, m)];
+        const double bnm = f * p_n;
+        const double bth = (n == m) ? f * (p_np1 - (m + 1) * xx * p_n) / yy
+                                    : f * ((n - m + 1) * p_np1 - (n + 1) * xx * p_n) / yy;
+        if (m == 0) {
+          const double a = sl[n * n];
+          g += rn * bnm * a;
+          gr += n * rn1 * bnm * a;
+          gth += rn * bth * a;
+        } else {
+          const double are = sl[n * n + 2 * m - 1], aim = sl[n * n + 2 * m];
+          const double re = cm * are - sm * aim;  // Re(e^{i m ph} L)
+          const double im = sm * are + cm * aim;  // Im(e^{i m ph} L)
+          g += 2 * rn * bnm * re;
+          gr += 2 * n * rn1 * bnm * re;
+          gth += 2 * rn * bth * re;
+          gph += -2 * m * rn * bnm * im;
+        }
+        const double pn2 = (xx * (2 * (n + 1) + 1) * p_np1 - (n + 1 + m) * p_n) / (n + 1 - m + 1);
+        p_n = p_np1;
+        p_np1 = pn2;
+        rn1 = rn;
+        rn *= rs;
+      }
+      pmm = -pmm * fact * s2;
+      fact += 2;
+      rm1 = rm;
+      rm *= rs;
+    }
+    const double st = sin(th), ct = cos(th), sp = sin(ph), cp = cos(ph);
+    const double ex = st * cp * gr + ct * cp / rs * gth - sp / rs / st * gph;
+    const double ey = st * sp * gr + ct * sp / rs * gth + cp / rs / st * gph;
+    const double ez = ct * gr - st / rs * gth;
+    const double c1 = s.coef / rb, c2 = s.coef / (rb * rb);
+    if (KER == FMMB_LAPLACE_GNI) {
+      const float4 nv = tnrm[i];
+      pot[i] = -c2 * ((double)nv.x * ex + (double)nv.y * ey + (double)nv.z * ez);
+    } else {
+      pot[i] = c1 * g;
+      if (KER == FMMB_LAPLACE_G && grad) {
+        grad[i] = c2 * ex;
+        grad[ni + i] = c2 * ey;
+        grad[2 * ni + i] = c2 * ez;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- outputs
+template <typename T>
+__global__ void finalize(int n, const int* perm, const double* pn, const double* pf, const double* gn, const double* gf,
+                         T* pot, T* grad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int o = perm[i];
+  pot[o] = (T)(pn[i] + pf[i]);
+  if (grad) {
+    grad[o] = (T)(gn[i] + gf[i]);
+    grad[n + o] = (T)(gn[n + i] + gf[n + i]);
+    grad[2 * n + o] = (T)(gn[2 * n + i] + gf[2 * n + i]);
+  }
+}
+
+// ---------------------------------------------------------------- direct
+template <int KER>
+__global__ void __launch_bounds__(128) direct_f64(int i0, int i1, const int* __restrict__ inv_i, const float4* __restrict__ tpos,
+                                                  const float4* __restrict__ tnrm, int nj, const float4* __restrict__ spos,
+                                                  const float4* __restrict__ snrm, const float* __restrict__ qs, Sem s,
+                                                  double* __restrict__ pot, double* __restrict__ grad) {
+  __shared__ float4 sp[128], sn[128];
+  __shared__ float sq[128];
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = i < i1;
+  const int si = act ? inv_i[i] : 0;
+  const float4 xi = tpos[si];
+  const float4 nv = tnrm[si];
+  double p = 0, fx = 0, fy = 0, fz = 0;
+  for (int j0 = 0; j0 < nj; j0 += 128) {
+    __syncthreads();
+    if (j0 + threadIdx.x < nj) {
+      sp[threadIdx.x] = spos[j0 + threadIdx.x];
+      sn[threadIdx.x] = snrm[j0 + threadIdx.x];
+      sq[threadIdx.x] = qs[j0 + threadIdx.x];
+    }
+    __syncthreads();
+    const int nl = min(128, nj - j0);
+    for (int jj = 0; jj < nl; jj++) {
+      const float4 xj = sp[jj];
+      double dx, dy, dz;
+      if (s.ref) {
+        dx = (double)__fsub_rn(xi.x, xj.x);
+        dy = (double)__fsub_rn(xi.y, xj.y);
+        dz = (double)__fsub_rn(xi.z, xj.z);
+      } else {
+        dx = (double)xi.x - (double)xj.x;
+        dy = (double)xi.y - (double)xj.y;
+        dz = (double)xi.z - (double)xj.z;
+      }
+      if (s.excl_self && dx == 0.0 && dy == 0.0 && dz == 0.0) continue;
+      const double r2 = dx * dx + dy * dy + dz * dz + s.eps2;
+      const double rinv = 1.0 / sqrt(r2);
+      const double qr = s.coef * (double)sq[jj] * rinv;
+      if (KER == FMMB_LAPLACE_G) {
+        p += qr;
+        const double qr3 = qr * rinv * rinv;
+        fx -= dx * qr3;
+        fy -= dy * qr3;
+        fz -= dz * qr3;
+      } else if (KER == FMMB_LAPLACE_GNI) {
+        p += (dx * nv.x + dy * nv.y + dz * nv.z) * qr * rinv * rinv;
+      } else {
+        const float4 nj4 = sn[jj];
+        p += (dx * nj4.x + dy * nj4.y + dz * nj4.z) * qr * rinv * rinv;
+      }
+    }
+  }
+  if (act) {
+    pot[i - i0] = p;
+    if (KER == FMMB_LAPLACE_G && grad) {
+      const int m = i1 - i0;
+      grad[i - i0] = fx;
+      grad[m + i - i0] = fy;
+      grad[2 * m + i - i0] = fz;
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- launchers
+void launch_gather_charges(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st) {
+  gather_charges<<<nblk(n, 256), 256, 0, st>>>(n, nrhs, perm, q, qs);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_p2p_f64(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
+                    const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot,
+                    double* grad, int ni, cudaStream_t st) {
+  if (nleaf <= 0) return;
+  if (kernel == FMMB_LAPLACE_G)
+    p2p_f64<FMMB_LAPLACE_G><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+  else if (kernel == FMMB_LAPLACE_GNI)
+    p2p_f64<FMMB_LAPLACE_GNI><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+  else
+    p2p_f64<FMMB_LAPLACE_GNJ><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_p2m(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos, const float4* snrm,
+                const float* qs, const double* fac, const Sem& s, const float* bbox, double rb, double* M, cudaStream_t st) {
+  if (nleaf <= 0) return;
+  const size_t sm = 4 * (size_t)K * sizeof(double);
+  if (kernel == FMMB_LAPLACE_GNJ)
+    p2m_f64<FMMB_LAPLACE_GNJ><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, s, bbox[0], bbox[1], bbox[2], rb, M);
+  else
+    p2m_f64<FMMB_LAPLACE_G><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, s, bbox[0], bbox[1], bbox[2], rb, M);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_m2m(int nparent, int K, const int* child_start, const int* child_count, const int* child_keys, const double* Mc,
+                const double* ops, double* Mp, cudaStream_t st) {
+  if (nparent <= 0) return;
+  m2m_f64<<<nparent, 128, K * sizeof(double), st>>>(K, child_start, child_count, child_keys, Mc, ops, Mp);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_l2l(int nchild, int K, const int* parent, const int* keys, const double* Lp, const double* ops, double* Lc,
+                cudaStream_t st) {
+  if (nchild <= 0) return;
+  l2l_f64<<<nchild, 128, K * sizeof(double), st>>>(K, parent, keys, Lp, ops, Lc);
+  FMMB_CHECK_LAUNCH();
+}
+
+int m2l_tile_size() { return kM2LTile; }
+
+void launch_m2l_f64(int ntile, int K, const int* tile_boxes, const int* tile_oct, const int* list, const int* slot_rel,
+                    const int* rel_to_op, const double* ops, const double* M, double* L, cudaStream_t st) {
+  if (ntile <= 0) return;
+  m2l_f64<<<ntile, kM2LThreads, 0, st>>>(K, ntile, tile_boxes, tile_oct, list, slot_rel, rel_to_op, ops, M, L);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_l2p(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos, const float4* tnrm,
+                const double* fac, const Sem& s, const float* bbox, double rb, const double* L, double* pot, double* grad,
+                int ni, cudaStream_t st) {
+  if (nleaf <= 0) return;
+  const size_t sm = (size_t)K * sizeof(double);
+  if (kernel == FMMB_LAPLACE_G)
+    l2p_f64<FMMB_LAPLACE_G><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, s, bbox[0], bbox[1], bbox[2], rb, L, pot, grad, ni);
+  else if (kernel == FMMB_LAPLACE_GNI)
+    l2p_f64<FMMB_LAPLACE_GNI><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, s, bbox[0], bbox[1], bbox[2], rb, L, pot, grad, ni);
+  else
+    l2p_f64<FMMB_LAPLACE_GNJ><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, s, bbox[0], bbox[1], bbox[2], rb, L, pot, grad, ni);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_finalize_f32(int n, const int* perm, const double* pn, const double* pf, const double* gn, const double* gf, float* pot,
+                         float* grad, cudaStream_t st) {
+  finalize<float><<<nblk(n, 256), 256, 0, st>>>(n, perm, pn, pf, gn, gf, pot, grad);
+  FMMB_CHECK_LAUNCH();
+}
+void launch_finalize_f64(int n, const int* perm, const double* pn, const double* pf, const double* gn, const double* gf, double* pot,
+                         double* grad, cudaStream_t st) {
+  finalize<double><<<nblk(n, 256), 256, 0, st>>>(n, perm, pn, pf, gn, gf, pot, grad);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float4* tpos, const float4* tnrm, int nj,
+                       const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot, double* grad,
+                       cudaStream_t st) {
+  const int m = i1 - i0;
+  if (m <= 0) return;
+  if (kernel == FMMB_LAPLACE_G)
+    direct_f64<FMMB_LAPLACE_G><<<nblk(m, 128), 128, 0, st>>>(i0, i1, inv_i, tpos, tnrm, nj, spos, snrm, qs, s, pot, grad);
+  else if (kernel == FMMB_LAPLACE_GNI)
+    direct_f64<FMMB_LAPLACE_GNI><<<nblk(m, 128), 128, 0, st>>>(i0, i1, inv_i, tpos, tnrm, nj, spos, snrm, qs, s, pot, grad);
+  else
+    direct_f64<FMMB_LAPLACE_GNJ><<<nblk(m, 128), 128, 0, st>>>(i0, i1, inv_i, tpos, tnrm, nj, spos, snrm, qs, s, pot, grad);
+  FMMB_CHECK_LAUNCH();
+}
+
+}  // namespace fmmb

@@ -1,0 +1,189 @@
+"""GPU parity of libfmmb against the oracle (restatement pinned to the
+reference) and the reference's golden vectors, through the C ABI.
+
+Tolerances:
+* tree, permutations, leaf ranges, lists: bit-exact;
+* expansions and potentials, FP64 form vs oracle on the same semantics:
+  1e-10 relative (rounding order only);
+* FP64 form vs the reference's own float outputs (golden): 1e-6 relative
+  (the reference accumulates its outputs in float);
+* accuracy vs the FP64 direct sum (accurate semantics): the FMM truncation
+  error of the order used, stated per test.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "ref_fmm_*.npz")))
+
+
+@pytest.fixture(scope="module")
+def ob():
+    import old_fmm_bem_b200 as ob
+    from old_fmm_bem_b200 import build
+    build.build()
+    return ob
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+
+def make_points(n, seed, kind="uniform"):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        t = rng.random((3, n), dtype=np.float32)
+        s = rng.random((3, n), dtype=np.float32)
+    else:  # clustered: uneven leaves and empty boxes
+        c = rng.random((3, 8))
+        t = np.clip(c[:, rng.integers(0, 8, n)] + 0.06 * rng.standard_normal((3, n)), 0, 1).astype(np.float32)
+        s = np.clip(c[:, rng.integers(0, 8, n)] + 0.06 * rng.standard_normal((3, n)), 0, 1).astype(np.float32)
+    tn = rng.standard_normal((3, n)).astype(np.float32)
+    tn /= np.linalg.norm(tn, axis=0)
+    sn = rng.standard_normal((3, n)).astype(np.float32)
+    sn /= np.linalg.norm(sn, axis=0)
+    q = rng.uniform(-1, 1, n).astype(np.float32)
+    return t, tn, s, sn, q
+
+
+def plan_for(ob, neq, p, lmax, t, tn, s, sn, bbox=(0, 0, 0, 1), **kw):
+    pl = ob.Plan(kernel=neq, p=p, lmax=lmax, **kw)
+    pl.set_geometry(t, s, tn if neq == 1 else None, sn if neq == 2 else None, bbox=bbox)
+    return pl
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_tree_and_potentials_match_reference_golden(path, ob, oracle):
+    d = np.load(path)
+    p, lmax = int(d["p"]), int(d["lmax"])
+    for neq in (0, 1, 2):
+        pl = plan_for(ob, neq, p, lmax, d["t"], d["tn"], d["s"], d["sn"])
+        if neq == 0:
+            assert np.array_equal(pl.tree(0), d["perm_i"])
+            assert np.array_equal(pl.tree(1), d["perm_j"])
+            assert np.array_equal(pl.tree(6), d["leaf_i"])
+            assert np.array_equal(pl.tree(7), d["leaf_j"])
+            la, lb = oracle.parse_lists(pl.tree(8)), oracle.parse_lists(d["lists"])
+            assert len(la) == len(lb)
+            for x, y in zip(la, lb):
+                assert x[0] == y[0] and x[1] == y[1] and x[3] == y[3]
+        v, g = pl.evaluate(d["q"], f64=True)
+        ref = d[f"v{neq}"].astype(np.float64)
+        assert rel(v, ref) < 1e-6
+        if neq == 0:
+            assert rel(g.reshape(3, -1), d["g0"]) < 1e-6
+        pl.close()
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clustered"])
+@pytest.mark.parametrize("lmax", [2, 3, 4])
+def test_tree_bit_exact_vs_oracle(kind, lmax, ob, oracle):
+    t, tn, s, sn, q = make_points(6000 if lmax < 4 else 20000, 30 + lmax, kind)
+    pl = plan_for(ob, 0, 4, lmax, t, tn, s, sn)
+    oracle.oracle_fmm(t, s, q, neq=0, p=4, lmax=lmax)
+    rec = oracle.oracle_records()
+    for k in (0, 1, 2, 3, 4, 5, 6, 7, 8):
+        assert np.array_equal(pl.tree(k), rec[k]), k
+    pl.close()
+
+
+@pytest.mark.parametrize("neq", [0, 1, 2])
+@pytest.mark.parametrize("semantics", [0, 1])
+def test_fp64_expansions_and_potential_vs_oracle(neq, semantics, ob, oracle):
+    """Per-operator parity: multipoles (P2P/P2M/M2M) and locals (M2L/L2L) of
+    every level, then the potentials, FP64 form vs the restated reference."""
+    t, tn, s, sn, q = make_points(8000, 40 + neq, "clustered")
+    p, lmax = 6, 3
+    ref_sem = semantics == 0
+    pl = plan_for(ob, neq, p, lmax, t, tn, s, sn, semantics=semantics)
+    v, g = pl.evaluate(q, f64=True)
+    vo, go = oracle.oracle_fmm(t, s, q, neq=neq, p=p, lmax=lmax, tn=tn, sn=sn, ref_semantics=ref_sem,
+                               eps2=oracle.EPS_REF if ref_sem else 0.0, exclude_self=not ref_sem)
+    Mo, Lo = oracle.oracle_expansions(0), oracle.oracle_expansions(1)
+    Mg, Lg = pl.expansions(0), pl.expansions(1)
+    assert rel(Mg, Mo) < 1e-10
+    assert rel(Lg, Lo) < 1e-10
+    # the oracle accumulates outputs in float in reference semantics
+    tol = 1e-6 if ref_sem else 1e-10
+    assert rel(v, vo) < tol
+    if neq == 0:
+        assert rel(g.reshape(3, -1), go) < tol
+    pl.close()
+
+
+def test_direct_matches_oracle(ob, oracle):
+    t, tn, s, sn, q = make_points(3000, 50)
+    for neq in (0, 1, 2):
+        pl = plan_for(ob, neq, 4, 2, t, tn, s, sn, semantics=1, exclude_self=True)
+        v, g = pl.direct(q, 100, 600)
+        vo, go = oracle.direct(t, s, q, neq=neq, eps2=0.0, exclude_self=True, tn=tn, sn=sn, targets=(100, 600))
+        assert rel(v, vo) < 1e-12
+        if neq == 0:
+            assert rel(g, go) < 1e-12
+        pl.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_accuracy_vs_fp64_direct(precision, ob, oracle):
+    """Accurate semantics, p=12: relative error of the potential below 1e-6
+    against the FP64 direct sum (self pairs excluded, no softening)."""
+    n = 20000
+    rng = np.random.default_rng(60)
+    x = rng.random((3, n), dtype=np.float32)
+    q = rng.uniform(-1, 1, n).astype(np.float32)
+    pl = ob.Plan(kernel=0, p=12, lmax=3, precision=precision, semantics=1, exclude_self=True)
+    pl.set_geometry(x, x, bbox=(0, 0, 0, 1))
+    v, g = pl.evaluate(q, f64=True)
+    vd, gd = oracle.direct(x, x, q, neq=0, eps2=0.0, exclude_self=True, targets=(0, 1024))
+    assert rel(v[:1024], vd) < 1e-6
+    assert rel(g.reshape(3, -1)[:, :1024], gd) < 1e-5
+    pl.close()
+
+
+def test_mixed_matches_fp64(ob):
+    t, tn, s, sn, q = make_points(30000, 70, "clustered")
+    for neq in (0, 1, 2):
+        out = []
+        for prec in (0, 1):
+            pl = plan_for(ob, neq, 10, 4, t, tn, s, sn, semantics=1, precision=prec, exclude_self=True)
+            out.append(pl.evaluate(q, f64=True))
+            pl.close()
+        assert rel(out[1][0], out[0][0]) < 1e-6
+
+
+def test_host_and_device_pointers_agree(ob):
+    torch = pytest.importorskip("torch")
+    t, tn, s, sn, q = make_points(5000, 80)
+    pl = plan_for(ob, 0, 8, 3, t, tn, s, sn)
+    vh, gh = pl.evaluate(q)
+    qd = torch.from_numpy(q).cuda()
+    vd = torch.zeros(5000, device="cuda")
+    gd = torch.zeros(15000, device="cuda")
+    pl.evaluate(qd, vd, gd)
+    torch.cuda.synchronize()
+    assert np.array_equal(vh, vd.cpu().numpy())
+    assert np.array_equal(gh, gd.cpu().numpy())
+    # geometry from device tensors gives the same tree
+    pl2 = ob.Plan(kernel=0, p=8, lmax=3)
+    pl2.set_geometry(torch.from_numpy(t).cuda(), torch.from_numpy(s).cuda(), bbox=(0, 0, 0, 1))
+    assert np.array_equal(pl2.tree(8), pl.tree(8))
+    pl.close()
+    pl2.close()
+
+
+def test_errors_are_reported_not_fatal(ob):
+    with pytest.raises(ob.FMMError):
+        ob.Plan(p=0)
+    with pytest.raises(ob.FMMError):
+        ob.Plan(lmax=1)
+    pl = ob.Plan(kernel=1)
+    t, tn, s, sn, q = make_points(100, 90)
+    with pytest.raises(ob.FMMError):  # Gni without target normals
+        pl.set_geometry(t, s)
+    with pytest.raises(ob.FMMError):  # evaluate before geometry
+        pl.evaluate(q)
+    pl.close()
