@@ -1,0 +1,321 @@
+#!/usr/bin/env python
+"""Benchmark: Laplace double-layer (Gnj) BEM matvec, FMM on one B200 per rank.
+
+Workload (one "step" = one FMM matvec over the whole surface):
+  icosphere of radius 1 subdivided 6 times (81,920 triangles), 3 Gauss points
+  per triangle (245,760 points), outward unit normals, panel densities
+  U[-1, 1] times the quadrature weights as charges; targets = the same points,
+  zero-distance pairs excluded; order p = 10, mixed precision.
+Metric: FMM matvec Mpts/s (targets per second of one matvec on a built tree).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own independent problem (a different
+density seed): the FMM of one surface does not shard, so N GPUs run N
+independent matvecs (weak scaling, no collective on the data path).  The
+reference arm (--impl reference) times the reference's own CPU fmm() (built
+from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P_ORDER = 10
+SUBDIV = 6
+LMAX = 5
+METRIC = "FMM matvec Mpts/s (Laplace Gn double-layer BEM, 245,760 pts, p=10)"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def workload(seed):
+    from old_fmm_bem_b200 import geometry
+    return geometry.bem_double_layer_problem(SUBDIV, seed=seed)
+
+
+# ------------------------------------------------------------------ reference arm
+def _ref_sample():
+    """Bounded sample of the workload for the CPU reference: the same surface
+    family at 4 subdivisions (5,120 triangles, 15,360 points), lmax 3."""
+    from old_fmm_bem_b200 import geometry
+    return geometry.bem_double_layer_problem(4, seed=1), 3
+
+
+def _ref_worker(args):
+    from oracle import pyoracle
+    rep = args
+    (x, n, q), lmax = _ref_sample()
+    lo = x.min(axis=1)
+    rd = float((x.max(axis=1) - lo).max() * (1 + 1e-5))
+    t0 = time.perf_counter()
+    for _ in range(rep):
+        pyoracle.ref_fmm(x, x, q, neq=2, p=P_ORDER, lmax=lmax, sn=n, bbox=(lo[0], lo[1], lo[2], rd))
+    return time.perf_counter() - t0, x.shape[1] * rep
+
+
+def cpu_reference_time(workers, rep=1, pool=None):
+    if pool is None:
+        return _ref_worker(rep)
+    res = pool.map(_ref_worker, [rep] * workers)
+    return max(r[0] for r in res), sum(r[1] for r in res)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    if not pyoracle.ref_available(P_ORDER):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference library not built"}))
+        return
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            cpu_reference_time(cores, 1, pool)
+        t0 = time.perf_counter()
+        pts = 0
+        for _ in range(args.steps):
+            dt, n = cpu_reference_time(cores, 1, pool)
+            pts += n
+        el = time.perf_counter() - t0
+    value = pts / el / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Laplace Gnj double-layer matvec, icosphere r=1, p=10 (reference CPU fmm(), "
+                                   "bounded sample: 4 subdivisions, 15,360 points, lmax 3, one process per core)",
+                       "points_per_process": 15360, "processes": cores},
+            "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "reference",
+                             "sample": "reference fmm(ni,nj,2) at p=10 on a 15,360-point icosphere, one per core"},
+            "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args, rank, world):
+    import torch
+    import old_fmm_bem_b200 as ob
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    x, n, q = workload(seed=rank)
+    npts = x.shape[1]
+    stream = torch.cuda.Stream()
+    plan = ob.Plan(kernel=ob.LAPLACE_GNJ, p=P_ORDER, lmax=LMAX, precision=ob.MIXED if args.precision == "mixed" else ob.FP64,
+                   semantics=ob.SEM_ACCURATE, exclude_self=True)
+    plan.set_stream(stream)
+    xd, nd = torch.from_numpy(x).cuda(), torch.from_numpy(n).cuda()
+    plan.set_geometry(xd, xd, source_normals=nd)
+    qd = torch.from_numpy(q).cuda()
+    pot = torch.zeros(npts, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        plan.evaluate(qd, pot)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+
+    # device-resident timed region: per-step CUDA events on the plan's stream,
+    # L2 flushed between steps (outside the events)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    phase = np.zeros(7)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                ev[k][0].record(stream)
+                step()
+                ev[k][1].record(stream)
+                stream.synchronize()
+                phase += np.array(list(plan.timings().values()))
+        torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    ms_step = float(np.mean(ms))
+    phase /= args.steps
+    launches = plan.stats()["launches"]
+    if world > 1:
+        t = torch.tensor([ms_step], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_step = float(t.item())
+
+    # end to end through the public API with host (pinned) buffers: the copy of
+    # the charges in and of the potentials out are inside the timed call
+    qh = torch.from_numpy(q).pin_memory()
+    ph = torch.zeros(npts).pin_memory()
+    e2e = []
+    for k in range(max(3, args.steps // 2)):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plan.evaluate(qh.numpy(), ph.numpy())
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e))
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    if rank != 0:
+        plan.close()
+        return
+    st = plan.stats()
+    peaks, peak_kind = measured_peaks()
+    names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
+    dom = int(np.argmax(phase[:6]))
+    if names[dom] == "m2l":
+        K = (P_ORDER + 1) ** 2
+        flops = 2.0 * K * K * st["m2l_pairs"]
+        achieved = flops / (phase[3] * 1e-3) / 1e12
+        peak = peaks["bf16_tflops"] / 2 if args.precision == "mixed" else None
+        roof = {"kernel": "m2l", "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None, "traffic": None,
+                "note": f"algorithmic 2*K^2 flops per box pair (K={K}); peak = TF32 dense = half of {peak_kind} bf16"}
+    else:
+        flops = 20.0 * st["p2p_pairs"]
+        achieved = flops / (phase[0] * 1e-3) / 1e12
+        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
+        roof = {"kernel": "p2p", "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": None,
+                "note": "20 flops per pair; peak = 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz (nominal)"}
+    # CPU baseline: the reference's own fmm() on a bounded sample, one core
+    cpu = None
+    if not args.no_cpu:
+        try:
+            from oracle import pyoracle
+            if pyoracle.ref_available(P_ORDER):
+                dt, npt = cpu_reference_time(1, rep=2)
+                cpu = {"value": npt / dt / 1e6, "unit": "Mpts/s", "cores": 1, "kind": "reference",
+                       "sample": "reference fmm(ni,nj,2) at p=10 on a 15,360-point icosphere (4 subdivisions, "
+                                 "lmax 3), 2 runs, 1 core"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"error": str(e)}
+    value = world * npts / (ms_step * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+tf32x3+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": "Laplace Gnj double-layer BEM matvec, icosphere r=1, 81,920 triangles x 3 Gauss "
+                               "points = 245,760 points, p=10, lmax=5, self pairs excluded",
+                   "precision": args.precision, "points": npts, "p": P_ORDER, "lmax": LMAX,
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "phase_ms": dict(zip(names + ["total"], [float(v) for v in phase])),
+        "stats": st,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * npts / e2e_s / 1e6, "unit": "Mpts/s", "h2d_bytes_per_step": 4 * npts,
+                "d2h_bytes_per_step": 4 * npts},
+        "gpu_launches": launches * args.steps,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+    plan.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+    if world > 1 and args.impl == "ours":
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -128,14 +128,16 @@ FMMB_API int fmmb_get_tree(fmmb_plan* plan, int kind, int* out);
 FMMB_API long fmmb_get_expansion_size(fmmb_plan* plan, int which);
 FMMB_API int fmmb_get_expansions(fmmb_plan* plan, int which, double* out);
 
-/* Device time in ms of the phases of the last evaluate:
- * [0] P2P, [1] P2M, [2] M2M, [3] M2L, [4] L2L, [5] L2P, [6] whole evaluate. */
+/* Device time in ms of the phases of the last evaluate, summed over the
+ * launches of each phase (all right-hand sides): [0] P2P, [1] P2M, [2] M2M,
+ * [3] M2L, [4] L2L, [5] L2P, [6] whole evaluate (P2P overlaps the far field). */
 FMMB_API int fmmb_get_timings(fmmb_plan* plan, float* ms7);
 
 /* Counts of the current geometry: [0] ni, [1] nj, [2] target leaves,
  * [3] source leaves, [4] P2P pairs (sum over near-field leaf pairs of
- * ni*nj), [5] M2L box pairs, [6] lmax. */
-FMMB_API int fmmb_get_stats(fmmb_plan* plan, long long* out7);
+ * ni*nj), [5] M2L box pairs, [6] lmax, [7] kernel launches of the last
+ * evaluate. */
+FMMB_API int fmmb_get_stats(fmmb_plan* plan, long long* out8);
 
 FMMB_API const char* fmmb_last_error(void);
 

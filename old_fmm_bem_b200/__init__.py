@@ -202,12 +202,12 @@ class Plan:
     def timings(self):
         ms = np.zeros(7, np.float32)
         _check(load().fmmb_get_timings(self._h, ms.ctypes.data))
-        return dict(zip(["p2p", "p2m", "m2m", "m2l_l2l", "l2l", "l2p", "total"], ms.tolist()))
+        return dict(zip(["p2p", "p2m", "m2m", "m2l", "l2l", "l2p", "total"], ms.tolist()))
 
     def stats(self):
-        o = np.zeros(7, np.int64)
+        o = np.zeros(8, np.int64)
         _check(load().fmmb_get_stats(self._h, o.ctypes.data))
-        return dict(zip(["ni", "nj", "leaves_i", "leaves_j", "p2p_pairs", "m2l_pairs", "lmax"], o.tolist()))
+        return dict(zip(["ni", "nj", "leaves_i", "leaves_j", "p2p_pairs", "m2l_pairs", "lmax", "launches"], o.tolist()))
 
 
 def fmm(xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, gxj, gyj, gzj, vj, neq, *, lmax, xmin, ymin, zmin, rd, p=8,

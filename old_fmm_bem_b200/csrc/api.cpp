@@ -147,6 +147,11 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.fork, cudaEventDisableTiming));
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.join, cudaEventDisableTiming));
       for (auto& e : pl->ev) FMMB_CUDA(cudaEventCreate(&e));
+      for (auto& e : pl->evp) FMMB_CUDA(cudaEventCreate(&e));
+      pl->d_err.alloc(1);
+      FMMB_CUDA(cudaMemset(pl->d_err.get(), 0, sizeof(int)));
+      FMMB_CUDA(cudaHostAlloc((void**)&pl->h_err, sizeof(int), cudaHostAllocDefault));
+      *pl->h_err = 0;
       build_static_operators(pl->ops, pl->p, pl->ref);
       upload_static_ops(pl);
       if (!pl->ref) {  // geometry-independent M2L set
@@ -170,6 +175,9 @@ int fmmb_plan_destroy(fmmb_plan* pl) {
   if (pl->st.join) cudaEventDestroy(pl->st.join);
   for (auto& e : pl->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : pl->evp)
+    if (e) cudaEventDestroy(e);
+  if (pl->h_err) cudaFreeHost(pl->h_err);
   delete pl;
   return FMMB_OK;
 }
@@ -246,6 +254,70 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         FMMB_CUDA(cudaMemcpy(pl->tile_oct[lev]->get(), to.data(), to.size() * sizeof(int), cudaMemcpyHostToDevice));
       }
     }
+    // tensor-core M2L (mixed precision, K <= 128): operator images and work items
+    pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= 128;
+    if (pl->use_tc) {
+      if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_opimg.get() == nullptr) {
+        std::vector<float> img;
+        build_m2l_images(pl->ops, img);
+        pl->d_opimg.alloc(img.size());
+        FMMB_CUDA(cudaMemcpy(pl->d_opimg.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
+        pl->opimg_sets = pl->ops.m2l_sets;
+        pl->opimg_rd = pl->ops.m2l_rd;
+      }
+      std::vector<int> lst((size_t)pl->tot_i * kM2LSlots);
+      FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+      const int TT = m2l_tc_tile();
+      std::vector<int> tb, to, tl;
+      std::vector<std::vector<int>> tslots;
+      for (int lev = 2; lev <= pl->lmax; lev++)
+        for (int oct = 0; oct < 8; oct++) {
+          std::vector<int> bx;
+          for (int b = 0; b < pl->nbox_i[lev]; b++)
+            if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
+          for (size_t k = 0; k < bx.size(); k += TT) {
+            std::vector<int> act;
+            for (int sl = 0; sl < kM2LSlots; sl++) {
+              bool any = false;
+              for (size_t t = k; t < std::min(bx.size(), k + TT) && !any; t++) any = lst[(size_t)bx[t] * kM2LSlots + sl] >= 0;
+              if (any) act.push_back(sl);
+            }
+            if (act.empty()) continue;
+            for (int t = 0; t < TT; t++) tb.push_back(k + t < bx.size() ? bx[k + t] : -1);
+            to.push_back(oct);
+            tl.push_back(lev);
+            tslots.push_back(act);
+          }
+        }
+      const int ntile = (int)to.size();
+      // split tiles over their slots so that the launch has ~2 work items per SM
+      int dev_sms = 148;
+      cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
+      pl->tc_nsplit = ntile > 0 ? std::max(1, std::min(8, (2 * dev_sms + ntile - 1) / ntile)) : 1;
+      std::vector<int> wt, off{0}, sl;
+      for (int t = 0; t < ntile; t++) {
+        const int n = (int)tslots[t].size();
+        for (int k = 0; k < pl->tc_nsplit; k++) {
+          const int a = (int)((long long)n * k / pl->tc_nsplit), b = (int)((long long)n * (k + 1) / pl->tc_nsplit);
+          if (b <= a) continue;
+          wt.push_back(t);
+          for (int i = a; i < b; i++) sl.push_back(tslots[t][i]);
+          off.push_back((int)sl.size());
+        }
+      }
+      pl->tc_nwork = (int)wt.size();
+      auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+        d.alloc(h.size());
+        if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+      };
+      up(pl->tc_boxes, tb);
+      up(pl->tc_oct, to);
+      up(pl->tc_level, tl);
+      up(pl->tc_work_tile, wt);
+      up(pl->tc_slot_off, off);
+      up(pl->tc_slots, sl);
+      pl->Mtf.alloc((size_t)pl->tot_j * 256);
+    }
     // inverse target permutation (caller -> sorted) for the direct sum
     {
       std::vector<int> perm(ni), inv(ni);
@@ -271,6 +343,28 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
 
 namespace {
 
+// Brackets one launch with a pair of pool events (phase 0..5 as in
+// fmmb_get_timings); silently stops timing when the pool is exhausted.
+struct PhaseTimer {
+  fmmb_plan* pl;
+  int phase, idx;
+  cudaStream_t s;
+  PhaseTimer(fmmb_plan* p, int ph, cudaStream_t st) : pl(p), phase(ph), idx(-1), s(st) {
+    if (pl->ev_used + 2 <= fmmb_plan::kEvPool) {
+      idx = pl->ev_used;
+      pl->ev_used += 2;
+      FMMB_CUDA(cudaEventRecord(pl->evp[idx], s));
+    }
+    pl->launches++;
+  }
+  ~PhaseTimer() {
+    if (idx >= 0) {
+      cudaEventRecord(pl->evp[idx + 1], s);
+      pl->ev_phase.push_back({phase, idx});
+    }
+  }
+};
+
 // Runs one right-hand side: qs (sorted, device) -> near/far sorted outputs.
 void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   const int K = pl->K, p = pl->p, lmax = pl->lmax, ker = pl->cfg.kernel;
@@ -285,41 +379,87 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
   FMMB_CUDA(cudaEventRecord(pl->ev[0], side));
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
+  {
+  PhaseTimer tm(pl, 0, side);
   if (pl->cfg.precision == FMMB_MIXED)
     launch_p2p_mixed(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
                      pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
   else
     launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
                    pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+  }
   FMMB_CUDA(cudaEventRecord(pl->ev[1], side));
   FMMB_CUDA(cudaEventRecord(pl->st.join, side));
 
   // far field on the main stream
   FMMB_CUDA(cudaEventRecord(pl->ev[2], m));
   const double rb_leaf = (double)(pl->bbox[3] / (float)(1 << lmax));
-  launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(), qs,
-             pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+  {
+    PhaseTimer tm(pl, 1, m);
+    launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(), qs,
+               pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+  }
   FMMB_CUDA(cudaEventRecord(pl->ev[3], m));
-  for (int lev = lmax - 1; lev >= 2; lev--)
+  for (int lev = lmax - 1; lev >= 2; lev--) {
+    PhaseTimer tm(pl, 2, m);
     launch_m2m(pl->nbox_j[lev], K, pl->child_start_j.get() + pl->off_j[lev], pl->child_count_j.get() + pl->off_j[lev],
                pl->key_j.get() + pl->off_j[lev + 1], pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->d_m2m.get(),
                pl->M.get() + (size_t)pl->off_j[lev] * K, m);
+  }
   FMMB_CUDA(cudaEventRecord(pl->ev[4], m));
-  const size_t opsz = (size_t)316 * K * K;
-  for (int lev = 2; lev <= lmax; lev++) {
-    double* Ll = pl->L.get() + (size_t)pl->off_i[lev] * K;
-    if (lev == 2) FMMB_CUDA(cudaMemsetAsync(Ll, 0, (size_t)pl->nbox_i[2] * K * sizeof(double), m));
-    else
-      launch_l2l(pl->nbox_i[lev], K, pl->parent_i.get() + pl->off_i[lev], pl->key_i.get() + pl->off_i[lev],
-                 pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->d_l2l.get(), Ll, m);
-    const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
-    launch_m2l_f64(pl->tile_n[lev], K, pl->tile_boxes[lev]->get(), pl->tile_oct[lev]->get(), pl->m2l_list.get(), pl->d_slot_rel.get(),
-                   pl->d_rel_to_op.get(), pl->d_m2l.get() + set * opsz, pl->M.get() + (size_t)pl->off_j[lev] * K,
-                   pl->L.get(), m);
+  // downward pass: M2L of every level into zeroed locals, then each level
+  // adds its parent's translated local (L2L), top down
+  FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * K * sizeof(double), m));
+  if (pl->use_tc) {
+    {
+      PhaseTimer tm(pl, 3, m);
+      launch_split_tf32(pl->tot_j, K, pl->M.get(), pl->Mtf.get(), m);
+    }
+    PhaseTimer tm(pl, 3, m);
+    M2LTcArgs a{};
+    a.nwork = pl->tc_nwork;
+    a.K = K;
+    a.atomic = pl->tc_nsplit > 1 ? 1 : 0;
+    a.tile_boxes = pl->tc_boxes.get();
+    a.tile_oct = pl->tc_oct.get();
+    a.tile_level = pl->tc_level.get();
+    a.work_tile = pl->tc_work_tile.get();
+    a.slot_off = pl->tc_slot_off.get();
+    a.slots = pl->tc_slots.get();
+    a.list = pl->m2l_list.get();
+    a.slot_rel = pl->d_slot_rel.get();
+    a.rel_to_op = pl->d_rel_to_op.get();
+    a.opimg = pl->d_opimg.get();
+    const long long set_floats = (long long)316 * 4 * 2 * 128 * 32;
+    for (int l = 0; l < 11; l++) {
+      a.op_set_off[l] = (pl->ops.m2l_sets > 1 && l >= 2) ? (long long)(l - 2) * set_floats : 0;
+      a.mtf_box_off[l] = (l >= 2 && l <= lmax) ? pl->off_j[l] : 0;
+    }
+    a.Mtf = pl->Mtf.get();
+    a.L = pl->L.get();
+    a.err = pl->d_err.get();
+    launch_m2l_tc(a, m);
+  } else {
+    const size_t opsz = (size_t)316 * K * K;
+    for (int lev = 2; lev <= lmax; lev++) {
+      PhaseTimer tm(pl, 3, m);
+      const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
+      launch_m2l_f64(pl->tile_n[lev], K, pl->tile_boxes[lev]->get(), pl->tile_oct[lev]->get(), pl->m2l_list.get(),
+                     pl->d_slot_rel.get(), pl->d_rel_to_op.get(), pl->d_m2l.get() + set * opsz,
+                     pl->M.get() + (size_t)pl->off_j[lev] * K, pl->L.get(), m);
+    }
+  }
+  for (int lev = 3; lev <= lmax; lev++) {
+    PhaseTimer tm(pl, 4, m);
+    launch_l2l(pl->nbox_i[lev], K, pl->parent_i.get() + pl->off_i[lev], pl->key_i.get() + pl->off_i[lev],
+               pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->d_l2l.get(), pl->L.get() + (size_t)pl->off_i[lev] * K, m);
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[5], m));
-  launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
-             pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
+  {
+    PhaseTimer tm(pl, 5, m);
+    launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
+               pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
+  }
   FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
   FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));
 }
@@ -332,9 +472,19 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     cudaStream_t m = pl->st.main;
     const int ni = pl->ni, nj = pl->nj, nr = pl->cfg.nrhs;
     const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
+    if (*pl->h_err) {  // reported by the tensor-core kernel of an earlier call
+      const int e = *pl->h_err;
+      *pl->h_err = 0;
+      FMMB_CUDA(cudaMemsetAsync(pl->d_err.get(), 0, sizeof(int), pl->st.main));
+      throw Error{FMMB_ERR_CUDA, "tensor-core M2L pipeline wait timed out (code " + std::to_string(e) + ")"};
+    }
+    pl->ev_used = 0;
+    pl->ev_phase.clear();
+    pl->launches = 0;
     FMMB_CUDA(cudaEventRecord(pl->ev[7], m));
     const float* qd = to_device(q, (size_t)nj * nr, pl->stage_f, m);
     launch_gather_charges(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
+    pl->launches++;
     const bool pot_dev = is_device_ptr(pot);
     const bool grad_dev = want_grad && is_device_ptr(grad);
     // device destinations (staged through the plan when the caller gave host memory)
@@ -362,7 +512,10 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
       else
         launch_finalize_f64(ni, pl->perm_i.get(), pn, pn + ni, want_grad ? gn : nullptr, want_grad ? gn + 3 * (size_t)ni : nullptr,
                             (double*)(pd + (size_t)r * ni), want_grad ? (double*)(gd + (size_t)3 * r * ni) : nullptr, m);
+      pl->launches++;
     }
+    FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
+    FMMB_CUDA(cudaMemcpyAsync(pl->h_err, pl->d_err.get(), sizeof(int), cudaMemcpyDeviceToHost, m));
     if (!pot_dev) FMMB_CUDA(cudaMemcpyAsync(pot, pd, (size_t)ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
     if (want_grad && !grad_dev) FMMB_CUDA(cudaMemcpyAsync(grad, gd, (size_t)3 * ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
     if (!pot_dev || (want_grad && !grad_dev) || !is_device_ptr(q)) FMMB_CUDA(cudaStreamSynchronize(m));
@@ -523,18 +676,16 @@ int fmmb_get_timings(fmmb_plan* pl, float* ms) {
     FMMB_REQUIRE(pl->timings_valid, FMMB_ERR_STATE, "no evaluate yet");
     FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
     FMMB_CUDA(cudaStreamSynchronize(pl->st.side));
-    auto el = [&](int a, int b) {
+    FMMB_REQUIRE(*pl->h_err == 0, FMMB_ERR_CUDA, "tensor-core M2L pipeline wait timed out");
+    for (int k = 0; k < 7; k++) ms[k] = 0.0f;
+    for (auto& ph : pl->ev_phase) {
       float t = 0;
-      FMMB_CUDA(cudaEventElapsedTime(&t, pl->ev[a], pl->ev[b]));
-      return t;
-    };
-    ms[0] = el(0, 1);
-    ms[1] = el(2, 3);
-    ms[2] = el(3, 4);
-    ms[3] = el(4, 5);  // M2L and L2L interleaved per level
-    ms[4] = 0.0f;
-    ms[5] = el(5, 6);
-    ms[6] = el(7, 6);
+      FMMB_CUDA(cudaEventElapsedTime(&t, pl->evp[ph.second], pl->evp[ph.second + 1]));
+      ms[ph.first] += t;
+    }
+    float tot = 0;
+    FMMB_CUDA(cudaEventElapsedTime(&tot, pl->ev[7], pl->ev[6]));
+    ms[6] = tot;
   });
 }
 
@@ -549,6 +700,7 @@ int fmmb_get_stats(fmmb_plan* pl, long long* o) {
     o[4] = pl->p2p_pairs;
     o[5] = pl->m2l_pairs;
     o[6] = pl->lmax;
+    o[7] = pl->launches;
   });
 }
 

@@ -91,6 +91,8 @@ void build_static_operators(Operators& ops, int p, bool ref_semantics);
 // M2L sets: one in accurate semantics; one per level 2..lmax in reference
 // semantics, where the distance carries an absolute eps (needs the root size).
 void build_m2l_operators(Operators& ops, int lmax, float rd);
+// TF32 hi/lo images of the M2L operators in the tensor-core operand layout
+void build_m2l_images(const Operators& ops, std::vector<float>& img);
 
 struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
@@ -106,6 +108,13 @@ struct fmmb_plan {
   fmmb::Stream2 st;
   bool own_stream = true;
   cudaEvent_t ev[8] = {};
+  // per-launch timing: event pairs recorded around each phase launch and
+  // summed per phase when fmmb_get_timings is called
+  static constexpr int kEvPool = 96;
+  cudaEvent_t evp[kEvPool] = {};
+  int ev_used = 0;
+  std::vector<std::pair<int, int>> ev_phase;  // (phase, first event index of the pair)
+  int launches = 0;                           // kernel launches of the last evaluate
 
   // host copies of the configuration-dependent constants
   double eps2 = 0, coef = 0, rho_eps = 0, ang_eps = 0, pi_ang = 0;
@@ -138,12 +147,19 @@ struct fmmb_plan {
   // operators on the device
   fmmb::DevBuf<double> d_fac, d_m2m, d_l2l, d_m2l;
   fmmb::DevBuf<int> d_slot_rel, d_rel_to_op;
-  fmmb::DevBuf<float> d_m2l_tf32;            // [sets][316][2][Kp][Kp] hi/lo (mixed)
+  fmmb::DevBuf<float> d_opimg;               // [sets][316][4 K-blocks][2][128*32] TF32 images (mixed)
 
   // evaluation buffers
   fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
   fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
-  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][Kp] tf32 hi/lo (mixed)
+  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][128] TF32 hi/lo (mixed)
+  fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
+  int* h_err = nullptr;                      // pinned copy, checked by the next call
+  bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)
+  int tc_nwork = 0, tc_nsplit = 1;
+  int opimg_sets = 0;
+  float opimg_rd = 0;
+  fmmb::DevBuf<int> tc_boxes, tc_oct, tc_level, tc_work_tile, tc_slot_off, tc_slots;
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging
   fmmb::DevBuf<double> stage_d;

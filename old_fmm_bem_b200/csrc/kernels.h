@@ -46,3 +46,21 @@ void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float
                        cudaStream_t st);
 
 }  // namespace fmmb
+
+namespace fmmb {
+// tensor-core M2L (m2l_tc.cu)
+int m2l_tc_tile();
+void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
+struct M2LTcArgs {
+  int nwork, K, atomic;
+  const int *tile_boxes, *tile_oct, *tile_level, *work_tile, *slot_off, *slots;
+  const int *list, *slot_rel, *rel_to_op;
+  const float* opimg;
+  long long op_set_off[11];
+  const float* Mtf;
+  int mtf_box_off[11];
+  double* L;
+  int* err;
+};
+void launch_m2l_tc(const M2LTcArgs& a, cudaStream_t st);
+}  // namespace fmmb

@@ -11,6 +11,8 @@
 // to rounding.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "internal.h"
 #include "kernels.h"
 
@@ -273,16 +275,21 @@ __global__ void __launch_bounds__(128) l2l_f64(int K, const int* __restrict__ pa
   for (int row = threadIdx.x; row < K; row += blockDim.x) {
     double a = 0;
     for (int k = 0; k < K; k++) a += T[(size_t)row * K + k] * v[k];
-    Lc[(size_t)b * K + row] = a;  // the reference assigns (kernel/l2l.cxx:75-77)
+    // the reference assigns the translated parent local and adds M2L after
+    // (kernel/l2l.cxx:75-77, kernel/m2l.cxx:79-81); here M2L runs first for
+    // every level and the parent's contribution is added
+    Lc[(size_t)b * K + row] += a;
   }
 }
 
 // ---------------------------------------------------------------- M2L (FP64)
 // Target-stationary: each block owns a tile of target boxes of one octant at
 // one level (so they share one slot -> operator map), keeps their locals in
-// registers and walks the 189 slots; per slot the operator is streamed
-// through shared memory in column panels and applied to the gathered source
-// multipoles of the tile (a batched K x K x tile DGEMM).
+// registers and walks its share of the 189 slots (grid.y splits the slots so
+// that small trees still fill the GPU; the shares are added with FP64
+// atomics); per slot the operator is streamed through shared memory in column
+// panels and applied to the gathered source multipoles of the tile (a batched
+// K x K x tile DGEMM).
 constexpr int kM2LTile = 32;   // target boxes per block
 constexpr int kM2LPanel = 16;  // operator columns per shared-memory panel
 constexpr int kM2LThreads = 256;
@@ -307,7 +314,8 @@ __global__ void __launch_bounds__(kM2LThreads) m2l_f64(int K, int ntile, const i
     double acc[RPT][2];
 #pragma unroll
     for (int r = 0; r < RPT; r++) acc[r][0] = acc[r][1] = 0.0;
-    for (int slot = 0; slot < kM2LSlots; slot++) {
+    const int s0 = (blockIdx.y * kM2LSlots) / gridDim.y, s1 = ((blockIdx.y + 1) * kM2LSlots) / gridDim.y;
+    for (int slot = s0; slot < s1; slot++) {
       __syncthreads();
       if (threadIdx.x < kM2LTile) {
         const int box = sBox[threadIdx.x];
@@ -348,8 +356,8 @@ __global__ void __launch_bounds__(kM2LThreads) m2l_f64(int K, int ntile, const i
       const int row = rb0 + ty + 16 * r;
       if (row < K) {
         const int b0 = sBox[tx], b1 = sBox[tx + 16];
-        if (b0 >= 0) L[(size_t)b0 * K + row] += acc[r][0];
-        if (b1 >= 0) L[(size_t)b1 * K + row] += acc[r][1];
+        if (b0 >= 0) atomicAdd(&L[(size_t)b0 * K + row], acc[r][0]);
+        if (b1 >= 0) atomicAdd(&L[(size_t)b1 * K + row], acc[r][1]);
       }
     }
   }
@@ -574,7 +582,9 @@ int m2l_tile_size() { return kM2LTile; }
 void launch_m2l_f64(int ntile, int K, const int* tile_boxes, const int* tile_oct, const int* list, const int* slot_rel,
                     const int* rel_to_op, const double* ops, const double* M, double* L, cudaStream_t st) {
   if (ntile <= 0) return;
-  m2l_f64<<<ntile, kM2LThreads, 0, st>>>(K, ntile, tile_boxes, tile_oct, list, slot_rel, rel_to_op, ops, M, L);
+  // enough blocks for ~8 per SM on 148 SMs
+  const int split = std::max(1, std::min(27, (8 * 148 + ntile - 1) / ntile));
+  m2l_f64<<<dim3(ntile, split), kM2LThreads, 0, st>>>(K, ntile, tile_boxes, tile_oct, list, slot_rel, rel_to_op, ops, M, L);
   FMMB_CHECK_LAUNCH();
 }
 

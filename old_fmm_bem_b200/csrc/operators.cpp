@@ -22,6 +22,7 @@
 // (kernel/m2l.cxx:54), so one M2L set per level is built.
 #include <cmath>
 #include <complex>
+#include <cstring>
 #include <thread>
 #include <vector>
 
@@ -318,6 +319,46 @@ void build_m2l_operators(Operators& ops, int lmax, float rd) {
       return SR(j, k, n) / std::pow(rho, j + n + 1);
     };
     compose(p, Wf[je], Wb[je], Z, nullptr, &ops.m2l[((size_t)set * nops + o) * K * K]);
+  });
+}
+
+}  // namespace fmmb
+
+namespace fmmb {
+
+// TF32 round-to-nearest (ties away from zero) of an FP32 value, the rounding
+// of cvt.rna.tf32.f32: keep 10 mantissa bits.
+static float tf32_rna_host(float x) {
+  uint32_t b;
+  std::memcpy(&b, &x, 4);
+  if ((b & 0x7f800000u) != 0x7f800000u) b = (b + 0x1000u) & 0xffffe000u;
+  float y;
+  std::memcpy(&y, &b, 4);
+  return y;
+}
+
+// M2L operators as TF32 (hi, lo) pairs laid out exactly like the tensor-core
+// kernel's shared-memory operand tiles: per operator, per K-block of 32
+// columns, per part, 128 rows of 128 bytes with the 16-byte chunk c of row r
+// stored at chunk c ^ (r & 7) (K-major SWIZZLE_128B).  Rows/columns >= K are 0.
+void build_m2l_images(const Operators& ops, std::vector<float>& img) {
+  const int K = ops.K, nops = (int)ops.op_rel.size();
+  const size_t per_op = (size_t)4 * 2 * 128 * 32;
+  img.assign((size_t)ops.m2l_sets * nops * per_op, 0.0f);
+  parallel_for(ops.m2l_sets * nops, [&](int w) {
+    const double* T = &ops.m2l[(size_t)w * K * K];
+    float* out = &img[(size_t)w * per_op];
+    for (int kb = 0; kb < 4; kb++)
+      for (int r = 0; r < 128; r++)
+        for (int j = 0; j < 32; j++) {
+          const int col = kb * 32 + j;
+          const double v = (r < K && col < K) ? T[(size_t)r * K + col] : 0.0;
+          const float hi = tf32_rna_host((float)v);
+          const float lo = tf32_rna_host((float)(v - (double)hi));
+          const size_t pos = (size_t)r * 32 + (size_t)(((j >> 2) ^ (r & 7)) << 2) + (j & 3);
+          out[(size_t)(kb * 2 + 0) * 4096 + pos] = hi;
+          out[(size_t)(kb * 2 + 1) * 4096 + pos] = lo;
+        }
   });
 }
 

@@ -251,13 +251,19 @@ __global__ void leaf_ranges(int nleaf, int n, const int* first, int2* leaf) {
   leaf[b] = make_int2(f, e - f);
 }
 
-// child ranges of each parent (children of one parent are contiguous)
-__global__ void child_ranges(int nchild, const int* parent, int* start, int* count) {
+// child ranges of each parent (children of one parent are contiguous and
+// every parent has at least one child): first the starts, then (next launch)
+// the counts from consecutive starts.
+__global__ void child_starts(int nchild, const int* parent, int* start) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nchild) return;
   const int p = parent[c];
   if (c == 0 || parent[c - 1] != p) start[p] = c;
-  if (c == nchild - 1 || parent[c + 1] != p) count[p] = c + 1 - start[p];
+}
+__global__ void child_counts(int nparent, int nchild, const int* start, int* count) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nparent) return;
+  count[p] = ((p + 1 < nparent) ? start[p + 1] : nchild) - start[p];
 }
 
 __device__ __forceinline__ int find_key(const int* keys, int n, int k) {
@@ -442,11 +448,33 @@ void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
     FMMB_CUDA(cudaMemsetAsync(pl->child_count_j.get(), 0, tot * sizeof(int), s));
     for (int lev = lmax; lev >= 3; lev--) {
       // children at lev, parents at lev-1 (indices within the level)
-      child_ranges<<<blocks(nbox[lev], 256), 256, 0, s>>>(nbox[lev], parent_all.get() + off[lev],
-                                                         pl->child_start_j.get() + off[lev - 1],
-                                                         pl->child_count_j.get() + off[lev - 1]);
+      child_starts<<<blocks(nbox[lev], 256), 256, 0, s>>>(nbox[lev], parent_all.get() + off[lev],
+                                                         pl->child_start_j.get() + off[lev - 1]);
+      FMMB_CHECK_LAUNCH();
+      child_counts<<<blocks(nbox[lev - 1], 256), 256, 0, s>>>(nbox[lev - 1], nbox[lev], pl->child_start_j.get() + off[lev - 1],
+                                                             pl->child_count_j.get() + off[lev - 1]);
       FMMB_CHECK_LAUNCH();
     }
+    // every parent must own 1..8 children: a cheap host check that keeps a
+    // broken tree from reaching the expansion kernels
+    std::vector<int> cc(tot);
+    FMMB_CUDA(cudaMemcpyAsync(cc.data(), pl->child_count_j.get(), tot * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    for (int lev = lmax - 1; lev >= 2; lev--)
+      for (int b = 0; b < nbox[lev]; b++) {
+        const int c = cc[off[lev] + b];
+        FMMB_REQUIRE(c >= 1 && c <= 8, FMMB_ERR_STATE, "tree build: inconsistent child count");
+      }
+  }
+  {
+    std::vector<int> pa(tot);
+    FMMB_CUDA(cudaMemcpyAsync(pa.data(), parent_all.get(), tot * sizeof(int), cudaMemcpyDeviceToHost, s));
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    for (int lev = lmax; lev >= 3; lev--)
+      for (int b = 0; b < nbox[lev]; b++) {
+        const int q = pa[off[lev] + b];
+        FMMB_REQUIRE(q >= 0 && q < nbox[lev - 1], FMMB_ERR_STATE, "tree build: parent index out of range");
+      }
   }
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
