@@ -224,35 +224,68 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       build_m2l_operators(pl->ops, pl->lmax, pl->bbox[3]);
       upload(pl->d_m2l, pl->ops.m2l, s);
     }
-    // M2L tiles: per level, target boxes grouped by octant, m2l_tile_size() per tile
-    std::vector<int> keys(pl->tot_i);
+    // FP64 translation tiles (M2L, M2M, L2L) per level
+    std::vector<int> keys(pl->tot_i), keys_j(pl->tot_j), par_j(pl->tot_j), lst((size_t)pl->tot_i * kM2LSlots);
     FMMB_CUDA(cudaMemcpy(keys.data(), pl->key_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
-    const int TS = m2l_tile_size();
-    pl->tile_n.assign(pl->lmax + 1, 0);
-    pl->tile_boxes.clear();
-    pl->tile_oct.clear();
-    for (int lev = 0; lev <= pl->lmax; lev++) {
-      pl->tile_boxes.emplace_back(new DevBuf<int>());
-      pl->tile_oct.emplace_back(new DevBuf<int>());
-    }
-    for (int lev = 2; lev <= pl->lmax; lev++) {
+    FMMB_CUDA(cudaMemcpy(keys_j.data(), pl->key_j.get(), pl->tot_j * sizeof(int), cudaMemcpyDeviceToHost));
+    FMMB_CUDA(cudaMemcpy(par_j.data(), pl->parent_j.get(), pl->tot_j * sizeof(int), cudaMemcpyDeviceToHost));
+    FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    const int XT = translate_tile_size();
+    auto make_tiles = [&](const std::vector<std::vector<int>>& groups, int nslots, auto op_of) {
+      std::unique_ptr<fmmb_plan::TileSet> ts(new fmmb_plan::TileSet());
       std::vector<int> tb, to;
-      for (int oct = 0; oct < 8; oct++) {
-        std::vector<int> bx;
-        for (int b = 0; b < pl->nbox_i[lev]; b++)
-          if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
-        for (size_t k = 0; k < bx.size(); k += TS) {
-          for (int t = 0; t < TS; t++) tb.push_back(k + t < bx.size() ? bx[k + t] : -1);
-          to.push_back(oct);
+      for (const auto& g : groups)
+        for (size_t k = 0; k < g.size(); k += XT) {
+          const size_t e = std::min(g.size(), k + XT);
+          std::vector<int> ops_row(nslots, -1);
+          bool any_slot = false;
+          for (int sl = 0; sl < nslots; sl++)
+            for (size_t t = k; t < e; t++) {
+              const int o = op_of(g[t], sl);
+              if (o >= 0) {
+                ops_row[sl] = o;
+                any_slot = true;
+                break;
+              }
+            }
+          if (!any_slot) continue;
+          for (int t = 0; t < XT; t++) tb.push_back(k + t < e ? g[k + t] : -1);
+          to.insert(to.end(), ops_row.begin(), ops_row.end());
         }
-      }
-      pl->tile_n[lev] = (int)to.size();
-      pl->tile_boxes[lev]->alloc(tb.size());
-      pl->tile_oct[lev]->alloc(to.size());
+      ts->ntile = (int)tb.size() / XT;
+      ts->boxes.alloc(tb.size());
+      ts->ops.alloc(to.size());
       if (!tb.empty()) {
-        FMMB_CUDA(cudaMemcpy(pl->tile_boxes[lev]->get(), tb.data(), tb.size() * sizeof(int), cudaMemcpyHostToDevice));
-        FMMB_CUDA(cudaMemcpy(pl->tile_oct[lev]->get(), to.data(), to.size() * sizeof(int), cudaMemcpyHostToDevice));
+        FMMB_CUDA(cudaMemcpy(ts->boxes.get(), tb.data(), tb.size() * sizeof(int), cudaMemcpyHostToDevice));
+        FMMB_CUDA(cudaMemcpy(ts->ops.get(), to.data(), to.size() * sizeof(int), cudaMemcpyHostToDevice));
       }
+      return ts;
+    };
+    // M2M child lists: [parent][octant] -> child within the child level
+    std::vector<int> m2m_list((size_t)pl->tot_j * 8, -1);
+    for (int lev = pl->lmax; lev >= 3; lev--)
+      for (int c = 0; c < pl->nbox_j[lev]; c++) {
+        const int par = par_j[pl->off_j[lev] + c];
+        m2m_list[(size_t)(pl->off_j[lev - 1] + par) * 8 + (keys_j[pl->off_j[lev] + c] & 7)] = c;
+      }
+    pl->m2m_list.alloc(m2m_list.size());
+    FMMB_CUDA(cudaMemcpy(pl->m2m_list.get(), m2m_list.data(), m2m_list.size() * sizeof(int), cudaMemcpyHostToDevice));
+    pl->m2l_tiles.clear();
+    pl->m2m_tiles.clear();
+    pl->l2l_tiles.clear();
+    for (int lev = 0; lev <= pl->lmax; lev++) {
+      std::vector<std::vector<int>> by_oct(8), all(1);
+      if (lev >= 2)
+        for (int b = 0; b < pl->nbox_i[lev]; b++) by_oct[keys[pl->off_i[lev] + b] & 7].push_back(pl->off_i[lev] + b);
+      pl->m2l_tiles.push_back(make_tiles(by_oct, kM2LSlots, [&](int box, int sl) {
+        if (lst[(size_t)box * kM2LSlots + sl] < 0) return -1;
+        return pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
+      }));
+      pl->l2l_tiles.push_back(make_tiles(lev >= 3 ? by_oct : std::vector<std::vector<int>>(), 1,
+                                         [&](int box, int) { return keys[box] & 7; }));
+      if (lev >= 2 && lev < pl->lmax)
+        for (int b = 0; b < pl->nbox_j[lev]; b++) all[0].push_back(pl->off_j[lev] + b);
+      pl->m2m_tiles.push_back(make_tiles(all, 8, [&](int box, int sl) { return m2m_list[(size_t)box * 8 + sl] >= 0 ? sl : -1; }));
     }
     // tensor-core M2L (mixed precision, K <= 128): operator images and work items
     pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= 128;
@@ -265,8 +298,6 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         pl->opimg_sets = pl->ops.m2l_sets;
         pl->opimg_rd = pl->ops.m2l_rd;
       }
-      std::vector<int> lst((size_t)pl->tot_i * kM2LSlots);
-      FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
       const int TT = m2l_tc_tile();
       std::vector<int> tb, to, tl;
       std::vector<std::vector<int>> tslots;
@@ -343,6 +374,12 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
 
 namespace {
 
+// Slot split of a translation launch: enough blocks for ~8 per SM on 148 SMs.
+int split_for(int ntile, int nslots) {
+  if (ntile <= 0) return 1;
+  return std::max(1, std::min(std::min(nslots, 27), (8 * 148 + ntile - 1) / ntile));
+}
+
 // Brackets one launch with a pair of pool events (phase 0..5 as in
 // fmmb_get_timings); silently stops timing when the pool is exhausted.
 struct PhaseTimer {
@@ -396,15 +433,23 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   const double rb_leaf = (double)(pl->bbox[3] / (float)(1 << lmax));
   {
     PhaseTimer tm(pl, 1, m);
-    launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(), qs,
-               pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+    if (pl->ref)  // the reference's spherical formulation, quirks included
+      launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(),
+                 qs, pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+    else
+      launch_p2m_cart(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
+                      pl->snrm.get(), qs, pl->d_fac.get(), pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[3], m));
+  // upward pass: parents accumulate their children (levels below lmax start at zero)
+  if (lmax > 2)
+    FMMB_CUDA(cudaMemsetAsync(pl->M.get() + (size_t)pl->off_j[lmax - 1] * K, 0,
+                              (size_t)(pl->tot_j - pl->off_j[lmax - 1]) * K * sizeof(double), m));
   for (int lev = lmax - 1; lev >= 2; lev--) {
     PhaseTimer tm(pl, 2, m);
-    launch_m2m(pl->nbox_j[lev], K, pl->child_start_j.get() + pl->off_j[lev], pl->child_count_j.get() + pl->off_j[lev],
-               pl->key_j.get() + pl->off_j[lev + 1], pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->d_m2m.get(),
-               pl->M.get() + (size_t)pl->off_j[lev] * K, m);
+    const auto& ts = *pl->m2m_tiles[lev];
+    launch_translate_f64(ts.ntile, split_for(ts.ntile, 8), K, 8, ts.boxes.get(), ts.ops.get(), pl->m2m_list.get(),
+                         pl->d_m2m.get(), pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->M.get(), m);
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[4], m));
   // downward pass: M2L of every level into zeroed locals, then each level
@@ -444,21 +489,28 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     for (int lev = 2; lev <= lmax; lev++) {
       PhaseTimer tm(pl, 3, m);
       const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
-      launch_m2l_f64(pl->tile_n[lev], K, pl->tile_boxes[lev]->get(), pl->tile_oct[lev]->get(), pl->m2l_list.get(),
-                     pl->d_slot_rel.get(), pl->d_rel_to_op.get(), pl->d_m2l.get() + set * opsz,
-                     pl->M.get() + (size_t)pl->off_j[lev] * K, pl->L.get(), m);
+      const auto& ts = *pl->m2l_tiles[lev];
+      launch_translate_f64(ts.ntile, split_for(ts.ntile, kM2LSlots), K, kM2LSlots, ts.boxes.get(), ts.ops.get(),
+                           pl->m2l_list.get(), pl->d_m2l.get() + set * opsz, pl->M.get() + (size_t)pl->off_j[lev] * K,
+                           pl->L.get(), m);
     }
   }
   for (int lev = 3; lev <= lmax; lev++) {
     PhaseTimer tm(pl, 4, m);
-    launch_l2l(pl->nbox_i[lev], K, pl->parent_i.get() + pl->off_i[lev], pl->key_i.get() + pl->off_i[lev],
-               pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->d_l2l.get(), pl->L.get() + (size_t)pl->off_i[lev] * K, m);
+    const auto& ts = *pl->l2l_tiles[lev];
+    launch_translate_f64(ts.ntile, 1, K, 1, ts.boxes.get(), ts.ops.get(), pl->parent_i.get(), pl->d_l2l.get(),
+                         pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->L.get(), m);
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);
-    launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
-               pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
+    if (pl->ref)
+      launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
+                 pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
+    else
+      launch_l2p_cart(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(),
+                      pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K,
+                      pot_far, g_far, pl->ni, m);
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
   FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));

@@ -1,0 +1,292 @@
+// P2M and L2P from Cartesian solid-harmonic recurrences (accurate semantics).
+//
+// The reference evaluates r^n fac(n,m) P_n^m(cos a) e^{-i m b} through
+// spherical angles (acos, atan, exp; kernel/multipole.cxx:7-35,
+// kernel/G_p2m.cxx:28-55) and the local-expansion gradient through spherical
+// derivatives with a 1/sin(theta) (kernel/G_l2p.cxx:44-70).  In exact
+// arithmetic the same quantities follow from the homogeneous polynomials
+//   S_n^m(x) = r^n P_n^m(cos theta) e^{i m phi}   (Condon-Shortley phase)
+// without any trigonometric function:
+//   S_m^m = -(2m-1) (x + i y) S_{m-1}^{m-1},   S_{m+1}^m = (2m+1) z S_m^m,
+//   (n-m) S_n^m = (2n-1) z S_{n-1}^m - (n+m-1) r^2 S_{n-2}^m,
+// with the ladder identities
+//   d/dz S_n^m = (n+m) S_{n-1}^m,  (d/dx + i d/dy) S_n^m = S_{n-1}^{m+1},
+//   (d/dx - i d/dy) S_n^m = -(n+m)(n+m-1) S_{n-1}^{m-1},
+//   S_{n}^{-1} = -conj(S_n^1) / (n (n+1)).
+// Multipole basis: fac(n,m) conj(S_n^m); local evaluation: Re sum w_m
+// fac(n,m) L_n^m S_n^m with w_0 = 1, w_m = 2.  This form has no singular
+// points (a target on a box axis or at a box centre is fine), so it is used
+// for accurate semantics; reference semantics keep the spherical kernels
+// of kernels_fp64.cu, which reproduce the reference's eps-shifted radius and
+// single-precision angles.
+#include <cuda_runtime.h>
+
+#include "internal.h"
+#include "kernels.h"
+
+namespace fmmb {
+namespace {
+
+struct cplx {
+  double re, im;
+};
+__device__ __forceinline__ cplx cmul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ cplx cscale(cplx a, double s) { return {a.re * s, a.im * s}; }
+
+__device__ __forceinline__ void box_center(int key, float xmin, float ymin, float zmin, double rb, double& xc, double& yc,
+                                           double& zc) {
+  int cx = 0, cy = 0, cz = 0;
+  for (int i = 0; i < 10; i++) {
+    cy |= ((key >> (3 * i)) & 1) << i;
+    cx |= ((key >> (3 * i + 1)) & 1) << i;
+    cz |= ((key >> (3 * i + 2)) & 1) << i;
+  }
+  xc = (double)xmin + (cx + 0.5) * rb;
+  yc = (double)ymin + (cy + 0.5) * rb;
+  zc = (double)zmin + (cz + 0.5) * rb;
+}
+
+// ------------------------------------------------------------------ P2M
+// One block (128 threads) per source leaf.  Lanes are grouped in segments of
+// SEG; lane m of a segment owns order m (column m of S) of one point, so a
+// block processes 128/SEG points at a time.  The dipole needs the neighbouring
+// columns m-1 and m+1 of the previous degree, which come from the adjacent
+// lanes by shuffles.  Each segment accumulates into its own shared-memory
+// copy of the multipole; the copies are summed at the end.
+template <int KER, int SEG>
+__global__ void __launch_bounds__(128) p2m_cart(int p, int K, const int* __restrict__ keys, const int2* __restrict__ leaf,
+                                                const float4* __restrict__ spos, const float4* __restrict__ snrm,
+                                                const float* __restrict__ qs, const double* __restrict__ fac, float xmin,
+                                                float ymin, float zmin, double rb, double* __restrict__ M) {
+  constexpr int G = 128 / SEG;
+  extern __shared__ double acc[];  // [G][K]
+  const int g = threadIdx.x / SEG, m = threadIdx.x % SEG;
+  for (int k = threadIdx.x; k < G * K; k += blockDim.x) acc[k] = 0.0;
+  __syncthreads();
+  const int b = blockIdx.x;
+  double xc, yc, zc;
+  box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
+  const int2 lf = leaf[b];
+  double* my = acc + g * K;
+  const double inv_rb = 1.0 / rb;
+  const unsigned segmask = 0xffffffffu;  // every lane of the warp runs the same loop trip counts
+  const int rounds = (lf.y + G - 1) / G;
+  for (int it = 0; it < rounds; it++) {
+    const int jj = it * G + g;
+    const bool act = jj < lf.y;
+    const int j = lf.x + (act ? jj : 0);
+    const float4 xs = spos[j];
+    const double q = act ? (double)qs[j] : 0.0;
+    const double x = ((double)xs.x - xc) * inv_rb, y = ((double)xs.y - yc) * inv_rb, z = ((double)xs.z - zc) * inv_rb;
+    const double r2 = x * x + y * y + z * z;
+    // S_m^m = prod_{k<m} -(2k+1) (x + i y)
+    cplx smm = {1.0, 0.0};
+    for (int k = 0; k < m; k++) smm = cscale(cmul(smm, cplx{x, y}), -(2.0 * k + 1.0));
+    cplx s1 = {0.0, 0.0}, s2 = {0.0, 0.0};  // S_{n-1}^m, S_{n-2}^m
+    double qnx = 0, qny = 0, qnz = 0;
+    if (KER == FMMB_LAPLACE_GNJ) {
+      const float4 nv = snrm[j];
+      const float qf = act ? qs[j] : 0.f;
+      qnx = (double)(qf * nv.x) * inv_rb;
+      qny = (double)(qf * nv.y) * inv_rb;
+      qnz = (double)(qf * nv.z) * inv_rb;
+    }
+    for (int n = 0; n <= p; n++) {
+      cplx sn;
+      if (n < m) sn = {0.0, 0.0};
+      else if (n == m) sn = smm;
+      else if (n == m + 1) sn = cscale(s1, (2.0 * m + 1.0) * z);
+      else {
+        const double a = (2.0 * n - 1.0) * z / (n - m), c = (n + m - 1.0) * r2 / (n - m);
+        sn = {a * s1.re - c * s2.re, a * s1.im - c * s2.im};
+      }
+      if (KER != FMMB_LAPLACE_GNJ) {
+        if (n >= m && m <= p) {
+          const double f = q * fac[ifull_d(n, m)];
+          if (m == 0) my[n * n] += f * sn.re;
+          else {
+            my[n * n + 2 * m - 1] += f * sn.re;
+            my[n * n + 2 * m] -= f * sn.im;
+          }
+        }
+      } else {
+        // n . grad S_n^m from degree n-1 (s1): columns m+1 (lane above) and
+        // m-1 (lane below; for m = 0 the conjugate of column 1)
+        cplx up, dn;
+        up.re = __shfl_down_sync(segmask, s1.re, 1, SEG);
+        up.im = __shfl_down_sync(segmask, s1.im, 1, SEG);
+        dn.re = __shfl_up_sync(segmask, s1.re, 1, SEG);
+        dn.im = __shfl_up_sync(segmask, s1.im, 1, SEG);
+        if (m == SEG - 1) up = {0.0, 0.0};
+        double cm;
+        if (m == 0) {
+          dn = {up.re, -up.im};
+          cm = 1.0;
+        } else {
+          cm = -(double)(n + m) * (double)(n + m - 1);
+        }
+        if (n >= 1 && n >= m && m <= p) {
+          // D = 1/2 (nx - i ny) up + 1/2 (nx + i ny) cm dn + nz (n+m) s1
+          const cplx a = cmul(cplx{0.5 * qnx, -0.5 * qny}, up);
+          const cplx c = cmul(cplx{0.5 * qnx * cm, 0.5 * qny * cm}, dn);
+          const double d = qnz * (n + m);
+          const double Dre = a.re + c.re + d * s1.re, Dim = a.im + c.im + d * s1.im;
+          const double f = fac[ifull_d(n, m)];
+          if (m == 0) my[n * n] += f * Dre;
+          else {
+            my[n * n + 2 * m - 1] += f * Dre;
+            my[n * n + 2 * m] -= f * Dim;
+          }
+        }
+      }
+      s2 = s1;
+      s1 = sn;
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    double t = 0.0;
+#pragma unroll
+    for (int gg = 0; gg < G; gg++) t += acc[gg * K + k];
+    M[(size_t)b * K + k] = t;
+  }
+}
+
+// ------------------------------------------------------------------ L2P
+// One block (64 threads) per target leaf.  The leaf's local expansion is
+// turned once into the coefficients of the potential and of the three
+// derivative expansions (ladder identities above), then each thread walks
+// the S_n^m of its point column by column.
+constexpr int kL2PThreads = 64;
+
+template <int KER>
+__global__ void __launch_bounds__(kL2PThreads) l2p_cart(int p, int K, const int* __restrict__ keys,
+                                                        const int2* __restrict__ leaf, const float4* __restrict__ tpos,
+                                                        const float4* __restrict__ tnrm, const double* __restrict__ fac,
+                                                        float xmin, float ymin, float zmin, double rb, double coef,
+                                                        const double* __restrict__ L, double* __restrict__ pot,
+                                                        double* __restrict__ grad, int ni) {
+  extern __shared__ double sm[];
+  const int P = (p + 1) * (p + 2) / 2;
+  cplx* Cphi = reinterpret_cast<cplx*>(sm);
+  cplx* Cz = Cphi + P;
+  cplx* Cp = Cz + P;
+  cplx* Cm = Cp + P;
+  double* Cs = reinterpret_cast<double*>(Cm + P);  // [p+1]
+  const int b = blockIdx.x;
+  const double* Lb = L + (size_t)b * K;
+  auto Lnm = [&](int n, int m) -> cplx {
+    if (m == 0) return {Lb[n * n], 0.0};
+    return {Lb[n * n + 2 * m - 1], Lb[n * n + 2 * m]};
+  };
+  for (int idx = threadIdx.x; idx < P; idx += blockDim.x) {
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= idx) n++;
+    const int m = idx - n * (n + 1) / 2;
+    const double wm = m ? 2.0 : 1.0;
+    Cphi[idx] = cscale(Lnm(n, m), wm * fac[ifull_d(n, m)]);
+    if (n < p) {
+      Cz[idx] = cscale(Lnm(n + 1, m), wm * fac[ifull_d(n + 1, m)] * (n + 1 + m));
+      Cp[idx] = (m >= 1) ? cscale(Lnm(n + 1, m - 1), (m - 1 ? 2.0 : 1.0) * fac[ifull_d(n + 1, m - 1)]) : cplx{0.0, 0.0};
+      Cm[idx] = cscale(Lnm(n + 1, m + 1), -2.0 * fac[ifull_d(n + 1, m + 1)] * (double)(n + m + 2) * (double)(n + m + 1));
+    } else {
+      Cz[idx] = Cp[idx] = Cm[idx] = cplx{0.0, 0.0};
+    }
+  }
+  for (int n = threadIdx.x; n <= p; n += blockDim.x) Cs[n] = (n < p) ? fac[ifull_d(n + 1, 0)] * Lb[(n + 1) * (n + 1)] : 0.0;
+  __syncthreads();
+  double xc, yc, zc;
+  box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
+  const int2 lf = leaf[b];
+  const double inv_rb = 1.0 / rb;
+  for (int ii = threadIdx.x; ii < lf.y; ii += blockDim.x) {
+    const int i = lf.x + ii;
+    const float4 xt = tpos[i];
+    const double x = ((double)xt.x - xc) * inv_rb, y = ((double)xt.y - yc) * inv_rb, z = ((double)xt.z - zc) * inv_rb;
+    const double r2 = x * x + y * y + z * z;
+    double F = 0, dzr = 0, dpr = 0, dpi = 0, dmr = 0, dmi = 0;
+    cplx smm = {1.0, 0.0};
+    for (int m = 0; m <= p; m++) {
+      if (m > 0) smm = cscale(cmul(smm, cplx{x, y}), -(2.0 * m - 1.0));
+      cplx s1 = {0.0, 0.0}, s2 = {0.0, 0.0};
+      for (int n = m; n <= p; n++) {
+        cplx sn;
+        if (n == m) sn = smm;
+        else if (n == m + 1) sn = cscale(s1, (2.0 * m + 1.0) * z);
+        else {
+          const double a = (2.0 * n - 1.0) * z / (n - m), c = (n + m - 1.0) * r2 / (n - m);
+          sn = {a * s1.re - c * s2.re, a * s1.im - c * s2.im};
+        }
+        const int idx = n * (n + 1) / 2 + m;
+        const cplx cf = Cphi[idx];
+        F += cf.re * sn.re - cf.im * sn.im;  // Re(C S)
+        if (n < p) {
+          const cplx cz = Cz[idx], cp = Cp[idx], cmm = Cm[idx];
+          dzr += cz.re * sn.re - cz.im * sn.im;
+          dpr += cp.re * sn.re - cp.im * sn.im;
+          dpi += cp.re * sn.im + cp.im * sn.re;
+          dmr += cmm.re * sn.re - cmm.im * sn.im;
+          dmi += cmm.re * sn.im + cmm.im * sn.re;
+          if (m == 1) {  // Cs[n] * conj(S_n^1)
+            dmr += Cs[n] * sn.re;
+            dmi -= Cs[n] * sn.im;
+          }
+        }
+        s2 = s1;
+        s1 = sn;
+      }
+    }
+    const double gx = 0.5 * (dpr + dmr), gy = 0.5 * (dpi - dmi), gz = dzr;
+    const double c1 = coef * inv_rb, c2 = coef * inv_rb * inv_rb;
+    if (KER == FMMB_LAPLACE_GNI) {
+      const float4 nv = tnrm[i];
+      pot[i] = -c2 * ((double)nv.x * gx + (double)nv.y * gy + (double)nv.z * gz);
+    } else {
+      pot[i] = c1 * F;
+      if (KER == FMMB_LAPLACE_G && grad) {
+        grad[i] = c2 * gx;
+        grad[ni + i] = c2 * gy;
+        grad[2 * ni + i] = c2 * gz;
+      }
+    }
+  }
+}
+
+}  // namespace
+
+void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
+                     const float4* snrm, const float* qs, const double* fac, const float* bbox, double rb, double* M,
+                     cudaStream_t st) {
+  if (nleaf <= 0) return;
+  if (p <= 14) {
+    const size_t sm = (size_t)(128 / 16) * K * sizeof(double);
+    if (kernel == FMMB_LAPLACE_GNJ)
+      p2m_cart<FMMB_LAPLACE_GNJ, 16><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, bbox[0], bbox[1], bbox[2], rb, M);
+    else
+      p2m_cart<FMMB_LAPLACE_G, 16><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, bbox[0], bbox[1], bbox[2], rb, M);
+  } else {
+    const size_t sm = (size_t)(128 / 32) * K * sizeof(double);
+    if (kernel == FMMB_LAPLACE_GNJ)
+      p2m_cart<FMMB_LAPLACE_GNJ, 32><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, bbox[0], bbox[1], bbox[2], rb, M);
+    else
+      p2m_cart<FMMB_LAPLACE_G, 32><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, bbox[0], bbox[1], bbox[2], rb, M);
+  }
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                     const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
+                     double* pot, double* grad, int ni, cudaStream_t st) {
+  if (nleaf <= 0) return;
+  const int P = (p + 1) * (p + 2) / 2;
+  const size_t sm = (size_t)4 * P * 2 * sizeof(double) + (p + 1) * sizeof(double);
+  if (kernel == FMMB_LAPLACE_G)
+    l2p_cart<FMMB_LAPLACE_G><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  else if (kernel == FMMB_LAPLACE_GNI)
+    l2p_cart<FMMB_LAPLACE_GNI><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  else
+    l2p_cart<FMMB_LAPLACE_GNJ><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  FMMB_CHECK_LAUNCH();
+}
+
+}  // namespace fmmb

@@ -166,9 +166,14 @@ struct fmmb_plan {
   fmmb::DevBuf<int> inv_i;                   // caller index -> sorted target position
   fmmb::DevBuf<char> stage_out;              // device staging of host outputs
   bool timings_valid = false;
-  // M2L tiles per level: target boxes of one octant, padded with -1
-  std::vector<int> tile_n;
-  std::vector<std::unique_ptr<fmmb::DevBuf<int>>> tile_boxes, tile_oct;
+  // FP64 translation tiles per level (kernels_fp64.cu translate_f64): output
+  // boxes [ntile][32] and per-tile operator index per slot [ntile][nslots]
+  struct TileSet {
+    int ntile = 0;
+    fmmb::DevBuf<int> boxes, ops;
+  };
+  std::vector<std::unique_ptr<TileSet>> m2l_tiles, m2m_tiles, l2l_tiles;  // index = level
+  fmmb::DevBuf<int> m2m_list;                                            // [tot_j][8] child (within level) or -1
 };
 
 namespace fmmb {

@@ -27,13 +27,17 @@ void launch_p2p_mixed(int kernel, int nleaf, const int2* leaf_i, const int2* lea
                       double* pot, double* grad, int ni, cudaStream_t st);
 void launch_p2m(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos, const float4* snrm,
                 const float* qs, const double* fac, const Sem& s, const float* bbox, double rb, double* M, cudaStream_t st);
-void launch_m2m(int nparent, int K, const int* child_start, const int* child_count, const int* child_keys, const double* Mc,
-                const double* ops, double* Mp, cudaStream_t st);
-void launch_l2l(int nchild, int K, const int* parent, const int* keys, const double* Lp, const double* ops, double* Lc,
-                cudaStream_t st);
-int m2l_tile_size();
-void launch_m2l_f64(int ntile, int K, const int* tile_boxes, const int* tile_oct, const int* list, const int* slot_rel,
-                    const int* rel_to_op, const double* ops, const double* M, double* L, cudaStream_t st);
+// trig-free Cartesian P2M / L2P (accurate semantics), expansions_cart.cu
+void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
+                     const float4* snrm, const float* qs, const double* fac, const float* bbox, double rb, double* M,
+                     cudaStream_t st);
+void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                     const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
+                     double* pot, double* grad, int ni, cudaStream_t st);
+int translate_tile_size();
+// batched FP64 translation (M2L / M2M / L2L), see kernels_fp64.cu
+void launch_translate_f64(int ntile, int nsplit, int K, int nslots, const int* tile_boxes, const int* tile_ops,
+                          const int* list, const double* ops, const double* in, double* out, cudaStream_t st);
 void launch_l2p(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos, const float4* tnrm,
                 const double* fac, const Sem& s, const float* bbox, double rb, const double* L, double* pot, double* grad,
                 int ni, cudaStream_t st);

@@ -232,115 +232,66 @@ __global__ void __launch_bounds__(128) p2m_f64(int p, int K, const int* __restri
   for (int k = threadIdx.x; k < K; k += blockDim.x) M[(size_t)b * K + k] = acc[k] + acc[K + k] + acc[2 * K + k] + acc[3 * K + k];
 }
 
-// ---------------------------------------------------------------- M2M / L2L
-// Dense K x K operator per child octant (operators.cpp).
-__global__ void __launch_bounds__(128) m2m_f64(int K, const int* __restrict__ child_start, const int* __restrict__ child_count,
-                                               const int* __restrict__ child_keys, const double* __restrict__ Mc,
-                                               const double* __restrict__ ops, double* __restrict__ Mp) {
-  extern __shared__ double v[];
-  const int b = blockIdx.x;
-  const int c0 = child_start[b], nc = child_count[b];
-  double acc[4] = {0, 0, 0, 0};
-  for (int c = c0; c < c0 + nc; c++) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < K; k += blockDim.x) v[k] = Mc[(size_t)c * K + k];
-    __syncthreads();
-    const double* T = ops + (size_t)(child_keys[c] & 7) * K * K;
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      const int row = threadIdx.x + r * 128;
-      if (row < K) {
-        double a = 0;
-        for (int k = 0; k < K; k++) a += T[(size_t)row * K + k] * v[k];
-        acc[r] += a;
-      }
-    }
-  }
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const int row = threadIdx.x + r * 128;
-    if (row < K) Mp[(size_t)b * K + row] = acc[r];
-  }
-}
+// ---------------------------------------------------------------- translations (FP64)
+// One kernel for the three box-to-box translations (M2L, M2M, L2L): a block
+// owns a tile of up to 32 output boxes and walks `nslots` slots; slot s of
+// output box b reads input box list[b*nslots + s] (an index into `in`, or
+// -1) through operator tile_ops[tile*nslots + s] (-1: no box of the tile uses
+// the slot).  Per slot the K x K operator is streamed through shared memory
+// in column panels and applied to the tile's gathered inputs -- a batched
+// K x K x 32 DGEMM whose operator is shared by the whole tile.  grid.y
+// splits the slots when there are few tiles; the shares are then added with
+// FP64 atomics.
+//   M2L: tiles of target boxes of one octant, 189 interaction slots
+//        (kernel/m2l.cxx:30-83);
+//   M2M: tiles of parent boxes, 8 child slots (kernel/m2m.cxx:28-62);
+//   L2L: tiles of child boxes of one octant, 1 parent slot (kernel/l2l.cxx:44-78).
+constexpr int kXTile = 32;    // output boxes per block
+constexpr int kXPanel = 16;   // operator columns per shared-memory panel
+constexpr int kXThreads = 256;
 
-__global__ void __launch_bounds__(128) l2l_f64(int K, const int* __restrict__ parent, const int* __restrict__ keys,
-                                               const double* __restrict__ Lp, const double* __restrict__ ops,
-                                               double* __restrict__ Lc) {
-  extern __shared__ double v[];
-  const int b = blockIdx.x;
-  const int pb = parent[b];
-  for (int k = threadIdx.x; k < K; k += blockDim.x) v[k] = Lp[(size_t)pb * K + k];
-  __syncthreads();
-  const double* T = ops + (size_t)(keys[b] & 7) * K * K;
-  for (int row = threadIdx.x; row < K; row += blockDim.x) {
-    double a = 0;
-    for (int k = 0; k < K; k++) a += T[(size_t)row * K + k] * v[k];
-    // the reference assigns the translated parent local and adds M2L after
-    // (kernel/l2l.cxx:75-77, kernel/m2l.cxx:79-81); here M2L runs first for
-    // every level and the parent's contribution is added
-    Lc[(size_t)b * K + row] += a;
-  }
-}
-
-// ---------------------------------------------------------------- M2L (FP64)
-// Target-stationary: each block owns a tile of target boxes of one octant at
-// one level (so they share one slot -> operator map), keeps their locals in
-// registers and walks its share of the 189 slots (grid.y splits the slots so
-// that small trees still fill the GPU; the shares are added with FP64
-// atomics); per slot the operator is streamed through shared memory in column
-// panels and applied to the gathered source multipoles of the tile (a batched
-// K x K x tile DGEMM).
-constexpr int kM2LTile = 32;   // target boxes per block
-constexpr int kM2LPanel = 16;  // operator columns per shared-memory panel
-constexpr int kM2LThreads = 256;
-
-__global__ void __launch_bounds__(kM2LThreads) m2l_f64(int K, int ntile, const int* __restrict__ tile_boxes,
-                                                       const int* __restrict__ tile_oct, const int* __restrict__ list,
-                                                       const int* __restrict__ slot_rel, const int* __restrict__ rel_to_op,
-                                                       const double* __restrict__ ops, const double* __restrict__ M,
-                                                       double* __restrict__ L) {
-  // rows of the output handled by this thread: row = ty + 16*r, boxes bx + 16*c
-  constexpr int RPT = 8;  // up to 128 rows (K <= 121 fits; larger K loops over row blocks)
-  __shared__ double sT[kM2LPanel][128 + 1];
-  __shared__ double sB[kM2LPanel][kM2LTile + 1];
-  __shared__ int sSrc[kM2LTile];
-  __shared__ int sBox[kM2LTile];
+__global__ void __launch_bounds__(kXThreads) translate_f64(int K, int nslots, const int* __restrict__ tile_boxes,
+                                                           const int* __restrict__ tile_ops, const int* __restrict__ list,
+                                                           const double* __restrict__ ops, const double* __restrict__ in,
+                                                           double* __restrict__ out) {
+  constexpr int RPT = 8;  // rows per thread: ty + 16*r covers 128 rows
+  __shared__ double sT[kXPanel][128 + 1];
+  __shared__ double sB[kXPanel][kXTile + 1];
+  __shared__ int sSrc[kXTile];
+  __shared__ int sBox[kXTile];
   const int tile = blockIdx.x;
-  const int oct = tile_oct[tile];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads
-  if (threadIdx.x < kM2LTile) sBox[threadIdx.x] = tile_boxes[tile * kM2LTile + threadIdx.x];
+  if (threadIdx.x < kXTile) sBox[threadIdx.x] = tile_boxes[tile * kXTile + threadIdx.x];
   __syncthreads();
+  const int s0 = (blockIdx.y * nslots) / gridDim.y, s1 = ((blockIdx.y + 1) * nslots) / gridDim.y;
   for (int rb0 = 0; rb0 < K; rb0 += 128) {
     double acc[RPT][2];
 #pragma unroll
     for (int r = 0; r < RPT; r++) acc[r][0] = acc[r][1] = 0.0;
-    const int s0 = (blockIdx.y * kM2LSlots) / gridDim.y, s1 = ((blockIdx.y + 1) * kM2LSlots) / gridDim.y;
     for (int slot = s0; slot < s1; slot++) {
+      const int op = tile_ops[(size_t)tile * nslots + slot];
+      if (op < 0) continue;
       __syncthreads();
-      if (threadIdx.x < kM2LTile) {
+      if (threadIdx.x < kXTile) {
         const int box = sBox[threadIdx.x];
-        sSrc[threadIdx.x] = box >= 0 ? list[(size_t)box * kM2LSlots + slot] : -1;
+        sSrc[threadIdx.x] = box >= 0 ? list[(size_t)box * nslots + slot] : -1;
       }
-      __syncthreads();
-      int any = 0;
-      for (int t = 0; t < kM2LTile; t++) any |= (sSrc[t] >= 0);
-      if (!any) continue;
-      const double* T = ops + (size_t)rel_to_op[slot_rel[oct * kM2LSlots + slot]] * K * K;
-      for (int k0 = 0; k0 < K; k0 += kM2LPanel) {
+      const double* T = ops + (size_t)op * K * K;
+      for (int k0 = 0; k0 < K; k0 += kXPanel) {
         __syncthreads();
-        for (int e = threadIdx.x; e < kM2LPanel * 128; e += kM2LThreads) {
-          const int row = e / kM2LPanel, kk = e % kM2LPanel;
+        for (int e = threadIdx.x; e < kXPanel * 128; e += kXThreads) {
+          const int row = e / kXPanel, kk = e % kXPanel;
           const int gr = rb0 + row, gk = k0 + kk;
           sT[kk][row] = (gr < K && gk < K) ? T[(size_t)gr * K + gk] : 0.0;
         }
-        for (int e = threadIdx.x; e < kM2LPanel * kM2LTile; e += kM2LThreads) {
-          const int t = e / kM2LPanel, kk = e % kM2LPanel;
+        for (int e = threadIdx.x; e < kXPanel * kXTile; e += kXThreads) {
+          const int t = e / kXPanel, kk = e % kXPanel;
           const int src = sSrc[t], gk = k0 + kk;
-          sB[kk][t] = (src >= 0 && gk < K) ? M[(size_t)src * K + gk] : 0.0;
+          sB[kk][t] = (src >= 0 && gk < K) ? in[(size_t)src * K + gk] : 0.0;
         }
         __syncthreads();
 #pragma unroll 4
-        for (int kk = 0; kk < kM2LPanel; kk++) {
+        for (int kk = 0; kk < kXPanel; kk++) {
           const double b0 = sB[kk][tx], b1 = sB[kk][tx + 16];
 #pragma unroll
           for (int r = 0; r < RPT; r++) {
@@ -356,8 +307,13 @@ __global__ void __launch_bounds__(kM2LThreads) m2l_f64(int K, int ntile, const i
       const int row = rb0 + ty + 16 * r;
       if (row < K) {
         const int b0 = sBox[tx], b1 = sBox[tx + 16];
-        if (b0 >= 0) atomicAdd(&L[(size_t)b0 * K + row], acc[r][0]);
-        if (b1 >= 0) atomicAdd(&L[(size_t)b1 * K + row], acc[r][1]);
+        if (gridDim.y > 1) {
+          if (b0 >= 0) atomicAdd(&out[(size_t)b0 * K + row], acc[r][0]);
+          if (b1 >= 0) atomicAdd(&out[(size_t)b1 * K + row], acc[r][1]);
+        } else {
+          if (b0 >= 0) out[(size_t)b0 * K + row] += acc[r][0];
+          if (b1 >= 0) out[(size_t)b1 * K + row] += acc[r][1];
+        }
       }
     }
   }
@@ -563,28 +519,12 @@ void launch_p2m(int kernel, int nleaf, int p, int K, const int* keys, const int2
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_m2m(int nparent, int K, const int* child_start, const int* child_count, const int* child_keys, const double* Mc,
-                const double* ops, double* Mp, cudaStream_t st) {
-  if (nparent <= 0) return;
-  m2m_f64<<<nparent, 128, K * sizeof(double), st>>>(K, child_start, child_count, child_keys, Mc, ops, Mp);
-  FMMB_CHECK_LAUNCH();
-}
+int translate_tile_size() { return kXTile; }
 
-void launch_l2l(int nchild, int K, const int* parent, const int* keys, const double* Lp, const double* ops, double* Lc,
-                cudaStream_t st) {
-  if (nchild <= 0) return;
-  l2l_f64<<<nchild, 128, K * sizeof(double), st>>>(K, parent, keys, Lp, ops, Lc);
-  FMMB_CHECK_LAUNCH();
-}
-
-int m2l_tile_size() { return kM2LTile; }
-
-void launch_m2l_f64(int ntile, int K, const int* tile_boxes, const int* tile_oct, const int* list, const int* slot_rel,
-                    const int* rel_to_op, const double* ops, const double* M, double* L, cudaStream_t st) {
+void launch_translate_f64(int ntile, int nsplit, int K, int nslots, const int* tile_boxes, const int* tile_ops,
+                          const int* list, const double* ops, const double* in, double* out, cudaStream_t st) {
   if (ntile <= 0) return;
-  // enough blocks for ~8 per SM on 148 SMs
-  const int split = std::max(1, std::min(27, (8 * 148 + ntile - 1) / ntile));
-  m2l_f64<<<dim3(ntile, split), kM2LThreads, 0, st>>>(K, ntile, tile_boxes, tile_oct, list, slot_rel, rel_to_op, ops, M, L);
+  translate_f64<<<dim3(ntile, std::max(1, nsplit)), kXThreads, 0, st>>>(K, nslots, tile_boxes, tile_ops, list, ops, in, out);
   FMMB_CHECK_LAUNCH();
 }
 

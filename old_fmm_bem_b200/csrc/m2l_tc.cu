@@ -6,12 +6,15 @@
 //
 //   L[:, tile] += sum over active slots d of  T_d (128 x 128) . M[src(tile, d)] (128 x 128)
 //
-// for a tile of 128 target boxes of one octant at one level (they share the
-// slot -> operator map).  The accumulator D (128 coefficients x 128 targets,
-// FP32) lives in tensor memory for the whole tile.  Each product is split
-// into three TF32 MMAs, A_hi.B_hi + A_hi.B_lo + A_lo.B_hi, where hi/lo are the
-// TF32 rounding of a value and of its remainder (an error of about 2^-21 per
-// product instead of 2^-11 for plain TF32).
+// for a tile of 64 target boxes of one octant at one level (they share the
+// slot -> operator map).  Each product is split into three TF32 MMAs,
+// A_hi.B_hi + A_hi.B_lo + A_lo.B_hi, where hi/lo are the TF32 rounding of a
+// value and of its remainder (about 2^-21 relative error per product instead
+// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 64
+// targets, 48 MMAs) is accumulated in FP32 in tensor memory; two such
+// accumulators alternate, and while the tensor core fills one the epilogue
+// warps drain the other into FP64 registers, so the FP32 accumulation depth
+// is one slot instead of ~100.
 //
 // Operands use the K-major SWIZZLE_128B shared-memory layout: per K-block of
 // 32 TF32 values a tile row is 128 bytes, 8-row groups are 1024 bytes apart,
@@ -20,12 +23,12 @@
 // cp.async.bulk per K-block loads them; the source multipoles are gathered by
 // the producer warps with 16-byte loads and swizzled stores.
 //
-// Warp roles (256 threads): warp 0 owns the tensor memory and one elected
-// lane issues the MMAs; warps 4..7 produce the stages; warps 0..3 read the
-// accumulator back (tcgen05.ld 32x32b: warp w sees TMEM lanes 32w..32w+31)
-// and add it into the FP64 locals.  Every mbarrier wait is bounded: on
-// timeout the kernel records an error code, skips the remaining work and
-// still frees its tensor memory.
+// Warp roles (288 threads): warps 0..3 drain the accumulators (tcgen05.ld
+// 32x32b: warp w sees TMEM lanes 32w..32w+31 = coefficients) and own the FP64
+// sums; warp 4 owns the tensor memory and one lane issues the MMAs; warps 5..8
+// produce the pipeline stages.  Every mbarrier wait is bounded: on timeout the
+// kernel records an error code, skips the remaining work and still frees its
+// tensor memory.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -36,15 +39,17 @@
 namespace fmmb {
 namespace tc {
 
-constexpr int kTile = 128;        // target boxes per tile (MMA N)
+constexpr int kTile = 64;         // target boxes per tile (MMA N)
 constexpr int kRows = 128;        // output coefficients (MMA M), K <= 128
 constexpr int kKB = 32;           // TF32 values per K-block (128 bytes)
 constexpr int kNKB = 4;           // K-blocks (K padded to 128)
-constexpr int kStages = 3;
-constexpr int kOpBytes = kRows * 128;               // one operand K-block image (16 KB)
-constexpr int kStageBytes = 4 * kOpBytes;           // A_hi, A_lo, B_hi, B_lo
+constexpr int kStages = 4;
+constexpr int kOpBytes = kRows * 128;               // operator K-block image (16 KB)
+constexpr int kBBytes = kTile * 128;                // gathered multipole K-block (8 KB)
+constexpr int kStageBytes = 2 * kOpBytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-constexpr int kThreads = 256;
+constexpr int kThreads = 288;
+constexpr int kTmemCols = 2 * kTile;                // two alternating accumulators
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
 
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major,
@@ -159,8 +164,9 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accf = empty + kStages;
-  uint32_t* tmem_slot = (uint32_t*)(accf + 1);
+  uint64_t* accf = empty + kStages;  // [2] accumulator b complete
+  uint64_t* acce = accf + 2;         // [2] accumulator b drained
+  uint32_t* tmem_slot = (uint32_t*)(acce + 2);
   __shared__ int sh_boxes[kTile];
   __shared__ int sh_fail;
 
@@ -172,7 +178,8 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
   const float* opimg = P.opimg + P.op_set_off[lev];
   const float* Mtf = P.Mtf + (size_t)P.mtf_box_off[lev] * 256;
   const int s_begin = P.slot_off[work], s_end = P.slot_off[work + 1];
-  const int nstage_total = (s_end - s_begin) * kNKB;
+  const int nslot = s_end - s_begin;
+  const int nstage_total = nslot * kNKB;
 
   if (threadIdx.x < kTile) sh_boxes[threadIdx.x] = P.tile_boxes[tile * kTile + threadIdx.x];
   if (threadIdx.x == 0) {
@@ -181,12 +188,15 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
       mbar_init(&full[s], 129);  // 128 producer arrivals + 1 expect_tx arrival
       mbar_init(&empty[s], 1);   // one tcgen05.commit
     }
-    mbar_init(accf, 1);
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&accf[b], 1);    // tcgen05.commit after a slot's MMAs
+      mbar_init(&acce[b], 128);  // every epilogue thread after its tcgen05.ld
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 4) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(kTile));
+                 "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   tc_fence_before();
@@ -194,9 +204,10 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= 4) {
-    // ------------------------------------------------ producers
-    const int pt = threadIdx.x - 128;  // 0..127
+  if (warp >= 5) {
+    // ------------------------------------------------ producers (128 threads)
+    const int pt = threadIdx.x - 160;        // 0..127
+    const int row = pt >> 1, part = pt & 1;  // one 128-byte row of B_hi or B_lo
     for (int st = 0; st < nstage_total; st++) {
       const int s = st % kStages;
       const uint32_t ph = (st / kStages) & 1;
@@ -217,96 +228,99 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
         bulk_g2s(stage, img, kOpBytes, &full[s]);
         bulk_g2s(stage + kOpBytes, img + kRows * kKB, kOpBytes, &full[s]);
       }
-      // gather row pt of B_hi and B_lo for this K-block
-      const int box = sh_boxes[pt];
+      const int box = sh_boxes[row];
       const int src = box >= 0 ? P.list[(size_t)box * kM2LSlots + slot] : -1;
-      unsigned char* bhi = stage + 2 * kOpBytes;
-      unsigned char* blo = stage + 3 * kOpBytes;
+      unsigned char* dst = stage + 2 * kOpBytes + part * kBBytes;
       if (src >= 0) {
-        const float4* g = reinterpret_cast<const float4*>(Mtf + (size_t)src * 256 + kb * kKB);
+        const float4* g = reinterpret_cast<const float4*>(Mtf + (size_t)src * 256 + part * 128 + kb * kKB);
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-          const float4 h = __ldg(g + c);
-          const float4 l = __ldg(g + 32 + c);  // lo part starts 128 floats later
-          *reinterpret_cast<float4*>(bhi + swz(pt, c)) = h;
-          *reinterpret_cast<float4*>(blo + swz(pt, c)) = l;
-        }
+        for (int c = 0; c < 8; c++) *reinterpret_cast<float4*>(dst + swz(row, c)) = __ldg(g + c);
       } else {
         const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-          *reinterpret_cast<float4*>(bhi + swz(pt, c)) = z;
-          *reinterpret_cast<float4*>(blo + swz(pt, c)) = z;
-        }
+        for (int c = 0; c < 8; c++) *reinterpret_cast<float4*>(dst + swz(row, c)) = z;
       }
       fence_async_smem();
       mbar_arrive(&full[s]);
     }
-  } else if (warp == 0) {
+  } else if (warp == 4) {
     // ------------------------------------------------ MMA issuer
-    uint32_t acc = 0;
-    for (int st = 0; st < nstage_total; st++) {
-      const int s = st % kStages;
-      const uint32_t ph = (st / kStages) & 1;
-      bool ok = true;
-      if (lane == 0) ok = mbar_wait(&full[s], ph);
-      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-      if (!ok) {
-        if (lane == 0) atomicExch(&sh_fail, 2);
-        break;
+    bool ok = true;
+    for (int g = 0; g < nslot && ok; g++) {
+      const int buf = g & 1;
+      const uint32_t dcol = tmem + (uint32_t)(buf * kTile);
+      if (g >= 2) {  // wait until the epilogue has drained this accumulator
+        if (lane == 0) ok = mbar_wait(&acce[buf], ((g >> 1) - 1) & 1);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) break;
+        tc_fence_after();
       }
-      tc_fence_after();
-      if (lane == 0) {
-        const uint32_t base = smem_u32(smem + s * kStageBytes);
-        const uint32_t ahi = base, alo = base + kOpBytes, bhi = base + 2 * kOpBytes, blo = base + 3 * kOpBytes;
+      for (int kb = 0; kb < kNKB && ok; kb++) {
+        const int st = g * kNKB + kb;
+        const int s = st % kStages;
+        const uint32_t ph = (st / kStages) & 1;
+        if (lane == 0) ok = mbar_wait(&full[s], ph);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) break;
+        tc_fence_after();
+        if (lane == 0) {
+          const uint32_t base = smem_u32(smem + s * kStageBytes);
+          const uint32_t ahi = base, alo = base + kOpBytes, bhi = base + 2 * kOpBytes, blo = bhi + kBBytes;
 #pragma unroll
-        for (int k = 0; k < kKB / 8; k++) {  // 4 MMAs of K=8 per 32-wide block
-          const uint32_t o = k * 32;           // 8 TF32 = 32 bytes along K
-          mma_tf32(tmem, make_desc(ahi + o), make_desc(bhi + o), acc);
-          acc = 1;
-          mma_tf32(tmem, make_desc(ahi + o), make_desc(blo + o), 1);
-          mma_tf32(tmem, make_desc(alo + o), make_desc(bhi + o), 1);
-        }
-        mma_commit(&empty[s]);  // frees the stage when these MMAs are done
-      }
-      __syncwarp();
-    }
-    if (lane == 0) mma_commit(accf);  // accumulator complete (or nothing issued)
-    __syncwarp();
-  }
-
-  // ------------------------------------------------ epilogue (warps 0..3)
-  if (warp < 4) {
-    bool ok = mbar_wait(accf, 0);
-    if (!ok) atomicExch(&sh_fail, 3);
-    tc_fence_after();
-    const int row = warp * 32 + lane;  // output coefficient of this thread
-    // tcgen05.ld is warp-collective: the predicate must be warp-uniform
-    ok = __all_sync(0xffffffffu, ok && *(volatile int*)&sh_fail == 0) != 0;
-    if (ok && nstage_total > 0) {
-#pragma unroll 1
-      for (int c0 = 0; c0 < kTile; c0 += 32) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-        if (row < P.K) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int box = sh_boxes[c0 + j];
-            if (box >= 0) {
-              double* dst = P.L + (size_t)box * P.K + row;
-              if (P.atomic) atomicAdd(dst, (double)v[j]);
-              else *dst += (double)v[j];
-            }
+          for (int k = 0; k < kKB / 8; k++) {  // 4 MMAs of K=8 per 32-wide block
+            const uint32_t o = k * 32;           // 8 TF32 = 32 bytes along K
+            mma_tf32(dcol, make_desc(ahi + o), make_desc(bhi + o), (kb | k) ? 1u : 0u);
+            mma_tf32(dcol, make_desc(ahi + o), make_desc(blo + o), 1u);
+            mma_tf32(dcol, make_desc(alo + o), make_desc(bhi + o), 1u);
           }
+          mma_commit(&empty[s]);  // frees the stage when these MMAs are done
+          if (kb == kNKB - 1) mma_commit(&accf[buf]);
+        }
+        __syncwarp();
+      }
+    }
+    if (!ok && lane == 0) atomicExch(&sh_fail, 2);
+  } else {
+    // ------------------------------------------------ epilogue (warps 0..3)
+    const int row = warp * 32 + lane;  // output coefficient of this thread
+    double acc[kTile];
+#pragma unroll
+    for (int j = 0; j < kTile; j++) acc[j] = 0.0;
+    bool ok = true;
+    for (int g = 0; g < nslot; g++) {
+      const int buf = g & 1;
+      bool w = mbar_wait(&accf[buf], (g >> 1) & 1);
+      ok = __all_sync(0xffffffffu, w && *(volatile int*)&sh_fail == 0) != 0;
+      if (!ok) break;
+      tc_fence_after();
+      float v[32];
+#pragma unroll
+      for (int h = 0; h < kTile / 32; h++) {
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * kTile + h * 32), v);
+#pragma unroll
+        for (int j = 0; j < 32; j++) acc[h * 32 + j] += (double)v[j];
+      }
+      tc_fence_before();
+      mbar_arrive(&acce[buf]);
+    }
+    if (!ok) atomicExch(&sh_fail, 3);
+    if (ok && row < P.K) {
+#pragma unroll
+      for (int j = 0; j < kTile; j++) {
+        const int box = sh_boxes[j];
+        if (box >= 0) {
+          double* dst = P.L + (size_t)box * P.K + row;
+          if (P.atomic) atomicAdd(dst, acc[j]);
+          else *dst += acc[j];
         }
       }
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 4) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTile));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
   }
   if (threadIdx.x == 0 && sh_fail) atomicExch(P.err, sh_fail);
 }

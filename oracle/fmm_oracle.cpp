@@ -460,7 +460,14 @@ int oracle_fmm(const oracle_config* cfg, int ni, int nj, const float* tx, const 
       for (int i = tr.li0[ii]; i <= tr.li1[ii]; i++) {
         double pij = 0, fx = 0, fy = 0, fz = 0;
         for (int j = tr.lj0[jj]; j <= tr.lj1[jj]; j++) {
-          double dx = X[i] - XJ[j], dy = Y[i] - YJ[j], dz = Z[i] - ZJ[j];
+          // float differences as the reference (kernel/G_p2p.cxx:21-23);
+          // exact FP64 differences in accurate semantics
+          double dx, dy, dz;
+          if (s.ref) {
+            dx = X[i] - XJ[j]; dy = Y[i] - YJ[j]; dz = Z[i] - ZJ[j];
+          } else {
+            dx = (double)X[i] - XJ[j]; dy = (double)Y[i] - YJ[j]; dz = (double)Z[i] - ZJ[j];
+          }
           if (s.excl_self && dx == 0 && dy == 0 && dz == 0) continue;
           double r2 = dx * dx + dy * dy + dz * dz + s.eps2;
           if (neq == 0) {
