@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -287,67 +288,142 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         for (int b = 0; b < pl->nbox_j[lev]; b++) all[0].push_back(pl->off_j[lev] + b);
       pl->m2m_tiles.push_back(make_tiles(all, 8, [&](int box, int sl) { return m2m_list[(size_t)box * 8 + sl] >= 0 ? sl : -1; }));
     }
-    // tensor-core M2L (mixed precision, K <= 128): operator images and work items
+    // tensor-core translations (mixed precision, K <= 128): operator images,
+    // split buffers with their tensor maps, and the work items of M2L (all
+    // levels), M2M and L2L (per level)
     pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= 128;
     if (pl->use_tc) {
-      if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_opimg.get() == nullptr) {
+      const int K = pl->K;
+      auto upload_img = [&](DevBuf<float>& d, const std::vector<double>& mats, int nmat) {
         std::vector<float> img;
-        build_m2l_images(pl->ops, img);
-        pl->d_opimg.alloc(img.size());
-        FMMB_CUDA(cudaMemcpy(pl->d_opimg.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
+        build_tc_images(mats, nmat, K, img);
+        d.alloc(img.size());
+        FMMB_CUDA(cudaMemcpy(d.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
+      };
+      if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_img_m2l.get() == nullptr) {
+        upload_img(pl->d_img_m2l, pl->ops.m2l, pl->ops.m2l_sets * 316);
+        upload_img(pl->d_img_m2m, pl->ops.m2m, 8);
+        upload_img(pl->d_img_l2l, pl->ops.l2l, 8);
         pl->opimg_sets = pl->ops.m2l_sets;
         pl->opimg_rd = pl->ops.m2l_rd;
       }
-      const int TT = m2l_tc_tile();
-      std::vector<int> tb, to, tl;
-      std::vector<std::vector<int>> tslots;
-      for (int lev = 2; lev <= pl->lmax; lev++)
-        for (int oct = 0; oct < 8; oct++) {
-          std::vector<int> bx;
-          for (int b = 0; b < pl->nbox_i[lev]; b++)
-            if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
-          for (size_t k = 0; k < bx.size(); k += TT) {
-            std::vector<int> act;
-            for (int sl = 0; sl < kM2LSlots; sl++) {
-              bool any = false;
-              for (size_t t = k; t < std::min(bx.size(), k + TT) && !any; t++) any = lst[(size_t)bx[t] * kM2LSlots + sl] >= 0;
-              if (any) act.push_back(sl);
-            }
-            if (act.empty()) continue;
-            for (int t = 0; t < TT; t++) tb.push_back(k + t < bx.size() ? bx[k + t] : -1);
-            to.push_back(oct);
-            tl.push_back(lev);
-            tslots.push_back(act);
-          }
-        }
-      const int ntile = (int)to.size();
-      // split tiles over their slots so that the launch has ~2 work items per SM
+      pl->Mtf.alloc((size_t)pl->tot_j * 256);
+      pl->Ltf.alloc((size_t)pl->tot_i * 256);
+      make_split_tmap(pl->tmap_M, pl->Mtf.get(), pl->tot_j);
+      make_split_tmap(pl->tmap_L, pl->Ltf.get(), pl->tot_i);
       int dev_sms = 148;
       cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
-      pl->tc_nsplit = ntile > 0 ? std::max(1, std::min(8, (2 * dev_sms + ntile - 1) / ntile)) : 1;
-      std::vector<int> wt, off{0}, sl;
-      for (int t = 0; t < ntile; t++) {
-        const int n = (int)tslots[t].size();
-        for (int k = 0; k < pl->tc_nsplit; k++) {
-          const int a = (int)((long long)n * k / pl->tc_nsplit), b = (int)((long long)n * (k + 1) / pl->tc_nsplit);
-          if (b <= a) continue;
-          wt.push_back(t);
-          for (int i = a; i < b; i++) sl.push_back(tslots[t][i]);
-          off.push_back((int)sl.size());
+      const int TT = tc_tile();
+      // groups of output boxes -> work items; slot(box, s) -> (operator, source row or -1)
+      auto build_job = [&](fmmb_plan::TcJob& job, const std::vector<std::vector<int>>& groups, int nslots,
+                           auto slot_fn, int oob_row) {
+        struct Tile {
+          std::vector<int> boxes;
+          std::vector<int> ops;                 // per active slot
+          std::vector<std::array<int, 64>> src;  // per active slot
+        };
+        std::vector<Tile> tiles;
+        for (const auto& g : groups)
+          for (size_t k = 0; k < g.size(); k += TT) {
+            Tile t;
+            for (int i = 0; i < TT; i++) t.boxes.push_back(k + i < g.size() ? g[k + i] : -1);
+            for (int sl = 0; sl < nslots; sl++) {
+              std::array<int, 64> rows;
+              int op = -1;
+              bool any = false;
+              for (int i = 0; i < TT; i++) {
+                rows[i] = oob_row;
+                if (t.boxes[i] < 0) continue;
+                int o = -1, r = -1;
+                slot_fn(t.boxes[i], sl, o, r);
+                if (r >= 0) {
+                  rows[i] = r;
+                  op = o;
+                  any = true;
+                }
+              }
+              if (any) {
+                t.ops.push_back(op);
+                t.src.push_back(rows);
+              }
+            }
+            if (!t.ops.empty()) tiles.push_back(std::move(t));
+          }
+        const int ntile = (int)tiles.size();
+        const int nsplit = ntile > 0 ? std::max(1, std::min(8, (2 * dev_sms + ntile - 1) / ntile)) : 1;
+        std::vector<int> ob, off{0}, so, ss;
+        for (const auto& t : tiles) {
+          const int n = (int)t.ops.size();
+          for (int k = 0; k < nsplit; k++) {
+            const int a0 = (int)((long long)n * k / nsplit), a1 = (int)((long long)n * (k + 1) / nsplit);
+            if (a1 <= a0) continue;
+            ob.insert(ob.end(), t.boxes.begin(), t.boxes.end());
+            for (int i = a0; i < a1; i++) {
+              so.push_back(t.ops[i]);
+              ss.insert(ss.end(), t.src[i].begin(), t.src[i].end());
+            }
+            off.push_back((int)so.size());
+          }
+        }
+        job.nwork = (int)off.size() - 1;
+        job.atomic = nsplit > 1 ? 1 : 0;
+        auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+          d.alloc(h.size());
+          if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+        };
+        up(job.out_boxes, ob);
+        up(job.slot_off, off);
+        up(job.slot_op, so);
+        up(job.slot_src, ss);
+      };
+      // M2L: target boxes by (level, octant); operator = set(level)*316 + position
+      {
+        std::vector<std::vector<int>> groups;
+        for (int lev = 2; lev <= pl->lmax; lev++)
+          for (int oct = 0; oct < 8; oct++) {
+            std::vector<int> bx;
+            for (int b = 0; b < pl->nbox_i[lev]; b++)
+              if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
+            groups.push_back(bx);
+          }
+        std::vector<int> lev_of(pl->tot_i);
+        for (int lev = 2; lev <= pl->lmax; lev++)
+          for (int b = 0; b < pl->nbox_i[lev]; b++) lev_of[pl->off_i[lev] + b] = lev;
+        build_job(pl->tc_m2l, groups, kM2LSlots, [&](int box, int sl, int& op, int& row) {
+          const int src = lst[(size_t)box * kM2LSlots + sl];
+          if (src < 0) return;
+          const int lev = lev_of[box];
+          const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
+          op = set * 316 + pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
+          row = pl->off_j[lev] + src;
+        }, pl->tot_j);
+      }
+      pl->tc_m2m.clear();
+      pl->tc_l2l.clear();
+      std::vector<int> par_i(pl->tot_i);
+      FMMB_CUDA(cudaMemcpy(par_i.data(), pl->parent_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int lev = 0; lev <= pl->lmax; lev++) {
+        pl->tc_m2m.emplace_back(new fmmb_plan::TcJob());
+        pl->tc_l2l.emplace_back(new fmmb_plan::TcJob());
+        if (lev >= 2 && lev < pl->lmax) {  // M2M into parents at lev
+          std::vector<std::vector<int>> groups(1);
+          for (int b = 0; b < pl->nbox_j[lev]; b++) groups[0].push_back(pl->off_j[lev] + b);
+          build_job(*pl->tc_m2m[lev], groups, 8, [&](int box, int sl, int& op, int& row) {
+            const int c = m2m_list[(size_t)box * 8 + sl];
+            if (c < 0) return;
+            op = sl;
+            row = pl->off_j[lev + 1] + c;
+          }, pl->tot_j);
+        }
+        if (lev >= 3) {  // L2L into children at lev, grouped by octant
+          std::vector<std::vector<int>> groups(8);
+          for (int b = 0; b < pl->nbox_i[lev]; b++) groups[keys[pl->off_i[lev] + b] & 7].push_back(pl->off_i[lev] + b);
+          build_job(*pl->tc_l2l[lev], groups, 1, [&](int box, int, int& op, int& row) {
+            op = keys[box] & 7;
+            row = pl->off_i[lev - 1] + par_i[box];
+          }, pl->tot_i);
         }
       }
-      pl->tc_nwork = (int)wt.size();
-      auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
-        d.alloc(h.size());
-        if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
-      };
-      up(pl->tc_boxes, tb);
-      up(pl->tc_oct, to);
-      up(pl->tc_level, tl);
-      up(pl->tc_work_tile, wt);
-      up(pl->tc_slot_off, off);
-      up(pl->tc_slots, sl);
-      pl->Mtf.alloc((size_t)pl->tot_j * 256);
     }
     // inverse target permutation (caller -> sorted) for the direct sum
     {
@@ -445,45 +521,50 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   if (lmax > 2)
     FMMB_CUDA(cudaMemsetAsync(pl->M.get() + (size_t)pl->off_j[lmax - 1] * K, 0,
                               (size_t)(pl->tot_j - pl->off_j[lmax - 1]) * K * sizeof(double), m));
-  for (int lev = lmax - 1; lev >= 2; lev--) {
-    PhaseTimer tm(pl, 2, m);
-    const auto& ts = *pl->m2m_tiles[lev];
-    launch_translate_f64(ts.ntile, split_for(ts.ntile, 8), K, 8, ts.boxes.get(), ts.ops.get(), pl->m2m_list.get(),
-                         pl->d_m2m.get(), pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->M.get(), m);
+  auto tc_run = [&](const fmmb_plan::TcJob& job, const float* img, const void* tmap, double* out, int phase) {
+    PhaseTimer tm(pl, phase, m);
+    TcJobArgs a{};
+    a.nwork = job.nwork;
+    a.K = K;
+    a.atomic = job.atomic;
+    a.out_boxes = job.out_boxes.get();
+    a.slot_off = job.slot_off.get();
+    a.slot_op = job.slot_op.get();
+    a.slot_src = job.slot_src.get();
+    a.opimg = img;
+    a.tmap = tmap;
+    a.out = out;
+    a.err = pl->d_err.get();
+    launch_translate_tc(a, m);
+  };
+  auto split = [&](const double* X, float* Xtf, int off, int n, int phase) {
+    PhaseTimer tm(pl, phase, m);
+    launch_split_tf32(n, K, X + (size_t)off * K, Xtf + (size_t)off * 256, m);
+  };
+  if (pl->use_tc) {
+    split(pl->M.get(), pl->Mtf.get(), pl->off_j[lmax], pl->nbox_j[lmax], 2);
+    for (int lev = lmax - 1; lev >= 2; lev--) {
+      tc_run(*pl->tc_m2m[lev], pl->d_img_m2m.get(), pl->tmap_M, pl->M.get(), 2);
+      split(pl->M.get(), pl->Mtf.get(), pl->off_j[lev], pl->nbox_j[lev], 2);
+    }
+  } else {
+    for (int lev = lmax - 1; lev >= 2; lev--) {
+      PhaseTimer tm(pl, 2, m);
+      const auto& ts = *pl->m2m_tiles[lev];
+      launch_translate_f64(ts.ntile, split_for(ts.ntile, 8), K, 8, ts.boxes.get(), ts.ops.get(), pl->m2m_list.get(),
+                           pl->d_m2m.get(), pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->M.get(), m);
+    }
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[4], m));
   // downward pass: M2L of every level into zeroed locals, then each level
   // adds its parent's translated local (L2L), top down
   FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * K * sizeof(double), m));
   if (pl->use_tc) {
-    {
-      PhaseTimer tm(pl, 3, m);
-      launch_split_tf32(pl->tot_j, K, pl->M.get(), pl->Mtf.get(), m);
+    tc_run(pl->tc_m2l, pl->d_img_m2l.get(), pl->tmap_M, pl->L.get(), 3);
+    for (int lev = 3; lev <= lmax; lev++) {
+      split(pl->L.get(), pl->Ltf.get(), pl->off_i[lev - 1], pl->nbox_i[lev - 1], 4);
+      tc_run(*pl->tc_l2l[lev], pl->d_img_l2l.get(), pl->tmap_L, pl->L.get(), 4);
     }
-    PhaseTimer tm(pl, 3, m);
-    M2LTcArgs a{};
-    a.nwork = pl->tc_nwork;
-    a.K = K;
-    a.atomic = pl->tc_nsplit > 1 ? 1 : 0;
-    a.tile_boxes = pl->tc_boxes.get();
-    a.tile_oct = pl->tc_oct.get();
-    a.tile_level = pl->tc_level.get();
-    a.work_tile = pl->tc_work_tile.get();
-    a.slot_off = pl->tc_slot_off.get();
-    a.slots = pl->tc_slots.get();
-    a.list = pl->m2l_list.get();
-    a.slot_rel = pl->d_slot_rel.get();
-    a.rel_to_op = pl->d_rel_to_op.get();
-    a.opimg = pl->d_opimg.get();
-    const long long set_floats = (long long)316 * 4 * 2 * 128 * 32;
-    for (int l = 0; l < 11; l++) {
-      a.op_set_off[l] = (pl->ops.m2l_sets > 1 && l >= 2) ? (long long)(l - 2) * set_floats : 0;
-      a.mtf_box_off[l] = (l >= 2 && l <= lmax) ? pl->off_j[l] : 0;
-    }
-    a.Mtf = pl->Mtf.get();
-    a.L = pl->L.get();
-    a.err = pl->d_err.get();
-    launch_m2l_tc(a, m);
   } else {
     const size_t opsz = (size_t)316 * K * K;
     for (int lev = 2; lev <= lmax; lev++) {
@@ -494,12 +575,12 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                            pl->m2l_list.get(), pl->d_m2l.get() + set * opsz, pl->M.get() + (size_t)pl->off_j[lev] * K,
                            pl->L.get(), m);
     }
-  }
-  for (int lev = 3; lev <= lmax; lev++) {
-    PhaseTimer tm(pl, 4, m);
-    const auto& ts = *pl->l2l_tiles[lev];
-    launch_translate_f64(ts.ntile, 1, K, 1, ts.boxes.get(), ts.ops.get(), pl->parent_i.get(), pl->d_l2l.get(),
-                         pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->L.get(), m);
+    for (int lev = 3; lev <= lmax; lev++) {
+      PhaseTimer tm(pl, 4, m);
+      const auto& ts = *pl->l2l_tiles[lev];
+      launch_translate_f64(ts.ntile, 1, K, 1, ts.boxes.get(), ts.ops.get(), pl->parent_i.get(), pl->d_l2l.get(),
+                           pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->L.get(), m);
+    }
   }
   FMMB_CUDA(cudaEventRecord(pl->ev[5], m));
   {

@@ -30,6 +30,14 @@ namespace {
 struct cplx {
   double re, im;
 };
+
+// 1/k for the Legendre-type recurrences (k = n - m <= 40): avoids FP64 divides
+__constant__ double c_inv[41] = {0.0,      1.0 / 1,  1.0 / 2,  1.0 / 3,  1.0 / 4,  1.0 / 5,  1.0 / 6,  1.0 / 7,
+                                 1.0 / 8,  1.0 / 9,  1.0 / 10, 1.0 / 11, 1.0 / 12, 1.0 / 13, 1.0 / 14, 1.0 / 15,
+                                 1.0 / 16, 1.0 / 17, 1.0 / 18, 1.0 / 19, 1.0 / 20, 1.0 / 21, 1.0 / 22, 1.0 / 23,
+                                 1.0 / 24, 1.0 / 25, 1.0 / 26, 1.0 / 27, 1.0 / 28, 1.0 / 29, 1.0 / 30, 1.0 / 31,
+                                 1.0 / 32, 1.0 / 33, 1.0 / 34, 1.0 / 35, 1.0 / 36, 1.0 / 37, 1.0 / 38, 1.0 / 39,
+                                 1.0 / 40};
 __device__ __forceinline__ cplx cmul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
 __device__ __forceinline__ cplx cscale(cplx a, double s) { return {a.re * s, a.im * s}; }
 
@@ -97,7 +105,8 @@ __global__ void __launch_bounds__(128) p2m_cart(int p, int K, const int* __restr
       else if (n == m) sn = smm;
       else if (n == m + 1) sn = cscale(s1, (2.0 * m + 1.0) * z);
       else {
-        const double a = (2.0 * n - 1.0) * z / (n - m), c = (n + m - 1.0) * r2 / (n - m);
+        const double inv = c_inv[n - m];
+        const double a = (2.0 * n - 1.0) * z * inv, c = (n + m - 1.0) * r2 * inv;
         sn = {a * s1.re - c * s2.re, a * s1.im - c * s2.im};
       }
       if (KER != FMMB_LAPLACE_GNJ) {
@@ -214,7 +223,8 @@ __global__ void __launch_bounds__(kL2PThreads) l2p_cart(int p, int K, const int*
         if (n == m) sn = smm;
         else if (n == m + 1) sn = cscale(s1, (2.0 * m + 1.0) * z);
         else {
-          const double a = (2.0 * n - 1.0) * z / (n - m), c = (n + m - 1.0) * r2 / (n - m);
+          const double inv = c_inv[n - m];
+        const double a = (2.0 * n - 1.0) * z * inv, c = (n + m - 1.0) * r2 * inv;
           sn = {a * s1.re - c * s2.re, a * s1.im - c * s2.im};
         }
         const int idx = n * (n + 1) / 2 + m;

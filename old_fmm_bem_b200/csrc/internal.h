@@ -91,8 +91,8 @@ void build_static_operators(Operators& ops, int p, bool ref_semantics);
 // M2L sets: one in accurate semantics; one per level 2..lmax in reference
 // semantics, where the distance carries an absolute eps (needs the root size).
 void build_m2l_operators(Operators& ops, int lmax, float rd);
-// TF32 hi/lo images of the M2L operators in the tensor-core operand layout
-void build_m2l_images(const Operators& ops, std::vector<float>& img);
+// TF32 hi/lo images of nmat K x K operators in the tensor-core operand layout
+void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vector<float>& img);
 
 struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
@@ -147,19 +147,26 @@ struct fmmb_plan {
   // operators on the device
   fmmb::DevBuf<double> d_fac, d_m2m, d_l2l, d_m2l;
   fmmb::DevBuf<int> d_slot_rel, d_rel_to_op;
-  fmmb::DevBuf<float> d_opimg;               // [sets][316][4 K-blocks][2][128*32] TF32 images (mixed)
+  fmmb::DevBuf<float> d_img_m2l;             // [sets*316][4 K-blocks][2][128*32] TF32 images (mixed)
+  fmmb::DevBuf<float> d_img_m2m, d_img_l2l;  // [8][...]
 
   // evaluation buffers
   fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
   fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
-  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][128] TF32 hi/lo (mixed)
+  fmmb::DevBuf<float> Mtf, Ltf;              // [tot][2][128] TF32 hi/lo splits (mixed)
+  alignas(128) unsigned char tmap_M[128] = {}, tmap_L[128] = {};  // CUtensorMap over Mtf / Ltf
   fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
   int* h_err = nullptr;                      // pinned copy, checked by the next call
   bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)
-  int tc_nwork = 0, tc_nsplit = 1;
   int opimg_sets = 0;
   float opimg_rd = 0;
-  fmmb::DevBuf<int> tc_boxes, tc_oct, tc_level, tc_work_tile, tc_slot_off, tc_slots;
+  // tensor-core translation jobs: work items of 64 output boxes with their slots
+  struct TcJob {
+    int nwork = 0, atomic = 0;
+    fmmb::DevBuf<int> out_boxes, slot_off, slot_op, slot_src;
+  };
+  TcJob tc_m2l;                                              // all levels
+  std::vector<std::unique_ptr<TcJob>> tc_m2m, tc_l2l;        // per level
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging
   fmmb::DevBuf<double> stage_d;

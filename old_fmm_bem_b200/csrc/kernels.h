@@ -52,19 +52,18 @@ void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float
 }  // namespace fmmb
 
 namespace fmmb {
-// tensor-core M2L (m2l_tc.cu)
-int m2l_tc_tile();
+// tensor-core translations (translate_tc.cu)
+int tc_tile();
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
-struct M2LTcArgs {
+// tmap_out: 128-byte aligned storage for a CUtensorMap
+void make_split_tmap(void* tmap_out, const float* base, int rows);
+struct TcJobArgs {
   int nwork, K, atomic;
-  const int *tile_boxes, *tile_oct, *tile_level, *work_tile, *slot_off, *slots;
-  const int *list, *slot_rel, *rel_to_op;
+  const int *out_boxes, *slot_off, *slot_op, *slot_src;
   const float* opimg;
-  long long op_set_off[11];
-  const float* Mtf;
-  int mtf_box_off[11];
-  double* L;
+  const void* tmap;  // CUtensorMap over the split inputs
+  double* out;
   int* err;
 };
-void launch_m2l_tc(const M2LTcArgs& a, cudaStream_t st);
+void launch_translate_tc(const TcJobArgs& a, cudaStream_t st);
 }  // namespace fmmb

@@ -337,16 +337,16 @@ static float tf32_rna_host(float x) {
   return y;
 }
 
-// M2L operators as TF32 (hi, lo) pairs laid out exactly like the tensor-core
-// kernel's shared-memory operand tiles: per operator, per K-block of 32
-// columns, per part, 128 rows of 128 bytes with the 16-byte chunk c of row r
-// stored at chunk c ^ (r & 7) (K-major SWIZZLE_128B).  Rows/columns >= K are 0.
-void build_m2l_images(const Operators& ops, std::vector<float>& img) {
-  const int K = ops.K, nops = (int)ops.op_rel.size();
+// Translation operators as TF32 (hi, lo) pairs laid out exactly like the
+// tensor-core kernel's shared-memory operand tiles: per operator, per K-block
+// of 32 columns, per part, 128 rows of 128 bytes with the 16-byte chunk c of
+// row r stored at chunk c ^ (r & 7) (K-major SWIZZLE_128B).  Rows/columns >= K
+// are 0.
+void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vector<float>& img) {
   const size_t per_op = (size_t)4 * 2 * 128 * 32;
-  img.assign((size_t)ops.m2l_sets * nops * per_op, 0.0f);
-  parallel_for(ops.m2l_sets * nops, [&](int w) {
-    const double* T = &ops.m2l[(size_t)w * K * K];
+  img.assign((size_t)nmat * per_op, 0.0f);
+  parallel_for(nmat, [&](int w) {
+    const double* T = &mats[(size_t)w * K * K];
     float* out = &img[(size_t)w * per_op];
     for (int kb = 0; kb < 4; kb++)
       for (int r = 0; r < 128; r++)

@@ -1,35 +1,28 @@
-// M2L on the 5th-generation tensor cores (tcgen05, TMEM accumulators), TF32x3.
+// Box-to-box translations (M2L, M2M, L2L) on the 5th-generation tensor
+// cores (tcgen05, TMEM accumulators) in TF32x3, for the mixed-precision form.
 //
-// Same operator as kernels_fp64.cu's m2l_f64 (the reference's
-// rotate / z-translate / rotate-back M2L of kernel/m2l.cxx:30-83 composed into
-// one real K x K matrix per relative position, operators.cpp), applied as
-//
-//   L[:, tile] += sum over active slots d of  T_d (128 x 128) . M[src(tile, d)] (128 x 128)
-//
-// for a tile of 64 target boxes of one octant at one level (they share the
-// slot -> operator map).  Each product is split into three TF32 MMAs,
+// Every translation is a dense real K x K operator (operators.cpp: the
+// reference's rotate / z-translate / rotate-back steps of kernel/m2l.cxx:30-83,
+// kernel/m2m.cxx:28-62 and kernel/l2l.cxx:44-78 composed into one matrix per
+// relative position).  A work item is a tile of 64 output boxes and a list of
+// slots; slot s contributes T_s (128 x 128) . X[src(s, box)] for the 64
+// boxes, X being the TF32 (hi, lo) split of the input expansions:
+//   M2L: output target boxes of one octant at one level, slots = interaction
+//        positions, input = multipoles of the same level;
+//   M2M: output parents, slots = the 8 child octants, input = children;
+//   L2L: output children of one octant, one slot, input = parents.
+// The operator index and the 64 source rows of every (work item, slot) are
+// precomputed with the tree.  Each product is split into three TF32 MMAs,
 // A_hi.B_hi + A_hi.B_lo + A_lo.B_hi, where hi/lo are the TF32 rounding of a
 // value and of its remainder (about 2^-21 relative error per product instead
-// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 64
-// targets, 48 MMAs) is accumulated in FP32 in tensor memory; two such
-// accumulators alternate, and while the tensor core fills one the epilogue
-// warps drain the other into FP64 registers, so the FP32 accumulation depth
-// is one slot instead of ~100.
+// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 64 boxes,
+// 48 MMAs) is accumulated in FP32 in tensor memory; two such accumulators
+// alternate, and while the tensor core fills one the epilogue warps drain the
+// other into FP64 registers, so the FP32 accumulation depth is one slot.
 //
-// Operands use the K-major SWIZZLE_128B shared-memory layout: per K-block of
-// 32 TF32 values a tile row is 128 bytes, 8-row groups are 1024 bytes apart,
-// and the 16-byte chunk c of row r sits at chunk c ^ (r & 7).  The operator
-// K-blocks are stored in global memory as exactly that image, so one
-// cp.async.bulk per K-block loads them; the source multipoles are gathered by
-// the producer warps with 16-byte loads and swizzled stores.
-//
-// Warp roles (288 threads): warps 0..3 drain the accumulators (tcgen05.ld
-// 32x32b: warp w sees TMEM lanes 32w..32w+31 = coefficients) and own the FP64
-// sums; warp 4 owns the tensor memory and one lane issues the MMAs; warps 5..8
-// produce the pipeline stages.  Every mbarrier wait is bounded: on timeout the
-// kernel records an error code, skips the remaining work and still frees its
-// tensor memory.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
 
@@ -48,7 +41,7 @@ constexpr int kOpBytes = kRows * 128;               // operator K-block image (1
 constexpr int kBBytes = kTile * 128;                // gathered multipole K-block (8 KB)
 constexpr int kStageBytes = 2 * kOpBytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-constexpr int kThreads = 288;
+constexpr int kThreads = 192;
 constexpr int kTmemCols = 2 * kTile;                // two alternating accumulators
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
 
@@ -140,26 +133,27 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
 __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
 struct Params {
-  int K;                        // real coefficients per expansion (<= 128)
-  const int* tile_boxes;        // [ntile][128] global target box index or -1
-  const int* tile_oct;          // [ntile] octant shared by the tile's boxes
-  const int* tile_level;        // [ntile]
-  const int* work_tile;         // [nwork] tile of each work item (a tile may be split over its slots)
-  const int* slot_off;          // [nwork + 1] CSR of the active slots of each work item
-  const int* slots;             // active slot numbers
-  const int* list;              // [tot_i][189] source box within the level or -1
-  const int* slot_rel;          // [8][189]
-  const int* rel_to_op;         // [343]
-  const float* opimg;           // operator images [sets][316][4][2][128*32]
-  long long op_set_off[11];     // float offset of each level's operator set
-  const float* Mtf;             // all-level source multipoles [tot_j][2][128] (hi, lo)
-  int mtf_box_off[11];          // first box of each level in Mtf
-  double* L;                    // all-level locals [tot_i][K]
-  int atomic;                   // 1 when a tile is split over several work items
-  int* err;                     // set to a nonzero code on timeout
+  int K;                  // real coefficients per expansion (<= 128)
+  const int* out_boxes;   // [nwork][64] output box (row of `out`) or -1
+  const int* slot_off;    // [nwork + 1] CSR of each work item's slots
+  const int* slot_op;     // operator image of each slot
+  const int* slot_src;    // [slots][64] input row of each output box (out of range = none)
+  const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
+  double* out;            // FP64 expansions, [rows][K]
+  int atomic;             // 1 when an output box appears in several work items
+  int* err;               // set to a nonzero code on timeout
 };
 
-__global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
+__device__ __forceinline__ void gather4(void* dst, const CUtensorMap* map, int x, int4 rows, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(rows.x), "r"(rows.y), "r"(rows.z), "r"(rows.w),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constant__ CUtensorMap src_map, Params P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
@@ -172,20 +166,15 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int work = blockIdx.x;
-  const int tile = P.work_tile[work];
-  const int oct = P.tile_oct[tile];
-  const int lev = P.tile_level[tile];
-  const float* opimg = P.opimg + P.op_set_off[lev];
-  const float* Mtf = P.Mtf + (size_t)P.mtf_box_off[lev] * 256;
   const int s_begin = P.slot_off[work], s_end = P.slot_off[work + 1];
   const int nslot = s_end - s_begin;
   const int nstage_total = nslot * kNKB;
 
-  if (threadIdx.x < kTile) sh_boxes[threadIdx.x] = P.tile_boxes[tile * kTile + threadIdx.x];
+  if (threadIdx.x < kTile) sh_boxes[threadIdx.x] = P.out_boxes[(size_t)work * kTile + threadIdx.x];
   if (threadIdx.x == 0) {
     sh_fail = 0;
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 129);  // 128 producer arrivals + 1 expect_tx arrival
+      mbar_init(&full[s], 1);    // the producer's expect_tx arrival (+ TMA bytes)
       mbar_init(&empty[s], 1);   // one tcgen05.commit
     }
     for (int b = 0; b < 2; b++) {
@@ -204,44 +193,32 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= 5) {
-    // ------------------------------------------------ producers (128 threads)
-    const int pt = threadIdx.x - 160;        // 0..127
-    const int row = pt >> 1, part = pt & 1;  // one 128-byte row of B_hi or B_lo
+  if (warp == 5) {
+    // ------------------------------------------------ producer warp
+    const int part = lane >> 4, g = lane & 15;  // lane: rows 4g..4g+3 of B_hi (part 0) / B_lo (part 1)
     for (int st = 0; st < nstage_total; st++) {
       const int s = st % kStages;
       const uint32_t ph = (st / kStages) & 1;
-      if (st >= kStages) {
-        if (!mbar_wait(&empty[s], ph ^ 1)) {
-          atomicExch(&sh_fail, 1);
-          break;
-        }
+      bool ok = true;
+      if (st >= kStages && lane == 0) ok = mbar_wait(&empty[s], ph ^ 1);
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      if (!ok) {
+        if (lane == 0) atomicExch(&sh_fail, 1);
+        break;
       }
       if (*(volatile int*)&sh_fail) break;
-      const int slot = P.slots[s_begin + st / kNKB];
+      const int sl = s_begin + st / kNKB;
       const int kb = st % kNKB;
       unsigned char* stage = smem + s * kStageBytes;
-      if (pt == 0) {
-        const int op = P.rel_to_op[P.slot_rel[oct * kM2LSlots + slot]];
-        const float* img = opimg + ((size_t)op * kNKB + kb) * 2 * (kRows * kKB);
-        mbar_arrive_tx(&full[s], 2 * kOpBytes);
+      if (lane == 0) {
+        const float* img = P.opimg + ((size_t)P.slot_op[sl] * kNKB + kb) * 2 * (kRows * kKB);
+        mbar_arrive_tx(&full[s], 2 * kOpBytes + 2 * kBBytes);
         bulk_g2s(stage, img, kOpBytes, &full[s]);
         bulk_g2s(stage + kOpBytes, img + kRows * kKB, kOpBytes, &full[s]);
       }
-      const int box = sh_boxes[row];
-      const int src = box >= 0 ? P.list[(size_t)box * kM2LSlots + slot] : -1;
-      unsigned char* dst = stage + 2 * kOpBytes + part * kBBytes;
-      if (src >= 0) {
-        const float4* g = reinterpret_cast<const float4*>(Mtf + (size_t)src * 256 + part * 128 + kb * kKB);
-#pragma unroll
-        for (int c = 0; c < 8; c++) *reinterpret_cast<float4*>(dst + swz(row, c)) = __ldg(g + c);
-      } else {
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-        for (int c = 0; c < 8; c++) *reinterpret_cast<float4*>(dst + swz(row, c)) = z;
-      }
-      fence_async_smem();
-      mbar_arrive(&full[s]);
+      __syncwarp();
+      const int4 rows = *reinterpret_cast<const int4*>(P.slot_src + (size_t)sl * kTile + 4 * g);
+      gather4(stage + 2 * kOpBytes + part * kBBytes + 4 * g * 128, &src_map, part * 128 + kb * kKB, rows, &full[s]);
     }
   } else if (warp == 4) {
     // ------------------------------------------------ MMA issuer
@@ -309,7 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1) m2l_tc_kernel(Params P) {
       for (int j = 0; j < kTile; j++) {
         const int box = sh_boxes[j];
         if (box >= 0) {
-          double* dst = P.L + (size_t)box * P.K + row;
+          double* dst = P.out + (size_t)box * P.K + row;
           if (P.atomic) atomicAdd(dst, acc[j]);
           else *dst += acc[j];
         }
@@ -350,7 +327,7 @@ __global__ void split_tf32(int nbox, int K, const double* __restrict__ M, float*
 
 }  // namespace tc
 
-int m2l_tc_tile() { return tc::kTile; }
+int tc_tile() { return tc::kTile; }
 
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st) {
   if (nbox <= 0) return;
@@ -359,30 +336,49 @@ void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_m2l_tc(const M2LTcArgs& a, cudaStream_t st) {
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    FMMB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    FMMB_REQUIRE(p && q == cudaDriverEntryPointSuccess, FMMB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+}  // namespace
+
+// Tensor map over split expansions [rows][256] FP32 (hi 0..127, lo 128..255):
+// boxes of 32 values x 1 row, 128-byte swizzle, zero fill out of range.
+void make_split_tmap(void* tmap_out, const float* base, int rows) {
+  CUtensorMap* m = reinterpret_cast<CUtensorMap*>(tmap_out);
+  const cuuint64_t dims[2] = {256, (cuuint64_t)(rows > 0 ? rows : 1)};
+  const cuuint64_t strides[1] = {256 * sizeof(float)};
+  const cuuint32_t box[2] = {32, 1};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  FMMB_REQUIRE(r == CUDA_SUCCESS, FMMB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+}
+
+void launch_translate_tc(const TcJobArgs& a, cudaStream_t st) {
   if (a.nwork <= 0) return;
-  FMMB_CUDA(cudaFuncSetAttribute(tc::m2l_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+  FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
   tc::Params P{};
   P.K = a.K;
-  P.tile_boxes = a.tile_boxes;
-  P.tile_oct = a.tile_oct;
-  P.tile_level = a.tile_level;
-  P.work_tile = a.work_tile;
+  P.out_boxes = a.out_boxes;
   P.slot_off = a.slot_off;
-  P.slots = a.slots;
-  P.list = a.list;
-  P.slot_rel = a.slot_rel;
-  P.rel_to_op = a.rel_to_op;
+  P.slot_op = a.slot_op;
+  P.slot_src = a.slot_src;
   P.opimg = a.opimg;
-  P.Mtf = a.Mtf;
-  for (int l = 0; l < 11; l++) {
-    P.op_set_off[l] = a.op_set_off[l];
-    P.mtf_box_off[l] = a.mtf_box_off[l];
-  }
-  P.L = a.L;
+  P.out = a.out;
   P.atomic = a.atomic;
   P.err = a.err;
-  tc::m2l_tc_kernel<<<a.nwork, tc::kThreads, tc::kSmemBytes, st>>>(P);
+  const CUtensorMap* m = reinterpret_cast<const CUtensorMap*>(a.tmap);
+  tc::translate_tc<<<a.nwork, tc::kThreads, tc::kSmemBytes, st>>>(*m, P);
   FMMB_CHECK_LAUNCH();
 }
 

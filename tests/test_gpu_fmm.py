@@ -193,14 +193,16 @@ def test_errors_are_reported_not_fatal(ob):
 
 
 @pytest.mark.parametrize("semantics", [0, 1])
-def test_tensor_core_m2l_locals_match_fp64(semantics, ob):
-    """The TF32x3 tensor-core M2L gives the FP64 locals of every level to
-    ~1e-6 (TF32x3 products carry ~2^-21 relative error, FP32 accumulation)."""
+def test_tensor_core_translations_match_fp64(semantics, ob):
+    """The TF32x3 tensor-core M2M, M2L and L2L give the FP64 multipoles and
+    locals of every level to ~1e-6 (TF32x3 products carry ~2^-21 relative
+    error; each slot is accumulated in FP32, slots in FP64)."""
     t, tn, s, sn, q = make_points(40000, 100, "clustered")
     out = []
     for prec in (0, 1):
         pl = plan_for(ob, 0, 10, 4, t, tn, s, sn, semantics=semantics, precision=prec)
         pl.evaluate(q, f64=True)
-        out.append(pl.expansions(1))
+        out.append((pl.expansions(0), pl.expansions(1)))
         pl.close()
-    assert rel(out[1], out[0]) < 2e-6
+    assert rel(out[1][0], out[0][0]) < 1e-6
+    assert rel(out[1][1], out[0][1]) < 2e-6
