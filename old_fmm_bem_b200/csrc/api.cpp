@@ -309,8 +309,6 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       }
       pl->Mtf.alloc((size_t)pl->tot_j * 256);
       pl->Ltf.alloc((size_t)pl->tot_i * 256);
-      make_split_tmap(pl->tmap_M, pl->Mtf.get(), pl->tot_j);
-      make_split_tmap(pl->tmap_L, pl->Ltf.get(), pl->tot_i);
       int dev_sms = 148;
       cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
       const int TT = tc_tile();
@@ -320,7 +318,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         struct Tile {
           std::vector<int> boxes;
           std::vector<int> ops;                 // per active slot
-          std::vector<std::array<int, 64>> src;  // per active slot
+          std::vector<std::vector<int>> src;     // per active slot, TT rows
         };
         std::vector<Tile> tiles;
         for (const auto& g : groups)
@@ -328,7 +326,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             Tile t;
             for (int i = 0; i < TT; i++) t.boxes.push_back(k + i < g.size() ? g[k + i] : -1);
             for (int sl = 0; sl < nslots; sl++) {
-              std::array<int, 64> rows;
+              std::vector<int> rows(TT);
               int op = -1;
               bool any = false;
               for (int i = 0; i < TT; i++) {
@@ -396,7 +394,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
           const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
           op = set * 316 + pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
           row = pl->off_j[lev] + src;
-        }, pl->tot_j);
+        }, -1);
       }
       pl->tc_m2m.clear();
       pl->tc_l2l.clear();
@@ -413,7 +411,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             if (c < 0) return;
             op = sl;
             row = pl->off_j[lev + 1] + c;
-          }, pl->tot_j);
+          }, -1);
         }
         if (lev >= 3) {  // L2L into children at lev, grouped by octant
           std::vector<std::vector<int>> groups(8);
@@ -421,7 +419,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
           build_job(*pl->tc_l2l[lev], groups, 1, [&](int box, int, int& op, int& row) {
             op = keys[box] & 7;
             row = pl->off_i[lev - 1] + par_i[box];
-          }, pl->tot_i);
+          }, -1);
         }
       }
     }
@@ -521,7 +519,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   if (lmax > 2)
     FMMB_CUDA(cudaMemsetAsync(pl->M.get() + (size_t)pl->off_j[lmax - 1] * K, 0,
                               (size_t)(pl->tot_j - pl->off_j[lmax - 1]) * K * sizeof(double), m));
-  auto tc_run = [&](const fmmb_plan::TcJob& job, const float* img, const void* tmap, double* out, int phase) {
+  auto tc_run = [&](const fmmb_plan::TcJob& job, const float* img, const float* xin, double* out, int phase) {
     PhaseTimer tm(pl, phase, m);
     TcJobArgs a{};
     a.nwork = job.nwork;
@@ -532,7 +530,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     a.slot_op = job.slot_op.get();
     a.slot_src = job.slot_src.get();
     a.opimg = img;
-    a.tmap = tmap;
+    a.xin = xin;
     a.out = out;
     a.err = pl->d_err.get();
     launch_translate_tc(a, m);
@@ -544,7 +542,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   if (pl->use_tc) {
     split(pl->M.get(), pl->Mtf.get(), pl->off_j[lmax], pl->nbox_j[lmax], 2);
     for (int lev = lmax - 1; lev >= 2; lev--) {
-      tc_run(*pl->tc_m2m[lev], pl->d_img_m2m.get(), pl->tmap_M, pl->M.get(), 2);
+      tc_run(*pl->tc_m2m[lev], pl->d_img_m2m.get(), pl->Mtf.get(), pl->M.get(), 2);
       split(pl->M.get(), pl->Mtf.get(), pl->off_j[lev], pl->nbox_j[lev], 2);
     }
   } else {
@@ -560,10 +558,10 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   // adds its parent's translated local (L2L), top down
   FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * K * sizeof(double), m));
   if (pl->use_tc) {
-    tc_run(pl->tc_m2l, pl->d_img_m2l.get(), pl->tmap_M, pl->L.get(), 3);
+    tc_run(pl->tc_m2l, pl->d_img_m2l.get(), pl->Mtf.get(), pl->L.get(), 3);
     for (int lev = 3; lev <= lmax; lev++) {
       split(pl->L.get(), pl->Ltf.get(), pl->off_i[lev - 1], pl->nbox_i[lev - 1], 4);
-      tc_run(*pl->tc_l2l[lev], pl->d_img_l2l.get(), pl->tmap_L, pl->L.get(), 4);
+      tc_run(*pl->tc_l2l[lev], pl->d_img_l2l.get(), pl->Ltf.get(), pl->L.get(), 4);
     }
   } else {
     const size_t opsz = (size_t)316 * K * K;

@@ -154,7 +154,6 @@ struct fmmb_plan {
   fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
   fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
   fmmb::DevBuf<float> Mtf, Ltf;              // [tot][2][128] TF32 hi/lo splits (mixed)
-  alignas(128) unsigned char tmap_M[128] = {}, tmap_L[128] = {};  // CUtensorMap over Mtf / Ltf
   fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
   int* h_err = nullptr;                      // pinned copy, checked by the next call
   bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)

@@ -55,13 +55,11 @@ namespace fmmb {
 // tensor-core translations (translate_tc.cu)
 int tc_tile();
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
-// tmap_out: 128-byte aligned storage for a CUtensorMap
-void make_split_tmap(void* tmap_out, const float* base, int rows);
 struct TcJobArgs {
   int nwork, K, atomic;
   const int *out_boxes, *slot_off, *slot_op, *slot_src;
   const float* opimg;
-  const void* tmap;  // CUtensorMap over the split inputs
+  const float* xin;  // TF32 split of the inputs [rows][2][128]
   double* out;
   int* err;
 };

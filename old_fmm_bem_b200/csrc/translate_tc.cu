@@ -15,14 +15,15 @@
 // precomputed with the tree.  Each product is split into three TF32 MMAs,
 // A_hi.B_hi + A_hi.B_lo + A_lo.B_hi, where hi/lo are the TF32 rounding of a
 // value and of its remainder (about 2^-21 relative error per product instead
-// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 64 boxes,
-// 48 MMAs) is accumulated in FP32 in tensor memory; two such accumulators
-// alternate, and while the tensor core fills one the epilogue warps drain the
-// other into FP64 registers, so the FP32 accumulation depth is one slot.
+// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 128
+// boxes, 48 MMAs) is accumulated in FP32 in tensor memory; two such
+// accumulators alternate, and while the tensor core fills one the epilogue
+// warps add the other into a running sum kept in tensor memory as an
+// unevaluated pair of FP32 numbers (hi + lo, updated by an error-free
+// two-sum), so the FP32 accumulation depth is one slot and the sum over
+// slots is exact to ~2^-44.
 //
-#include <cuda.h>
 #include <cuda_runtime.h>
-#include <cudaTypedefs.h>
 
 #include <cstdint>
 
@@ -32,17 +33,20 @@
 namespace fmmb {
 namespace tc {
 
-constexpr int kTile = 64;         // target boxes per tile (MMA N)
+constexpr int kTile = 128;        // output boxes per tile (MMA N)
 constexpr int kRows = 128;        // output coefficients (MMA M), K <= 128
 constexpr int kKB = 32;           // TF32 values per K-block (128 bytes)
 constexpr int kNKB = 4;           // K-blocks (K padded to 128)
-constexpr int kStages = 4;
+constexpr int kStages = 3;
 constexpr int kOpBytes = kRows * 128;               // operator K-block image (16 KB)
-constexpr int kBBytes = kTile * 128;                // gathered multipole K-block (8 KB)
+constexpr int kBBytes = kTile * 128;                // gathered input K-block (16 KB)
 constexpr int kStageBytes = 2 * kOpBytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-constexpr int kThreads = 192;
-constexpr int kTmemCols = 2 * kTile;                // two alternating accumulators
+constexpr int kThreads = 288;
+// tensor memory: two alternating FP32 slot accumulators, then the running
+// sum as an unevaluated FP32 pair (hi, lo)
+constexpr int kColP0 = 0, kColP1 = kTile, kColHi = 2 * kTile, kColLo = 3 * kTile;
+constexpr int kTmemCols = 4 * kTile;
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
 
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major,
@@ -129,6 +133,37 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// 32 consecutive accumulator columns of this thread's TMEM lane, raw (no wait).
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]),
+      "r"(r[19]), "r"(r[20]), "r"(r[21]), "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]),
+      "r"(r[28]), "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // Swizzled byte offset of 16-byte chunk c of row r in a K-block tile.
 __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
@@ -137,29 +172,21 @@ struct Params {
   const int* out_boxes;   // [nwork][64] output box (row of `out`) or -1
   const int* slot_off;    // [nwork + 1] CSR of each work item's slots
   const int* slot_op;     // operator image of each slot
-  const int* slot_src;    // [slots][64] input row of each output box (out of range = none)
+  const int* slot_src;    // [slots][128] input row of each output box (-1 = none)
   const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
+  const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
   double* out;            // FP64 expansions, [rows][K]
   int atomic;             // 1 when an output box appears in several work items
   int* err;               // set to a nonzero code on timeout
 };
 
-__device__ __forceinline__ void gather4(void* dst, const CUtensorMap* map, int x, int4 rows, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes "
-      "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(rows.x), "r"(rows.y), "r"(rows.z), "r"(rows.w),
-      "r"(smem_u32(bar))
-      : "memory");
-}
-
-__global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constant__ CUtensorMap src_map, Params P) {
+__global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accf = empty + kStages;  // [2] accumulator b complete
-  uint64_t* acce = accf + 2;         // [2] accumulator b drained
+  uint64_t* accf = empty + kStages;  // [2] slot accumulator b complete
+  uint64_t* acce = accf + 2;         // [2] slot accumulator b folded into the sum
   uint32_t* tmem_slot = (uint32_t*)(acce + 2);
   __shared__ int sh_boxes[kTile];
   __shared__ int sh_fail;
@@ -174,12 +201,12 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constan
   if (threadIdx.x == 0) {
     sh_fail = 0;
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 1);    // the producer's expect_tx arrival (+ TMA bytes)
+      mbar_init(&full[s], 129);  // 128 producer arrivals + the expect_tx arrival (+ bulk bytes)
       mbar_init(&empty[s], 1);   // one tcgen05.commit
     }
     for (int b = 0; b < 2; b++) {
       mbar_init(&accf[b], 1);    // tcgen05.commit after a slot's MMAs
-      mbar_init(&acce[b], 128);  // every epilogue thread after its tcgen05.ld
+      mbar_init(&acce[b], 128);  // every epilogue thread after folding the slot
     }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -193,40 +220,66 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constan
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 5) {
-    // ------------------------------------------------ producer warp
-    const int part = lane >> 4, g = lane & 15;  // lane: rows 4g..4g+3 of B_hi (part 0) / B_lo (part 1)
-    for (int st = 0; st < nstage_total; st++) {
+  if (warp >= 5) {
+    // ------------------------------------------------ producers (128 threads)
+    // thread pt gathers row pt (hi and lo parts) with cp.async, keeping two
+    // stages in flight: the arrival for stage st-1 follows the wait for it.
+    const int pt = threadIdx.x - 160;
+    int st = 0;
+    for (; st < nstage_total; st++) {
       const int s = st % kStages;
       const uint32_t ph = (st / kStages) & 1;
       bool ok = true;
       if (st >= kStages && lane == 0) ok = mbar_wait(&empty[s], ph ^ 1);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-      if (!ok) {
-        if (lane == 0) atomicExch(&sh_fail, 1);
-        break;
-      }
-      if (*(volatile int*)&sh_fail) break;
+      if (!ok) atomicExch(&sh_fail, 1);
+      if (!ok || *(volatile int*)&sh_fail) break;
       const int sl = s_begin + st / kNKB;
       const int kb = st % kNKB;
       unsigned char* stage = smem + s * kStageBytes;
-      if (lane == 0) {
+      if (pt == 0) {
         const float* img = P.opimg + ((size_t)P.slot_op[sl] * kNKB + kb) * 2 * (kRows * kKB);
-        mbar_arrive_tx(&full[s], 2 * kOpBytes + 2 * kBBytes);
+        mbar_arrive_tx(&full[s], 2 * kOpBytes);
         bulk_g2s(stage, img, kOpBytes, &full[s]);
         bulk_g2s(stage + kOpBytes, img + kRows * kKB, kOpBytes, &full[s]);
       }
-      __syncwarp();
-      const int4 rows = *reinterpret_cast<const int4*>(P.slot_src + (size_t)sl * kTile + 4 * g);
-      gather4(stage + 2 * kOpBytes + part * kBBytes + 4 * g * 128, &src_map, part * 128 + kb * kKB, rows, &full[s]);
+      const int src = P.slot_src[(size_t)sl * kTile + pt];
+      unsigned char* bhi = stage + 2 * kOpBytes;
+      unsigned char* blo = bhi + kBBytes;
+      if (src >= 0) {
+        const float* g = P.xin + (size_t)src * 256 + kb * kKB;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          cp_async16(bhi + swz(pt, c), g + 4 * c);
+          cp_async16(blo + swz(pt, c), g + 128 + 4 * c);
+        }
+      } else {
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          *reinterpret_cast<float4*>(bhi + swz(pt, c)) = z;
+          *reinterpret_cast<float4*>(blo + swz(pt, c)) = z;
+        }
+      }
+      cp_async_commit();
+      if (st > 0) {
+        cp_async_wait<1>();  // stage st-1 landed
+        fence_async_smem();
+        mbar_arrive(&full[(st - 1) % kStages]);
+      }
+    }
+    cp_async_wait<0>();
+    if (st > 0) {
+      fence_async_smem();
+      mbar_arrive(&full[(st - 1) % kStages]);
     }
   } else if (warp == 4) {
     // ------------------------------------------------ MMA issuer
     bool ok = true;
     for (int g = 0; g < nslot && ok; g++) {
       const int buf = g & 1;
-      const uint32_t dcol = tmem + (uint32_t)(buf * kTile);
-      if (g >= 2) {  // wait until the epilogue has drained this accumulator
+      const uint32_t dcol = tmem + (uint32_t)(buf ? kColP1 : kColP0);
+      if (g >= 2) {  // wait until the epilogue has folded this accumulator
         if (lane == 0) ok = mbar_wait(&acce[buf], ((g >> 1) - 1) & 1);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         if (!ok) break;
@@ -259,10 +312,10 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constan
     if (!ok && lane == 0) atomicExch(&sh_fail, 2);
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
+    // folds each slot's FP32 accumulator into the (hi, lo) running sum with
+    // an error-free two-sum, then writes hi + lo in FP64 at the end.
     const int row = warp * 32 + lane;  // output coefficient of this thread
-    double acc[kTile];
-#pragma unroll
-    for (int j = 0; j < kTile; j++) acc[j] = 0.0;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     bool ok = true;
     for (int g = 0; g < nslot; g++) {
       const int buf = g & 1;
@@ -270,25 +323,59 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(const __grid_constan
       ok = __all_sync(0xffffffffu, w && *(volatile int*)&sh_fail == 0) != 0;
       if (!ok) break;
       tc_fence_after();
-      float v[32];
-#pragma unroll
+#pragma unroll 1
       for (int h = 0; h < kTile / 32; h++) {
-        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(buf * kTile + h * 32), v);
+        uint32_t pv[32], hv[32], lv[32];
+        tmem_ld32_nowait(lane_base + (uint32_t)((buf ? kColP1 : kColP0) + h * 32), pv);
+        if (g > 0) {
+          tmem_ld32_nowait(lane_base + (uint32_t)(kColHi + h * 32), hv);
+          tmem_ld32_nowait(lane_base + (uint32_t)(kColLo + h * 32), lv);
+        }
+        tmem_wait_ld();
+        if (g == 0) {
 #pragma unroll
-        for (int j = 0; j < 32; j++) acc[h * 32 + j] += (double)v[j];
+          for (int j = 0; j < 32; j++) {
+            hv[j] = pv[j];
+            lv[j] = 0u;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const float a = __uint_as_float(hv[j]), b = __uint_as_float(pv[j]);
+            const float s = __fadd_rn(a, b);
+            const float bb = __fsub_rn(s, a);
+            const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+            hv[j] = __float_as_uint(s);
+            lv[j] = __float_as_uint(__fadd_rn(__uint_as_float(lv[j]), e));
+          }
+        }
+        tmem_st32(lane_base + (uint32_t)(kColHi + h * 32), hv);
+        tmem_st32(lane_base + (uint32_t)(kColLo + h * 32), lv);
       }
+      tmem_wait_st();
       tc_fence_before();
       mbar_arrive(&acce[buf]);
     }
     if (!ok) atomicExch(&sh_fail, 3);
-    if (ok && row < P.K) {
+    if (ok && nslot > 0) {
+      tc_fence_after();
+#pragma unroll 1
+      for (int h = 0; h < kTile / 32; h++) {
+        uint32_t hv[32], lv[32];
+        tmem_ld32_nowait(lane_base + (uint32_t)(kColHi + h * 32), hv);
+        tmem_ld32_nowait(lane_base + (uint32_t)(kColLo + h * 32), lv);
+        tmem_wait_ld();
+        if (row < P.K) {
 #pragma unroll
-      for (int j = 0; j < kTile; j++) {
-        const int box = sh_boxes[j];
-        if (box >= 0) {
-          double* dst = P.out + (size_t)box * P.K + row;
-          if (P.atomic) atomicAdd(dst, acc[j]);
-          else *dst += acc[j];
+          for (int j = 0; j < 32; j++) {
+            const int box = sh_boxes[h * 32 + j];
+            if (box >= 0) {
+              const double v = (double)__uint_as_float(hv[j]) + (double)__uint_as_float(lv[j]);
+              double* dst = P.out + (size_t)box * P.K + row;
+              if (P.atomic) atomicAdd(dst, v);
+              else *dst += v;
+            }
+          }
         }
       }
     }
@@ -336,34 +423,6 @@ void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_
   FMMB_CHECK_LAUNCH();
 }
 
-namespace {
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    FMMB_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    FMMB_REQUIRE(p && q == cudaDriverEntryPointSuccess, FMMB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
-  return fn;
-}
-}  // namespace
-
-// Tensor map over split expansions [rows][256] FP32 (hi 0..127, lo 128..255):
-// boxes of 32 values x 1 row, 128-byte swizzle, zero fill out of range.
-void make_split_tmap(void* tmap_out, const float* base, int rows) {
-  CUtensorMap* m = reinterpret_cast<CUtensorMap*>(tmap_out);
-  const cuuint64_t dims[2] = {256, (cuuint64_t)(rows > 0 ? rows : 1)};
-  const cuuint64_t strides[1] = {256 * sizeof(float)};
-  const cuuint32_t box[2] = {32, 1};
-  const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
-                                 estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                                 CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  FMMB_REQUIRE(r == CUDA_SUCCESS, FMMB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-}
-
 void launch_translate_tc(const TcJobArgs& a, cudaStream_t st) {
   if (a.nwork <= 0) return;
   FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
@@ -374,11 +433,11 @@ void launch_translate_tc(const TcJobArgs& a, cudaStream_t st) {
   P.slot_op = a.slot_op;
   P.slot_src = a.slot_src;
   P.opimg = a.opimg;
+  P.xin = a.xin;
   P.out = a.out;
   P.atomic = a.atomic;
   P.err = a.err;
-  const CUtensorMap* m = reinterpret_cast<const CUtensorMap*>(a.tmap);
-  tc::translate_tc<<<a.nwork, tc::kThreads, tc::kSmemBytes, st>>>(*m, P);
+  tc::translate_tc<<<a.nwork, tc::kThreads, tc::kSmemBytes, st>>>(P);
   FMMB_CHECK_LAUNCH();
 }
 
