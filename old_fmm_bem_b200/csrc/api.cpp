@@ -510,7 +510,9 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     if (pl->ref)  // the reference's spherical formulation, quirks included
       launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(),
                  qs, pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
-    else
+    else if (!(pl->cfg.precision == FMMB_MIXED &&
+               launch_p2m_f32(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
+                              pl->snrm.get(), qs, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m)))
       launch_p2m_cart(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
                       pl->snrm.get(), qs, pl->d_fac.get(), pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
   }

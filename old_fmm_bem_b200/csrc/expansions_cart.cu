@@ -21,6 +21,8 @@
 // single-precision angles.
 #include <cuda_runtime.h>
 
+#include <cmath>
+
 #include "internal.h"
 #include "kernels.h"
 
@@ -161,6 +163,146 @@ __global__ void __launch_bounds__(128) p2m_cart(int p, int K, const int* __restr
   }
 }
 
+// ------------------------------------------------------------------ P2M (FP32)
+// Mixed-precision P2M: one thread per source point evaluates every S_n^m of
+// its point in FP32 with the degree rows held in registers (order P fixed at
+// compile time, runtime order p <= P), writes its contributions to shared
+// memory, and the block reduces the columns in FP64.  The multipole of a leaf
+// carries FP32 rounding of each point's terms (relative 1e-7) -- below the
+// TF32x3 error of the translations that consume it.
+__constant__ float c_fac32[21 * 21 + 21];  // fac(n, m) at n*n+n+m, n <= 20
+
+constexpr int kP2MThreads = 64;
+
+template <int KER, int P>
+__global__ void __launch_bounds__(kP2MThreads) p2m_f32(int p, int K, const int* __restrict__ keys,
+                                                       const int2* __restrict__ leaf, const float4* __restrict__ spos,
+                                                       const float4* __restrict__ snrm, const float* __restrict__ qs,
+                                                       float xmin, float ymin, float zmin, double rb,
+                                                       double* __restrict__ M) {
+  extern __shared__ float contrib[];  // [kP2MThreads][K]
+  const int b = blockIdx.x;
+  double xc, yc, zc;
+  box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
+  const int2 lf = leaf[b];
+  const double inv_rb = 1.0 / rb;
+  double acc0 = 0.0, acc1 = 0.0;  // columns threadIdx.x and threadIdx.x + 64 (K <= 128 per pass)
+  double acc[(P + 1) * (P + 1) / kP2MThreads + 1];
+#pragma unroll
+  for (int i = 0; i < (P + 1) * (P + 1) / kP2MThreads + 1; i++) acc[i] = 0.0;
+  (void)acc0;
+  (void)acc1;
+  float* my = contrib + threadIdx.x * K;
+  for (int j0 = 0; j0 < lf.y; j0 += kP2MThreads) {
+    const int jj = j0 + threadIdx.x;
+    const bool act = jj < lf.y;
+    const int j = lf.x + (act ? jj : 0);
+    const float4 xs = spos[j];
+    const float q = act ? qs[j] : 0.f;
+    const float x = (float)(((double)xs.x - xc) * inv_rb), y = (float)(((double)xs.y - yc) * inv_rb),
+                z = (float)(((double)xs.z - zc) * inv_rb);
+    const float r2 = x * x + y * y + z * z;
+    float qnx = 0.f, qny = 0.f, qnz = 0.f;
+    if (KER == FMMB_LAPLACE_GNJ) {
+      const float4 nv = snrm[j];
+      const float s = q * (float)inv_rb;
+      qnx = s * nv.x;
+      qny = s * nv.y;
+      qnz = s * nv.z;
+    }
+    float r1re[P + 1], r1im[P + 1], r2re[P + 1], r2im[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) r1re[m] = r1im[m] = r2re[m] = r2im[m] = 0.f;
+#pragma unroll
+    for (int n = 0; n <= P; n++) {
+      float cre[P + 1], cim[P + 1];
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        cre[m] = cim[m] = 0.f;
+        if (m > n) continue;
+        if (n == 0) {
+          cre[0] = 1.f;
+        } else if (m == n) {  // S_n^n = -(2n-1) (x + i y) S_{n-1}^{n-1}
+          const float a = -(2.f * n - 1.f);
+          cre[m] = a * (x * r1re[n - 1] - y * r1im[n - 1]);
+          cim[m] = a * (x * r1im[n - 1] + y * r1re[n - 1]);
+        } else if (m == n - 1) {
+          const float a = (2.f * n - 1.f) * z;
+          cre[m] = a * r1re[m];
+          cim[m] = a * r1im[m];
+        } else {
+          const float inv = 1.f / (float)(n - m);
+          const float a = (2.f * n - 1.f) * z * inv, c = (float)(n + m - 1) * r2 * inv;
+          cre[m] = a * r1re[m] - c * r2re[m];
+          cim[m] = a * r1im[m] - c * r2im[m];
+        }
+        if (n > p) continue;
+        float vre, vim;
+        if (KER != FMMB_LAPLACE_GNJ) {
+          const float f = q * c_fac32[n * n + n + m];
+          vre = f * cre[m];
+          vim = -f * cim[m];
+        } else {
+          if (n == 0) {
+            vre = vim = 0.f;
+          } else {
+            // n . grad S_n^m from degree n-1
+            const float upr = (m + 1 <= n - 1) ? r1re[m + 1 <= P ? m + 1 : P] : 0.f;
+            const float upi = (m + 1 <= n - 1) ? r1im[m + 1 <= P ? m + 1 : P] : 0.f;
+            float dnr, dni, cm;
+            if (m == 0) {  // conj(S_{n-1}^1)
+              dnr = (n - 1 >= 1) ? r1re[1 <= P ? 1 : P] : 0.f;
+              dni = (n - 1 >= 1) ? -r1im[1 <= P ? 1 : P] : 0.f;
+              cm = 1.f;
+            } else {
+              dnr = r1re[m - 1 >= 0 ? m - 1 : 0];
+              dni = r1im[m - 1 >= 0 ? m - 1 : 0];
+              cm = -(float)(n + m) * (float)(n + m - 1);
+            }
+            const float s1r = (m <= n - 1) ? r1re[m] : 0.f, s1i = (m <= n - 1) ? r1im[m] : 0.f;
+            // D = 1/2 (nx - i ny) up + 1/2 cm (nx + i ny) dn + nz (n+m) s1
+            const float Dre = 0.5f * (qnx * upr + qny * upi) + 0.5f * cm * (qnx * dnr - qny * dni) + qnz * (n + m) * s1r;
+            const float Dim = 0.5f * (qnx * upi - qny * upr) + 0.5f * cm * (qnx * dni + qny * dnr) + qnz * (n + m) * s1i;
+            const float f = c_fac32[n * n + n + m];
+            vre = f * Dre;
+            vim = -f * Dim;
+          }
+        }
+        if (m == 0) my[n * n] = vre;
+        else {
+          my[n * n + 2 * m - 1] = vre;
+          my[n * n + 2 * m] = vim;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        r2re[m] = r1re[m];
+        r2im[m] = r1im[m];
+        r1re[m] = cre[m];
+        r1im[m] = cim[m];
+      }
+    }
+    __syncthreads();
+    // column sums over the chunk's points (inactive points contributed zeros)
+#pragma unroll
+    for (int i = 0; i < (P + 1) * (P + 1) / kP2MThreads + 1; i++) {
+      const int k = threadIdx.x + i * kP2MThreads;
+      if (k < K) {
+        float t = 0.f;
+        const int npt = min(kP2MThreads, lf.y - j0);
+        for (int pt = 0; pt < npt; pt++) t += contrib[pt * K + k];
+        acc[i] += (double)t;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < (P + 1) * (P + 1) / kP2MThreads + 1; i++) {
+    const int k = threadIdx.x + i * kP2MThreads;
+    if (k < K) M[(size_t)b * K + k] = acc[i];
+  }
+}
+
 // ------------------------------------------------------------------ L2P
 // One block (64 threads) per target leaf.  The leaf's local expansion is
 // turned once into the coefficients of the potential and of the three
@@ -282,6 +424,45 @@ void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const
       p2m_cart<FMMB_LAPLACE_G, 32><<<nleaf, 128, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, fac, bbox[0], bbox[1], bbox[2], rb, M);
   }
   FMMB_CHECK_LAUNCH();
+}
+
+namespace {
+template <int P>
+void p2m_f32_launch(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
+                    const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
+  const size_t sm = (size_t)kP2MThreads * K * sizeof(float);
+  if (kernel == FMMB_LAPLACE_GNJ)
+    p2m_f32<FMMB_LAPLACE_GNJ, P><<<nleaf, kP2MThreads, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
+  else
+    p2m_f32<FMMB_LAPLACE_G, P><<<nleaf, kP2MThreads, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
+}
+}  // namespace
+
+void init_fac32() {
+  static bool done = false;
+  if (done) return;
+  float h[21 * 21 + 21] = {};
+  for (int n = 0; n <= 20; n++)
+    for (int m = 0; m <= n; m++) {
+      double f = 1.0;  // sqrt((n-m)!/(n+m)!)
+      for (int k = n - m + 1; k <= n + m; k++) f /= k;
+      h[n * n + n + m] = (float)std::sqrt(f);
+    }
+  FMMB_CUDA(cudaMemcpyToSymbol(c_fac32, h, sizeof(h)));
+  done = true;
+}
+
+bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
+                    const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
+  if (nleaf <= 0) return true;
+  init_fac32();
+  if (p <= 8) p2m_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else if (p <= 10) p2m_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else if (p <= 12) p2m_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else if (p <= 16) p2m_f32_launch<16>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else return false;
+  FMMB_CHECK_LAUNCH();
+  return true;
 }
 
 void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
