@@ -78,7 +78,8 @@ FMMB_API int fmmb_config_init(fmmb_config* cfg);
 FMMB_API int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** plan);
 FMMB_API int fmmb_plan_destroy(fmmb_plan* plan);
 
-/* Work of this plan is queued on `stream` (a cudaStream_t; NULL = the plan's own). */
+/* Work of this plan is queued on `stream` (a cudaStream_t; NULL = the plan's own;
+ * cudaStreamLegacy for the legacy default stream). */
 FMMB_API int fmmb_set_stream(fmmb_plan* plan, void* stream);
 
 /* Builds the octree on the GPU (replaces fmm/boxn.cxx, sort/csort.cxx,

@@ -141,6 +141,20 @@ class Plan:
         """Queue the plan's work on a cudaStream_t (int handle or torch stream)."""
         h = getattr(stream, "cuda_stream", stream)
         _check(load().fmmb_set_stream(self._h, ctypes.c_void_p(h)))
+        self._stream = h
+
+    def _follow_torch(self, *arrays):
+        """With torch CUDA tensors among the arguments, queue the plan's work on
+        torch's current stream, so that it is ordered after the kernels that
+        produced the inputs and before those that read the outputs."""
+        if any(getattr(a, "is_cuda", False) for a in arrays):
+            import torch
+            # torch's default stream is the legacy default stream, handle 0,
+            # which fmmb_set_stream reads as "the plan's own": pass
+            # cudaStreamLegacy ((cudaStream_t)1) for it instead.
+            h = torch.cuda.current_stream().cuda_stream or 1
+            if h != getattr(self, "_stream", None):
+                self.set_stream(h)
 
     def set_geometry(self, targets, sources, target_normals=None, source_normals=None, bbox=None):
         """targets/sources: (3, n) float32 (numpy or torch); bbox = (xmin, ymin, zmin, rd)."""
@@ -150,6 +164,7 @@ class Plan:
         sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
         bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
         ni, nj = len(targets[0]), len(sources[0])
+        self._follow_torch(*targets, *sources)
         _check(load().fmmb_set_geometry(self._h, ni, t[0][0], t[1][0], t[2][0], tn[0][0], tn[1][0], tn[2][0], nj,
                                         s[0][0], s[1][0], s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0]))
         self.ni, self.nj = ni, nj
@@ -168,6 +183,7 @@ class Plan:
         pp, pk = _ptr(pot, dt)
         gp, gk = _ptr(grad, dt) if self.kernel == LAPLACE_G else (None, None)
         fn = load().fmmb_evaluate_f64 if f64 else load().fmmb_evaluate
+        self._follow_torch(q, pot, grad)
         _check(fn(self._h, qp, pp, gp))
         return pk, gk
 
@@ -177,6 +193,7 @@ class Plan:
         qp, qk = _ptr(q, np.float32)
         pot = np.zeros(i1 - i0)
         grad = np.zeros(3 * (i1 - i0))
+        self._follow_torch(q)
         _check(load().fmmb_direct_f64(self._h, qp, i0, i1, pot.ctypes.data,
                                       grad.ctypes.data if self.kernel == LAPLACE_G else None))
         return pot, (grad.reshape(3, -1) if self.kernel == LAPLACE_G else None)
