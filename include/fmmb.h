@@ -109,6 +109,27 @@ FMMB_API int fmmb_evaluate_f64(fmmb_plan* plan, const float* q, double* pot, dou
  * the geometry and the first right-hand side of q; targets [i0, i1). */
 FMMB_API int fmmb_direct_f64(fmmb_plan* plan, const float* q, int i0, int i1, double* pot, double* grad);
 
+/* Direct sum without a plan that allocates nothing (no cudaMalloc/cudaFree,
+ * no allocating library routine).  It has no counterpart in the reference:
+ * it serves callers that must not allocate, such as a stream about to be
+ * captured into a CUDA graph.  Same arithmetic as fmmb_direct_f64 (FP64, the
+ * kernel, semantics, eps2 and exclude_self of cfg; the other fields are
+ * ignored), float outputs pot[ni] and, for FMMB_LAPLACE_G, grad[3*ni] (may be
+ * NULL).  Every pointer must be device (or managed) memory; work is queued on
+ * `stream` (a cudaStream_t, NULL = the legacy default stream).
+ * The FP64 partial sums of its source split live in one static device array of
+ * FMMB_STATIC_SCRATCH_BYTES per device: ncomp * ni must not exceed
+ * FMMB_STATIC_SCRATCH_BYTES / 8 (ncomp = 4 for G with grad, else 1), larger
+ * sizes return FMMB_ERR_CAPACITY.  All calls on a device share that array:
+ * calls that overlap on the GPU race and must be ordered by the caller.  The
+ * first call on a device (that device current) looks the array up with
+ * cudaGetSymbolAddress; make it before any stream capture. */
+#define FMMB_STATIC_SCRATCH_BYTES (16u << 20)
+FMMB_API int fmmb_direct_static(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                                const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,
+                                const float* sy, const float* sz, const float* snx, const float* sny,
+                                const float* snz, const float* q, float* pot, float* grad, void* stream);
+
 /* ---- inspection (tests, tooling) ---- */
 
 /* Tree of the current geometry.  kind: 0 target permutation (sorted position

@@ -31,7 +31,7 @@ SEM_REFERENCE, SEM_ACCURATE = 0, 1
 EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_set_stream", "fmmb_set_geometry",
            "fmmb_evaluate", "fmmb_evaluate_f64", "fmmb_direct_f64", "fmmb_get_tree_size", "fmmb_get_tree",
            "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
-           "fmmb_last_error"]
+           "fmmb_last_error", "fmmb_direct_static"]
 
 
 def lib_path() -> str:
@@ -69,6 +69,8 @@ def load():
     lib.fmmb_evaluate.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_evaluate_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_direct_f64.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_direct_static.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
+        [_vp] * 6 + [_vp, _vp, _vp, _vp]
     lib.fmmb_get_tree_size.argtypes = [_vp, ctypes.c_int]
     lib.fmmb_get_tree_size.restype = ctypes.c_long
     lib.fmmb_get_tree.argtypes = [_vp, ctypes.c_int, _vp]
