@@ -312,89 +312,51 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       int dev_sms = 148;
       cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
       const int TT = tc_tile();
-      // groups of output boxes -> work items; slot(box, s) -> (operator, source row or -1)
-      auto build_job = [&](fmmb_plan::TcJob& job, const std::vector<std::vector<int>>& groups, int nslots,
-                           auto slot_fn, int oob_row) {
-        struct Tile {
-          std::vector<int> boxes;
-          std::vector<int> ops;                 // per active slot
-          std::vector<std::vector<int>> src;     // per active slot, TT rows
-        };
-        std::vector<Tile> tiles;
-        for (const auto& g : groups)
-          for (size_t k = 0; k < g.size(); k += TT) {
-            Tile t;
-            for (int i = 0; i < TT; i++) t.boxes.push_back(k + i < g.size() ? g[k + i] : -1);
-            for (int sl = 0; sl < nslots; sl++) {
-              std::vector<int> rows(TT);
-              int op = -1;
-              bool any = false;
-              for (int i = 0; i < TT; i++) {
-                rows[i] = oob_row;
-                if (t.boxes[i] < 0) continue;
-                int o = -1, r = -1;
-                slot_fn(t.boxes[i], sl, o, r);
-                if (r >= 0) {
-                  rows[i] = r;
-                  op = o;
-                  any = true;
-                }
-              }
-              if (any) {
-                t.ops.push_back(op);
-                t.src.push_back(rows);
-              }
+      pl->nsm = dev_sms;
+      auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+        d.alloc(h.size());
+        if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+      };
+      // box pairs {operator, input row, output row} -> tiles of TT pairs of one
+      // operator each (operators ascending, pairs in output order within one)
+      using Pair = std::array<int, 3>;
+      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs, int atomic) {
+        std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x[0] < y[0]; });
+        std::vector<int> top, tsrc, tdst;
+        for (size_t i = 0; i < pairs.size();) {
+          size_t j = i;
+          while (j < pairs.size() && pairs[j][0] == pairs[i][0]) j++;
+          for (size_t k = i; k < j; k += TT) {
+            top.push_back(pairs[i][0]);
+            for (int c = 0; c < TT; c++) {
+              tsrc.push_back(k + c < j ? pairs[k + c][1] : -1);
+              tdst.push_back(k + c < j ? pairs[k + c][2] : -1);
             }
-            if (!t.ops.empty()) tiles.push_back(std::move(t));
           }
-        const int ntile = (int)tiles.size();
-        const int nsplit = ntile > 0 ? std::max(1, std::min(8, (2 * dev_sms + ntile - 1) / ntile)) : 1;
-        std::vector<int> ob, off{0}, so, ss;
-        for (const auto& t : tiles) {
-          const int n = (int)t.ops.size();
-          for (int k = 0; k < nsplit; k++) {
-            const int a0 = (int)((long long)n * k / nsplit), a1 = (int)((long long)n * (k + 1) / nsplit);
-            if (a1 <= a0) continue;
-            ob.insert(ob.end(), t.boxes.begin(), t.boxes.end());
-            for (int i = a0; i < a1; i++) {
-              so.push_back(t.ops[i]);
-              ss.insert(ss.end(), t.src[i].begin(), t.src[i].end());
+          i = j;
+        }
+        job.ntile = (int)top.size();
+        job.atomic = atomic;
+        up(job.tile_op, top);
+        up(job.tile_src, tsrc);
+        up(job.tile_dst, tdst);
+      };
+      // M2L, all levels in one job: operator = set(level)*316 + relative position
+      {
+        std::vector<Pair> pairs;
+        for (int lev = 2; lev <= pl->lmax; lev++) {
+          const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
+          for (int b = 0; b < pl->nbox_i[lev]; b++) {
+            const int box = pl->off_i[lev] + b;
+            for (int sl = 0; sl < kM2LSlots; sl++) {
+              const int src = lst[(size_t)box * kM2LSlots + sl];
+              if (src < 0) continue;
+              const int op = set * 316 + pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
+              pairs.push_back({op, pl->off_j[lev] + src, box});
             }
-            off.push_back((int)so.size());
           }
         }
-        job.nwork = (int)off.size() - 1;
-        job.atomic = nsplit > 1 ? 1 : 0;
-        auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
-          d.alloc(h.size());
-          if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
-        };
-        up(job.out_boxes, ob);
-        up(job.slot_off, off);
-        up(job.slot_op, so);
-        up(job.slot_src, ss);
-      };
-      // M2L: target boxes by (level, octant); operator = set(level)*316 + position
-      {
-        std::vector<std::vector<int>> groups;
-        for (int lev = 2; lev <= pl->lmax; lev++)
-          for (int oct = 0; oct < 8; oct++) {
-            std::vector<int> bx;
-            for (int b = 0; b < pl->nbox_i[lev]; b++)
-              if ((keys[pl->off_i[lev] + b] & 7) == oct) bx.push_back(pl->off_i[lev] + b);
-            groups.push_back(bx);
-          }
-        std::vector<int> lev_of(pl->tot_i);
-        for (int lev = 2; lev <= pl->lmax; lev++)
-          for (int b = 0; b < pl->nbox_i[lev]; b++) lev_of[pl->off_i[lev] + b] = lev;
-        build_job(pl->tc_m2l, groups, kM2LSlots, [&](int box, int sl, int& op, int& row) {
-          const int src = lst[(size_t)box * kM2LSlots + sl];
-          if (src < 0) return;
-          const int lev = lev_of[box];
-          const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
-          op = set * 316 + pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
-          row = pl->off_j[lev] + src;
-        }, -1);
+        build_job(pl->tc_m2l, pairs, 1);
       }
       pl->tc_m2m.clear();
       pl->tc_l2l.clear();
@@ -403,23 +365,24 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       for (int lev = 0; lev <= pl->lmax; lev++) {
         pl->tc_m2m.emplace_back(new fmmb_plan::TcJob());
         pl->tc_l2l.emplace_back(new fmmb_plan::TcJob());
-        if (lev >= 2 && lev < pl->lmax) {  // M2M into parents at lev
-          std::vector<std::vector<int>> groups(1);
-          for (int b = 0; b < pl->nbox_j[lev]; b++) groups[0].push_back(pl->off_j[lev] + b);
-          build_job(*pl->tc_m2m[lev], groups, 8, [&](int box, int sl, int& op, int& row) {
-            const int c = m2m_list[(size_t)box * 8 + sl];
-            if (c < 0) return;
-            op = sl;
-            row = pl->off_j[lev + 1] + c;
-          }, -1);
+        if (lev >= 2 && lev < pl->lmax) {  // M2M into parents at lev: operator = child octant
+          std::vector<Pair> pairs;
+          for (int b = 0; b < pl->nbox_j[lev]; b++) {
+            const int box = pl->off_j[lev] + b;
+            for (int sl = 0; sl < 8; sl++) {
+              const int c = m2m_list[(size_t)box * 8 + sl];
+              if (c >= 0) pairs.push_back({sl, pl->off_j[lev + 1] + c, box});
+            }
+          }
+          build_job(*pl->tc_m2m[lev], pairs, 1);
         }
-        if (lev >= 3) {  // L2L into children at lev, grouped by octant
-          std::vector<std::vector<int>> groups(8);
-          for (int b = 0; b < pl->nbox_i[lev]; b++) groups[keys[pl->off_i[lev] + b] & 7].push_back(pl->off_i[lev] + b);
-          build_job(*pl->tc_l2l[lev], groups, 1, [&](int box, int, int& op, int& row) {
-            op = keys[box] & 7;
-            row = pl->off_i[lev - 1] + par_i[box];
-          }, -1);
+        if (lev >= 3) {  // L2L into children at lev (one pair per child): operator = child octant
+          std::vector<Pair> pairs;
+          for (int b = 0; b < pl->nbox_i[lev]; b++) {
+            const int box = pl->off_i[lev] + b;
+            pairs.push_back({keys[box] & 7, pl->off_i[lev - 1] + par_i[box], box});
+          }
+          build_job(*pl->tc_l2l[lev], pairs, 0);
         }
       }
     }
@@ -524,18 +487,17 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   auto tc_run = [&](const fmmb_plan::TcJob& job, const float* img, const float* xin, double* out, int phase) {
     PhaseTimer tm(pl, phase, m);
     TcJobArgs a{};
-    a.nwork = job.nwork;
+    a.ntile = job.ntile;
     a.K = K;
     a.atomic = job.atomic;
-    a.out_boxes = job.out_boxes.get();
-    a.slot_off = job.slot_off.get();
-    a.slot_op = job.slot_op.get();
-    a.slot_src = job.slot_src.get();
+    a.tile_op = job.tile_op.get();
+    a.tile_src = job.tile_src.get();
+    a.tile_dst = job.tile_dst.get();
     a.opimg = img;
     a.xin = xin;
     a.out = out;
     a.err = pl->d_err.get();
-    launch_translate_tc(a, m);
+    launch_translate_tc(a, pl->nsm, m);
   };
   auto split = [&](const double* X, float* Xtf, int off, int n, int phase) {
     PhaseTimer tm(pl, phase, m);

@@ -160,11 +160,12 @@ struct fmmb_plan {
   int opimg_sets = 0;
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots
-  struct TcJob {
-    int nwork = 0, atomic = 0;
-    fmmb::DevBuf<int> out_boxes, slot_off, slot_op, slot_src;
+  struct TcJob {  // pair tiles of one tensor-core translation launch (translate_tc.cu)
+    int ntile = 0, atomic = 0;
+    fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
   };
   TcJob tc_m2l;                                              // all levels
+  int nsm = 148;                                             // SMs of the plan's device
   std::vector<std::unique_ptr<TcJob>> tc_m2m, tc_l2l;        // per level
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging

@@ -60,12 +60,12 @@ namespace fmmb {
 int tc_tile();
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
 struct TcJobArgs {
-  int nwork, K, atomic;
-  const int *out_boxes, *slot_off, *slot_op, *slot_src;
+  int ntile, K, atomic;
+  const int *tile_op, *tile_src, *tile_dst;  // [ntile], [ntile][128], [ntile][128]
   const float* opimg;
   const float* xin;  // TF32 split of the inputs [rows][2][128]
   double* out;
   int* err;
 };
-void launch_translate_tc(const TcJobArgs& a, cudaStream_t st);
+void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st);
 }  // namespace fmmb

@@ -4,25 +4,27 @@
 // Every translation is a dense real K x K operator (operators.cpp: the
 // reference's rotate / z-translate / rotate-back steps of kernel/m2l.cxx:30-83,
 // kernel/m2m.cxx:28-62 and kernel/l2l.cxx:44-78 composed into one matrix per
-// relative position).  A work item is a tile of 64 output boxes and a list of
-// slots; slot s contributes T_s (128 x 128) . X[src(s, box)] for the 64
-// boxes, X being the TF32 (hi, lo) split of the input expansions:
-//   M2L: output target boxes of one octant at one level, slots = interaction
-//        positions, input = multipoles of the same level;
-//   M2M: output parents, slots = the 8 child octants, input = children;
-//   L2L: output children of one octant, one slot, input = parents.
-// The operator index and the 64 source rows of every (work item, slot) are
-// precomputed with the tree.  Each product is split into three TF32 MMAs,
-// A_hi.B_hi + A_hi.B_lo + A_lo.B_hi, where hi/lo are the TF32 rounding of a
-// value and of its remainder (about 2^-21 relative error per product instead
-// of 2^-11 for plain TF32).  One slot's product (128 coefficients x 128
-// boxes, 48 MMAs) is accumulated in FP32 in tensor memory; two such
-// accumulators alternate, and while the tensor core fills one the epilogue
-// warps add the other into a running sum kept in tensor memory as an
-// unevaluated pair of FP32 numbers (hi + lo, updated by an error-free
-// two-sum), so the FP32 accumulation depth is one slot and the sum over
-// slots is exact to ~2^-44.
+// relative position).  The work is a list of box pairs (output row, input
+// row, operator), grouped by operator and cut into tiles of 128 pairs: one
+// tile is one GEMM  D (128 coefficients x 128 pairs) = T_op . X[inputs],
+// X being the TF32 (hi, lo) split of the input expansions, and its columns
+// are added into the FP64 output rows in the epilogue (atomically when an
+// output row receives several pairs: M2L, M2M; plainly for L2L).  Grouping by
+// operator keeps the tiles full whatever the geometry (on a surface most of
+// the 189 interaction positions of a box are empty, so tiles of output boxes
+// would be mostly zero columns).  Each product is split into three TF32 MMAs,
+// A_hi.B_hi + A_hi.B_lo + A_lo.B_hi (about 2^-21 relative error per product
+// instead of 2^-11 for plain TF32), accumulated in FP32 in tensor memory over
+// the K coefficients of one pair only; the sum over pairs is FP64.
 //
+// A persistent CTA takes a contiguous range of tiles, so consecutive tiles
+// mostly share their operator: the operator (4 K-blocks x hi/lo, 128 KB)
+// stays resident in shared memory and is reloaded (bulk copies) only when the
+// operator changes.  The input columns stream through a 3-stage ring, one
+// K-block (hi + lo, 32 KB) per stage, gathered with cp.async by three
+// producer groups (group s fills ring slot s), so up to three stages are in
+// flight while the tensor core works.  Two TMEM accumulators alternate
+// between the MMA warp and the four epilogue warps.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,23 +32,23 @@
 #include "internal.h"
 #include "kernels.h"
 
+
 namespace fmmb {
 namespace tc {
 
-constexpr int kTile = 128;        // output boxes per tile (MMA N)
+constexpr int kTile = 128;        // pairs per tile (MMA N)
 constexpr int kRows = 128;        // output coefficients (MMA M), K <= 128
 constexpr int kKB = 32;           // TF32 values per K-block (128 bytes)
 constexpr int kNKB = 4;           // K-blocks (K padded to 128)
-constexpr int kStages = 3;
-constexpr int kOpBytes = kRows * 128;               // operator K-block image (16 KB)
-constexpr int kBBytes = kTile * 128;                // gathered input K-block (16 KB)
-constexpr int kStageBytes = 2 * kOpBytes + 2 * kBBytes;  // A_hi, A_lo, B_hi, B_lo
-constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-constexpr int kThreads = 288;
-// tensor memory: two alternating FP32 slot accumulators, then the running
-// sum as an unevaluated FP32 pair (hi, lo)
-constexpr int kColP0 = 0, kColP1 = kTile, kColHi = 2 * kTile, kColLo = 3 * kTile;
-constexpr int kTmemCols = 4 * kTile;
+constexpr int kStages = 3;        // input ring
+constexpr int kHalf = kTile * 128;                  // one 128 x 128-byte K-block tile (16 KB)
+constexpr int kABytes = kNKB * 2 * kHalf;           // resident operator, hi/lo per K-block (128 KB)
+constexpr int kStageBytes = 2 * kHalf;              // input K-block, hi and lo (32 KB)
+constexpr int kBarBytes = 128;
+constexpr int kSmemBytes = kABytes + kStages * kStageBytes + kBarBytes + 1024;
+constexpr int kProducerWarps = 4 * kStages;         // one 128-thread group per ring slot
+constexpr int kThreads = 32 * (5 + kProducerWarps); // 4 epilogue + 1 MMA + producers
+constexpr int kTmemCols = 2 * kTile;                // two alternating FP32 accumulators
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
 
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major,
@@ -169,45 +171,49 @@ __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 12
 
 struct Params {
   int K;                  // real coefficients per expansion (<= 128)
-  const int* out_boxes;   // [nwork][64] output box (row of `out`) or -1
-  const int* slot_off;    // [nwork + 1] CSR of each work item's slots
-  const int* slot_op;     // operator image of each slot
-  const int* slot_src;    // [slots][128] input row of each output box (-1 = none)
+  int ntile;              // pair tiles
+  const int* tile_op;     // [ntile] operator of each tile (tiles sorted by operator)
+  const int* tile_src;    // [ntile][128] input row of each pair (-1 = empty column)
+  const int* tile_dst;    // [ntile][128] output row of each pair (-1 = empty column)
   const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
   const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
   double* out;            // FP64 expansions, [rows][K]
-  int atomic;             // 1 when an output box appears in several work items
+  int atomic;             // 1 when an output row receives several pairs
   int* err;               // set to a nonzero code on timeout
 };
 
 __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = (uint64_t*)(smem + kStages * kStageBytes);
+  unsigned char* sA = smem;                       // resident operator
+  unsigned char* sB = smem + kABytes;             // input ring
+  uint64_t* full = (uint64_t*)(sB + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accf = empty + kStages;  // [2] slot accumulator b complete
-  uint64_t* acce = accf + 2;         // [2] slot accumulator b folded into the sum
-  uint32_t* tmem_slot = (uint32_t*)(acce + 2);
-  __shared__ int sh_boxes[kTile];
+  uint64_t* accf = empty + kStages;  // [2] accumulator b holds a finished tile
+  uint64_t* acce = accf + 2;         // [2] accumulator b read out by the epilogue
+  uint64_t* a_full = acce + 2;       // operator image landed
+  uint64_t* a_free = a_full + 1;     // MMAs reading the previous operator done
+  uint32_t* tmem_slot = (uint32_t*)(a_free + 1);
   __shared__ int sh_fail;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int work = blockIdx.x;
-  const int s_begin = P.slot_off[work], s_end = P.slot_off[work + 1];
-  const int nslot = s_end - s_begin;
-  const int nstage_total = nslot * kNKB;
+  const int t_begin = (int)((long long)P.ntile * blockIdx.x / gridDim.x);
+  const int t_end = (int)((long long)P.ntile * (blockIdx.x + 1) / gridDim.x);
+  const int ntile = t_end - t_begin;
+  const int nstage_total = ntile * kNKB;
 
-  if (threadIdx.x < kTile) sh_boxes[threadIdx.x] = P.out_boxes[(size_t)work * kTile + threadIdx.x];
   if (threadIdx.x == 0) {
     sh_fail = 0;
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 129);  // 128 producer arrivals + the expect_tx arrival (+ bulk bytes)
+      mbar_init(&full[s], 128);  // the 128 producers of ring slot s
       mbar_init(&empty[s], 1);   // one tcgen05.commit
     }
     for (int b = 0; b < 2; b++) {
-      mbar_init(&accf[b], 1);    // tcgen05.commit after a slot's MMAs
-      mbar_init(&acce[b], 128);  // every epilogue thread after folding the slot
+      mbar_init(&accf[b], 1);    // tcgen05.commit after a tile's MMAs
+      mbar_init(&acce[b], 128);  // every epilogue thread after reading the tile
     }
+    mbar_init(a_full, 1);        // expect_tx arrival + operator bytes
+    mbar_init(a_free, 1);        // tcgen05.commit
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 4) {
@@ -221,37 +227,29 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   const uint32_t tmem = *tmem_slot;
 
   if (warp >= 5) {
-    // ------------------------------------------------ producers (128 threads)
-    // thread pt gathers row pt (hi and lo parts) with cp.async, keeping two
-    // stages in flight: the arrival for stage st-1 follows the wait for it.
-    const int pt = threadIdx.x - 160;
-    int st = 0;
-    for (; st < nstage_total; st++) {
-      const int s = st % kStages;
+    // ------------------------------------------------ producers
+    // group s (128 threads) fills ring slot s for stages s, s+3, s+6, ...;
+    // thread pt gathers column pt (hi and lo parts of one K-block).
+    const int grp = (warp - 5) >> 2;
+    const int pt = threadIdx.x - 160 - grp * 128;
+    unsigned char* bhi = sB + grp * kStageBytes;
+    unsigned char* blo = bhi + kHalf;
+    for (int st = grp; st < nstage_total; st += kStages) {
       const uint32_t ph = (st / kStages) & 1;
       bool ok = true;
-      if (st >= kStages && lane == 0) ok = mbar_wait(&empty[s], ph ^ 1);
+      if (st >= kStages && lane == 0) ok = mbar_wait(&empty[grp], ph ^ 1);
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) atomicExch(&sh_fail, 1);
       if (!ok || *(volatile int*)&sh_fail) break;
-      const int sl = s_begin + st / kNKB;
+      const int g = t_begin + st / kNKB;
       const int kb = st % kNKB;
-      unsigned char* stage = smem + s * kStageBytes;
-      if (pt == 0) {
-        const float* img = P.opimg + ((size_t)P.slot_op[sl] * kNKB + kb) * 2 * (kRows * kKB);
-        mbar_arrive_tx(&full[s], 2 * kOpBytes);
-        bulk_g2s(stage, img, kOpBytes, &full[s]);
-        bulk_g2s(stage + kOpBytes, img + kRows * kKB, kOpBytes, &full[s]);
-      }
-      const int src = P.slot_src[(size_t)sl * kTile + pt];
-      unsigned char* bhi = stage + 2 * kOpBytes;
-      unsigned char* blo = bhi + kBBytes;
+      const int src = P.tile_src[(size_t)g * kTile + pt];
       if (src >= 0) {
-        const float* g = P.xin + (size_t)src * 256 + kb * kKB;
+        const float* x = P.xin + (size_t)src * 256 + kb * kKB;
 #pragma unroll
         for (int c = 0; c < 8; c++) {
-          cp_async16(bhi + swz(pt, c), g + 4 * c);
-          cp_async16(blo + swz(pt, c), g + 128 + 4 * c);
+          cp_async16(bhi + swz(pt, c), x + 4 * c);
+          cp_async16(blo + swz(pt, c), x + 128 + 4 * c);
         }
       } else {
         const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -262,40 +260,54 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
         }
       }
       cp_async_commit();
-      if (st > 0) {
-        cp_async_wait<1>();  // stage st-1 landed
-        fence_async_smem();
-        mbar_arrive(&full[(st - 1) % kStages]);
-      }
+      cp_async_wait<0>();
+      fence_async_smem();
+      mbar_arrive(&full[grp]);
     }
     cp_async_wait<0>();
-    if (st > 0) {
-      fence_async_smem();
-      mbar_arrive(&full[(st - 1) % kStages]);
-    }
   } else if (warp == 4) {
-    // ------------------------------------------------ MMA issuer
+    // ------------------------------------------------ MMA issuer (+ operator loads)
     bool ok = true;
-    for (int g = 0; g < nslot && ok; g++) {
-      const int buf = g & 1;
-      const uint32_t dcol = tmem + (uint32_t)(buf ? kColP1 : kColP0);
-      if (g >= 2) {  // wait until the epilogue has folded this accumulator
-        if (lane == 0) ok = mbar_wait(&acce[buf], ((g >> 1) - 1) & 1);
+    int cur_op = -1, nload = 0;
+    for (int i = 0; i < ntile && ok; i++) {
+      const int g = t_begin + i;
+      const int buf = i & 1;
+      const uint32_t dcol = tmem + (uint32_t)(buf * kTile);
+      const int op = P.tile_op[g];
+      if (op != cur_op) {  // reload the resident operator once the MMAs reading it are done
+        if (lane == 0) {
+          if (nload > 0) {
+            mma_commit(a_free);
+            ok = mbar_wait(a_free, (nload - 1) & 1);
+          }
+          if (ok) {
+            const unsigned char* img = (const unsigned char*)(P.opimg + (size_t)op * kNKB * 2 * (kRows * kKB));
+            mbar_arrive_tx(a_full, kABytes);
+            for (int c = 0; c < kNKB * 2; c++) bulk_g2s(sA + c * kHalf, img + (size_t)c * kHalf, kHalf, a_full);
+            ok = mbar_wait(a_full, nload & 1);
+          }
+        }
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         if (!ok) break;
-        tc_fence_after();
+        cur_op = op;
+        nload++;
       }
+      if (i >= 2) {  // wait until the epilogue has read this accumulator
+        if (lane == 0) ok = mbar_wait(&acce[buf], ((i >> 1) - 1) & 1);
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        if (!ok) break;
+      }
+      tc_fence_after();
       for (int kb = 0; kb < kNKB && ok; kb++) {
-        const int st = g * kNKB + kb;
+        const int st = i * kNKB + kb;
         const int s = st % kStages;
-        const uint32_t ph = (st / kStages) & 1;
-        if (lane == 0) ok = mbar_wait(&full[s], ph);
+        if (lane == 0) ok = mbar_wait(&full[s], (st / kStages) & 1);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         if (!ok) break;
         tc_fence_after();
         if (lane == 0) {
-          const uint32_t base = smem_u32(smem + s * kStageBytes);
-          const uint32_t ahi = base, alo = base + kOpBytes, bhi = base + 2 * kOpBytes, blo = bhi + kBBytes;
+          const uint32_t ahi = smem_u32(sA + kb * 2 * kHalf), alo = ahi + kHalf;
+          const uint32_t bhi = smem_u32(sB + s * kStageBytes), blo = bhi + kHalf;
 #pragma unroll
           for (int k = 0; k < kKB / 8; k++) {  // 4 MMAs of K=8 per 32-wide block
             const uint32_t o = k * 32;           // 8 TF32 = 32 bytes along K
@@ -303,82 +315,58 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
             mma_tf32(dcol, make_desc(ahi + o), make_desc(blo + o), 1u);
             mma_tf32(dcol, make_desc(alo + o), make_desc(bhi + o), 1u);
           }
-          mma_commit(&empty[s]);  // frees the stage when these MMAs are done
+          mma_commit(&empty[s]);  // frees the ring slot when these MMAs are done
           if (kb == kNKB - 1) mma_commit(&accf[buf]);
         }
         __syncwarp();
       }
     }
     if (!ok && lane == 0) atomicExch(&sh_fail, 2);
+    // drain: every MMA issued above completes before tensor memory is freed
+    if (lane == 0 && nload > 0) {
+      mma_commit(a_free);
+      mbar_wait(a_free, (nload - 1) & 1);
+    }
+    __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
-    // folds each slot's FP32 accumulator into the (hi, lo) running sum with
-    // an error-free two-sum, then writes hi + lo in FP64 at the end.
-    const int row = warp * 32 + lane;  // output coefficient of this thread
+    // thread `row` owns output coefficient row; column j of a tile adds into
+    // output row tile_dst[j] (lane l holds tile_dst[32h + l], broadcast by shuffle).
+    const int row = warp * 32 + lane;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     bool ok = true;
-    for (int g = 0; g < nslot; g++) {
-      const int buf = g & 1;
-      bool w = mbar_wait(&accf[buf], (g >> 1) & 1);
+    for (int i = 0; i < ntile; i++) {
+      const int g = t_begin + i;
+      const int buf = i & 1;
+      int dl[kTile / 32];
+#pragma unroll
+      for (int h = 0; h < kTile / 32; h++) dl[h] = P.tile_dst[(size_t)g * kTile + h * 32 + lane];
+      const bool w = mbar_wait(&accf[buf], (i >> 1) & 1);
       ok = __all_sync(0xffffffffu, w && *(volatile int*)&sh_fail == 0) != 0;
       if (!ok) break;
       tc_fence_after();
-#pragma unroll 1
+#pragma unroll
       for (int h = 0; h < kTile / 32; h++) {
-        uint32_t pv[32], hv[32], lv[32];
-        tmem_ld32_nowait(lane_base + (uint32_t)((buf ? kColP1 : kColP0) + h * 32), pv);
-        if (g > 0) {
-          tmem_ld32_nowait(lane_base + (uint32_t)(kColHi + h * 32), hv);
-          tmem_ld32_nowait(lane_base + (uint32_t)(kColLo + h * 32), lv);
-        }
+        uint32_t v[32];
+        tmem_ld32_nowait(lane_base + (uint32_t)(buf * kTile + h * 32), v);
         tmem_wait_ld();
-        if (g == 0) {
+        if (h == kTile / 32 - 1) {  // the accumulator is free once read
+          tc_fence_before();
+          mbar_arrive(&acce[buf]);
+        }
 #pragma unroll
-          for (int j = 0; j < 32; j++) {
-            hv[j] = pv[j];
-            lv[j] = 0u;
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const float a = __uint_as_float(hv[j]), b = __uint_as_float(pv[j]);
-            const float s = __fadd_rn(a, b);
-            const float bb = __fsub_rn(s, a);
-            const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
-            hv[j] = __float_as_uint(s);
-            lv[j] = __float_as_uint(__fadd_rn(__uint_as_float(lv[j]), e));
+        for (int j = 0; j < 32; j++) {
+          const int dst = __shfl_sync(0xffffffffu, dl[h], j);
+          if (dst >= 0 && row < P.K) {
+            double* o = P.out + (size_t)dst * P.K + row;
+            const double val = (double)__uint_as_float(v[j]);
+            if (P.atomic) atomicAdd(o, val);
+            else *o += val;
           }
         }
-        tmem_st32(lane_base + (uint32_t)(kColHi + h * 32), hv);
-        tmem_st32(lane_base + (uint32_t)(kColLo + h * 32), lv);
       }
-      tmem_wait_st();
-      tc_fence_before();
-      mbar_arrive(&acce[buf]);
     }
     if (!ok) atomicExch(&sh_fail, 3);
-    if (ok && nslot > 0) {
-      tc_fence_after();
-#pragma unroll 1
-      for (int h = 0; h < kTile / 32; h++) {
-        uint32_t hv[32], lv[32];
-        tmem_ld32_nowait(lane_base + (uint32_t)(kColHi + h * 32), hv);
-        tmem_ld32_nowait(lane_base + (uint32_t)(kColLo + h * 32), lv);
-        tmem_wait_ld();
-        if (row < P.K) {
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const int box = sh_boxes[h * 32 + j];
-            if (box >= 0) {
-              const double v = (double)__uint_as_float(hv[j]) + (double)__uint_as_float(lv[j]);
-              double* dst = P.out + (size_t)box * P.K + row;
-              if (P.atomic) atomicAdd(dst, v);
-              else *dst += v;
-            }
-          }
-        }
-      }
-    }
   }
   tc_fence_before();
   __syncthreads();
@@ -423,21 +411,22 @@ void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_translate_tc(const TcJobArgs& a, cudaStream_t st) {
-  if (a.nwork <= 0) return;
+void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st) {
+  if (a.ntile <= 0) return;
   FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
   tc::Params P{};
   P.K = a.K;
-  P.out_boxes = a.out_boxes;
-  P.slot_off = a.slot_off;
-  P.slot_op = a.slot_op;
-  P.slot_src = a.slot_src;
+  P.ntile = a.ntile;
+  P.tile_op = a.tile_op;
+  P.tile_src = a.tile_src;
+  P.tile_dst = a.tile_dst;
   P.opimg = a.opimg;
   P.xin = a.xin;
   P.out = a.out;
   P.atomic = a.atomic;
   P.err = a.err;
-  tc::translate_tc<<<a.nwork, tc::kThreads, tc::kSmemBytes, st>>>(P);
+  const int grid = a.ntile < nsm ? a.ntile : nsm;
+  tc::translate_tc<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(P);
   FMMB_CHECK_LAUNCH();
 }
 
