@@ -320,7 +320,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       // box pairs {operator, input row, output row} -> tiles of TT pairs of one
       // operator each (operators ascending, pairs in output order within one)
       using Pair = std::array<int, 3>;
-      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs, int atomic) {
+      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs) {
         std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x[0] < y[0]; });
         std::vector<int> top, tsrc, tdst;
         for (size_t i = 0; i < pairs.size();) {
@@ -336,7 +336,6 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
           i = j;
         }
         job.ntile = (int)top.size();
-        job.atomic = atomic;
         up(job.tile_op, top);
         up(job.tile_src, tsrc);
         up(job.tile_dst, tdst);
@@ -356,7 +355,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             }
           }
         }
-        build_job(pl->tc_m2l, pairs, 1);
+        build_job(pl->tc_m2l, pairs);
       }
       pl->tc_m2m.clear();
       pl->tc_l2l.clear();
@@ -374,7 +373,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
               if (c >= 0) pairs.push_back({sl, pl->off_j[lev + 1] + c, box});
             }
           }
-          build_job(*pl->tc_m2m[lev], pairs, 1);
+          build_job(*pl->tc_m2m[lev], pairs);
         }
         if (lev >= 3) {  // L2L into children at lev (one pair per child): operator = child octant
           std::vector<Pair> pairs;
@@ -382,7 +381,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             const int box = pl->off_i[lev] + b;
             pairs.push_back({keys[box] & 7, pl->off_i[lev - 1] + par_i[box], box});
           }
-          build_job(*pl->tc_l2l[lev], pairs, 0);
+          build_job(*pl->tc_l2l[lev], pairs);
         }
       }
     }
@@ -489,7 +488,6 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     TcJobArgs a{};
     a.ntile = job.ntile;
     a.K = K;
-    a.atomic = job.atomic;
     a.tile_op = job.tile_op.get();
     a.tile_src = job.tile_src.get();
     a.tile_dst = job.tile_dst.get();

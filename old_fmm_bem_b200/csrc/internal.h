@@ -161,7 +161,7 @@ struct fmmb_plan {
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots
   struct TcJob {  // pair tiles of one tensor-core translation launch (translate_tc.cu)
-    int ntile = 0, atomic = 0;
+    int ntile = 0;
     fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
   };
   TcJob tc_m2l;                                              // all levels

@@ -60,7 +60,7 @@ namespace fmmb {
 int tc_tile();
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
 struct TcJobArgs {
-  int ntile, K, atomic;
+  int ntile, K;
   const int *tile_op, *tile_src, *tile_dst;  // [ntile], [ntile][128], [ntile][128]
   const float* opimg;
   const float* xin;  // TF32 split of the inputs [rows][2][128]

@@ -8,8 +8,8 @@
 // row, operator), grouped by operator and cut into tiles of 128 pairs: one
 // tile is one GEMM  D (128 coefficients x 128 pairs) = T_op . X[inputs],
 // X being the TF32 (hi, lo) split of the input expansions, and its columns
-// are added into the FP64 output rows in the epilogue (atomically when an
-// output row receives several pairs: M2L, M2M; plainly for L2L).  Grouping by
+// are added into the FP64 output rows in the epilogue by reductions at the L2
+// (an output row receives several pairs in M2L and M2M).  Grouping by
 // operator keeps the tiles full whatever the geometry (on a surface most of
 // the 189 interaction positions of a box are empty, so tiles of output boxes
 // would be mostly zero columns).  Each product is split into three TF32 MMAs,
@@ -166,6 +166,16 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// out[0] += v at the L2 when pred (fire and forget).
+__device__ __forceinline__ void red_add_f64(double* out, double v, bool pred) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %2, 0;\n\t"
+      "@p red.global.add.f64 [%0], %1;\n\t}" ::"l"(out),
+      "d"(v), "r"((int)pred)
+      : "memory");
+}
+
 // Swizzled byte offset of 16-byte chunk c of row r in a K-block tile.
 __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
@@ -178,7 +188,6 @@ struct Params {
   const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
   const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
   double* out;            // FP64 expansions, [rows][K]
-  int atomic;             // 1 when an output row receives several pairs
   int* err;               // set to a nonzero code on timeout
 };
 
@@ -330,9 +339,12 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
-    // thread `row` owns output coefficient row; column j of a tile adds into
-    // output row tile_dst[j] (lane l holds tile_dst[32h + l], broadcast by shuffle).
+    // thread `row` owns output coefficient row; column j of a tile is added
+    // into output row tile_dst[j] (lane l holds tile_dst[32h + l], broadcast by
+    // shuffle) with a predicated FP64 reduction at the L2: no branch per
+    // column, and no read-back of the output.
     const int row = warp * 32 + lane;
+    const bool row_ok = row < P.K;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     bool ok = true;
     for (int i = 0; i < ntile; i++) {
@@ -354,15 +366,13 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
           tc_fence_before();
           mbar_arrive(&acce[buf]);
         }
+        int d[32];
+#pragma unroll
+        for (int j = 0; j < 32; j++) d[j] = __shfl_sync(0xffffffffu, dl[h], j);
 #pragma unroll
         for (int j = 0; j < 32; j++) {
-          const int dst = __shfl_sync(0xffffffffu, dl[h], j);
-          if (dst >= 0 && row < P.K) {
-            double* o = P.out + (size_t)dst * P.K + row;
-            const double val = (double)__uint_as_float(v[j]);
-            if (P.atomic) atomicAdd(o, val);
-            else *o += val;
-          }
+          const bool pj = row_ok && d[j] >= 0;
+          red_add_f64(P.out + (size_t)(pj ? d[j] : 0) * P.K + row, (double)__uint_as_float(v[j]), pj);
         }
       }
     }
@@ -423,7 +433,6 @@ void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st) {
   P.opimg = a.opimg;
   P.xin = a.xin;
   P.out = a.out;
-  P.atomic = a.atomic;
   P.err = a.err;
   const int grid = a.ntile < nsm ? a.ntile : nsm;
   tc::translate_tc<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(P);
