@@ -320,7 +320,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       // box pairs {operator, input row, output row} -> tiles of TT pairs of one
       // operator each (operators ascending, pairs in output order within one)
       using Pair = std::array<int, 3>;
-      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs) {
+      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs, bool pair_rows) {
         std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x[0] < y[0]; });
         std::vector<int> top, tsrc, tdst;
         for (size_t i = 0; i < pairs.size();) {
@@ -339,6 +339,27 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         up(job.tile_op, top);
         up(job.tile_src, tsrc);
         up(job.tile_dst, tdst);
+        job.nred = 0;
+        if (pair_rows) {  // per output row, its pair positions in tile order
+          std::vector<std::array<int, 2>> pos;
+          for (size_t k = 0; k < tdst.size(); k++)
+            if (tdst[k] >= 0) pos.push_back({tdst[k], (int)k});
+          std::sort(pos.begin(), pos.end());
+          std::vector<int> rows, ptr, idx;
+          for (size_t k = 0; k < pos.size(); k++) {
+            if (k == 0 || pos[k][0] != pos[k - 1][0]) {
+              rows.push_back(pos[k][0]);
+              ptr.push_back((int)k);
+            }
+            idx.push_back(pos[k][1]);
+          }
+          ptr.push_back((int)pos.size());
+          job.nred = (int)rows.size();
+          up(job.red_rows, rows);
+          up(job.red_ptr, ptr);
+          up(job.red_idx, idx);
+          pl->tc_y.alloc((size_t)job.ntile * TT * 128);
+        }
       };
       // M2L, all levels in one job: operator = set(level)*316 + relative position
       {
@@ -355,7 +376,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             }
           }
         }
-        build_job(pl->tc_m2l, pairs);
+        build_job(pl->tc_m2l, pairs, true);
       }
       pl->tc_m2m.clear();
       pl->tc_l2l.clear();
@@ -373,7 +394,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
               if (c >= 0) pairs.push_back({sl, pl->off_j[lev + 1] + c, box});
             }
           }
-          build_job(*pl->tc_m2m[lev], pairs);
+          build_job(*pl->tc_m2m[lev], pairs, false);
         }
         if (lev >= 3) {  // L2L into children at lev (one pair per child): operator = child octant
           std::vector<Pair> pairs;
@@ -381,7 +402,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             const int box = pl->off_i[lev] + b;
             pairs.push_back({keys[box] & 7, pl->off_i[lev - 1] + par_i[box], box});
           }
-          build_job(*pl->tc_l2l[lev], pairs);
+          build_job(*pl->tc_l2l[lev], pairs, false);
         }
       }
     }
@@ -494,8 +515,13 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     a.opimg = img;
     a.xin = xin;
     a.out = out;
+    a.y = job.nred > 0 ? pl->tc_y.get() : nullptr;
     a.err = pl->d_err.get();
     launch_translate_tc(a, pl->nsm, m);
+    if (job.nred > 0) {
+      launch_reduce_pairs(job.nred, job.red_rows.get(), job.red_ptr.get(), job.red_idx.get(), pl->tc_y.get(), K, out, m);
+      pl->launches++;
+    }
   };
   auto split = [&](const double* X, float* Xtf, int off, int n, int phase) {
     PhaseTimer tm(pl, phase, m);

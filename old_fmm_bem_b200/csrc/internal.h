@@ -163,7 +163,12 @@ struct fmmb_plan {
   struct TcJob {  // pair tiles of one tensor-core translation launch (translate_tc.cu)
     int ntile = 0;
     fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
+    // when nred > 0 the launch stores pair rows to tc_y and reduce_pairs sums
+    // them per output row: rows, CSR offsets, pair positions (tile*128 + column)
+    int nred = 0;
+    fmmb::DevBuf<int> red_rows, red_ptr, red_idx;
   };
+  fmmb::DevBuf<float> tc_y;                                  // pair rows of the M2L launch
   TcJob tc_m2l;                                              // all levels
   int nsm = 148;                                             // SMs of the plan's device
   std::vector<std::unique_ptr<TcJob>> tc_m2m, tc_l2l;        // per level

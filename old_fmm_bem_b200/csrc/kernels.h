@@ -65,7 +65,11 @@ struct TcJobArgs {
   const float* opimg;
   const float* xin;  // TF32 split of the inputs [rows][2][128]
   double* out;
+  float* y;  // pair rows [ntile*128][128] instead of reductions into out (nullptr: reductions)
   int* err;
 };
 void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st);
+// out[rows[w]] += sum of the pair rows y[idx[ptr[w]..ptr[w+1])] (FP64, list order)
+void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int K, double* out,
+                         cudaStream_t st);
 }  // namespace fmmb

@@ -188,6 +188,7 @@ struct Params {
   const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
   const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
   double* out;            // FP64 expansions, [rows][K]
+  float* y;               // when set: column j of tile g goes to y[(g*128 + j)*128 + row] instead
   int* err;               // set to a nonzero code on timeout
 };
 
@@ -339,10 +340,11 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
-    // thread `row` owns output coefficient row; column j of a tile is added
-    // into output row tile_dst[j] (lane l holds tile_dst[32h + l], broadcast by
-    // shuffle) with a predicated FP64 reduction at the L2: no branch per
-    // column, and no read-back of the output.
+    // thread `row` owns output coefficient row.  Either column j of a tile is
+    // added into output row tile_dst[j] (lane l holds tile_dst[32h + l],
+    // broadcast by shuffle) with a predicated FP64 reduction at the L2 -- no
+    // branch per column, no read-back -- or, for launches whose outputs
+    // receive many pairs (M2L), the column is stored to its pair row of y.
     const int row = warp * 32 + lane;
     const bool row_ok = row < P.K;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
@@ -366,13 +368,19 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
           tc_fence_before();
           mbar_arrive(&acce[buf]);
         }
-        int d[32];
+        if (P.y) {  // pair-indexed FP32 rows: plain coalesced stores, summed per output by reduce_pairs
+          float* yb = P.y + ((size_t)g * kTile + h * 32) * kRows + row;
 #pragma unroll
-        for (int j = 0; j < 32; j++) d[j] = __shfl_sync(0xffffffffu, dl[h], j);
+          for (int j = 0; j < 32; j++) yb[(size_t)j * kRows] = __uint_as_float(v[j]);
+        } else {
+          int d[32];
 #pragma unroll
-        for (int j = 0; j < 32; j++) {
-          const bool pj = row_ok && d[j] >= 0;
-          red_add_f64(P.out + (size_t)(pj ? d[j] : 0) * P.K + row, (double)__uint_as_float(v[j]), pj);
+          for (int j = 0; j < 32; j++) d[j] = __shfl_sync(0xffffffffu, dl[h], j);
+#pragma unroll
+          for (int j = 0; j < 32; j++) {
+            const bool pj = row_ok && d[j] >= 0;
+            red_add_f64(P.out + (size_t)(pj ? d[j] : 0) * P.K + row, (double)__uint_as_float(v[j]), pj);
+          }
         }
       }
     }
@@ -410,9 +418,54 @@ __global__ void split_tf32(int nbox, int K, const double* __restrict__ M, float*
   Mtf[b * 256 + 128 + k] = lo;
 }
 
+// out[rows[w]][0..K) += sum over e in [ptr[w], ptr[w+1]) of y[idx[e]][0..K), in
+// FP64 and in list order (deterministic); one warp per output row, lane l
+// holding coefficients 4l..4l+3.
+__global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* __restrict__ ptr,
+                             const int* __restrict__ idx, const float* __restrict__ y, int K,
+                             double* __restrict__ out) {
+  const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nrow) return;
+  double a[4] = {0, 0, 0, 0};
+  const int e0 = ptr[w], e1 = ptr[w + 1];
+  int e = e0;
+  for (; e + 4 <= e1; e += 4) {
+    float4 v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = __ldg(reinterpret_cast<const float4*>(y + (size_t)idx[e + u] * kRows) + lane);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      a[0] += v[u].x;
+      a[1] += v[u].y;
+      a[2] += v[u].z;
+      a[3] += v[u].w;
+    }
+  }
+  for (; e < e1; e++) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(y + (size_t)idx[e] * kRows) + lane);
+    a[0] += v.x;
+    a[1] += v.y;
+    a[2] += v.z;
+    a[3] += v.w;
+  }
+  double* o = out + (size_t)rows[w] * K;
+#pragma unroll
+  for (int c = 0; c < 4; c++)
+    if (4 * lane + c < K) o[4 * lane + c] += a[c];
+}
+
 }  // namespace tc
 
 int tc_tile() { return tc::kTile; }
+
+void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int K, double* out,
+                         cudaStream_t st) {
+  if (nrow <= 0) return;
+  const size_t threads = (size_t)nrow * 32;
+  tc::reduce_pairs<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(nrow, rows, ptr, idx, y, K, out);
+  FMMB_CHECK_LAUNCH();
+}
 
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st) {
   if (nbox <= 0) return;
@@ -433,6 +486,7 @@ void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st) {
   P.opimg = a.opimg;
   P.xin = a.xin;
   P.out = a.out;
+  P.y = a.y;
   P.err = a.err;
   const int grid = a.ntile < nsm ? a.ntile : nsm;
   tc::translate_tc<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(P);
