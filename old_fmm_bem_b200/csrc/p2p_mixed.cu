@@ -7,10 +7,15 @@
 // into FP64 accumulators, so the accumulated rounding stays at the FP32 level
 // of one 32-term sum whatever the number of sources.
 //
-// Layout: one block of 128 threads per target leaf.  Threads 0..63 and
-// 64..127 take the same 64 targets and split each staged source chunk in two
-// halves; the halves are combined through shared memory at the end (leaves are
-// ~64 points, so one thread per target would idle half the block).
+// Layout: one block of 4 warps per target leaf.  The sources of all
+// neighbour leaves are staged once into shared memory as one list -- the
+// leaf's own source leaf first, padded to a multiple of 32 with far,
+// zero-charge points, then the other neighbours, padded likewise -- so that
+// every run of 32 sources needs no bounds check, and only runs of the own leaf
+// test for coincident points (points at zero distance share a leaf).  Each
+// lane holds two targets (a pass covers 64), so one shared-memory read of a
+// source serves two pairs; warp w takes runs w, w+4, ... and the four warps'
+// FP64 partial sums are added through shared memory at the end of a pass.
 #include <cuda_runtime.h>
 
 #include "internal.h"
@@ -20,8 +25,54 @@ namespace fmmb {
 namespace {
 
 constexpr int kThreads = 128;
-constexpr int kTeam = 64;      // targets per pass
-constexpr int kChunk = 256;    // sources staged per pass
+constexpr int kWarps = kThreads / 32;
+constexpr int kPass = 64;     // targets per pass (two per lane)
+constexpr int kCap = 1024;    // staged sources per chunk (multiple of 32)
+constexpr int kSelfSlot = 13; // offset (0, 0, 0) in the 27-slot list
+constexpr float kFar = 1e18f; // padding sources: r^2 ~ 3e36 stays finite in FP32
+
+__device__ __forceinline__ int pad32(int n) { return (n + 31) & ~31; }
+
+template <int KER>
+struct Acc {
+  float p, fx, fy, fz;
+};
+
+// One run of 32 staged sources against the thread's two targets.
+template <int KER, bool EXCL>
+__device__ __forceinline__ void run32(const float4* __restrict__ sp, const float4* __restrict__ sm, float4 xa,
+                                      float4 xb, float4 na, float4 nb, float eps2, Acc<KER>& a, Acc<KER>& b) {
+#pragma unroll 8
+  for (int k = 0; k < 32; k++) {
+    const float4 xj = sp[k];
+    float4 mj = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (KER == FMMB_LAPLACE_GNJ) mj = sm[k];
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const float4 xi = t ? xb : xa;
+      Acc<KER>& c = t ? b : a;
+      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+      float rinv = rsqrtf(r2);
+      if (EXCL) rinv = (r2 > 0.f) ? rinv : 0.f;
+      if (KER == FMMB_LAPLACE_G) {
+        const float qr = xj.w * rinv;
+        const float qr3 = qr * rinv * rinv;
+        c.p += qr;
+        c.fx = fmaf(dx, qr3, c.fx);
+        c.fy = fmaf(dy, qr3, c.fy);
+        c.fz = fmaf(dz, qr3, c.fz);
+      } else if (KER == FMMB_LAPLACE_GNI) {
+        const float4 nv = t ? nb : na;
+        const float qr3 = xj.w * rinv * rinv * rinv;
+        c.p = fmaf(fmaf(dx, nv.x, fmaf(dy, nv.y, dz * nv.z)), qr3, c.p);
+      } else {
+        const float r3 = rinv * rinv * rinv;
+        c.p = fmaf(fmaf(dx, mj.x, fmaf(dy, mj.y, dz * mj.z)), r3, c.p);
+      }
+    }
+  }
+}
 
 template <int KER, bool EXCL>
 __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ leaf_i, const int2* __restrict__ leaf_j,
@@ -30,95 +81,130 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ l
                                                       const float4* __restrict__ snrm, const float* __restrict__ qs,
                                                       float eps2, double coef, double* __restrict__ pot,
                                                       double* __restrict__ grad, int ni) {
-  __shared__ float4 sp[kChunk];
-  __shared__ float4 sn[KER == FMMB_LAPLACE_GNJ ? kChunk : 1];
-  __shared__ double red[4][kTeam];
+  constexpr int NC = KER == FMMB_LAPLACE_G ? 4 : 1;  // accumulated components
+  __shared__ float4 sp[kCap];                                   // x, y, z, q (Gnj: q unused)
+  __shared__ float4 sm[KER == FMMB_LAPLACE_GNJ ? kCap : 1];     // q * n_j (Gnj)
+  __shared__ double red[kWarps - 1][NC][kPass];
+  __shared__ int2 seg[kP2PSlots];                               // (first source, count), own leaf first
+  __shared__ int nseg_sh;
+
   const int b = blockIdx.x;
   const int2 li = leaf_i[b];
-  const int t = threadIdx.x & (kTeam - 1);
-  const int half = threadIdx.x / kTeam;
-  int slots[kP2PSlots];
-  int nslot = 0;
-  for (int s = 0; s < kP2PSlots; s++) {
-    const int jl = list[(size_t)b * kP2PSlots + s];
-    if (jl >= 0) slots[nslot++] = jl;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    int n = 0;
+    const int self = list[(size_t)b * kP2PSlots + kSelfSlot];
+    seg[n++] = self >= 0 ? leaf_j[self] : make_int2(0, 0);
+    for (int s = 0; s < kP2PSlots; s++) {
+      const int jl = list[(size_t)b * kP2PSlots + s];
+      if (s != kSelfSlot && jl >= 0) seg[n++] = leaf_j[jl];
+    }
+    nseg_sh = n;
   }
-  for (int t0 = 0; t0 < li.y; t0 += kTeam) {
-    const bool act = t0 + t < li.y;
-    const int i = li.x + t0 + t;
-    const float4 xi = act ? tpos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 nv = (KER == FMMB_LAPLACE_GNI && act) ? tnrm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    double P = 0, FX = 0, FY = 0, FZ = 0;
-    for (int s = 0; s < nslot; s++) {
-      const int2 lj = leaf_j[slots[s]];
-      for (int j0 = 0; j0 < lj.y; j0 += kChunk) {
-        const int nld = min(kChunk, lj.y - j0);
+  __syncthreads();
+  const int nseg = nseg_sh;
+  int n_other = 0;
+  for (int s = 1; s < nseg; s++) n_other += seg[s].y;
+  const int self_end = pad32(seg[0].y);                  // virtual list: [own | pad | others | pad]
+  const int vlen = self_end + pad32(n_other);
+  const int nchunk = (vlen + kCap - 1) / kCap;
+
+  for (int t0 = 0; t0 < li.y; t0 += kPass) {
+    const int ia = t0 + lane, ib = t0 + 32 + lane;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 xa = ia < li.y ? tpos[li.x + ia] : z4;
+    const float4 xb = ib < li.y ? tpos[li.x + ib] : z4;
+    float4 na = z4, nb = z4;
+    if (KER == FMMB_LAPLACE_GNI) {
+      if (ia < li.y) na = tnrm[li.x + ia];
+      if (ib < li.y) nb = tnrm[li.x + ib];
+    }
+    double PA[NC], PB[NC];
+#pragma unroll
+    for (int c = 0; c < NC; c++) PA[c] = PB[c] = 0.0;
+
+    for (int ch = 0; ch < nchunk; ch++) {
+      const int c0 = ch * kCap, c1 = min(vlen, c0 + kCap);
+      if (nchunk > 1 || t0 == 0) {
+        // stage virtual sources [c0, c1): far zero-charge points, then every
+        // segment's part of the chunk
         __syncthreads();
-        for (int e = threadIdx.x; e < nld; e += kThreads) {
-          const int j = lj.x + j0 + e;
-          float4 v = spos[j];
-          v.w = qs[j];
-          sp[e] = v;
-          if (KER == FMMB_LAPLACE_GNJ) sn[e] = snrm[j];
+        for (int e = threadIdx.x; e < c1 - c0; e += kThreads) {
+          sp[e] = make_float4(kFar, kFar, kFar, 0.f);
+          if (KER == FMMB_LAPLACE_GNJ) sm[e] = z4;
         }
         __syncthreads();
-        // this half's share of the chunk, in runs of 32
-        const int mid = (nld + 1) >> 1;
-        const int jb = half ? mid : 0, je = half ? nld : mid;
-        for (int r0 = jb; r0 < je; r0 += 32) {
-          const int r1 = min(je, r0 + 32);
-          float p = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
-#pragma unroll 8
-          for (int jj = r0; jj < r1; jj++) {
-            const float4 xj = sp[jj];
-            const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-            float rinv = rsqrtf(r2);
-            if (EXCL) rinv = (r2 > 0.f) ? rinv : 0.f;
-            if (KER == FMMB_LAPLACE_G) {
-              const float qr = xj.w * rinv;
-              const float qr3 = qr * rinv * rinv;
-              p += qr;
-              fx = fmaf(dx, qr3, fx);
-              fy = fmaf(dy, qr3, fy);
-              fz = fmaf(dz, qr3, fz);
-            } else if (KER == FMMB_LAPLACE_GNI) {
-              const float qr3 = xj.w * rinv * rinv * rinv;
-              p = fmaf(fmaf(dx, nv.x, fmaf(dy, nv.y, dz * nv.z)), qr3, p);
-            } else {
-              const float4 nj = sn[jj];
-              const float qr3 = xj.w * rinv * rinv * rinv;
-              p = fmaf(fmaf(dx, nj.x, fmaf(dy, nj.y, dz * nj.z)), qr3, p);
+        int v0 = 0;  // virtual start of the segment
+        for (int s = 0; s < nseg; s++) {
+          const int2 sg = seg[s];
+          const int lo = max(v0, c0), hi = min(v0 + sg.y, c1);
+          for (int v = lo + threadIdx.x; v < hi; v += kThreads) {
+            const int j = sg.x + (v - v0);
+            float4 x = spos[j];
+            const float q = qs[j];
+            x.w = q;
+            sp[v - c0] = x;
+            if (KER == FMMB_LAPLACE_GNJ) {
+              const float4 nj = snrm[j];
+              sm[v - c0] = make_float4(q * nj.x, q * nj.y, q * nj.z, 0.f);
             }
           }
-          P += (double)p;
-          if (KER == FMMB_LAPLACE_G) {
-            FX += (double)fx;
-            FY += (double)fy;
-            FZ += (double)fz;
+          v0 = (s == 0) ? self_end : v0 + sg.y;
+        }
+        __syncthreads();
+      }
+      // runs of 32 sources: warp w takes runs w, w + 4, ...
+      for (int r0 = c0 + warp * 32; r0 < c1; r0 += kWarps * 32) {
+        Acc<KER> a{0.f, 0.f, 0.f, 0.f}, bb{0.f, 0.f, 0.f, 0.f};
+        if (EXCL && r0 < self_end)
+          run32<KER, true>(sp + (r0 - c0), sm + (KER == FMMB_LAPLACE_GNJ ? r0 - c0 : 0), xa, xb, na, nb, eps2, a, bb);
+        else
+          run32<KER, false>(sp + (r0 - c0), sm + (KER == FMMB_LAPLACE_GNJ ? r0 - c0 : 0), xa, xb, na, nb, eps2, a, bb);
+        PA[0] += (double)a.p;
+        PB[0] += (double)bb.p;
+        if (KER == FMMB_LAPLACE_G) {
+          PA[1] += (double)a.fx;
+          PA[2] += (double)a.fy;
+          PA[3] += (double)a.fz;
+          PB[1] += (double)bb.fx;
+          PB[2] += (double)bb.fy;
+          PB[3] += (double)bb.fz;
+        }
+      }
+    }
+    // add the warps' partial sums
+    if (warp > 0) {
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        red[warp - 1][c][lane] = PA[c];
+        red[warp - 1][c][32 + lane] = PB[c];
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+      for (int w = 0; w < kWarps - 1; w++)
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          PA[c] += red[w][c][lane];
+          PB[c] += red[w][c][32 + lane];
+        }
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const int it = t ? ib : ia;
+        if (it < li.y) {
+          const int i = li.x + it;
+          const double* P = t ? PB : PA;
+          pot[i] = coef * P[0];
+          if (KER == FMMB_LAPLACE_G && grad) {
+            grad[i] = -coef * P[1];
+            grad[ni + i] = -coef * P[2];
+            grad[2 * (size_t)ni + i] = -coef * P[3];
           }
         }
       }
     }
-    // combine the two halves
     __syncthreads();
-    if (half) {
-      red[0][t] = P;
-      if (KER == FMMB_LAPLACE_G) {
-        red[1][t] = FX;
-        red[2][t] = FY;
-        red[3][t] = FZ;
-      }
-    }
-    __syncthreads();
-    if (!half && act) {
-      pot[i] = coef * (P + red[0][t]);
-      if (KER == FMMB_LAPLACE_G && grad) {
-        grad[i] = -coef * (FX + red[1][t]);
-        grad[ni + i] = -coef * (FY + red[2][t]);
-        grad[2 * ni + i] = -coef * (FZ + red[3][t]);
-      }
-    }
   }
 }
 
