@@ -79,12 +79,26 @@ void upload(DevBuf<double>& d, const std::vector<double>& h, cudaStream_t s) {
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
+// Doubles per operator in the transposed M2M/L2L arrays: K*K rounded up to a
+// 16-byte multiple, so each operator can be bulk-copied.
+size_t pair_op_stride(int K) { return ((size_t)K * K + 1) & ~(size_t)1; }
+
 void upload_static_ops(fmmb_plan* pl) {
   const Operators& o = pl->ops;
   cudaStream_t s = pl->st.main;
   upload(pl->d_fac, o.fac, s);
-  upload(pl->d_m2m, o.m2m, s);
-  upload(pl->d_l2l, o.l2l, s);
+  const int K = pl->K;
+  const size_t ostride = pair_op_stride(K);
+  auto transposed = [&](const std::vector<double>& a) {  // [op][r][c] -> [op][c][r], op stride ostride
+    const size_t nop = a.size() / ((size_t)K * K);
+    std::vector<double> t(nop * ostride, 0.0);
+    for (size_t op = 0; op < nop; op++)
+      for (int r = 0; r < K; r++)
+        for (int c = 0; c < K; c++) t[op * ostride + (size_t)c * K + r] = a[(op * K + r) * K + c];
+    return t;
+  };
+  upload(pl->d_m2m_t, transposed(o.m2m), s);
+  upload(pl->d_l2l_t, transposed(o.l2l), s);
   pl->d_slot_rel.alloc(o.slot_rel.size());
   FMMB_CUDA(cudaMemcpyAsync(pl->d_slot_rel.get(), o.slot_rel.data(), o.slot_rel.size() * sizeof(int), cudaMemcpyHostToDevice, s));
   pl->d_rel_to_op.alloc(o.rel_to_op.size());
@@ -143,8 +157,14 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       pl->ang_eps = pl->ref ? kEpsF : 0.0;
       pl->pi_ang = pl->ref ? kPiF : M_PI;
       FMMB_CUDA(cudaGetDevice(&pl->device));
-      FMMB_CUDA(cudaStreamCreateWithFlags(&pl->st.main, cudaStreamNonBlocking));
-      FMMB_CUDA(cudaStreamCreateWithFlags(&pl->st.side, cudaStreamNonBlocking));
+      // the far field (main / capture stream) outranks the near field (side
+      // stream): its short dependent launches take SMs first and the P2P
+      // blocks fill the rest
+      int prio_low = 0, prio_high = 0;
+      FMMB_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+      FMMB_CUDA(cudaStreamCreateWithPriority(&pl->st.main, cudaStreamNonBlocking, prio_high));
+      FMMB_CUDA(cudaStreamCreateWithPriority(&pl->st.side, cudaStreamNonBlocking, prio_low));
+      FMMB_CUDA(cudaStreamCreateWithPriority(&pl->st.cap, cudaStreamNonBlocking, prio_high));
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.fork, cudaEventDisableTiming));
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.join, cudaEventDisableTiming));
       for (auto& e : pl->ev) FMMB_CUDA(cudaEventCreate(&e));
@@ -170,8 +190,11 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
 int fmmb_plan_destroy(fmmb_plan* pl) {
   if (!pl) return FMMB_OK;
   cudaDeviceSynchronize();
+  for (auto& g : pl->gexec)
+    if (g) cudaGraphExecDestroy(g);
   if (pl->own_stream && pl->st.main) cudaStreamDestroy(pl->st.main);
   if (pl->st.side) cudaStreamDestroy(pl->st.side);
+  if (pl->st.cap) cudaStreamDestroy(pl->st.cap);
   if (pl->st.fork) cudaEventDestroy(pl->st.fork);
   if (pl->st.join) cudaEventDestroy(pl->st.join);
   for (auto& e : pl->ev)
@@ -199,6 +222,13 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
   return guarded([&] {
     FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
     FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
+    for (int w = 0; w < 2; w++) {  // captured evaluates refer to the old buffers
+      if (pl->gexec[w]) {
+        FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
+        cudaGraphExecDestroy(pl->gexec[w]);
+        pl->gexec[w] = nullptr;
+      }
+    }
     FMMB_REQUIRE(tx && ty && tz && sx && sy && sz, FMMB_ERR_ARG, "null coordinates");
     FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNI || (tnx && tny && tnz), FMMB_ERR_ARG, "Gni needs target normals");
     FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNJ || (snx && sny && snz), FMMB_ERR_ARG, "Gnj needs source normals");
@@ -272,26 +302,79 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
     pl->m2m_list.alloc(m2m_list.size());
     FMMB_CUDA(cudaMemcpy(pl->m2m_list.get(), m2m_list.data(), m2m_list.size() * sizeof(int), cudaMemcpyHostToDevice));
     pl->m2l_tiles.clear();
-    pl->m2m_tiles.clear();
-    pl->l2l_tiles.clear();
     for (int lev = 0; lev <= pl->lmax; lev++) {
-      std::vector<std::vector<int>> by_oct(8), all(1);
+      std::vector<std::vector<int>> by_oct(8);
       if (lev >= 2)
         for (int b = 0; b < pl->nbox_i[lev]; b++) by_oct[keys[pl->off_i[lev] + b] & 7].push_back(pl->off_i[lev] + b);
       pl->m2l_tiles.push_back(make_tiles(by_oct, kM2LSlots, [&](int box, int sl) {
         if (lst[(size_t)box * kM2LSlots + sl] < 0) return -1;
         return pl->ops.rel_to_op[pl->ops.slot_rel[(keys[box] & 7) * kM2LSlots + sl]];
       }));
-      pl->l2l_tiles.push_back(make_tiles(lev >= 3 ? by_oct : std::vector<std::vector<int>>(), 1,
-                                         [&](int box, int) { return keys[box] & 7; }));
-      if (lev >= 2 && lev < pl->lmax)
-        for (int b = 0; b < pl->nbox_j[lev]; b++) all[0].push_back(pl->off_j[lev] + b);
-      pl->m2m_tiles.push_back(make_tiles(all, 8, [&](int box, int sl) { return m2m_list[(size_t)box * 8 + sl] >= 0 ? sl : -1; }));
     }
-    // tensor-core translations (mixed precision, K <= 128): operator images,
-    // split buffers with their tensor maps, and the work items of M2L (all
-    // levels), M2M and L2L (per level)
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
+    pl->nsm = dev_sms;
+    // M2M / L2L pair tiles: {operator = child octant, input row, output row},
+    // grouped by operator, tiles of tp pairs
+    {
+      using P3 = std::array<int, 3>;
+      auto pair_job = [&](std::vector<P3>& pairs) {
+        std::unique_ptr<fmmb_plan::PairJob> job(new fmmb_plan::PairJob());
+        std::stable_sort(pairs.begin(), pairs.end(), [](const P3& x, const P3& y) { return x[0] < y[0]; });
+        const int tp = pairs_f64_tile(pl->K, (int)pairs.size(), dev_sms);
+        std::vector<int> top, tsrc, tdst;
+        for (size_t i = 0; i < pairs.size();) {
+          size_t j = i;
+          while (j < pairs.size() && pairs[j][0] == pairs[i][0]) j++;
+          for (size_t k = i; k < j; k += tp) {
+            top.push_back(pairs[i][0]);
+            for (int c = 0; c < tp; c++) {
+              tsrc.push_back(k + c < j ? pairs[k + c][1] : -1);
+              tdst.push_back(k + c < j ? pairs[k + c][2] : -1);
+            }
+          }
+          i = j;
+        }
+        job->ntile = (int)top.size();
+        job->tp = tp;
+        auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+          d.alloc(h.size());
+          if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+        };
+        up(job->tile_op, top);
+        up(job->tile_src, tsrc);
+        up(job->tile_dst, tdst);
+        return job;
+      };
+      std::vector<int> par_i(pl->tot_i);
+      FMMB_CUDA(cudaMemcpy(par_i.data(), pl->parent_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
+      pl->m2m_pairs.clear();
+      pl->l2l_pairs.clear();
+      for (int lev = 0; lev <= pl->lmax; lev++) {
+        std::vector<P3> up_pairs, down_pairs;
+        if (lev >= 2 && lev < pl->lmax)
+          for (int b = 0; b < pl->nbox_j[lev]; b++) {
+            const int box = pl->off_j[lev] + b;
+            for (int sl = 0; sl < 8; sl++) {
+              const int c = m2m_list[(size_t)box * 8 + sl];
+              if (c >= 0) up_pairs.push_back({sl, pl->off_j[lev + 1] + c, box});
+            }
+          }
+        if (lev >= 3)
+          for (int b = 0; b < pl->nbox_i[lev]; b++) {
+            const int box = pl->off_i[lev] + b;
+            down_pairs.push_back({keys[box] & 7, pl->off_i[lev - 1] + par_i[box], box});
+          }
+        pl->m2m_pairs.push_back(pair_job(up_pairs));
+        pl->l2l_pairs.push_back(pair_job(down_pairs));
+      }
+    }
+    // tensor-core M2L (mixed precision, K <= 128): operator images, the TF32
+    // split of M, and the pair tiles of all levels
     pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= 128;
+    init_fac32();
+    prepare_translate_pairs_f64();
+    if (pl->use_tc) prepare_translate_tc();
     if (pl->use_tc) {
       const int K = pl->K;
       auto upload_img = [&](DevBuf<float>& d, const std::vector<double>& mats, int nmat) {
@@ -302,17 +385,11 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
       };
       if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_img_m2l.get() == nullptr) {
         upload_img(pl->d_img_m2l, pl->ops.m2l, pl->ops.m2l_sets * 316);
-        upload_img(pl->d_img_m2m, pl->ops.m2m, 8);
-        upload_img(pl->d_img_l2l, pl->ops.l2l, 8);
         pl->opimg_sets = pl->ops.m2l_sets;
         pl->opimg_rd = pl->ops.m2l_rd;
       }
       pl->Mtf.alloc((size_t)pl->tot_j * 256);
-      pl->Ltf.alloc((size_t)pl->tot_i * 256);
-      int dev_sms = 148;
-      cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, pl->device);
       const int TT = tc_tile();
-      pl->nsm = dev_sms;
       auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
         d.alloc(h.size());
         if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -378,33 +455,6 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         }
         build_job(pl->tc_m2l, pairs, true);
       }
-      pl->tc_m2m.clear();
-      pl->tc_l2l.clear();
-      std::vector<int> par_i(pl->tot_i);
-      FMMB_CUDA(cudaMemcpy(par_i.data(), pl->parent_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
-      for (int lev = 0; lev <= pl->lmax; lev++) {
-        pl->tc_m2m.emplace_back(new fmmb_plan::TcJob());
-        pl->tc_l2l.emplace_back(new fmmb_plan::TcJob());
-        if (lev >= 2 && lev < pl->lmax) {  // M2M into parents at lev: operator = child octant
-          std::vector<Pair> pairs;
-          for (int b = 0; b < pl->nbox_j[lev]; b++) {
-            const int box = pl->off_j[lev] + b;
-            for (int sl = 0; sl < 8; sl++) {
-              const int c = m2m_list[(size_t)box * 8 + sl];
-              if (c >= 0) pairs.push_back({sl, pl->off_j[lev + 1] + c, box});
-            }
-          }
-          build_job(*pl->tc_m2m[lev], pairs, false);
-        }
-        if (lev >= 3) {  // L2L into children at lev (one pair per child): operator = child octant
-          std::vector<Pair> pairs;
-          for (int b = 0; b < pl->nbox_i[lev]; b++) {
-            const int box = pl->off_i[lev] + b;
-            pairs.push_back({keys[box] & 7, pl->off_i[lev - 1] + par_i[box], box});
-          }
-          build_job(*pl->tc_l2l[lev], pairs, false);
-        }
-      }
     }
     // inverse target permutation (caller -> sorted) for the direct sum
     {
@@ -439,6 +489,12 @@ int split_for(int ntile, int nslots) {
 
 // Brackets one launch with a pair of pool events (phase 0..5 as in
 // fmmb_get_timings); silently stops timing when the pool is exhausted.
+// Records a timing event; while the evaluate is being captured into a graph,
+// as an event-record node (a plain record would only become a dependency).
+cudaError_t time_mark(const fmmb_plan* pl, cudaEvent_t e, cudaStream_t s) {
+  return cudaEventRecordWithFlags(e, s, pl->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+}
+
 struct PhaseTimer {
   fmmb_plan* pl;
   int phase, idx;
@@ -447,13 +503,13 @@ struct PhaseTimer {
     if (pl->ev_used + 2 <= fmmb_plan::kEvPool) {
       idx = pl->ev_used;
       pl->ev_used += 2;
-      FMMB_CUDA(cudaEventRecord(pl->evp[idx], s));
+      FMMB_CUDA(time_mark(pl, pl->evp[idx], s));
     }
     pl->launches++;
   }
   ~PhaseTimer() {
     if (idx >= 0) {
-      cudaEventRecord(pl->evp[idx + 1], s);
+      time_mark(pl, pl->evp[idx + 1], s);
       pl->ev_phase.push_back({phase, idx});
     }
   }
@@ -471,7 +527,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   // near field on the side stream
   FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
   FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
-  FMMB_CUDA(cudaEventRecord(pl->ev[0], side));
+  FMMB_CUDA(time_mark(pl, pl->ev[0], side));
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
   {
   PhaseTimer tm(pl, 0, side);
@@ -482,11 +538,11 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
                    pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
   }
-  FMMB_CUDA(cudaEventRecord(pl->ev[1], side));
+  FMMB_CUDA(time_mark(pl, pl->ev[1], side));
   FMMB_CUDA(cudaEventRecord(pl->st.join, side));
 
   // far field on the main stream
-  FMMB_CUDA(cudaEventRecord(pl->ev[2], m));
+  FMMB_CUDA(time_mark(pl, pl->ev[2], m));
   const double rb_leaf = (double)(pl->bbox[3] / (float)(1 << lmax));
   {
     PhaseTimer tm(pl, 1, m);
@@ -499,7 +555,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
       launch_p2m_cart(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
                       pl->snrm.get(), qs, pl->d_fac.get(), pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
   }
-  FMMB_CUDA(cudaEventRecord(pl->ev[3], m));
+  FMMB_CUDA(time_mark(pl, pl->ev[3], m));
   // upward pass: parents accumulate their children (levels below lmax start at zero)
   if (lmax > 2)
     FMMB_CUDA(cudaMemsetAsync(pl->M.get() + (size_t)pl->off_j[lmax - 1] * K, 0,
@@ -527,30 +583,34 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     PhaseTimer tm(pl, phase, m);
     launch_split_tf32(n, K, X + (size_t)off * K, Xtf + (size_t)off * 256, m);
   };
-  if (pl->use_tc) {
-    split(pl->M.get(), pl->Mtf.get(), pl->off_j[lmax], pl->nbox_j[lmax], 2);
-    for (int lev = lmax - 1; lev >= 2; lev--) {
-      tc_run(*pl->tc_m2m[lev], pl->d_img_m2m.get(), pl->Mtf.get(), pl->M.get(), 2);
-      split(pl->M.get(), pl->Mtf.get(), pl->off_j[lev], pl->nbox_j[lev], 2);
-    }
-  } else {
-    for (int lev = lmax - 1; lev >= 2; lev--) {
-      PhaseTimer tm(pl, 2, m);
-      const auto& ts = *pl->m2m_tiles[lev];
-      launch_translate_f64(ts.ntile, split_for(ts.ntile, 8), K, 8, ts.boxes.get(), ts.ops.get(), pl->m2m_list.get(),
-                           pl->d_m2m.get(), pl->M.get() + (size_t)pl->off_j[lev + 1] * K, pl->M.get(), m);
-    }
-  }
-  FMMB_CUDA(cudaEventRecord(pl->ev[4], m));
+  auto pairs_run = [&](const fmmb_plan::PairJob& job, const double* opT, const double* xin, double* out, int atomic,
+                       int phase) {
+    if (job.ntile <= 0) return;
+    PhaseTimer tm(pl, phase, m);
+    PairArgs a{};
+    a.ntile = job.ntile;
+    a.tp = job.tp;
+    a.K = K;
+    a.atomic = atomic;
+    a.tile_op = job.tile_op.get();
+    a.tile_src = job.tile_src.get();
+    a.tile_dst = job.tile_dst.get();
+    a.opT = opT;
+    a.ostride = pair_op_stride(K);
+    a.xin = xin;
+    a.out = out;
+    a.err = pl->d_err.get();
+    launch_translate_pairs_f64(a, m);
+  };
+  for (int lev = lmax - 1; lev >= 2; lev--)  // parents at lev from their children (several per parent)
+    pairs_run(*pl->m2m_pairs[lev], pl->d_m2m_t.get(), pl->M.get(), pl->M.get(), 1, 2);
+  if (pl->use_tc) split(pl->M.get(), pl->Mtf.get(), 0, pl->tot_j, 2);  // every level, for the M2L
+  FMMB_CUDA(time_mark(pl, pl->ev[4], m));
   // downward pass: M2L of every level into zeroed locals, then each level
   // adds its parent's translated local (L2L), top down
   FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * K * sizeof(double), m));
   if (pl->use_tc) {
     tc_run(pl->tc_m2l, pl->d_img_m2l.get(), pl->Mtf.get(), pl->L.get(), 3);
-    for (int lev = 3; lev <= lmax; lev++) {
-      split(pl->L.get(), pl->Ltf.get(), pl->off_i[lev - 1], pl->nbox_i[lev - 1], 4);
-      tc_run(*pl->tc_l2l[lev], pl->d_img_l2l.get(), pl->Ltf.get(), pl->L.get(), 4);
-    }
   } else {
     const size_t opsz = (size_t)316 * K * K;
     for (int lev = 2; lev <= lmax; lev++) {
@@ -561,14 +621,9 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                            pl->m2l_list.get(), pl->d_m2l.get() + set * opsz, pl->M.get() + (size_t)pl->off_j[lev] * K,
                            pl->L.get(), m);
     }
-    for (int lev = 3; lev <= lmax; lev++) {
-      PhaseTimer tm(pl, 4, m);
-      const auto& ts = *pl->l2l_tiles[lev];
-      launch_translate_f64(ts.ntile, 1, K, 1, ts.boxes.get(), ts.ops.get(), pl->parent_i.get(), pl->d_l2l.get(),
-                           pl->L.get() + (size_t)pl->off_i[lev - 1] * K, pl->L.get(), m);
-    }
   }
-  FMMB_CUDA(cudaEventRecord(pl->ev[5], m));
+  for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
+    pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);  FMMB_CUDA(time_mark(pl, pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);
     if (pl->ref)
@@ -579,8 +634,57 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                       pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K,
                       pot_far, g_far, pl->ni, m);
   }
-  FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
+  FMMB_CUDA(time_mark(pl, pl->ev[6], m));
   FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));
+}
+
+// One right-hand side through its captured graph: captured on first use
+// after each fmmb_set_geometry (run_one with the plan's private capture stream
+// standing in for the main stream, in thread-local capture mode, the side
+// stream joining through the fork/join events), then replayed with one launch
+// on the main stream (which may be a legacy default stream, where capture is
+// not possible).  A graph that fails to instantiate turns graphs off for the
+// plan and runs the evaluate directly.
+void run_graph(fmmb_plan* pl, bool want_grad) {
+  const int w = want_grad ? 1 : 0;
+  cudaStream_t m = pl->st.main;
+  if (!pl->gexec[w]) {
+    cudaStream_t c = pl->st.cap;
+    FMMB_CUDA(cudaStreamBeginCapture(c, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t graph = nullptr;
+    pl->st.main = c;
+    pl->capturing = true;
+    try {
+      run_one(pl, pl->qs.get(), want_grad);
+    } catch (...) {
+      pl->st.main = m;
+      pl->capturing = false;
+      cudaStreamEndCapture(c, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      throw;
+    }
+    pl->st.main = m;
+    pl->capturing = false;
+    FMMB_CUDA(cudaStreamEndCapture(c, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      pl->use_graph = false;
+      pl->ev_used = 0;
+      pl->ev_phase.clear();
+      run_one(pl, pl->qs.get(), want_grad);
+      return;
+    }
+    pl->gexec[w] = exec;
+    pl->gphase[w] = pl->ev_phase;
+    pl->glaunches[w] = pl->launches;
+  }
+  pl->ev_phase = pl->gphase[w];
+  pl->launches = pl->glaunches[w];
+  FMMB_CUDA(cudaGraphLaunch(pl->gexec[w], m));
 }
 
 template <typename T>
@@ -622,7 +726,10 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
       if (want_grad && !grad_dev) gd = (T*)base;
     }
     for (int r = 0; r < nr; r++) {
-      run_one(pl, pl->qs.get() + (size_t)r * nj, want_grad);
+      if (nr == 1 && pl->use_graph)
+        run_graph(pl, want_grad);
+      else
+        run_one(pl, pl->qs.get() + (size_t)r * nj, want_grad);
       const double* pn = pl->pot_s.get();
       const double* gn = pl->grad_s.get();
       if (sizeof(T) == 4)

@@ -439,8 +439,10 @@ void p2m_f32_launch(int kernel, int nleaf, int p, int K, const int* keys, const 
 }  // namespace
 
 void init_fac32() {
-  static bool done = false;
-  if (done) return;
+  static bool done[64] = {};
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && done[dev]) return;
   float h[21 * 21 + 21] = {};
   for (int n = 0; n <= 20; n++)
     for (int m = 0; m <= n; m++) {
@@ -449,13 +451,12 @@ void init_fac32() {
       h[n * n + n + m] = (float)std::sqrt(f);
     }
   FMMB_CUDA(cudaMemcpyToSymbol(c_fac32, h, sizeof(h)));
-  done = true;
+  if (dev < 64) done[dev] = true;
 }
 
 bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
                     const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
   if (nleaf <= 0) return true;
-  init_fac32();
   if (p <= 8) p2m_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
   else if (p <= 10) p2m_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
   else if (p <= 12) p2m_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);

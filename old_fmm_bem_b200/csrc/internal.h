@@ -96,6 +96,7 @@ void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vect
 
 struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
+  cudaStream_t cap = nullptr;  // private stream the evaluate graphs are captured on
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 
@@ -145,18 +146,27 @@ struct fmmb_plan {
   fmmb::DevBuf<int> child_count_j;
 
   // operators on the device
-  fmmb::DevBuf<double> d_fac, d_m2m, d_l2l, d_m2l;
+  fmmb::DevBuf<double> d_fac, d_m2l;
+  fmmb::DevBuf<double> d_m2m_t, d_l2l_t;    // [8][column][row] (transposed for translate_pairs_f64)
   fmmb::DevBuf<int> d_slot_rel, d_rel_to_op;
   fmmb::DevBuf<float> d_img_m2l;             // [sets*316][4 K-blocks][2][128*32] TF32 images (mixed)
-  fmmb::DevBuf<float> d_img_m2m, d_img_l2l;  // [8][...]
 
   // evaluation buffers
   fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
   fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
-  fmmb::DevBuf<float> Mtf, Ltf;              // [tot][2][128] TF32 hi/lo splits (mixed)
+  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][128] TF32 hi/lo split of M (mixed, M2L input)
   fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
   int* h_err = nullptr;                      // pinned copy, checked by the next call
   bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)
+  // The plan-internal part of a one-right-hand-side evaluate (sorted charges ->
+  // sorted outputs, plan-owned buffers only) captured once per geometry as a
+  // CUDA graph, without / with gradient, with the phase-timer records and the
+  // launch count of the capturing call.
+  bool use_graph = true;
+  bool capturing = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  std::vector<std::pair<int, int>> gphase[2];
+  int glaunches[2] = {0, 0};
   int opimg_sets = 0;
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots
@@ -171,7 +181,13 @@ struct fmmb_plan {
   fmmb::DevBuf<float> tc_y;                                  // pair rows of the M2L launch
   TcJob tc_m2l;                                              // all levels
   int nsm = 148;                                             // SMs of the plan's device
-  std::vector<std::unique_ptr<TcJob>> tc_m2m, tc_l2l;        // per level
+  // FP64 pair tiles of M2M (into parents at a level) and L2L (into children
+  // at a level), index = level
+  struct PairJob {
+    int ntile = 0, tp = 0;
+    fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
+  };
+  std::vector<std::unique_ptr<PairJob>> m2m_pairs, l2l_pairs;
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging
   fmmb::DevBuf<double> stage_d;
@@ -184,7 +200,7 @@ struct fmmb_plan {
     int ntile = 0;
     fmmb::DevBuf<int> boxes, ops;
   };
-  std::vector<std::unique_ptr<TileSet>> m2l_tiles, m2m_tiles, l2l_tiles;  // index = level
+  std::vector<std::unique_ptr<TileSet>> m2l_tiles;  // index = level
   fmmb::DevBuf<int> m2m_list;                                            // [tot_j][8] child (within level) or -1
 };
 

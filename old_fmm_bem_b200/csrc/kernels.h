@@ -58,6 +58,23 @@ void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float
 namespace fmmb {
 // tensor-core translations (translate_tc.cu)
 int tc_tile();
+// FP64 box-pair translations (M2M, L2L): tiles of tp pairs of one operator
+struct PairArgs {
+  int ntile, tp, K, atomic;
+  const int *tile_op, *tile_src, *tile_dst;  // [ntile], [ntile][tp], [ntile][tp]
+  const double* opT;                         // operators transposed, [op][column][row], op stride ostride
+  size_t ostride;                            // K*K rounded up to even (16-byte multiple)
+  const double* xin;                         // input expansions [rows][K]
+  double* out;                               // output expansions [rows][K]
+  int* err;                                  // set to 4 on a timed-out operator copy
+};
+// pairs per tile for npair pairs: enough tiles for the SMs, shared memory <= 48 KB
+int pairs_f64_tile(int K, int npair, int nsm);
+// once per device, before any launch (and outside stream capture)
+void prepare_translate_pairs_f64();
+void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st);
+// constant table of the FP32 P2M, once per device (outside stream capture)
+void init_fac32();
 void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
 struct TcJobArgs {
   int ntile, K;
@@ -68,6 +85,8 @@ struct TcJobArgs {
   float* y;  // pair rows [ntile*128][128] instead of reductions into out (nullptr: reductions)
   int* err;
 };
+// once per device, before any launch (and outside stream capture)
+void prepare_translate_tc();
 void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st);
 // out[rows[w]] += sum of the pair rows y[idx[ptr[w]..ptr[w+1])] (FP64, list order)
 void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int K, double* out,

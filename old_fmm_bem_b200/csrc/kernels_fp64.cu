@@ -553,6 +553,179 @@ void launch_finalize_f64(int n, const int* perm, const double* pn, const double*
   FMMB_CHECK_LAUNCH();
 }
 
+namespace {
+
+// Box-pair translations on the FP64 CUDA cores (M2M, L2L): a block takes a
+// tile of TP pairs sharing one operator, stages their input expansions in
+// shared memory (transposed, [coefficient][pair], row stride TP + 2 against
+// bank conflicts) and forms output coefficient r of the pairs, reading column
+// c of the operator once (opT[op][c][r], consecutive over r) for all of them.
+// STAGED: the whole operator is first brought into shared memory with one
+// bulk copy (orders whose K x K operator fits); otherwise its columns are read
+// from global memory, the next 8 while the current 8 are used.  256 threads:
+// thread t forms row t % 128 for half t / 128 of the pairs.  Outputs are
+// added (atomically when an output row receives several pairs, M2M).
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+template <int TP, bool STAGED>
+__global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
+  extern __shared__ __align__(16) double dsm[];
+  __shared__ __align__(8) uint64_t bar;
+  constexpr int S = TP + 2, TH = TP / 2;
+  const int g = blockIdx.x, K = P.K;
+  const int op = P.tile_op[g];
+  const int* src = P.tile_src + (size_t)g * TP;
+  const int* dst = P.tile_dst + (size_t)g * TP;
+  double* xs = STAGED ? dsm + P.ostride : dsm;
+  const double* T = P.opT + (size_t)op * P.ostride;
+  if (STAGED) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                   "r"((uint32_t)(P.ostride * sizeof(double)))
+                   : "memory");
+      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                       smem_addr(dsm)),
+                   "l"(T), "r"((uint32_t)(P.ostride * sizeof(double))), "r"(smem_addr(&bar))
+                   : "memory");
+    }
+  }
+  for (int e = threadIdx.x; e < K * TP; e += blockDim.x) {
+    const int j = e / K, c = e - j * K;
+    const int sj = src[j];
+    xs[c * S + j] = sj >= 0 ? P.xin[(size_t)sj * K + c] : 0.0;
+  }
+  __syncthreads();
+  if (STAGED) {  // bounded wait for the operator
+    bool done = false;
+    for (unsigned it = 0; it < (1u << 22) && !done; it++) {
+      uint32_t ok;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+          "selp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(ok)
+          : "r"(smem_addr(&bar))
+          : "memory");
+      done = ok != 0;
+    }
+    if (!done) {
+      if (threadIdx.x == 0) atomicExch(P.err, 4);
+      return;  // the copy may still be landing: nothing below reads it
+    }
+    T = dsm;
+  }
+  const int half = threadIdx.x >> 7;
+  const double* xh = xs + half * TH;
+  for (int r = threadIdx.x & 127; r < K; r += 128) {
+    double acc[TH];
+#pragma unroll
+    for (int j = 0; j < TH; j++) acc[j] = 0.0;
+    if (STAGED) {
+#pragma unroll 4
+      for (int c = 0; c < K; c++) {
+        const double t = T[(size_t)c * K + r];
+        const double2* xc = reinterpret_cast<const double2*>(xh + c * S);
+#pragma unroll
+        for (int j2 = 0; j2 < TH / 2; j2++) {
+          const double2 v = xc[j2];
+          acc[2 * j2] = fma(t, v.x, acc[2 * j2]);
+          acc[2 * j2 + 1] = fma(t, v.y, acc[2 * j2 + 1]);
+        }
+      }
+    } else {
+      constexpr int CU = 8;  // operator columns per chunk; the next chunk is loaded while this one is used
+      double tc[CU], tn[CU];
+#pragma unroll
+      for (int u = 0; u < CU; u++) tc[u] = u < K ? __ldg(T + (size_t)u * K + r) : 0.0;
+      for (int c0 = 0; c0 < K; c0 += CU) {
+#pragma unroll
+        for (int u = 0; u < CU; u++) {
+          const int c = c0 + CU + u;
+          tn[u] = c < K ? __ldg(T + (size_t)c * K + r) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < CU; u++) {
+          if (c0 + u < K) {
+            const double2* xc = reinterpret_cast<const double2*>(xh + (c0 + u) * S);
+#pragma unroll
+            for (int j2 = 0; j2 < TH / 2; j2++) {
+              const double2 v = xc[j2];
+              acc[2 * j2] = fma(tc[u], v.x, acc[2 * j2]);
+              acc[2 * j2 + 1] = fma(tc[u], v.y, acc[2 * j2 + 1]);
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < CU; u++) tc[u] = tn[u];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < TH; j++) {
+      const int d = dst[half * TH + j];
+      if (d >= 0) {
+        double* o = P.out + (size_t)d * K + r;
+        if (P.atomic) atomicAdd(o, acc[j]);
+        else *o += acc[j];
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int pairs_f64_tile(int K, int npair, int nsm) {
+  int tp = 32;
+  while (tp > 4 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
+  while (tp > 4 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
+  return tp;
+}
+
+namespace {
+size_t pairs_smem(int K, int tp, size_t ostride, bool staged) {
+  return (staged ? ostride * sizeof(double) : 0) + (size_t)K * (tp + 2) * sizeof(double);
+}
+constexpr size_t kPairsSmemMax = 224 * 1024;  // below the 227 KB opt-in limit, which includes static shared memory
+
+template <int TP>
+void launch_tp(const PairArgs& a, cudaStream_t st) {
+  const bool staged = pairs_smem(a.K, TP, a.ostride, true) <= kPairsSmemMax;
+  if (staged)
+    translate_pairs_f64<TP, true><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride, true), st>>>(a);
+  else
+    translate_pairs_f64<TP, false><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride, false), st>>>(a);
+}
+
+template <int TP>
+void prepare_tp() {
+  FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kPairsSmemMax));
+  FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 48 * 1024));
+}
+}  // namespace
+
+void prepare_translate_pairs_f64() {
+  prepare_tp<32>();
+  prepare_tp<16>();
+  prepare_tp<8>();
+  prepare_tp<4>();
+}
+
+void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
+  if (a.ntile <= 0) return;
+  switch (a.tp) {
+    case 32: launch_tp<32>(a, st); break;
+    case 16: launch_tp<16>(a, st); break;
+    case 8: launch_tp<8>(a, st); break;
+    default: launch_tp<4>(a, st); break;
+  }
+  FMMB_CHECK_LAUNCH();
+}
+
 void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float4* tpos, const float4* tnrm, int nj,
                        const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot, double* grad,
                        cudaStream_t st) {

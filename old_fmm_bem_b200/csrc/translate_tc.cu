@@ -474,9 +474,12 @@ void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_
   FMMB_CHECK_LAUNCH();
 }
 
+void prepare_translate_tc() {
+  FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+}
+
 void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st) {
   if (a.ntile <= 0) return;
-  FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
   tc::Params P{};
   P.K = a.K;
   P.ntile = a.ntile;
