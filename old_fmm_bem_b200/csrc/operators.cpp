@@ -337,28 +337,29 @@ static float tf32_rna_host(float x) {
   return y;
 }
 
-// Translation operators as TF32 (hi, lo) pairs laid out exactly like the
-// tensor-core kernel's shared-memory operand tiles: per operator, per K-block
-// of 32 columns, per part, 128 rows of 128 bytes with the 16-byte chunk c of
-// row r stored at chunk c ^ (r & 7) (K-major SWIZZLE_128B).  Rows/columns >= K
-// are 0.
+// Translation operators as TF32 (hi, lo) pairs for the tensor-core kernel,
+// zero padded to 128 x 128; per operator 2 x 16384 floats:
+//  * hi (TF32 rounding of the FP64 entry) laid out like the kernel's
+//    shared-memory operand tiles: per K-block of 32 columns, 128 rows of 128
+//    bytes with the 16-byte chunk c of row r stored at chunk c ^ (r & 7)
+//    (K-major SWIZZLE_128B), 4 K-blocks;
+//  * lo (TF32 rounding of the remainder) row-major, 128 rows of 128 values,
+//    which the kernel writes into tensor-memory lane r.
 void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vector<float>& img) {
-  const size_t per_op = (size_t)4 * 2 * 128 * 32;
+  const size_t per_op = (size_t)2 * 128 * 128;
   img.assign((size_t)nmat * per_op, 0.0f);
   parallel_for(nmat, [&](int w) {
     const double* T = &mats[(size_t)w * K * K];
     float* out = &img[(size_t)w * per_op];
-    for (int kb = 0; kb < 4; kb++)
-      for (int r = 0; r < 128; r++)
-        for (int j = 0; j < 32; j++) {
-          const int col = kb * 32 + j;
-          const double v = (r < K && col < K) ? T[(size_t)r * K + col] : 0.0;
-          const float hi = tf32_rna_host((float)v);
-          const float lo = tf32_rna_host((float)(v - (double)hi));
-          const size_t pos = (size_t)r * 32 + (size_t)(((j >> 2) ^ (r & 7)) << 2) + (j & 3);
-          out[(size_t)(kb * 2 + 0) * 4096 + pos] = hi;
-          out[(size_t)(kb * 2 + 1) * 4096 + pos] = lo;
-        }
+    for (int r = 0; r < K; r++)
+      for (int col = 0; col < K; col++) {
+        const double v = T[(size_t)r * K + col];
+        const float hi = tf32_rna_host((float)v);
+        const float lo = tf32_rna_host((float)(v - (double)hi));
+        const int kb = col / 32, j = col % 32;
+        out[(size_t)kb * 4096 + (size_t)r * 32 + (size_t)(((j >> 2) ^ (r & 7)) << 2) + (j & 3)] = hi;
+        out[(size_t)4 * 4096 + (size_t)r * 128 + col] = lo;
+      }
   });
 }
 

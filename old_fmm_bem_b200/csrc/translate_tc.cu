@@ -18,13 +18,15 @@
 // the K coefficients of one pair only; the sum over pairs is FP64.
 //
 // A persistent CTA takes a contiguous range of tiles, so consecutive tiles
-// mostly share their operator: the operator (4 K-blocks x hi/lo, 128 KB)
-// stays resident in shared memory and is reloaded (bulk copies) only when the
-// operator changes.  The input columns stream through a 3-stage ring, one
-// K-block (hi + lo, 32 KB) per stage, gathered with cp.async by three
-// producer groups (group s fills ring slot s), so up to three stages are in
-// flight while the tensor core works.  Two TMEM accumulators alternate
-// between the MMA warp and the four epilogue warps.
+// mostly share their operator, which stays resident and is reloaded by the
+// epilogue warps only when it changes: its hi part in shared memory (4
+// K-blocks, 64 KB, one bulk copy each), its lo part in tensor memory (lane =
+// output coefficient, 128 columns), so the A_lo.B_hi product reads A from
+// tensor memory and shared memory keeps room for a 5-stage ring of input
+// K-blocks (hi + lo, 32 KB each).  Five producer groups (group s fills ring
+// slot s) gather the input rows with cp.async, so up to five stages are in
+// flight while the tensor core works.  Tensor memory (512 columns): three
+// alternating FP32 accumulators (MMA warp / four epilogue warps) and A_lo.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -40,15 +42,20 @@ constexpr int kTile = 128;        // pairs per tile (MMA N)
 constexpr int kRows = 128;        // output coefficients (MMA M), K <= 128
 constexpr int kKB = 32;           // TF32 values per K-block (128 bytes)
 constexpr int kNKB = 4;           // K-blocks (K padded to 128)
-constexpr int kStages = 3;        // input ring
+constexpr int kStages = 5;        // input ring
 constexpr int kHalf = kTile * 128;                  // one 128 x 128-byte K-block tile (16 KB)
-constexpr int kABytes = kNKB * 2 * kHalf;           // resident operator, hi/lo per K-block (128 KB)
+constexpr int kABytes = kNKB * kHalf;               // resident operator hi part (64 KB)
 constexpr int kStageBytes = 2 * kHalf;              // input K-block, hi and lo (32 KB)
-constexpr int kBarBytes = 128;
+constexpr int kBarBytes = 256;                      // 18 mbarriers + the TMEM address
 constexpr int kSmemBytes = kABytes + kStages * kStageBytes + kBarBytes + 1024;
-constexpr int kProducerWarps = 4 * kStages;         // one 128-thread group per ring slot
-constexpr int kThreads = 32 * (5 + kProducerWarps); // 4 epilogue + 1 MMA + producers
-constexpr int kTmemCols = 2 * kTile;                // two alternating FP32 accumulators
+constexpr int kGroupWarps = 2;                      // producer warps per ring slot
+constexpr int kGroupThreads = 32 * kGroupWarps;
+constexpr int kThreads = 32 * (5 + kStages * kGroupWarps);  // 4 epilogue + 1 MMA + producers
+constexpr int kTmemCols = 512;
+constexpr int kNAcc = 3;                            // alternating FP32 accumulators
+constexpr int kColAlo = 2 * kTile;                  // operator lo part
+__host__ __device__ constexpr int acc_col(int b) { return b < 2 ? b * kTile : 3 * kTile; }  // around A_lo
+constexpr int kImgFloats = 2 * kRows * kKB * kNKB;  // per operator: hi image (swizzled) + lo rows
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
 
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major,
@@ -112,6 +119,24 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(kIdesc), "r"(accumulate)
       : "memory");
+}
+
+// D (+)= A . B with A read from tensor memory (lane = row, one TF32 per column).
+__device__ __forceinline__ void mma_tf32_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(db), "r"(kIdesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
@@ -185,25 +210,57 @@ struct Params {
   const int* tile_op;     // [ntile] operator of each tile (tiles sorted by operator)
   const int* tile_src;    // [ntile][128] input row of each pair (-1 = empty column)
   const int* tile_dst;    // [ntile][128] output row of each pair (-1 = empty column)
-  const float* opimg;     // operator images [ops][4 K-blocks][2][128*32]
+  const float* opimg;     // operators [ops][kImgFloats]: hi K-block images, then lo rows [128][128]
   const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
   double* out;            // FP64 expansions, [rows][K]
   float* y;               // when set: column j of tile g goes to y[(g*128 + j)*128 + row] instead
   int* err;               // set to a nonzero code on timeout
 };
 
+// The epilogue warps make operator `op` resident: thread 0 bulk-copies the hi
+// images into shared memory (their bytes counted on a_full), every thread
+// writes its row of the lo part into tensor memory, then arrives on a_full.
+__device__ __forceinline__ void load_operator(const Params& P, int op, int row, uint32_t lane_base,
+                                              unsigned char* sA, uint64_t* a_full) {
+  const float* img = P.opimg + (size_t)op * kImgFloats;
+  if (row == 0) {
+    mbar_expect_tx(a_full, kABytes);
+    for (int c = 0; c < kNKB; c++) bulk_g2s(sA + c * kHalf, img + (size_t)c * (kRows * kKB), kHalf, a_full);
+  }
+  const float4* lo = reinterpret_cast<const float4*>(img + kNKB * kRows * kKB + (size_t)row * kRows);
+#pragma unroll 1
+  for (int c = 0; c < kNKB; c += 2) {  // two chunks of 32 columns per batch of loads
+    uint32_t r[2][32];
+#pragma unroll
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        const float4 v = __ldg(lo + (c + u) * 8 + q);
+        r[u][4 * q] = __float_as_uint(v.x);
+        r[u][4 * q + 1] = __float_as_uint(v.y);
+        r[u][4 * q + 2] = __float_as_uint(v.z);
+        r[u][4 * q + 3] = __float_as_uint(v.w);
+      }
+#pragma unroll
+    for (int u = 0; u < 2; u++) tmem_st32(lane_base + (uint32_t)(kColAlo + (c + u) * 32), r[u]);
+  }
+  tmem_wait_st();
+  tc_fence_before();
+  mbar_arrive(a_full);
+}
+
 __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* sA = smem;                       // resident operator
+  unsigned char* sA = smem;                       // resident operator, hi part
   unsigned char* sB = smem + kABytes;             // input ring
   uint64_t* full = (uint64_t*)(sB + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
-  uint64_t* accf = empty + kStages;  // [2] accumulator b holds a finished tile
-  uint64_t* acce = accf + 2;         // [2] accumulator b read out by the epilogue
-  uint64_t* a_full = acce + 2;       // operator image landed
-  uint64_t* a_free = a_full + 1;     // MMAs reading the previous operator done
-  uint32_t* tmem_slot = (uint32_t*)(a_free + 1);
+  uint64_t* accf = empty + kStages;  // [kNAcc] accumulator b holds a finished tile
+  uint64_t* acce = accf + kNAcc;     // [kNAcc] accumulator b read out by the epilogue
+  uint64_t* a_full = acce + kNAcc;   // operator resident (hi bytes landed, lo rows written)
+  uint64_t* drain = a_full + 1;      // all MMAs done (before tensor memory is freed)
+  uint32_t* tmem_slot = (uint32_t*)(drain + 1);
   __shared__ int sh_fail;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -215,16 +272,24 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   if (threadIdx.x == 0) {
     sh_fail = 0;
     for (int s = 0; s < kStages; s++) {
-      mbar_init(&full[s], 128);  // the 128 producers of ring slot s
-      mbar_init(&empty[s], 1);   // one tcgen05.commit
+      mbar_init(&full[s], kGroupThreads);  // the producers of ring slot s
+      mbar_init(&empty[s], 1);             // one tcgen05.commit
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kNAcc; b++) {
       mbar_init(&accf[b], 1);    // tcgen05.commit after a tile's MMAs
       mbar_init(&acce[b], 128);  // every epilogue thread after reading the tile
     }
-    mbar_init(a_full, 1);        // expect_tx arrival + operator bytes
-    mbar_init(a_free, 1);        // tcgen05.commit
+    mbar_init(a_full, 128);      // every epilogue thread (+ the hi bytes)
+    mbar_init(drain, 1);         // tcgen05.commit
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    // this CTA's pair lists and operator images, into L2 ahead of their use
+    prefetch_l2(P.tile_src + (size_t)t_begin * kTile, (uint32_t)(ntile * kTile * sizeof(int)));
+    prefetch_l2(P.tile_dst + (size_t)t_begin * kTile, (uint32_t)(ntile * kTile * sizeof(int)));
+    for (int i = 0, prev = -1; i < ntile; i++) {
+      const int op = P.tile_op[t_begin + i];
+      if (op != prev) prefetch_l2(P.opimg + (size_t)op * kImgFloats, (uint32_t)(kImgFloats * sizeof(float)));
+      prev = op;
+    }
   }
   if (warp == 4) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -238,12 +303,15 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
 
   if (warp >= 5) {
     // ------------------------------------------------ producers
-    // group s (128 threads) fills ring slot s for stages s, s+3, s+6, ...;
-    // thread pt gathers column pt (hi and lo parts of one K-block).
-    const int grp = (warp - 5) >> 2;
-    const int pt = threadIdx.x - 160 - grp * 128;
-    unsigned char* bhi = sB + grp * kStageBytes;
-    unsigned char* blo = bhi + kHalf;
+    // group s (2 warps) fills ring slot s for stages s, s+5, s+10, ...  A
+    // stage is 128 input rows x (hi, lo) x 128 bytes; one warp instruction
+    // copies two rows: lanes 0-7 the hi line of the first row, 8-15 its lo
+    // line, 16-31 the same for the second, so it touches four whole lines.
+    const int grp = (warp - 5) / kGroupWarps;
+    const int gw = (warp - 5) % kGroupWarps;
+    const int part = (lane >> 3) & 1, chunk = lane & 7;
+    constexpr int kRowsPerThread = kTile / (2 * kGroupWarps);  // 32
+    unsigned char* bdst = sB + grp * kStageBytes + part * kHalf;
     for (int st = grp; st < nstage_total; st += kStages) {
       const uint32_t ph = (st / kStages) & 1;
       bool ok = true;
@@ -253,21 +321,18 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
       if (!ok || *(volatile int*)&sh_fail) break;
       const int g = t_begin + st / kNKB;
       const int kb = st % kNKB;
-      const int src = P.tile_src[(size_t)g * kTile + pt];
-      if (src >= 0) {
-        const float* x = P.xin + (size_t)src * 256 + kb * kKB;
+      const int* tsrc = P.tile_src + (size_t)g * kTile;
+      int src[kRowsPerThread];
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-          cp_async16(bhi + swz(pt, c), x + 4 * c);
-          cp_async16(blo + swz(pt, c), x + 128 + 4 * c);
-        }
-      } else {
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int k = 0; k < kRowsPerThread; k++) src[k] = __ldg(tsrc + k * 2 * kGroupWarps + gw * 2 + (lane >> 4));
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-          *reinterpret_cast<float4*>(bhi + swz(pt, c)) = z;
-          *reinterpret_cast<float4*>(blo + swz(pt, c)) = z;
-        }
+      for (int k = 0; k < kRowsPerThread; k++) {
+        const int r = k * 2 * kGroupWarps + gw * 2 + (lane >> 4);
+        unsigned char* d = bdst + swz(r, chunk);
+        if (src[k] >= 0)
+          cp_async16(d, P.xin + (size_t)src[k] * 256 + part * 128 + kb * kKB + 4 * chunk);
+        else
+          *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       cp_async_commit();
       cp_async_wait<0>();
@@ -276,34 +341,23 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     }
     cp_async_wait<0>();
   } else if (warp == 4) {
-    // ------------------------------------------------ MMA issuer (+ operator loads)
+    // ------------------------------------------------ MMA issuer
     bool ok = true;
     int cur_op = -1, nload = 0;
     for (int i = 0; i < ntile && ok; i++) {
       const int g = t_begin + i;
-      const int buf = i & 1;
-      const uint32_t dcol = tmem + (uint32_t)(buf * kTile);
+      const int buf = i % kNAcc;
+      const uint32_t dcol = tmem + (uint32_t)acc_col(buf);
       const int op = P.tile_op[g];
-      if (op != cur_op) {  // reload the resident operator once the MMAs reading it are done
-        if (lane == 0) {
-          if (nload > 0) {
-            mma_commit(a_free);
-            ok = mbar_wait(a_free, (nload - 1) & 1);
-          }
-          if (ok) {
-            const unsigned char* img = (const unsigned char*)(P.opimg + (size_t)op * kNKB * 2 * (kRows * kKB));
-            mbar_arrive_tx(a_full, kABytes);
-            for (int c = 0; c < kNKB * 2; c++) bulk_g2s(sA + c * kHalf, img + (size_t)c * kHalf, kHalf, a_full);
-            ok = mbar_wait(a_full, nload & 1);
-          }
-        }
+      if (op != cur_op) {  // the epilogue makes each new operator resident once the MMAs using the old one are done
+        if (lane == 0) ok = mbar_wait(a_full, nload & 1);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         if (!ok) break;
         cur_op = op;
         nload++;
       }
-      if (i >= 2) {  // wait until the epilogue has read this accumulator
-        if (lane == 0) ok = mbar_wait(&acce[buf], ((i >> 1) - 1) & 1);
+      if (i >= kNAcc) {  // wait until the epilogue has read this accumulator
+        if (lane == 0) ok = mbar_wait(&acce[buf], (i / kNAcc - 1) & 1);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
         if (!ok) break;
       }
@@ -316,14 +370,15 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
         if (!ok) break;
         tc_fence_after();
         if (lane == 0) {
-          const uint32_t ahi = smem_u32(sA + kb * 2 * kHalf), alo = ahi + kHalf;
+          const uint32_t ahi = smem_u32(sA + kb * kHalf);
+          const uint32_t alo = tmem + (uint32_t)(kColAlo + kb * kKB);
           const uint32_t bhi = smem_u32(sB + s * kStageBytes), blo = bhi + kHalf;
 #pragma unroll
           for (int k = 0; k < kKB / 8; k++) {  // 4 MMAs of K=8 per 32-wide block
-            const uint32_t o = k * 32;           // 8 TF32 = 32 bytes along K
+            const uint32_t o = k * 32;           // 8 TF32 = 32 bytes along K in shared memory
             mma_tf32(dcol, make_desc(ahi + o), make_desc(bhi + o), (kb | k) ? 1u : 0u);
             mma_tf32(dcol, make_desc(ahi + o), make_desc(blo + o), 1u);
-            mma_tf32(dcol, make_desc(alo + o), make_desc(bhi + o), 1u);
+            mma_tf32_ta(dcol, alo + k * 8, make_desc(bhi + o), 1u);
           }
           mma_commit(&empty[s]);  // frees the ring slot when these MMAs are done
           if (kb == kNKB - 1) mma_commit(&accf[buf]);
@@ -333,36 +388,40 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     }
     if (!ok && lane == 0) atomicExch(&sh_fail, 2);
     // drain: every MMA issued above completes before tensor memory is freed
-    if (lane == 0 && nload > 0) {
-      mma_commit(a_free);
-      mbar_wait(a_free, (nload - 1) & 1);
+    if (lane == 0) {
+      mma_commit(drain);
+      mbar_wait(drain, 0);
     }
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
-    // thread `row` owns output coefficient row.  Either column j of a tile is
-    // added into output row tile_dst[j] (lane l holds tile_dst[32h + l],
+    // thread `row` owns output coefficient row (tensor memory lane `row`).  It
+    // makes each new operator resident, then for each tile either adds column
+    // j into output row tile_dst[j] (lane l holds tile_dst[32h + l],
     // broadcast by shuffle) with a predicated FP64 reduction at the L2 -- no
     // branch per column, no read-back -- or, for launches whose outputs
-    // receive many pairs (M2L), the column is stored to its pair row of y.
+    // receive many pairs (M2L), stores the column to its pair row of y.
     const int row = warp * 32 + lane;
     const bool row_ok = row < P.K;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     bool ok = true;
+    if (ntile > 0) load_operator(P, P.tile_op[t_begin], row, lane_base, sA, a_full);
     for (int i = 0; i < ntile; i++) {
       const int g = t_begin + i;
-      const int buf = i & 1;
+      const int buf = i % kNAcc;
       int dl[kTile / 32];
 #pragma unroll
       for (int h = 0; h < kTile / 32; h++) dl[h] = P.tile_dst[(size_t)g * kTile + h * 32 + lane];
-      const bool w = mbar_wait(&accf[buf], (i >> 1) & 1);
+      const bool w = mbar_wait(&accf[buf], (i / kNAcc) & 1);
       ok = __all_sync(0xffffffffu, w && *(volatile int*)&sh_fail == 0) != 0;
       if (!ok) break;
       tc_fence_after();
+      if (i + 1 < ntile && P.tile_op[g + 1] != P.tile_op[g])  // every MMA up to tile i is done
+        load_operator(P, P.tile_op[g + 1], row, lane_base, sA, a_full);
 #pragma unroll
       for (int h = 0; h < kTile / 32; h++) {
         uint32_t v[32];
-        tmem_ld32_nowait(lane_base + (uint32_t)(buf * kTile + h * 32), v);
+        tmem_ld32_nowait(lane_base + (uint32_t)(acc_col(buf) + h * 32), v);
         tmem_wait_ld();
         if (h == kTile / 32 - 1) {  // the accumulator is free once read
           tc_fence_before();
