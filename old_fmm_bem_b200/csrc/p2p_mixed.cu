@@ -35,6 +35,16 @@ constexpr float kFar = 1e18f; // padding sources: r^2 ~ 3e36 stays finite in FP3
 
 __device__ __forceinline__ int pad32(int n) { return (n + 31) & ~31; }
 
+// 1/sqrt(x) from the hardware approximation, subnormal inputs flushed to zero
+// (r^2 is either 0 -- coincident points, handled by the caller -- or far
+// above the subnormal range for any pair of distinct float positions in
+// neighbouring leaves), so no subnormal fix-up instructions are emitted.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 template <int KER>
 struct Acc {
   float p, fx, fy, fz;
@@ -55,7 +65,7 @@ __device__ __forceinline__ void run32(const float4* __restrict__ sp, const float
       Acc<KER>& c = acc[t];
       const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
       const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-      float rinv = rsqrtf(r2);
+      float rinv = rsqrt_ftz(r2);
       if (EXCL) rinv = (r2 > 0.f) ? rinv : 0.f;
       if (KER == FMMB_LAPLACE_G) {
         const float qr = xj.w * rinv;
