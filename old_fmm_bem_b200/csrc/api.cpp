@@ -623,13 +623,17 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     }
   }
   for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
-    pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);  FMMB_CUDA(time_mark(pl, pl->ev[5], m));
+    pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);
+  FMMB_CUDA(time_mark(pl, pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);
     if (pl->ref)
       launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
                  pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
-    else
+    else if (!(pl->cfg.precision == FMMB_MIXED &&
+               launch_l2p_f32(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(),
+                              pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef,
+                              pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m)))
       launch_l2p_cart(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(),
                       pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K,
                       pot_far, g_far, pl->ni, m);

@@ -404,6 +404,163 @@ __global__ void __launch_bounds__(kL2PThreads) l2p_cart(int p, int K, const int*
   }
 }
 
+// FP32 L2P for the mixed form: the same coefficient arrays as l2p_cart
+// (computed in FP64, stored as FP32 pairs), the solid harmonics S_n^m of a
+// point by the P2M recurrence in FP32 registers (fully unrolled to order P),
+// each degree's partial sums in FP32 and promoted to FP64 accumulators.
+constexpr int kL2PF32Threads = 64;
+
+// Shared-memory coefficient read that the compiler may not hoist out of the
+// point loop (hoisting all of them would need hundreds of registers).
+__device__ __forceinline__ float2 lds2(const float2* p) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+               : "=f"(v.x), "=f"(v.y)
+               : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
+  return v;
+}
+__device__ __forceinline__ float lds1(const float* p) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
+  return v;
+}
+
+template <int KER, int P>
+__global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const int* __restrict__ keys,
+                                                          const int2* __restrict__ leaf, const float4* __restrict__ tpos,
+                                                          const float4* __restrict__ tnrm, const double* __restrict__ fac,
+                                                          float xmin, float ymin, float zmin, double rb, double coef,
+                                                          const double* __restrict__ L, double* __restrict__ pot,
+                                                          double* __restrict__ grad, int ni) {
+  constexpr int NT = (P + 1) * (P + 2) / 2;
+  constexpr bool DER = KER != FMMB_LAPLACE_GNJ;  // derivative sums needed
+  __shared__ float2 Cphi[NT], Cz[DER ? NT : 1], Cp[DER ? NT : 1], Cm[DER ? NT : 1];
+  __shared__ float Cs[P + 1];
+  const int b = blockIdx.x;
+  const double* Lb = L + (size_t)b * K;
+  auto Lnm = [&](int n, int m) -> cplx {
+    if (m == 0) return {Lb[n * n], 0.0};
+    return {Lb[n * n + 2 * m - 1], Lb[n * n + 2 * m]};
+  };
+  auto f2 = [](cplx c) { return make_float2((float)c.re, (float)c.im); };
+  for (int idx = threadIdx.x; idx < NT; idx += blockDim.x) {
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= idx) n++;
+    const int m = idx - n * (n + 1) / 2;
+    const double wm = m ? 2.0 : 1.0;
+    Cphi[idx] = n <= p ? f2(cscale(Lnm(n, m), wm * fac[ifull_d(n, m)])) : make_float2(0.f, 0.f);
+    if (DER) {
+      if (n < p) {
+        Cz[idx] = f2(cscale(Lnm(n + 1, m), wm * fac[ifull_d(n + 1, m)] * (n + 1 + m)));
+        Cp[idx] = (m >= 1) ? f2(cscale(Lnm(n + 1, m - 1), (m - 1 ? 2.0 : 1.0) * fac[ifull_d(n + 1, m - 1)]))
+                           : make_float2(0.f, 0.f);
+        Cm[idx] = f2(cscale(Lnm(n + 1, m + 1), -2.0 * fac[ifull_d(n + 1, m + 1)] * (double)(n + m + 2) * (double)(n + m + 1)));
+      } else {
+        Cz[idx] = Cp[idx] = Cm[idx] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  for (int n = threadIdx.x; n <= P; n += blockDim.x) Cs[n] = (n < p) ? (float)(fac[ifull_d(n + 1, 0)] * Lb[(n + 1) * (n + 1)]) : 0.f;
+  __syncthreads();
+  double xc, yc, zc;
+  box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
+  const int2 lf = leaf[b];
+  const double inv_rb = 1.0 / rb;
+  for (int ii = threadIdx.x; ii < lf.y; ii += blockDim.x) {
+    const int i = lf.x + ii;
+    const float4 xt = tpos[i];
+    const float x = (float)(((double)xt.x - xc) * inv_rb), y = (float)(((double)xt.y - yc) * inv_rb),
+                z = (float)(((double)xt.z - zc) * inv_rb);
+    const float r2 = x * x + y * y + z * z;
+    double F = 0, dzr = 0, dpr = 0, dpi = 0, dmr = 0, dmi = 0;
+    float r1re[P + 1], r1im[P + 1], r2re[P + 1], r2im[P + 1];
+#pragma unroll
+    for (int m = 0; m <= P; m++) r1re[m] = r1im[m] = r2re[m] = r2im[m] = 0.f;
+#pragma unroll
+    for (int n = 0; n <= P; n++) {
+      float cre[P + 1], cim[P + 1];
+      float fn = 0.f, zn = 0.f, pr = 0.f, pi = 0.f, mr = 0.f, mi = 0.f;
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        cre[m] = cim[m] = 0.f;
+        if (m > n) continue;
+        if (n == 0) {
+          cre[0] = 1.f;
+        } else if (m == n) {  // S_n^n = -(2n-1) (x + i y) S_{n-1}^{n-1}
+          const float a = -(2.f * n - 1.f);
+          cre[m] = a * (x * r1re[n - 1] - y * r1im[n - 1]);
+          cim[m] = a * (x * r1im[n - 1] + y * r1re[n - 1]);
+        } else if (m == n - 1) {
+          const float a = (2.f * n - 1.f) * z;
+          cre[m] = a * r1re[m];
+          cim[m] = a * r1im[m];
+        } else {
+          const float inv = 1.f / (float)(n - m);
+          const float a = (2.f * n - 1.f) * z * inv, c = (float)(n + m - 1) * r2 * inv;
+          cre[m] = a * r1re[m] - c * r2re[m];
+          cim[m] = a * r1im[m] - c * r2im[m];
+        }
+        const int idx = n * (n + 1) / 2 + m;
+        const float2 cf = lds2(Cphi + idx);
+        fn = fmaf(cf.x, cre[m], fmaf(-cf.y, cim[m], fn));
+        if (DER) {
+          const float2 cz = lds2(Cz + idx), cp = lds2(Cp + idx), cmm = lds2(Cm + idx);
+          zn = fmaf(cz.x, cre[m], fmaf(-cz.y, cim[m], zn));
+          pr = fmaf(cp.x, cre[m], fmaf(-cp.y, cim[m], pr));
+          pi = fmaf(cp.x, cim[m], fmaf(cp.y, cre[m], pi));
+          mr = fmaf(cmm.x, cre[m], fmaf(-cmm.y, cim[m], mr));
+          mi = fmaf(cmm.x, cim[m], fmaf(cmm.y, cre[m], mi));
+          if (m == 1) {  // Cs[n] * conj(S_n^1)
+            const float cs = lds1(Cs + n);
+            mr = fmaf(cs, cre[m], mr);
+            mi = fmaf(-cs, cim[m], mi);
+          }
+        }
+      }
+      F += (double)fn;
+      if (DER) {
+        dzr += (double)zn;
+        dpr += (double)pr;
+        dpi += (double)pi;
+        dmr += (double)mr;
+        dmi += (double)mi;
+      }
+#pragma unroll
+      for (int m = 0; m <= P; m++) {
+        r2re[m] = r1re[m];
+        r2im[m] = r1im[m];
+        r1re[m] = cre[m];
+        r1im[m] = cim[m];
+      }
+    }
+    const double gx = 0.5 * (dpr + dmr), gy = 0.5 * (dpi - dmi), gz = dzr;
+    const double c1 = coef * inv_rb, c2 = coef * inv_rb * inv_rb;
+    if (KER == FMMB_LAPLACE_GNI) {
+      const float4 nv = tnrm[i];
+      pot[i] = -c2 * ((double)nv.x * gx + (double)nv.y * gy + (double)nv.z * gz);
+    } else {
+      pot[i] = c1 * F;
+      if (KER == FMMB_LAPLACE_G && grad) {
+        grad[i] = c2 * gx;
+        grad[ni + i] = c2 * gy;
+        grad[2 * ni + i] = c2 * gz;
+      }
+    }
+  }
+}
+
+template <int P>
+void l2p_f32_launch(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
+                    double* pot, double* grad, int ni, cudaStream_t st) {
+  if (kernel == FMMB_LAPLACE_G)
+    l2p_f32<FMMB_LAPLACE_G, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  else if (kernel == FMMB_LAPLACE_GNI)
+    l2p_f32<FMMB_LAPLACE_GNI, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  else
+    l2p_f32<FMMB_LAPLACE_GNJ, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+}
+
 }  // namespace
 
 void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
@@ -479,6 +636,19 @@ void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const
   else
     l2p_cart<FMMB_LAPLACE_GNJ><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
   FMMB_CHECK_LAUNCH();
+}
+
+bool launch_l2p_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
+                    double* pot, double* grad, int ni, cudaStream_t st) {
+  if (nleaf <= 0) return true;
+  if (p <= 8) l2p_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else if (p <= 10) l2p_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else if (p <= 12) l2p_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else if (p <= 16) l2p_f32_launch<16>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else return false;
+  FMMB_CHECK_LAUNCH();
+  return true;
 }
 
 }  // namespace fmmb

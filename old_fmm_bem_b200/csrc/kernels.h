@@ -38,6 +38,10 @@ void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const
 // returns false when p is outside its range
 bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
                     const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st);
+// FP32 L2P for the mixed form (accurate semantics, p <= 16); false outside its range
+bool launch_l2p_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
+                    double* pot, double* grad, int ni, cudaStream_t st);
 int translate_tile_size();
 // batched FP64 translation (M2L / M2M / L2L), see kernels_fp64.cu
 void launch_translate_f64(int ntile, int nsplit, int K, int nslots, const int* tile_boxes, const int* tile_ops,
