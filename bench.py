@@ -38,6 +38,9 @@ SUBDIV = 6
 LMAX = 5
 METRIC = "FMM matvec Mpts/s (Laplace Gn double-layer BEM, 245,760 pts, p=10)"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+# DRAM bytes (read + write) of one launch on this workload, from the ncu
+# captures summarised in profiles/
+NCU_TRAFFIC = {"p2p_mixed": 13.41e6, "translate_tc": 175.89e6}  # bytes; profiles/p2p_mixed_bem245k_p10.md, profiles/translate_tc_m2l_bem245k_p10.md
 
 
 def measured_peaks():
@@ -49,57 +52,55 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while running."""
+    """Polls the SM clock and the clock-event (throttle) reasons of one GPU
+    through NVML every `period` seconds while the timed region runs (the same
+    counters nvidia-smi's clocks.sm / clocks_event_reasons.* report)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.lines = []
+    def __init__(self, gpu_index, period=0.002):
+        self.gpu, self.period = gpu_index, period
+        self.sm, self.mask, self.smax = [], 0, None
+        self._stop = threading.Event()
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "20"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._poll, daemon=True)
             self.t.start()
         except Exception:
-            self.proc = None
+            self.nv = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll(self):
+        nv = self.nv
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                self.mask |= int(get_reasons(self.h))
+            except Exception:
+                pass
+            time.sleep(self.period)
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self.nv:
+            self.t.join(timeout=2)
             try:
-                self.proc.wait(timeout=5)
+                self.nv.nvmlShutdown()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = sorted(nm for bit, nm in self.REASONS.items() if self.mask & bit)
+        return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax,
+                "reasons": reasons, "samples": len(self.sm), "source": "NVML, 2 ms polling"}
 
 
 def workload(seed):
@@ -241,22 +242,34 @@ def run_ours(args, rank, world):
     st = plan.stats()
     peaks, peak_kind = measured_peaks()
     names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
+    K = (P_ORDER + 1) ** 2
+    # Rooflines of the two dominant kernels, from their CUDA-event durations in
+    # the timed steps above (phase timers on the launching streams).
+    #  * p2p_mixed: 20 flops per algorithmic pair (3 sub, 3 fma for r^2, rsqrt,
+    #    r^-3, the normal dot and the accumulation); bound by the FP32 pipes
+    #    (peak 148 SMs x 128 lanes x 2 flops at the maximum SM clock).
+    #  * M2L (translate_tc + its pair-row reduction): 2 K^2 algorithmic flops per
+    #    box pair on the tensor cores; TF32 peak = half the measured dense bf16.
+    # traffic: DRAM bytes of one launch from ncu (profiles/*.md), or None.
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    p2p_ach = 20.0 * st["p2p_pairs"] / (phase[0] * 1e-3) / 1e12
+    tf32_peak = peaks["bf16_tflops"] / 2
+    m2l_ach = 2.0 * K * K * st["m2l_pairs"] / (phase[3] * 1e-3) / 1e12
+    roof_p2p = {"kernel": "p2p_mixed", "bound": "fp32", "achieved": p2p_ach, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": p2p_ach / fp32_peak, "traffic": NCU_TRAFFIC.get("p2p_mixed"),
+                "ms": float(phase[0]),
+                "note": f"20 flops per algorithmic pair ({st['p2p_pairs']} pairs); peak = nominal FP32 at "
+                        f"{sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)"}
+    roof_m2l = {"kernel": "translate_tc+reduce_pairs (M2L)", "bound": "tensor", "achieved": m2l_ach,
+                "peak": tf32_peak if args.precision == "mixed" else None, "unit": "TFLOP/s",
+                "frac": (m2l_ach / tf32_peak) if args.precision == "mixed" else None,
+                "traffic": NCU_TRAFFIC.get("translate_tc"), "ms": float(phase[3]),
+                "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
+                        f"execute 3 TF32 MMAs per product on 128x128 padded operators; peak = TF32 dense = half of "
+                        f"{peak_kind} bf16"}
     dom = int(np.argmax(phase[:6]))
-    if names[dom] == "m2l":
-        K = (P_ORDER + 1) ** 2
-        flops = 2.0 * K * K * st["m2l_pairs"]
-        achieved = flops / (phase[3] * 1e-3) / 1e12
-        peak = peaks["bf16_tflops"] / 2 if args.precision == "mixed" else None
-        roof = {"kernel": "m2l", "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if peak else None, "traffic": None,
-                "note": f"algorithmic 2*K^2 flops per box pair (K={K}); peak = TF32 dense = half of {peak_kind} bf16"}
-    else:
-        flops = 20.0 * st["p2p_pairs"]
-        achieved = flops / (phase[0] * 1e-3) / 1e12
-        fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12
-        roof = {"kernel": "p2p", "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp32_peak, "traffic": None,
-                "note": "20 flops per pair; peak = 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz (nominal)"}
+    roof = roof_m2l if names[dom] == "m2l" else roof_p2p
     # CPU baseline: the reference's own fmm() on a bounded sample, one core
     cpu = None
     if not args.no_cpu:
@@ -281,6 +294,7 @@ def run_ours(args, rank, world):
         "phase_ms": dict(zip(names + ["total"], [float(v) for v in phase])),
         "stats": st,
         "roofline": roof,
+        "roofline_secondary": roof_p2p if roof is roof_m2l else roof_m2l,
         "cpu_baseline": cpu,
         "e2e": {"value": world * npts / e2e_s / 1e6, "unit": "Mpts/s", "h2d_bytes_per_step": 4 * npts,
                 "d2h_bytes_per_step": 4 * npts},
@@ -294,7 +308,7 @@ def run_ours(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])

@@ -524,22 +524,26 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   double* pot_far = pl->pot_s.get() + pl->ni;
   double* g_near = want_grad ? pl->grad_s.get() : nullptr;
   double* g_far = want_grad ? pl->grad_s.get() + 3 * (size_t)pl->ni : nullptr;
-  // near field on the side stream
-  FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
-  FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
-  FMMB_CUDA(time_mark(pl, pl->ev[0], side));
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
-  {
-  PhaseTimer tm(pl, 0, side);
-  if (pl->cfg.precision == FMMB_MIXED)
-    launch_p2p_mixed(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
-                     pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
-  else
-    launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
-                   pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
-  }
-  FMMB_CUDA(time_mark(pl, pl->ev[1], side));
-  FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+  // near field on the side stream, forked from the main stream once the
+  // tensor-core M2L (which needs whole SMs) has been issued: P2P then fills
+  // the SMs that the latency-bound L2L / L2P launches leave idle
+  auto near_field = [&]() {
+    FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
+    FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
+    FMMB_CUDA(time_mark(pl, pl->ev[0], side));
+    {
+      PhaseTimer tm(pl, 0, side);
+      if (pl->cfg.precision == FMMB_MIXED)
+        launch_p2p_mixed(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
+                         pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+      else
+        launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
+                       pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+    }
+    FMMB_CUDA(time_mark(pl, pl->ev[1], side));
+    FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+  };
 
   // far field on the main stream
   FMMB_CUDA(time_mark(pl, pl->ev[2], m));
@@ -622,6 +626,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                            pl->L.get(), m);
     }
   }
+  near_field();
   for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
     pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));

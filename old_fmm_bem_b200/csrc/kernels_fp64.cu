@@ -593,10 +593,34 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
                    : "memory");
     }
   }
-  for (int e = threadIdx.x; e < K * TP; e += blockDim.x) {
-    const int j = e / K, c = e - j * K;
-    const int sj = src[j];
-    xs[c * S + j] = sj >= 0 ? P.xin[(size_t)sj * K + c] : 0.0;
+  // input expansions of the tile: source rows first, then every element's
+  // load issued before any is stored (one round trip instead of a chain)
+  __shared__ int ssrc[TP];
+  if (threadIdx.x < TP) ssrc[threadIdx.x] = src[threadIdx.x];
+  __syncthreads();
+  {
+    constexpr int kPer = 16;  // elements per thread per round (K*TP <= 16*256 for K <= 128)
+    for (int e0 = 0; e0 < K * TP; e0 += kPer * 256) {
+      double v[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = e0 + u * 256 + threadIdx.x;
+        v[u] = 0.0;
+        if (e < K * TP) {
+          const int j = e / K, c = e - j * K;
+          const int sj = ssrc[j];
+          if (sj >= 0) v[u] = __ldg(P.xin + (size_t)sj * K + c);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = e0 + u * 256 + threadIdx.x;
+        if (e < K * TP) {
+          const int j = e / K, c = e - j * K;
+          xs[c * S + j] = v[u];
+        }
+      }
+    }
   }
   __syncthreads();
   if (STAGED) {  // bounded wait for the operator
