@@ -79,9 +79,10 @@ void upload(DevBuf<double>& d, const std::vector<double>& h, cudaStream_t s) {
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
-// Doubles per operator in the transposed M2M/L2L arrays: K*K rounded up to a
-// 16-byte multiple, so each operator can be bulk-copied.
-size_t pair_op_stride(int K) { return ((size_t)K * K + 1) & ~(size_t)1; }
+// Doubles per operator in the transposed M2M/L2L arrays: K columns of KP = K
+// rounded up to even rows (16-byte aligned row pairs; a 16-byte multiple in
+// all, so each operator can be bulk-copied).
+size_t pair_op_stride(int K) { return (size_t)K * (size_t)((K + 1) & ~1); }
 
 void upload_static_ops(fmmb_plan* pl) {
   const Operators& o = pl->ops;
@@ -89,12 +90,13 @@ void upload_static_ops(fmmb_plan* pl) {
   upload(pl->d_fac, o.fac, s);
   const int K = pl->K;
   const size_t ostride = pair_op_stride(K);
-  auto transposed = [&](const std::vector<double>& a) {  // [op][r][c] -> [op][c][r], op stride ostride
+  const int KP = (K + 1) & ~1;
+  auto transposed = [&](const std::vector<double>& a) {  // [op][r][c] -> [op][c][r], row stride KP
     const size_t nop = a.size() / ((size_t)K * K);
     std::vector<double> t(nop * ostride, 0.0);
     for (size_t op = 0; op < nop; op++)
       for (int r = 0; r < K; r++)
-        for (int c = 0; c < K; c++) t[op * ostride + (size_t)c * K + r] = a[(op * K + r) * K + c];
+        for (int c = 0; c < K; c++) t[op * ostride + (size_t)c * KP + r] = a[(op * K + r) * K + c];
     return t;
   };
   upload(pl->d_m2m_t, transposed(o.m2m), s);
@@ -525,25 +527,36 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   double* g_near = want_grad ? pl->grad_s.get() : nullptr;
   double* g_far = want_grad ? pl->grad_s.get() + 3 * (size_t)pl->ni : nullptr;
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
-  // near field on the side stream, forked from the main stream once the
-  // tensor-core M2L (which needs whole SMs) has been issued: P2P then fills
-  // the SMs that the latency-bound L2L / L2P launches leave idle
-  auto near_field = [&]() {
+  // Near field on the low-priority side stream, in two halves of the target
+  // leaves: the first overlaps the upward pass (P2M / M2M, short dependent
+  // launches that leave SMs idle), the second the downward tail (L2L / L2P);
+  // the tensor-core M2L, which needs whole SMs, runs between them.
+  auto near_field = [&](int l0, int l1, bool last) {
+    if (l1 <= l0) {
+      if (last) FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+      return;
+    }
     FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
     FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
-    FMMB_CUDA(time_mark(pl, pl->ev[0], side));
+    if (l0 == 0) FMMB_CUDA(time_mark(pl, pl->ev[0], side));
     {
       PhaseTimer tm(pl, 0, side);
+      const int2* li = pl->leaf_i.get() + l0;
+      const int* lst = pl->p2p_list.get() + (size_t)l0 * kP2PSlots;
       if (pl->cfg.precision == FMMB_MIXED)
-        launch_p2p_mixed(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
-                         pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+        launch_p2p_mixed(ker, l1 - l0, li, pl->leaf_j.get(), lst, pl->tpos.get(), pl->tnrm.get(), pl->spos.get(),
+                         pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
       else
-        launch_p2p_f64(ker, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
-                       pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+        launch_p2p_f64(ker, l1 - l0, li, pl->leaf_j.get(), lst, pl->tpos.get(), pl->tnrm.get(), pl->spos.get(),
+                       pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
     }
-    FMMB_CUDA(time_mark(pl, pl->ev[1], side));
-    FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+    if (last) {
+      FMMB_CUDA(time_mark(pl, pl->ev[1], side));
+      FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+    }
   };
+  const int p2p_split = nleaf_i / 2;
+  near_field(0, p2p_split, false);
 
   // far field on the main stream
   FMMB_CUDA(time_mark(pl, pl->ev[2], m));
@@ -626,7 +639,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                            pl->L.get(), m);
     }
   }
-  near_field();
+  near_field(p2p_split, nleaf_i, true);
   for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
     pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));

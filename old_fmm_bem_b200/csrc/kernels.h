@@ -66,8 +66,8 @@ int tc_tile();
 struct PairArgs {
   int ntile, tp, K, atomic;
   const int *tile_op, *tile_src, *tile_dst;  // [ntile], [ntile][tp], [ntile][tp]
-  const double* opT;                         // operators transposed, [op][column][row], op stride ostride
-  size_t ostride;                            // K*K rounded up to even (16-byte multiple)
+  const double* opT;                         // operators transposed, [op][column][row], row stride K rounded up to even
+  size_t ostride;                            // doubles per operator: K * (K rounded up to even)
   const double* xin;                         // input expansions [rows][K]
   double* out;                               // output expansions [rows][K]
   int* err;                                  // set to 4 on a timed-out operator copy

@@ -557,14 +557,15 @@ namespace {
 
 // Box-pair translations on the FP64 CUDA cores (M2M, L2L): a block takes a
 // tile of TP pairs sharing one operator, stages their input expansions in
-// shared memory (transposed, [coefficient][pair], row stride TP + 2 against
-// bank conflicts) and forms output coefficient r of the pairs, reading column
-// c of the operator once (opT[op][c][r], consecutive over r) for all of them.
-// STAGED: the whole operator is first brought into shared memory with one
-// bulk copy (orders whose K x K operator fits); otherwise its columns are read
-// from global memory, the next 8 while the current 8 are used.  256 threads:
-// thread t forms row t % 128 for half t / 128 of the pairs.  Outputs are
-// added (atomically when an output row receives several pairs, M2M).
+// shared memory (transposed, [coefficient][pair], row stride TP + 2) and forms
+// the outputs with a register tile per thread of 2 consecutive output rows x
+// J = TP / 4 pairs: per operator column c one 16-byte read of
+// T[c][2rp..2rp+1] and J/2 broadcast reads of the inputs feed 2J FMAs.
+// Thread t takes row pair t % 64 and pair group t / 64.  The transposed operator
+// (opT[op][c][r], row stride KP = K rounded up to even) is first brought into
+// shared memory with one bulk copy when it fits (STAGED), else read from
+// global memory.  Outputs are added (atomically when an output row receives
+// several pairs, M2M).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -573,51 +574,54 @@ template <int TP, bool STAGED>
 __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
   extern __shared__ __align__(16) double dsm[];
   __shared__ __align__(8) uint64_t bar;
-  constexpr int S = TP + 2, TH = TP / 2;
-  const int g = blockIdx.x, K = P.K;
+  __shared__ int ssrc[TP];
+  constexpr int S = TP + 2;
+  constexpr int J = TP / 4 < 2 ? 2 : TP / 4;  // pairs per thread
+  constexpr int G = TP / J;                    // pair groups (4: all 256 threads busy)
+  const int g = blockIdx.x, K = P.K, KP = (K + 1) & ~1;
   const int op = P.tile_op[g];
   const int* src = P.tile_src + (size_t)g * TP;
   const int* dst = P.tile_dst + (size_t)g * TP;
   double* xs = STAGED ? dsm + P.ostride : dsm;
   const double* T = P.opT + (size_t)op * P.ostride;
-  if (STAGED) {
-    if (threadIdx.x == 0) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
-                   "r"((uint32_t)(P.ostride * sizeof(double)))
-                   : "memory");
-      asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                       smem_addr(dsm)),
-                   "l"(T), "r"((uint32_t)(P.ostride * sizeof(double))), "r"(smem_addr(&bar))
-                   : "memory");
-    }
+  if (STAGED && threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                 "r"((uint32_t)(P.ostride * sizeof(double)))
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dsm)),
+                 "l"(T), "r"((uint32_t)(P.ostride * sizeof(double))), "r"(smem_addr(&bar))
+                 : "memory");
   }
-  // input expansions of the tile: source rows first, then every element's
-  // load issued before any is stored (one round trip instead of a chain)
-  __shared__ int ssrc[TP];
+  // input expansions of the tile: warp w copies pairs w, w+8, ..., its lanes
+  // consecutive coefficients (coalesced), all loads of a warp issued before
+  // its stores
   if (threadIdx.x < TP) ssrc[threadIdx.x] = src[threadIdx.x];
   __syncthreads();
   {
-    constexpr int kPer = 16;  // elements per thread per round (K*TP <= 16*256 for K <= 128)
-    for (int e0 = 0; e0 < K * TP; e0 += kPer * 256) {
-      double v[kPer];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    constexpr int kPW = (TP + 7) / 8;  // pairs per warp
+    for (int c0 = 0; c0 < K; c0 += 128) {
+      double v[kPW][4];
 #pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = e0 + u * 256 + threadIdx.x;
-        v[u] = 0.0;
-        if (e < K * TP) {
-          const int j = e / K, c = e - j * K;
-          const int sj = ssrc[j];
-          if (sj >= 0) v[u] = __ldg(P.xin + (size_t)sj * K + c);
+      for (int q = 0; q < kPW; q++) {
+        const int j = w + 8 * q;
+        const int sj = j < TP ? ssrc[j] : -1;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int c = c0 + l + 32 * u;
+          v[q][u] = (sj >= 0 && c < K) ? __ldg(P.xin + (size_t)sj * K + c) : 0.0;
         }
       }
 #pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = e0 + u * 256 + threadIdx.x;
-        if (e < K * TP) {
-          const int j = e / K, c = e - j * K;
-          xs[c * S + j] = v[u];
+      for (int q = 0; q < kPW; q++) {
+        const int j = w + 8 * q;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int c = c0 + l + 32 * u;
+          if (j < TP && c < K) xs[c * S + j] = v[q][u];
         }
       }
     }
@@ -642,58 +646,38 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
     }
     T = dsm;
   }
-  const int half = threadIdx.x >> 7;
-  const double* xh = xs + half * TH;
-  for (int r = threadIdx.x & 127; r < K; r += 128) {
-    double acc[TH];
+  const int grp = threadIdx.x >> 6, rp = threadIdx.x & 63;
+  if (grp >= G) return;
+  const double* xg = xs + grp * J;
+  for (int r0 = 2 * rp; r0 < K; r0 += 128) {
+    double a0[J], a1[J];
 #pragma unroll
-    for (int j = 0; j < TH; j++) acc[j] = 0.0;
-    if (STAGED) {
+    for (int j = 0; j < J; j++) a0[j] = a1[j] = 0.0;
 #pragma unroll 4
-      for (int c = 0; c < K; c++) {
-        const double t = T[(size_t)c * K + r];
-        const double2* xc = reinterpret_cast<const double2*>(xh + c * S);
+    for (int c = 0; c < K; c++) {
+      const double2 t = STAGED ? *reinterpret_cast<const double2*>(T + (size_t)c * KP + r0)
+                               : __ldg(reinterpret_cast<const double2*>(T + (size_t)c * KP + r0));
+      const double2* xc = reinterpret_cast<const double2*>(xg + c * S);
 #pragma unroll
-        for (int j2 = 0; j2 < TH / 2; j2++) {
-          const double2 v = xc[j2];
-          acc[2 * j2] = fma(t, v.x, acc[2 * j2]);
-          acc[2 * j2 + 1] = fma(t, v.y, acc[2 * j2 + 1]);
-        }
-      }
-    } else {
-      constexpr int CU = 8;  // operator columns per chunk; the next chunk is loaded while this one is used
-      double tc[CU], tn[CU];
-#pragma unroll
-      for (int u = 0; u < CU; u++) tc[u] = u < K ? __ldg(T + (size_t)u * K + r) : 0.0;
-      for (int c0 = 0; c0 < K; c0 += CU) {
-#pragma unroll
-        for (int u = 0; u < CU; u++) {
-          const int c = c0 + CU + u;
-          tn[u] = c < K ? __ldg(T + (size_t)c * K + r) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < CU; u++) {
-          if (c0 + u < K) {
-            const double2* xc = reinterpret_cast<const double2*>(xh + (c0 + u) * S);
-#pragma unroll
-            for (int j2 = 0; j2 < TH / 2; j2++) {
-              const double2 v = xc[j2];
-              acc[2 * j2] = fma(tc[u], v.x, acc[2 * j2]);
-              acc[2 * j2 + 1] = fma(tc[u], v.y, acc[2 * j2 + 1]);
-            }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < CU; u++) tc[u] = tn[u];
+      for (int j2 = 0; j2 < J / 2; j2++) {
+        const double2 v = xc[j2];
+        a0[2 * j2] = fma(t.x, v.x, a0[2 * j2]);
+        a0[2 * j2 + 1] = fma(t.x, v.y, a0[2 * j2 + 1]);
+        a1[2 * j2] = fma(t.y, v.x, a1[2 * j2]);
+        a1[2 * j2 + 1] = fma(t.y, v.y, a1[2 * j2 + 1]);
       }
     }
 #pragma unroll
-    for (int j = 0; j < TH; j++) {
-      const int d = dst[half * TH + j];
-      if (d >= 0) {
-        double* o = P.out + (size_t)d * K + r;
-        if (P.atomic) atomicAdd(o, acc[j]);
-        else *o += acc[j];
+    for (int j = 0; j < J; j++) {
+      const int d = dst[grp * J + j];
+      if (d < 0) continue;
+      double* o = P.out + (size_t)d * K + r0;
+      if (P.atomic) {
+        atomicAdd(o, a0[j]);
+        if (r0 + 1 < K) atomicAdd(o + 1, a1[j]);
+      } else {
+        o[0] += a0[j];
+        if (r0 + 1 < K) o[1] += a1[j];
       }
     }
   }
@@ -703,8 +687,8 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
 
 int pairs_f64_tile(int K, int npair, int nsm) {
   int tp = 32;
-  while (tp > 4 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
-  while (tp > 4 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
+  while (tp > 8 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
+  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
   return tp;
 }
 
@@ -736,7 +720,6 @@ void prepare_translate_pairs_f64() {
   prepare_tp<32>();
   prepare_tp<16>();
   prepare_tp<8>();
-  prepare_tp<4>();
 }
 
 void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
@@ -744,8 +727,7 @@ void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
   switch (a.tp) {
     case 32: launch_tp<32>(a, st); break;
     case 16: launch_tp<16>(a, st); break;
-    case 8: launch_tp<8>(a, st); break;
-    default: launch_tp<4>(a, st); break;
+    default: launch_tp<8>(a, st); break;
   }
   FMMB_CHECK_LAUNCH();
 }
