@@ -166,6 +166,26 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------------ accuracy
+def rel_err_vs_direct(ob, kernel, x_t, x_s, q, pot_fmm, grad_fmm=None, n_t=None, n_s=None, ntarget=1024, seed=7):
+    """Relative 2-norm error of FMM potentials (and gradients) at `ntarget`
+    random targets against the FP64 direct sum on the GPU (fmmb_direct_f64,
+    itself checked against the oracle by the test suite), zero-distance pairs
+    excluded and no softening, like the FMM plans measured here."""
+    rng = np.random.default_rng(seed)
+    sel = np.sort(rng.choice(x_t.shape[1], size=min(ntarget, x_t.shape[1]), replace=False))
+    pd = ob.Plan(kernel=kernel, p=4, lmax=2, precision=ob.FP64, semantics=ob.SEM_ACCURATE, exclude_self=True)
+    pd.set_geometry(np.ascontiguousarray(x_t[:, sel]), x_s,
+                    np.ascontiguousarray(n_t[:, sel]) if n_t is not None else None, n_s)
+    vd, gd = pd.direct(q)
+    pd.close()
+    out = {"pot": float(np.linalg.norm(pot_fmm[sel] - vd) / np.linalg.norm(vd)), "targets": int(len(sel))}
+    if grad_fmm is not None and gd is not None:
+        g = grad_fmm.reshape(3, -1)[:, sel]
+        out["grad"] = float(np.linalg.norm(g - gd) / np.linalg.norm(gd))
+    return out
+
+
 # ------------------------------------------------------------------ our arm
 def run_ours(args, rank, world):
     import torch
@@ -239,6 +259,8 @@ def run_ours(args, rank, world):
     if rank != 0:
         plan.close()
         return
+    pot64, _ = plan.evaluate(q, f64=True)
+    err = rel_err_vs_direct(ob, ob.LAPLACE_GNJ, x, x, q, pot64, n_s=n)
     st = plan.stats()
     peaks, peak_kind = measured_peaks()
     names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
@@ -291,6 +313,7 @@ def run_ours(args, rank, world):
                                "points = 245,760 points, p=10, lmax=5, self pairs excluded",
                    "precision": args.precision, "points": npts, "p": P_ORDER, "lmax": LMAX,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "rel_err_vs_fp64_direct": err,
         "phase_ms": dict(zip(names + ["total"], [float(v) for v in phase])),
         "stats": st,
         "roofline": roof,
@@ -305,6 +328,112 @@ def run_ours(args, rank, world):
     plan.close()
 
 
+# ------------------------------------------------------------------ other configurations
+def _timed(step, stream, steps, warmup, flush):
+    """Mean CUDA-event time (ms) of `step` on `stream`, L2 flushed before each."""
+    import torch
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            step()
+    torch.cuda.synchronize()
+    ms = []
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+    return float(np.mean(ms))
+
+
+def uniform_cube(n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.random((3, n), dtype=np.float32), rng.uniform(-1, 1, n).astype(np.float32)
+
+
+def gaussian_clusters(n, seed, nclusters=32, sigma=0.02):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.1, 0.9, (3, nclusters))
+    lab = rng.integers(0, nclusters, n)
+    x = np.clip(c[:, lab] + sigma * rng.standard_normal((3, n)), 0.0, 1.0).astype(np.float32)
+    return x, rng.standard_normal(n).astype(np.float32)
+
+
+def run_c1(args):
+    """Plain Laplace G potential FMM in FP64: 32,768 points uniform in [0,1]^3,
+    charges U[-1,1], p = 8, lmax 3 (64 points per leaf)."""
+    import torch
+    import old_fmm_bem_b200 as ob
+    x, q = uniform_cube(32768, 11)
+    stream = torch.cuda.Stream()
+    plan = ob.Plan(kernel=ob.LAPLACE_G, p=8, lmax=3, precision=ob.FP64, semantics=ob.SEM_ACCURATE, exclude_self=True)
+    plan.set_stream(stream)
+    xd, qd = torch.from_numpy(x).cuda(), torch.from_numpy(q).cuda()
+    plan.set_geometry(xd, xd, bbox=(0, 0, 0, 1))
+    pot = torch.zeros(x.shape[1], device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        ms = _timed(lambda: plan.evaluate(qd, pot), stream, args.steps, max(3, args.warmup), flush)
+    pot64, _ = plan.evaluate(q, f64=True)
+    err = rel_err_vs_direct(ob, ob.LAPLACE_G, x, x, q, pot64)
+    print(json.dumps({"metric": "FMM matvec Mpts/s (Laplace G potential, 32,768 uniform points, p=8, FP64)",
+                      "value": x.shape[1] / (ms * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1, "steps": args.steps,
+                      "ms_per_step": ms, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "Laplace G, 32,768 points U[0,1]^3, q U[-1,1], p=8, lmax=3, FP64, "
+                                             "self pairs excluded"},
+                      "rel_err_vs_fp64_direct": err, "phase_ms": plan.timings(), "clocks": clk.summary()}))
+    plan.close()
+
+
+def run_c3(args):
+    """Adjoint: Laplace G as a torch.autograd operator, 1,048,576 points from 32
+    Gaussian clusters (sigma 0.02) in the unit cube, charges N(0,1), p = 10,
+    lmax 6; one step = forward + backward (gradients w.r.t. charges and
+    positions), mixed and FP64 forms."""
+    import torch
+    import old_fmm_bem_b200 as ob
+    from old_fmm_bem_b200.autograd import FMMOperator
+    x, q = gaussian_clusters(1 << 20, 13)
+    n = x.shape[1]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    w = torch.randn(n, device="cuda", dtype=torch.float64, generator=torch.Generator("cuda").manual_seed(5))
+    res = {}
+    for name, prec in (("mixed", ob.MIXED), ("fp64", ob.FP64)):
+        X = torch.from_numpy(x).cuda().requires_grad_(True)
+        Q = torch.from_numpy(q).cuda().to(torch.float64).requires_grad_(True)
+        op = FMMOperator(X, X, kernel=ob.LAPLACE_G, p=10, lmax=6, precision=prec, bbox=(0, 0, 0, 1))
+        box = {}
+
+        def fwd():
+            box["pot"] = op(Q)
+
+        def fwd_bwd():
+            X.grad = None
+            Q.grad = None
+            (op(Q) * w).sum().backward()
+
+        t_f = _timed(fwd, stream, args.steps, max(3, args.warmup), flush)
+        t_fb = _timed(fwd_bwd, stream, args.steps, max(3, args.warmup), flush)
+        pot = box["pot"].detach().cpu().numpy()
+        field = op.plan.evaluate(q, f64=True)[1]
+        res[name] = {"forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": (t_fb - t_f) / t_f,
+                     "rel_err_vs_fp64_direct": rel_err_vs_direct(ob, ob.LAPLACE_G, x, x, q, pot, field)}
+        op.close()
+    m, f = res["mixed"], res["fp64"]
+    print(json.dumps({"metric": "FMM matvec + adjoint Mpts/s (Laplace G, 1,048,576 clustered points, p=10)",
+                      "value": n / (m["forward_backward_ms"] * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1,
+                      "steps": args.steps, "dtype": "f32+tf32x3+f64", "data": "synthetic",
+                      "config": {"workload": "Laplace G, 1,048,576 points from 32 Gaussian clusters (sigma 0.02) in "
+                                             "[0,1]^3, q N(0,1), p=10, lmax=6; step = forward + backward (charges "
+                                             "and positions)"},
+                      "mixed": m, "fp64": f,
+                      "mixed_speedup_over_fp64": f["forward_backward_ms"] / m["forward_backward_ms"]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -313,6 +442,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m"],
+                    help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "
+                         "points; adjoint1m: forward + backward on 1,048,576 clustered points")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -324,6 +456,10 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.config == "uniform32k":
+        run_c1(args)
+    elif args.config == "adjoint1m":
+        run_c3(args)
     else:
         run_ours(args, rank, world)
     if world > 1 and args.impl == "ours":

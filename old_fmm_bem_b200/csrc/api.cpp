@@ -371,74 +371,78 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         pl->l2l_pairs.push_back(pair_job(down_pairs));
       }
     }
-    // tensor-core M2L (mixed precision, K <= 128): operator images, the TF32
-    // split of M, and the pair tiles of all levels
-    pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= 128;
+    // tensor-core M2L (mixed precision, K <= tc_max_k()): operator images (one
+    // per operator and block of 128 output rows), the TF32 split of M, and
+    // the work items over the pair tiles of all levels
+    pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= tc_max_k();
     init_fac32();
     prepare_translate_pairs_f64();
     if (pl->use_tc) prepare_translate_tc();
     if (pl->use_tc) {
-      const int K = pl->K;
-      auto upload_img = [&](DevBuf<float>& d, const std::vector<double>& mats, int nmat) {
-        std::vector<float> img;
-        build_tc_images(mats, nmat, K, img);
-        d.alloc(img.size());
-        FMMB_CUDA(cudaMemcpy(d.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
-      };
+      const int K = pl->K, kpad = tc_kpad(K), nrb = (K + 127) / 128;
       if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_img_m2l.get() == nullptr) {
-        upload_img(pl->d_img_m2l, pl->ops.m2l, pl->ops.m2l_sets * 316);
+        std::vector<float> img;
+        build_tc_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, kpad, img);
+        pl->d_img_m2l.alloc(img.size());
+        FMMB_CUDA(cudaMemcpy(pl->d_img_m2l.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
         pl->opimg_sets = pl->ops.m2l_sets;
         pl->opimg_rd = pl->ops.m2l_rd;
       }
-      pl->Mtf.alloc((size_t)pl->tot_j * 256);
+      pl->Mtf.alloc((size_t)pl->tot_j * 2 * kpad);
       const int TT = tc_tile();
       auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
         d.alloc(h.size());
         if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
       };
       // box pairs {operator, input row, output row} -> tiles of TT pairs of one
-      // operator each (operators ascending, pairs in output order within one)
+      // operator each (operators ascending, pairs in output order within one);
+      // a work item is a tile and a block of 128 output rows (operator image
+      // op * nrb + block), items of one operator and block consecutive
       using Pair = std::array<int, 3>;
-      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs, bool pair_rows) {
+      auto build_job = [&](fmmb_plan::TcJob& job, std::vector<Pair>& pairs) {
         std::stable_sort(pairs.begin(), pairs.end(), [](const Pair& x, const Pair& y) { return x[0] < y[0]; });
-        std::vector<int> top, tsrc, tdst;
+        std::vector<int> wop, wsrc, wy, tdst;
+        int ntile = 0;
         for (size_t i = 0; i < pairs.size();) {
           size_t j = i;
           while (j < pairs.size() && pairs[j][0] == pairs[i][0]) j++;
-          for (size_t k = i; k < j; k += TT) {
-            top.push_back(pairs[i][0]);
-            for (int c = 0; c < TT; c++) {
-              tsrc.push_back(k + c < j ? pairs[k + c][1] : -1);
-              tdst.push_back(k + c < j ? pairs[k + c][2] : -1);
+          const int t0 = ntile;
+          for (size_t k = i; k < j; k += TT, ntile++)
+            for (int c = 0; c < TT; c++) tdst.push_back(k + c < j ? pairs[k + c][2] : -1);
+          for (int h = 0; h < nrb; h++)
+            for (int t = t0; t < ntile; t++) {
+              const size_t k = i + (size_t)(t - t0) * TT;
+              wop.push_back(pairs[i][0] * nrb + h);
+              for (int c = 0; c < TT; c++) wsrc.push_back(k + c < j ? pairs[k + c][1] : -1);
+              wy.push_back(t * TT);
+              wy.push_back(128 * h);
             }
-          }
           i = j;
         }
-        job.ntile = (int)top.size();
-        up(job.tile_op, top);
-        up(job.tile_src, tsrc);
-        up(job.tile_dst, tdst);
-        job.nred = 0;
-        if (pair_rows) {  // per output row, its pair positions in tile order
-          std::vector<std::array<int, 2>> pos;
-          for (size_t k = 0; k < tdst.size(); k++)
-            if (tdst[k] >= 0) pos.push_back({tdst[k], (int)k});
-          std::sort(pos.begin(), pos.end());
-          std::vector<int> rows, ptr, idx;
-          for (size_t k = 0; k < pos.size(); k++) {
-            if (k == 0 || pos[k][0] != pos[k - 1][0]) {
-              rows.push_back(pos[k][0]);
-              ptr.push_back((int)k);
-            }
-            idx.push_back(pos[k][1]);
+        job.ntile = (int)wop.size();
+        up(job.tile_op, wop);
+        up(job.tile_src, wsrc);
+        up(job.tile_y, wy);
+        // per output row, its pair rows (tile * TT + column)
+        std::vector<std::array<int, 2>> pos;
+        for (size_t k = 0; k < tdst.size(); k++)
+          if (tdst[k] >= 0) pos.push_back({tdst[k], (int)k});
+        std::sort(pos.begin(), pos.end());
+        std::vector<int> rows, ptr, idx;
+        for (size_t k = 0; k < pos.size(); k++) {
+          if (k == 0 || pos[k][0] != pos[k - 1][0]) {
+            rows.push_back(pos[k][0]);
+            ptr.push_back((int)k);
           }
-          ptr.push_back((int)pos.size());
-          job.nred = (int)rows.size();
-          up(job.red_rows, rows);
-          up(job.red_ptr, ptr);
-          up(job.red_idx, idx);
-          pl->tc_y.alloc((size_t)job.ntile * TT * 128);
+          idx.push_back(pos[k][1]);
         }
+        ptr.push_back((int)pos.size());
+        job.nred = (int)rows.size();
+        up(job.red_rows, rows);
+        up(job.red_ptr, ptr);
+        up(job.red_idx, idx);
+        job.ys = 128 * nrb;
+        pl->tc_y.alloc((size_t)ntile * TT * job.ys);
       };
       // M2L, all levels in one job: operator = set(level)*316 + relative position
       {
@@ -455,7 +459,7 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
             }
           }
         }
-        build_job(pl->tc_m2l, pairs, true);
+        build_job(pl->tc_m2l, pairs);
       }
     }
     // inverse target permutation (caller -> sorted) for the direct sum
@@ -584,21 +588,20 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     a.K = K;
     a.tile_op = job.tile_op.get();
     a.tile_src = job.tile_src.get();
-    a.tile_dst = job.tile_dst.get();
+    a.tile_y = reinterpret_cast<const int2*>(job.tile_y.get());
     a.opimg = img;
     a.xin = xin;
-    a.out = out;
-    a.y = job.nred > 0 ? pl->tc_y.get() : nullptr;
+    a.y = pl->tc_y.get();
+    a.ys = job.ys;
     a.err = pl->d_err.get();
     launch_translate_tc(a, pl->nsm, m);
-    if (job.nred > 0) {
-      launch_reduce_pairs(job.nred, job.red_rows.get(), job.red_ptr.get(), job.red_idx.get(), pl->tc_y.get(), K, out, m);
-      pl->launches++;
-    }
+    launch_reduce_pairs(job.nred, job.red_rows.get(), job.red_ptr.get(), job.red_idx.get(), pl->tc_y.get(), job.ys, K,
+                        out, m);
+    pl->launches++;
   };
   auto split = [&](const double* X, float* Xtf, int off, int n, int phase) {
     PhaseTimer tm(pl, phase, m);
-    launch_split_tf32(n, K, X + (size_t)off * K, Xtf + (size_t)off * 256, m);
+    launch_split_tf32(n, K, tc_kpad(K), X + (size_t)off * K, Xtf + (size_t)off * 2 * tc_kpad(K), m);
   };
   auto pairs_run = [&](const fmmb_plan::PairJob& job, const double* opT, const double* xin, double* out, int atomic,
                        int phase) {

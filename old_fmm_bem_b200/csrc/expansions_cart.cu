@@ -614,6 +614,7 @@ void init_fac32() {
 bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
                     const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
   if (nleaf <= 0) return true;
+  if ((size_t)kP2MThreads * K * sizeof(float) > 48 * 1024) return false;  // per-point rows staged in shared memory
   if (p <= 8) p2m_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
   else if (p <= 10) p2m_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
   else if (p <= 12) p2m_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);

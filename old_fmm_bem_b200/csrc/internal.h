@@ -92,7 +92,7 @@ void build_static_operators(Operators& ops, int p, bool ref_semantics);
 // semantics, where the distance carries an absolute eps (needs the root size).
 void build_m2l_operators(Operators& ops, int lmax, float rd);
 // TF32 hi/lo images of nmat K x K operators in the tensor-core operand layout
-void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vector<float>& img);
+void build_tc_images(const std::vector<double>& mats, int nmat, int K, int kpad, std::vector<float>& img);
 
 struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
@@ -154,7 +154,7 @@ struct fmmb_plan {
   // evaluation buffers
   fmmb::DevBuf<float> qs;                    // sorted charges [nrhs][nj]
   fmmb::DevBuf<double> M, L;                 // [tot][K] scaled real-packed
-  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][128] TF32 hi/lo split of M (mixed, M2L input)
+  fmmb::DevBuf<float> Mtf;                   // [tot_j][2][tc_kpad(K)] TF32 hi/lo split of M (mixed, M2L input)
   fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
   int* h_err = nullptr;                      // pinned copy, checked by the next call
   bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)
@@ -170,12 +170,12 @@ struct fmmb_plan {
   int opimg_sets = 0;
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots
-  struct TcJob {  // pair tiles of one tensor-core translation launch (translate_tc.cu)
-    int ntile = 0;
-    fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
-    // when nred > 0 the launch stores pair rows to tc_y and reduce_pairs sums
-    // them per output row: rows, CSR offsets, pair positions (tile*128 + column)
-    int nred = 0;
+  struct TcJob {  // work items of the tensor-core M2L (translate_tc.cu)
+    int ntile = 0;                               // work items (pair tile x block of 128 output rows)
+    fmmb::DevBuf<int> tile_op, tile_src, tile_y; // operator image, input rows, (pair row, row offset)
+    // the launch stores pair rows of ys floats to tc_y and reduce_pairs sums
+    // them per output row: rows, CSR offsets, pair rows (tile*128 + column)
+    int nred = 0, ys = 128;
     fmmb::DevBuf<int> red_rows, red_ptr, red_idx;
   };
   fmmb::DevBuf<float> tc_y;                                  // pair rows of the M2L launch

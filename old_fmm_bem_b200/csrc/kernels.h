@@ -34,8 +34,9 @@ void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const
 void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
                      const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
                      double* pot, double* grad, int ni, cudaStream_t st);
-// FP32 point-per-thread P2M for the mixed form (accurate semantics, p <= 16);
-// returns false when p is outside its range
+// FP32 point-per-thread P2M for the mixed form (accurate semantics, p <= 11:
+// its 64 x K staging must fit 48 KB of shared memory); returns false outside
+// that range
 bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
                     const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st);
 // FP32 L2P for the mixed form (accurate semantics, p <= 16); false outside its range
@@ -79,20 +80,25 @@ void prepare_translate_pairs_f64();
 void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st);
 // constant table of the FP32 P2M, once per device (outside stream capture)
 void init_fac32();
-void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st);
+void launch_split_tf32(int nbox, int K, int kpad, const double* M, float* Mtf, cudaStream_t st);
 struct TcJobArgs {
-  int ntile, K;
-  const int *tile_op, *tile_src, *tile_dst;  // [ntile], [ntile][128], [ntile][128]
-  const float* opimg;
-  const float* xin;  // TF32 split of the inputs [rows][2][128]
-  double* out;
-  float* y;  // pair rows [ntile*128][128] instead of reductions into out (nullptr: reductions)
+  int ntile, K;                 // work items, real coefficients per expansion (<= tc_max_k())
+  const int* tile_op;           // [ntile] operator image per work item
+  const int* tile_src;          // [ntile][128] input rows
+  const int2* tile_y;           // [ntile] (first pair row of y, coefficient offset)
+  const float* opimg;           // operator images, see translate_tc.cu
+  const float* xin;             // TF32 split of the inputs [rows][2][tc_kpad(K)]
+  float* y;                     // pair rows [pairs][ys]
+  int ys;                       // floats per pair row
   int* err;
 };
 // once per device, before any launch (and outside stream capture)
 void prepare_translate_tc();
 void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st);
-// out[rows[w]] += sum of the pair rows y[idx[ptr[w]..ptr[w+1])] (FP64, list order)
-void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int K, double* out,
-                         cudaStream_t st);
+// out[rows[w]] += sum of the pair rows y[idx[ptr[w]..ptr[w+1])] (rows of ys floats; FP64, list order)
+void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int ys, int K,
+                         double* out, cudaStream_t st);
+// K padded for the tensor-core operands (128, or a multiple of 32 up to tc_max_k())
+int tc_kpad(int K);
+int tc_max_k();
 }  // namespace fmmb

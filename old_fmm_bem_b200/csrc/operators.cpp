@@ -338,28 +338,36 @@ static float tf32_rna_host(float x) {
 }
 
 // Translation operators as TF32 (hi, lo) pairs for the tensor-core kernel,
-// zero padded to 128 x 128; per operator 2 x 16384 floats:
+// zero padded to kpad columns; one image per operator and block of 128 output
+// rows (nrb = ceil(K / 128) blocks, image index op * nrb + block), each of
+// 2 x 128 x kpad floats:
 //  * hi (TF32 rounding of the FP64 entry) laid out like the kernel's
 //    shared-memory operand tiles: per K-block of 32 columns, 128 rows of 128
 //    bytes with the 16-byte chunk c of row r stored at chunk c ^ (r & 7)
-//    (K-major SWIZZLE_128B), 4 K-blocks;
-//  * lo (TF32 rounding of the remainder) row-major, 128 rows of 128 values,
+//    (K-major SWIZZLE_128B), kpad / 32 K-blocks;
+//  * lo (TF32 rounding of the remainder) row-major, 128 rows of kpad values,
 //    which the kernel writes into tensor-memory lane r.
-void build_tc_images(const std::vector<double>& mats, int nmat, int K, std::vector<float>& img) {
-  const size_t per_op = (size_t)2 * 128 * 128;
-  img.assign((size_t)nmat * per_op, 0.0f);
+void build_tc_images(const std::vector<double>& mats, int nmat, int K, int kpad, std::vector<float>& img) {
+  const int nrb = (K + 127) / 128, nkb = kpad / 32;
+  const size_t per_img = (size_t)2 * 128 * kpad;
+  img.assign((size_t)nmat * nrb * per_img, 0.0f);
   parallel_for(nmat, [&](int w) {
     const double* T = &mats[(size_t)w * K * K];
-    float* out = &img[(size_t)w * per_op];
-    for (int r = 0; r < K; r++)
-      for (int col = 0; col < K; col++) {
-        const double v = T[(size_t)r * K + col];
-        const float hi = tf32_rna_host((float)v);
-        const float lo = tf32_rna_host((float)(v - (double)hi));
-        const int kb = col / 32, j = col % 32;
-        out[(size_t)kb * 4096 + (size_t)r * 32 + (size_t)(((j >> 2) ^ (r & 7)) << 2) + (j & 3)] = hi;
-        out[(size_t)4 * 4096 + (size_t)r * 128 + col] = lo;
+    for (int blk = 0; blk < nrb; blk++) {
+      float* out = &img[((size_t)w * nrb + blk) * per_img];
+      for (int rr = 0; rr < 128; rr++) {
+        const int r = blk * 128 + rr;
+        if (r >= K) break;
+        for (int col = 0; col < K; col++) {
+          const double v = T[(size_t)r * K + col];
+          const float hi = tf32_rna_host((float)v);
+          const float lo = tf32_rna_host((float)(v - (double)hi));
+          const int kb = col / 32, j = col % 32;
+          out[(size_t)kb * 4096 + (size_t)rr * 32 + (size_t)(((j >> 2) ^ (rr & 7)) << 2) + (j & 3)] = hi;
+          out[(size_t)nkb * 4096 + (size_t)rr * kpad + col] = lo;
+        }
       }
+    }
   });
 }
 

@@ -39,24 +39,33 @@ namespace fmmb {
 namespace tc {
 
 constexpr int kTile = 128;        // pairs per tile (MMA N)
-constexpr int kRows = 128;        // output coefficients (MMA M), K <= 128
+constexpr int kRows = 128;        // output coefficients per work item (MMA M)
 constexpr int kKB = 32;           // TF32 values per K-block (128 bytes)
-constexpr int kNKB = 4;           // K-blocks (K padded to 128)
-constexpr int kStages = 5;        // input ring
 constexpr int kHalf = kTile * 128;                  // one 128 x 128-byte K-block tile (16 KB)
-constexpr int kABytes = kNKB * kHalf;               // resident operator hi part (64 KB)
 constexpr int kStageBytes = 2 * kHalf;              // input K-block, hi and lo (32 KB)
-constexpr int kBarBytes = 256;                      // 18 mbarriers + the TMEM address
-constexpr int kSmemBytes = kABytes + kStages * kStageBytes + kBarBytes + 1024;
+constexpr int kBarBytes = 256;                      // <= 18 mbarriers + the TMEM address
 constexpr int kGroupWarps = 2;                      // producer warps per ring slot
 constexpr int kGroupThreads = 32 * kGroupWarps;
-constexpr int kThreads = 32 * (5 + kStages * kGroupWarps);  // 4 epilogue + 1 MMA + producers
 constexpr int kTmemCols = 512;
-constexpr int kNAcc = 3;                            // alternating FP32 accumulators
-constexpr int kColAlo = 2 * kTile;                  // operator lo part
-__host__ __device__ constexpr int acc_col(int b) { return b < 2 ? b * kTile : 3 * kTile; }  // around A_lo
-constexpr int kImgFloats = 2 * kRows * kKB * kNKB;  // per operator: hi image (swizzled) + lo rows
+constexpr int kMaxNKB = 8;                          // K <= 256 (p <= 15)
 constexpr unsigned kSpinLimit = 1u << 22;           // bounded waits (seconds at most)
+
+// Layout for operators of NKB K-blocks (K padded to 32 NKB): the hi part is
+// resident in shared memory (NKB x 16 KB), the input ring takes what is left
+// of 224 KB; the lo part takes the last 32 NKB tensor-memory columns and the
+// accumulators (128 columns each) the rest.
+template <int NKB>
+struct Cfg {
+  static constexpr int kKPad = NKB * kKB;
+  static constexpr int kABytes = NKB * kHalf;
+  static constexpr int kStages = (224 * 1024 - kABytes) / kStageBytes;
+  static constexpr int kSmemBytes = kABytes + kStages * kStageBytes + kBarBytes + 1024;
+  static constexpr int kThreads = 32 * (5 + kStages * kGroupWarps);  // 4 epilogue + 1 MMA + producers
+  static constexpr int kColAlo = kTmemCols - NKB * kKB;
+  static constexpr int kNAcc = kColAlo / kTile < 3 ? kColAlo / kTile : 3;
+  static constexpr int kImgFloats = 2 * kRows * kKPad;  // hi image (swizzled K-blocks) + lo rows
+  static_assert(kStages >= 2 && kNAcc >= 2, "operator too large for the tensor-core layout");
+};
 
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major,
 // N = 128 (bits 17..22 hold N>>3), M = 128 (bits 24..28 hold M>>4)
@@ -191,69 +200,64 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// out[0] += v at the L2 when pred (fire and forget).
-__device__ __forceinline__ void red_add_f64(double* out, double v, bool pred) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %2, 0;\n\t"
-      "@p red.global.add.f64 [%0], %1;\n\t}" ::"l"(out),
-      "d"(v), "r"((int)pred)
-      : "memory");
-}
-
 // Swizzled byte offset of 16-byte chunk c of row r in a K-block tile.
 __device__ __forceinline__ uint32_t swz(int r, int c) { return (uint32_t)(r * 128 + ((c ^ (r & 7)) << 4)); }
 
 struct Params {
-  int K;                  // real coefficients per expansion (<= 128)
-  int ntile;              // pair tiles
-  const int* tile_op;     // [ntile] operator of each tile (tiles sorted by operator)
+  int ntile;              // work items: (pair tile, row block of the operator)
+  const int* tile_op;     // [ntile] operator image of each work item (sorted)
   const int* tile_src;    // [ntile][128] input row of each pair (-1 = empty column)
-  const int* tile_dst;    // [ntile][128] output row of each pair (-1 = empty column)
-  const float* opimg;     // operators [ops][kImgFloats]: hi K-block images, then lo rows [128][128]
-  const float* xin;       // TF32 split of the inputs [rows][2][128] (hi, lo)
-  double* out;            // FP64 expansions, [rows][K]
-  float* y;               // when set: column j of tile g goes to y[(g*128 + j)*128 + row] instead
+  const int2* tile_y;     // [ntile] (first pair row in y, coefficient offset in the row)
+  const float* opimg;     // operator images [ops][Cfg::kImgFloats]: hi K-block images, then lo rows [128][kKPad]
+  const float* xin;       // TF32 split of the inputs [rows][2][kKPad] (hi, lo)
+  float* y;               // pair rows: column j of work item g goes to y[(tile_y.x + j)*ys + tile_y.y + row]
+  int ys;                 // floats per pair row of y
   int* err;               // set to a nonzero code on timeout
 };
 
-// The epilogue warps make operator `op` resident: thread 0 bulk-copies the hi
-// images into shared memory (their bytes counted on a_full), every thread
-// writes its row of the lo part into tensor memory, then arrives on a_full.
+// The epilogue warps make operator image `op` resident: thread 0 bulk-copies
+// the hi images into shared memory (their bytes counted on a_full), every
+// thread writes its row of the lo part into tensor memory, then arrives.
+template <int NKB>
 __device__ __forceinline__ void load_operator(const Params& P, int op, int row, uint32_t lane_base,
                                               unsigned char* sA, uint64_t* a_full) {
-  const float* img = P.opimg + (size_t)op * kImgFloats;
+  using C = Cfg<NKB>;
+  const float* img = P.opimg + (size_t)op * C::kImgFloats;
   if (row == 0) {
-    mbar_expect_tx(a_full, kABytes);
-    for (int c = 0; c < kNKB; c++) bulk_g2s(sA + c * kHalf, img + (size_t)c * (kRows * kKB), kHalf, a_full);
+    mbar_expect_tx(a_full, C::kABytes);
+    for (int c = 0; c < NKB; c++) bulk_g2s(sA + c * kHalf, img + (size_t)c * (kRows * kKB), kHalf, a_full);
   }
-  const float4* lo = reinterpret_cast<const float4*>(img + kNKB * kRows * kKB + (size_t)row * kRows);
+  const float4* lo = reinterpret_cast<const float4*>(img + NKB * kRows * kKB + (size_t)row * C::kKPad);
 #pragma unroll 1
-  for (int c = 0; c < kNKB; c += 2) {  // two chunks of 32 columns per batch of loads
+  for (int c = 0; c < NKB; c += 2) {  // two chunks of 32 columns per batch of loads
     uint32_t r[2][32];
 #pragma unroll
     for (int u = 0; u < 2; u++)
 #pragma unroll
       for (int q = 0; q < 8; q++) {
-        const float4 v = __ldg(lo + (c + u) * 8 + q);
+        const float4 v = c + u < NKB ? __ldg(lo + (c + u) * 8 + q) : make_float4(0.f, 0.f, 0.f, 0.f);
         r[u][4 * q] = __float_as_uint(v.x);
         r[u][4 * q + 1] = __float_as_uint(v.y);
         r[u][4 * q + 2] = __float_as_uint(v.z);
         r[u][4 * q + 3] = __float_as_uint(v.w);
       }
 #pragma unroll
-    for (int u = 0; u < 2; u++) tmem_st32(lane_base + (uint32_t)(kColAlo + (c + u) * 32), r[u]);
+    for (int u = 0; u < 2; u++)
+      if (c + u < NKB) tmem_st32(lane_base + (uint32_t)(C::kColAlo + (c + u) * 32), r[u]);
   }
   tmem_wait_st();
   tc_fence_before();
   mbar_arrive(a_full);
 }
 
-__global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
+template <int NKB>
+__global__ void __launch_bounds__(Cfg<NKB>::kThreads, 1) translate_tc(Params P) {
+  using C = Cfg<NKB>;
+  constexpr int kStages = C::kStages, kNAcc = C::kNAcc;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sA = smem;                       // resident operator, hi part
-  unsigned char* sB = smem + kABytes;             // input ring
+  unsigned char* sB = smem + C::kABytes;          // input ring
   uint64_t* full = (uint64_t*)(sB + kStages * kStageBytes);
   uint64_t* empty = full + kStages;
   uint64_t* accf = empty + kStages;  // [kNAcc] accumulator b holds a finished tile
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
   const int t_begin = (int)((long long)P.ntile * blockIdx.x / gridDim.x);
   const int t_end = (int)((long long)P.ntile * (blockIdx.x + 1) / gridDim.x);
   const int ntile = t_end - t_begin;
-  const int nstage_total = ntile * kNKB;
+  const int nstage_total = ntile * NKB;
 
   if (threadIdx.x == 0) {
     sh_fail = 0;
@@ -284,10 +288,9 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     // this CTA's pair lists and operator images, into L2 ahead of their use
     prefetch_l2(P.tile_src + (size_t)t_begin * kTile, (uint32_t)(ntile * kTile * sizeof(int)));
-    prefetch_l2(P.tile_dst + (size_t)t_begin * kTile, (uint32_t)(ntile * kTile * sizeof(int)));
     for (int i = 0, prev = -1; i < ntile; i++) {
       const int op = P.tile_op[t_begin + i];
-      if (op != prev) prefetch_l2(P.opimg + (size_t)op * kImgFloats, (uint32_t)(kImgFloats * sizeof(float)));
+      if (op != prev) prefetch_l2(P.opimg + (size_t)op * C::kImgFloats, (uint32_t)(C::kImgFloats * sizeof(float)));
       prev = op;
     }
   }
@@ -303,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
 
   if (warp >= 5) {
     // ------------------------------------------------ producers
-    // group s (2 warps) fills ring slot s for stages s, s+5, s+10, ...  A
+    // group s (2 warps) fills ring slot s for stages s, s+kStages, ...  A
     // stage is 128 input rows x (hi, lo) x 128 bytes; one warp instruction
     // copies two rows: lanes 0-7 the hi line of the first row, 8-15 its lo
     // line, 16-31 the same for the second, so it touches four whole lines.
@@ -319,8 +322,8 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
       ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
       if (!ok) atomicExch(&sh_fail, 1);
       if (!ok || *(volatile int*)&sh_fail) break;
-      const int g = t_begin + st / kNKB;
-      const int kb = st % kNKB;
+      const int g = t_begin + st / NKB;
+      const int kb = st % NKB;
       const int* tsrc = P.tile_src + (size_t)g * kTile;
       int src[kRowsPerThread];
 #pragma unroll
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
         const int r = k * 2 * kGroupWarps + gw * 2 + (lane >> 4);
         unsigned char* d = bdst + swz(r, chunk);
         if (src[k] >= 0)
-          cp_async16(d, P.xin + (size_t)src[k] * 256 + part * 128 + kb * kKB + 4 * chunk);
+          cp_async16(d, P.xin + (size_t)src[k] * (2 * C::kKPad) + part * C::kKPad + kb * kKB + 4 * chunk);
         else
           *reinterpret_cast<float4*>(d) = make_float4(0.f, 0.f, 0.f, 0.f);
       }
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     for (int i = 0; i < ntile && ok; i++) {
       const int g = t_begin + i;
       const int buf = i % kNAcc;
-      const uint32_t dcol = tmem + (uint32_t)acc_col(buf);
+      const uint32_t dcol = tmem + (uint32_t)(buf * kTile);
       const int op = P.tile_op[g];
       if (op != cur_op) {  // the epilogue makes each new operator resident once the MMAs using the old one are done
         if (lane == 0) ok = mbar_wait(a_full, nload & 1);
@@ -362,8 +365,8 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
         if (!ok) break;
       }
       tc_fence_after();
-      for (int kb = 0; kb < kNKB && ok; kb++) {
-        const int st = i * kNKB + kb;
+      for (int kb = 0; kb < NKB && ok; kb++) {
+        const int st = i * NKB + kb;
         const int s = st % kStages;
         if (lane == 0) ok = mbar_wait(&full[s], (st / kStages) & 1);
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
         tc_fence_after();
         if (lane == 0) {
           const uint32_t ahi = smem_u32(sA + kb * kHalf);
-          const uint32_t alo = tmem + (uint32_t)(kColAlo + kb * kKB);
+          const uint32_t alo = tmem + (uint32_t)(C::kColAlo + kb * kKB);
           const uint32_t bhi = smem_u32(sB + s * kStageBytes), blo = bhi + kHalf;
 #pragma unroll
           for (int k = 0; k < kKB / 8; k++) {  // 4 MMAs of K=8 per 32-wide block
@@ -381,7 +384,7 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
             mma_tf32_ta(dcol, alo + k * 8, make_desc(bhi + o), 1u);
           }
           mma_commit(&empty[s]);  // frees the ring slot when these MMAs are done
-          if (kb == kNKB - 1) mma_commit(&accf[buf]);
+          if (kb == NKB - 1) mma_commit(&accf[buf]);
         }
         __syncwarp();
       }
@@ -395,52 +398,36 @@ __global__ void __launch_bounds__(kThreads, 1) translate_tc(Params P) {
     __syncwarp();
   } else {
     // ------------------------------------------------ epilogue (warps 0..3)
-    // thread `row` owns output coefficient row (tensor memory lane `row`).  It
-    // makes each new operator resident, then for each tile either adds column
-    // j into output row tile_dst[j] (lane l holds tile_dst[32h + l],
-    // broadcast by shuffle) with a predicated FP64 reduction at the L2 -- no
-    // branch per column, no read-back -- or, for launches whose outputs
-    // receive many pairs (M2L), stores the column to its pair row of y.
+    // thread `row` owns output coefficient row (tensor memory lane `row`): it
+    // makes each new operator resident, then stores column j of every tile to
+    // its pair row of y (plain coalesced FP32 stores; reduce_pairs sums the
+    // pair rows of each output box in FP64).
     const int row = warp * 32 + lane;
-    const bool row_ok = row < P.K;
     const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     bool ok = true;
-    if (ntile > 0) load_operator(P, P.tile_op[t_begin], row, lane_base, sA, a_full);
+    if (ntile > 0) load_operator<NKB>(P, P.tile_op[t_begin], row, lane_base, sA, a_full);
     for (int i = 0; i < ntile; i++) {
       const int g = t_begin + i;
       const int buf = i % kNAcc;
-      int dl[kTile / 32];
-#pragma unroll
-      for (int h = 0; h < kTile / 32; h++) dl[h] = P.tile_dst[(size_t)g * kTile + h * 32 + lane];
+      const int2 ty = P.tile_y[g];
       const bool w = mbar_wait(&accf[buf], (i / kNAcc) & 1);
       ok = __all_sync(0xffffffffu, w && *(volatile int*)&sh_fail == 0) != 0;
       if (!ok) break;
       tc_fence_after();
       if (i + 1 < ntile && P.tile_op[g + 1] != P.tile_op[g])  // every MMA up to tile i is done
-        load_operator(P, P.tile_op[g + 1], row, lane_base, sA, a_full);
+        load_operator<NKB>(P, P.tile_op[g + 1], row, lane_base, sA, a_full);
 #pragma unroll
       for (int h = 0; h < kTile / 32; h++) {
         uint32_t v[32];
-        tmem_ld32_nowait(lane_base + (uint32_t)(acc_col(buf) + h * 32), v);
+        tmem_ld32_nowait(lane_base + (uint32_t)(buf * kTile + h * 32), v);
         tmem_wait_ld();
         if (h == kTile / 32 - 1) {  // the accumulator is free once read
           tc_fence_before();
           mbar_arrive(&acce[buf]);
         }
-        if (P.y) {  // pair-indexed FP32 rows: plain coalesced stores, summed per output by reduce_pairs
-          float* yb = P.y + ((size_t)g * kTile + h * 32) * kRows + row;
+        float* yb = P.y + ((size_t)ty.x + h * 32) * P.ys + ty.y + row;
 #pragma unroll
-          for (int j = 0; j < 32; j++) yb[(size_t)j * kRows] = __uint_as_float(v[j]);
-        } else {
-          int d[32];
-#pragma unroll
-          for (int j = 0; j < 32; j++) d[j] = __shfl_sync(0xffffffffu, dl[h], j);
-#pragma unroll
-          for (int j = 0; j < 32; j++) {
-            const bool pj = row_ok && d[j] >= 0;
-            red_add_f64(P.out + (size_t)(pj ? d[j] : 0) * P.K + row, (double)__uint_as_float(v[j]), pj);
-          }
-        }
+        for (int j = 0; j < 32; j++) yb[(size_t)j * P.ys] = __uint_as_float(v[j]);
       }
     }
     if (!ok) atomicExch(&sh_fail, 3);
@@ -461,97 +448,137 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(r);
 }
 
-// M (FP64, [nbox][K]) -> Mtf ([nbox][2][128] FP32: TF32 hi, TF32 lo, zero padded)
-__global__ void split_tf32(int nbox, int K, const double* __restrict__ M, float* __restrict__ Mtf) {
+// M (FP64, [nbox][K]) -> Mtf ([nbox][2][kpad] FP32: TF32 hi, TF32 lo, zero padded)
+__global__ void split_tf32(int nbox, int K, int kpad, const double* __restrict__ M, float* __restrict__ Mtf) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= (size_t)nbox * 128) return;
-  const size_t b = i / 128;
-  const int k = (int)(i % 128);
+  if (i >= (size_t)nbox * kpad) return;
+  const size_t b = i / kpad;
+  const int k = (int)(i % kpad);
   float hi = 0.f, lo = 0.f;
   if (k < K) {
     const double x = M[b * K + k];
     hi = tf32_rna((float)x);
     lo = tf32_rna((float)(x - (double)hi));
   }
-  Mtf[b * 256 + k] = hi;
-  Mtf[b * 256 + 128 + k] = lo;
+  Mtf[b * 2 * kpad + k] = hi;
+  Mtf[b * 2 * kpad + kpad + k] = lo;
 }
 
-// out[rows[w]][0..K) += sum over e in [ptr[w], ptr[w+1]) of y[idx[e]][0..K), in
-// FP64 and in list order (deterministic); one warp per output row, lane l
-// holding coefficients 4l..4l+3.
+// out[rows[w]][0..K) += sum over e in [ptr[w], ptr[w+1]) of y[idx[e]][0..K)
+// (pair rows of ys floats), in FP64 and in list order (deterministic); one warp
+// per output row, lane l holding coefficients 128c + 4l .. 128c + 4l + 3 of
+// each 128-coefficient chunk c (K <= 256).
 __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* __restrict__ ptr,
-                             const int* __restrict__ idx, const float* __restrict__ y, int K,
+                             const int* __restrict__ idx, const float* __restrict__ y, int ys, int K,
                              double* __restrict__ out) {
   const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (w >= nrow) return;
-  double a[4] = {0, 0, 0, 0};
+  const int nch = (K + 127) / 128;
+  double a[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   const int e0 = ptr[w], e1 = ptr[w + 1];
   int e = e0;
   for (; e + 4 <= e1; e += 4) {
-    float4 v[4];
-#pragma unroll
-    for (int u = 0; u < 4; u++) v[u] = __ldg(reinterpret_cast<const float4*>(y + (size_t)idx[e + u] * kRows) + lane);
+    float4 v[4][2];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      a[0] += v[u].x;
-      a[1] += v[u].y;
-      a[2] += v[u].z;
-      a[3] += v[u].w;
+      const float4* yr = reinterpret_cast<const float4*>(y + (size_t)idx[e + u] * ys);
+      v[u][0] = __ldg(yr + lane);
+      v[u][1] = nch > 1 ? __ldg(yr + 32 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
     }
+#pragma unroll
+    for (int u = 0; u < 4; u++)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        a[c][0] += v[u][c].x;
+        a[c][1] += v[u][c].y;
+        a[c][2] += v[u][c].z;
+        a[c][3] += v[u][c].w;
+      }
   }
   for (; e < e1; e++) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(y + (size_t)idx[e] * kRows) + lane);
-    a[0] += v.x;
-    a[1] += v.y;
-    a[2] += v.z;
-    a[3] += v.w;
+    const float4* yr = reinterpret_cast<const float4*>(y + (size_t)idx[e] * ys);
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      if (c >= nch) break;
+      const float4 v = __ldg(yr + 32 * c + lane);
+      a[c][0] += v.x;
+      a[c][1] += v.y;
+      a[c][2] += v.z;
+      a[c][3] += v.w;
+    }
   }
   double* o = out + (size_t)rows[w] * K;
 #pragma unroll
-  for (int c = 0; c < 4; c++)
-    if (4 * lane + c < K) o[4 * lane + c] += a[c];
+  for (int c = 0; c < 2; c++)
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int k = 128 * c + 4 * lane + u;
+      if (k < K) o[k] += a[c][u];
+    }
 }
 
 }  // namespace tc
 
 int tc_tile() { return tc::kTile; }
+int tc_kpad(int K) { return K <= 128 ? 128 : ((K + tc::kKB - 1) / tc::kKB) * tc::kKB; }
+int tc_max_k() { return tc::kMaxNKB * tc::kKB; }
 
-void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int K, double* out,
-                         cudaStream_t st) {
+void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int ys, int K,
+                         double* out, cudaStream_t st) {
   if (nrow <= 0) return;
   const size_t threads = (size_t)nrow * 32;
-  tc::reduce_pairs<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(nrow, rows, ptr, idx, y, K, out);
+  tc::reduce_pairs<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(nrow, rows, ptr, idx, y, ys, K, out);
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_split_tf32(int nbox, int K, const double* M, float* Mtf, cudaStream_t st) {
+void launch_split_tf32(int nbox, int K, int kpad, const double* M, float* Mtf, cudaStream_t st) {
   if (nbox <= 0) return;
-  const size_t n = (size_t)nbox * 128;
-  tc::split_tf32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nbox, K, M, Mtf);
+  const size_t n = (size_t)nbox * kpad;
+  tc::split_tf32<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nbox, K, kpad, M, Mtf);
   FMMB_CHECK_LAUNCH();
 }
+
+namespace {
+template <int NKB>
+void prepare_nkb() {
+  FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc<NKB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc::Cfg<NKB>::kSmemBytes));
+}
+template <int NKB>
+void launch_nkb(const tc::Params& P, int grid, cudaStream_t st) {
+  tc::translate_tc<NKB><<<grid, tc::Cfg<NKB>::kThreads, tc::Cfg<NKB>::kSmemBytes, st>>>(P);
+}
+}  // namespace
 
 void prepare_translate_tc() {
-  FMMB_CUDA(cudaFuncSetAttribute(tc::translate_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kSmemBytes));
+  prepare_nkb<4>();
+  prepare_nkb<5>();
+  prepare_nkb<6>();
+  prepare_nkb<7>();
+  prepare_nkb<8>();
 }
 
 void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st) {
   if (a.ntile <= 0) return;
   tc::Params P{};
-  P.K = a.K;
   P.ntile = a.ntile;
   P.tile_op = a.tile_op;
   P.tile_src = a.tile_src;
-  P.tile_dst = a.tile_dst;
+  P.tile_y = a.tile_y;
   P.opimg = a.opimg;
   P.xin = a.xin;
-  P.out = a.out;
   P.y = a.y;
+  P.ys = a.ys;
   P.err = a.err;
   const int grid = a.ntile < nsm ? a.ntile : nsm;
-  tc::translate_tc<<<grid, tc::kThreads, tc::kSmemBytes, st>>>(P);
+  switch (tc_kpad(a.K) / tc::kKB) {
+    case 4: launch_nkb<4>(P, grid, st); break;
+    case 5: launch_nkb<5>(P, grid, st); break;
+    case 6: launch_nkb<6>(P, grid, st); break;
+    case 7: launch_nkb<7>(P, grid, st); break;
+    default: launch_nkb<8>(P, grid, st); break;
+  }
   FMMB_CHECK_LAUNCH();
 }
 
