@@ -130,6 +130,20 @@ FMMB_API int fmmb_direct_static(const fmmb_config* cfg, int ni, const float* tx,
                                 const float* sy, const float* sz, const float* snx, const float* sny,
                                 const float* snz, const float* q, float* pot, float* grad, void* stream);
 
+/* Chooses the octree depth for a geometry: for each lmax in [lmin, lmax_hi]
+ * (0, 0 = a range around 64 points per leaf) builds the tree of the given
+ * targets / sources (arguments as for fmmb_set_geometry) with the settings of
+ * cfg, times `reps` evaluates of fixed pseudo-random charges with CUDA events
+ * and returns the fastest depth in *best; ms_out (may be NULL) receives the
+ * milliseconds per evaluate of each candidate (-1 for a depth that did not fit
+ * in device memory).  The reference fixes lmax from a table of N
+ * (fmm/nlevel.cxx:5-31); this is the tuned replacement. */
+FMMB_API int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                                const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,
+                                const float* sy, const float* sz, const float* snx, const float* sny,
+                                const float* snz, const float* bbox, int lmin, int lmax_hi, int reps, int* best,
+                                float* ms_out);
+
 /* ---- inspection (tests, tooling) ---- */
 
 /* Tree of the current geometry.  kind: 0 target permutation (sorted position

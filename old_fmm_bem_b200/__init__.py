@@ -31,7 +31,7 @@ SEM_REFERENCE, SEM_ACCURATE = 0, 1
 EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_set_stream", "fmmb_set_geometry",
            "fmmb_evaluate", "fmmb_evaluate_f64", "fmmb_direct_f64", "fmmb_get_tree_size", "fmmb_get_tree",
            "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
-           "fmmb_last_error", "fmmb_direct_static"]
+           "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax"]
 
 
 def lib_path() -> str:
@@ -69,6 +69,8 @@ def load():
     lib.fmmb_evaluate.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_evaluate_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_direct_f64.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_autotune_lmax.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
+        [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
     lib.fmmb_direct_static.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
         [_vp] * 6 + [_vp, _vp, _vp, _vp]
     lib.fmmb_get_tree_size.argtypes = [_vp, ctypes.c_int]
@@ -227,6 +229,35 @@ class Plan:
         o = np.zeros(8, np.int64)
         _check(load().fmmb_get_stats(self._h, o.ctypes.data))
         return dict(zip(["ni", "nj", "leaves_i", "leaves_j", "p2p_pairs", "m2l_pairs", "lmax", "launches"], o.tolist()))
+
+
+def autotune_lmax(targets, sources, *, kernel=LAPLACE_G, target_normals=None, source_normals=None, p=8,
+                  precision=FP64, semantics=SEM_REFERENCE, eps2=0.0, exclude_self=False, bbox=None, lmin=0, lmax=0,
+                  reps=3):
+    """Fastest octree depth for this geometry (fmmb_autotune_lmax); returns
+    (best_lmax, {lmax: ms per evaluate})."""
+    lib = load()
+    cfg = _Config()
+    lib.fmmb_config_init(ctypes.byref(cfg))
+    cfg.kernel, cfg.p, cfg.precision, cfg.semantics = kernel, p, precision, semantics
+    cfg.eps2, cfg.exclude_self = eps2, int(exclude_self)
+    t = [_ptr(targets[k], np.float32) for k in range(3)]
+    s = [_ptr(sources[k], np.float32) for k in range(3)]
+    tn = [_ptr(target_normals[k], np.float32) for k in range(3)] if target_normals is not None else [(None, None)] * 3
+    sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
+    bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
+    ni, nj = len(targets[0]), len(sources[0])
+    best = ctypes.c_int(-1)
+    ms = np.zeros(16, np.float32)
+    _check(lib.fmmb_autotune_lmax(ctypes.byref(cfg), ni, t[0][0], t[1][0], t[2][0], tn[0][0], tn[1][0], tn[2][0], nj,
+                                  s[0][0], s[1][0], s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0], lmin, lmax, reps,
+                                  ctypes.byref(best), ms.ctypes.data))
+    if lmin <= 0 or lmax <= 0:  # the library chose the range around its estimate
+        l = 2
+        while l < 10 and max(ni, nj) / 8.0 ** l > 64.0:
+            l += 1
+        lmin, lmax = max(2, l - 1), min(10, l + 2)
+    return best.value, {l: float(ms[l - lmin]) for l in range(lmin, lmax + 1)}
 
 
 def fmm(xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, gxj, gyj, gzj, vj, neq, *, lmax, xmin, ymin, zmin, rd, p=8,

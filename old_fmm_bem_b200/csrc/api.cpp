@@ -784,6 +784,79 @@ int fmmb_evaluate_f64(fmmb_plan* pl, const float* q, double* pot, double* grad) 
   return evaluate_impl<double>(pl, q, pot, grad);
 }
 
+int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                       const float* tnx, const float* tny, const float* tnz, int nj, const float* sx, const float* sy,
+                       const float* sz, const float* snx, const float* sny, const float* snz, const float* bbox,
+                       int lmin, int lmax_hi, int reps, int* best, float* ms_out) {
+  return guarded([&] {
+    FMMB_REQUIRE(cfg && best, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
+    if (lmin <= 0 || lmax_hi <= 0) {  // around 64 points per leaf of a uniform cloud, then one coarser / two finer
+      int l = 2;
+      while (l < 10 && (double)std::max(ni, nj) / std::pow(8.0, l) > 64.0) l++;
+      lmin = std::max(2, l - 1);
+      lmax_hi = std::min(10, l + 2);
+    }
+    FMMB_REQUIRE(2 <= lmin && lmin <= lmax_hi && lmax_hi <= 10, FMMB_ERR_ARG, "lmax range must lie in [2, 10]");
+    reps = std::max(1, reps);
+    // random charges on the device (caller order), one FP64 output buffer
+    std::vector<float> hq((size_t)nj * std::max(1, cfg->nrhs));
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    for (auto& v : hq) {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      v = (float)((st >> 40) * (2.0 / 16777216.0) - 1.0);
+    }
+    DevBuf<float> dq;
+    dq.alloc(hq.size());
+    FMMB_CUDA(cudaMemcpy(dq.get(), hq.data(), hq.size() * sizeof(float), cudaMemcpyHostToDevice));
+    DevBuf<float> dpot, dgrad;
+    dpot.alloc((size_t)ni * std::max(1, cfg->nrhs));
+    dgrad.alloc((size_t)3 * ni * std::max(1, cfg->nrhs));
+    cudaEvent_t e0, e1;
+    FMMB_CUDA(cudaEventCreate(&e0));
+    FMMB_CUDA(cudaEventCreate(&e1));
+    float best_ms = 0.f;
+    *best = -1;
+    for (int l = lmin; l <= lmax_hi; l++) {
+      fmmb_config c = *cfg;
+      c.lmax = l;
+      fmmb_plan* pl = nullptr;
+      int rc = fmmb_plan_create(&c, &pl);
+      if (rc == FMMB_OK)
+        rc = fmmb_set_geometry(pl, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+      float ms = -1.f;
+      if (rc == FMMB_OK) {
+        float* g = cfg->kernel == FMMB_LAPLACE_G ? dgrad.get() : nullptr;
+        rc = fmmb_evaluate(pl, dq.get(), dpot.get(), g);  // warm-up (captures the graph)
+        if (rc == FMMB_OK) {
+          FMMB_CUDA(cudaEventRecord(e0, pl->st.main));
+          for (int r = 0; r < reps && rc == FMMB_OK; r++) rc = fmmb_evaluate(pl, dq.get(), dpot.get(), g);
+          FMMB_CUDA(cudaEventRecord(e1, pl->st.main));
+          FMMB_CUDA(cudaEventSynchronize(e1));
+          FMMB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          ms /= reps;
+        }
+      }
+      const std::string err = rc == FMMB_OK ? std::string() : std::string(fmmb_last_error());
+      if (pl) fmmb_plan_destroy(pl);
+      if (rc == FMMB_ERR_NOMEM || rc == FMMB_ERR_CAPACITY) ms = -1.f;  // this depth does not fit: skip it
+      else if (rc != FMMB_OK) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw Error{rc, "autotune at lmax " + std::to_string(l) + ": " + err};
+      }
+      if (ms_out) ms_out[l - lmin] = ms;
+      if (ms >= 0.f && (*best < 0 || ms < best_ms)) {
+        best_ms = ms;
+        *best = l;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    FMMB_REQUIRE(*best >= 0, FMMB_ERR_NOMEM, "no octree depth in the range fits on the device");
+  });
+}
+
 int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, double* grad) {
   return guarded([&] {
     FMMB_REQUIRE(pl && q && pot, FMMB_ERR_ARG, "null argument");

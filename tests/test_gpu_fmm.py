@@ -209,3 +209,14 @@ def test_tensor_core_translations_match_fp64(semantics, p, ob):
         pl.close()
     assert rel(out[1][0], out[0][0]) < 1e-6
     assert rel(out[1][1], out[0][1]) < 2e-6 * max(1.0, ((p + 1) ** 2 / 121) ** 0.5)
+
+
+def test_autotune_lmax_picks_a_measured_depth(ob):
+    """fmmb_autotune_lmax times every depth of the range on the given geometry
+    and returns the fastest one."""
+    rng = np.random.default_rng(90)
+    x = rng.random((3, 30000), dtype=np.float32)
+    best, ms = ob.autotune_lmax(x, x, kernel=0, p=6, precision=1, semantics=1, exclude_self=True,
+                                bbox=(0, 0, 0, 1), lmin=2, lmax=4, reps=2)
+    assert set(ms) == {2, 3, 4} and all(v > 0 for v in ms.values())
+    assert best == min(ms, key=ms.get)
