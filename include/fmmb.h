@@ -103,6 +103,24 @@ FMMB_API int fmmb_evaluate(fmmb_plan* plan, const float* q, float* pot, float* g
 /* Same with FP64 outputs. */
 FMMB_API int fmmb_evaluate_f64(fmmb_plan* plan, const float* q, double* pot, double* grad);
 
+/* Transposed matvec (the charge adjoint): out[nj] = A^T w for w[ni] (nrhs
+ * blocks), A being this plan's FMM.  G is symmetric, so A^T is the G-FMM from
+ * the targets to the sources; for the normal-derivative kernels
+ * d/dx_j G = -d/dx_i G gives Gni^T = -Gnj and Gnj^T = -Gni with the point
+ * sets swapped.  grad[3 nj] (Laplace G only, may be NULL) receives the
+ * gradient of A^T w at the sources.  The transposed plan (same root cube,
+ * same settings) is built on the first call after fmmb_set_geometry.  No
+ * counterpart in the reference (its fmm() has no adjoint). */
+FMMB_API int fmmb_evaluate_transpose(fmmb_plan* plan, const float* w, float* out, float* grad);
+FMMB_API int fmmb_evaluate_transpose_f64(fmmb_plan* plan, const float* w, double* out, double* grad);
+
+/* Position gradients of L = sum_i w_i pot_i for the Laplace G kernel, one
+ * right-hand side: dxt[3 ni] = w * grad(pot)(x_t) and dxs[3 nj] =
+ * q * grad(psi)(x_s), psi = A^T w (either output may be NULL; when targets and
+ * sources are the same points the caller adds the two).  Costs one matvec and
+ * one transposed matvec, both with gradient.  No reference counterpart. */
+FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w, double* dxt, double* dxs);
+
 /* Direct O(ni*nj) sum on the GPU with the plan's kernel and semantics
  * (replaces G_dir/Gni_dir/Gnj_dir, kernel/G_dir.cxx:6-30,
  * kernel/Gni_dir.cxx:6-21, kernel/Gnj_dir.cxx:6-21), FP64 arithmetic.  Uses

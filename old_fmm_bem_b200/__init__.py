@@ -31,7 +31,8 @@ SEM_REFERENCE, SEM_ACCURATE = 0, 1
 EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_set_stream", "fmmb_set_geometry",
            "fmmb_evaluate", "fmmb_evaluate_f64", "fmmb_direct_f64", "fmmb_get_tree_size", "fmmb_get_tree",
            "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
-           "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax"]
+           "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
+           "fmmb_evaluate_transpose_f64", "fmmb_position_grad"]
 
 
 def lib_path() -> str:
@@ -69,6 +70,9 @@ def load():
     lib.fmmb_evaluate.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_evaluate_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_direct_f64.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_evaluate_transpose.argtypes = [_vp, _vp, _vp, _vp]
+    lib.fmmb_evaluate_transpose_f64.argtypes = [_vp, _vp, _vp, _vp]
+    lib.fmmb_position_grad.argtypes = [_vp, _vp, _vp, _vp, _vp]
     lib.fmmb_autotune_lmax.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
         [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
     lib.fmmb_direct_static.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
@@ -190,6 +194,38 @@ class Plan:
         self._follow_torch(q, pot, grad)
         _check(fn(self._h, qp, pp, gp))
         return pk, gk
+
+    def evaluate_transpose(self, w, out=None, grad=None, f64=False):
+        """Charge adjoint A^T w (fmmb_evaluate_transpose): w (nrhs*ni,) ->
+        (out (nrhs*nj,), grad (3*nrhs*nj,) for LAPLACE_G or None)."""
+        dt = np.float64 if f64 else np.float32
+        wp, wk = _ptr(w, np.float32)
+        nj = self.nj * self.nrhs
+        if out is None:
+            out = np.zeros(nj, dt)
+        if grad is None and self.kernel == LAPLACE_G:
+            grad = np.zeros(3 * nj, dt)
+        op_, ok = _ptr(out, dt)
+        gp, gk = _ptr(grad, dt) if self.kernel == LAPLACE_G else (None, None)
+        fn = load().fmmb_evaluate_transpose_f64 if f64 else load().fmmb_evaluate_transpose
+        self._follow_torch(w, out, grad)
+        _check(fn(self._h, wp, op_, gp))
+        return ok, gk
+
+    def position_grad(self, q, w, dxt=None, dxs=None):
+        """Laplace G position gradients of sum(w * pot) (fmmb_position_grad):
+        returns (dxt (3, ni), dxs (3, nj)) in FP64."""
+        qp, qk = _ptr(q, np.float32)
+        wp, wk = _ptr(w, np.float32)
+        if dxt is None:
+            dxt = np.zeros(3 * self.ni)
+        if dxs is None:
+            dxs = np.zeros(3 * self.nj)
+        tp, tk = _ptr(dxt, np.float64)
+        sp, sk = _ptr(dxs, np.float64)
+        self._follow_torch(q, w, dxt, dxs)
+        _check(load().fmmb_position_grad(self._h, qp, wp, tp, sp))
+        return tk.reshape(3, -1), sk.reshape(3, -1)
 
     def direct(self, q, i0=0, i1=None):
         """FP64 direct sum on the GPU for targets [i0, i1) (caller order)."""

@@ -21,10 +21,10 @@ backward, for L = sum_i w_i pot_i with w = dL/dpot:
   derivatives of the kernel and are not provided: their positions must not
   require grad.)
 
-An FMMOperator builds the forward and the transposed plan (both trees) once;
-every call reuses them, so the geometry (positions, normals) must stay as it was
-at construction.  Expansions are recomputed by each matvec, nothing of size
-N*P is stored between the passes.
+An FMMOperator builds the plan (and, through fmmb_evaluate_transpose, its
+transposed plan) once; every call reuses the trees, so the geometry
+(positions, normals) must stay as it was at construction.  Expansions are
+recomputed by each matvec, nothing of size N*P is stored between the passes.
 """
 from __future__ import annotations
 
@@ -33,9 +33,6 @@ import torch
 from . import FP64, LAPLACE_G, LAPLACE_GNI, LAPLACE_GNJ, MIXED, SEM_ACCURATE, Plan
 
 __all__ = ["FMMOperator", "fmm_potential", "FMMFunction"]
-
-_TRANSPOSED = {LAPLACE_G: LAPLACE_G, LAPLACE_GNI: LAPLACE_GNJ, LAPLACE_GNJ: LAPLACE_GNI}
-
 
 def _col(t):
     return [t[k].contiguous() for k in range(3)]
@@ -59,11 +56,6 @@ class FMMOperator:
         self.plan = Plan(kernel=kernel, **kw)
         self.plan.set_geometry(_col(xt), _col(xs), _col(nt) if kernel == LAPLACE_GNI else None,
                                _col(ns) if kernel == LAPLACE_GNJ else None, bbox=bbox)
-        tk = _TRANSPOSED[kernel]
-        self.sign = 1.0 if kernel == LAPLACE_G else -1.0
-        self.plan_t = Plan(kernel=tk, **kw)
-        self.plan_t.set_geometry(_col(xs), _col(xt), _col(ns) if tk == LAPLACE_GNI else None,
-                                 _col(nt) if tk == LAPLACE_GNJ else None, bbox=bbox)
 
     def __call__(self, q):
         """Potential at the targets (FP64 accumulation, returned in q's dtype);
@@ -73,7 +65,6 @@ class FMMOperator:
 
     def close(self):
         self.plan.close()
-        self.plan_t.close()
 
 
 class FMMFunction(torch.autograd.Function):
@@ -97,12 +88,13 @@ class FMMFunction(torch.autograd.Function):
         (qd,) = ctx.saved_tensors
         op = ctx.op
         wd = w.detach().to(torch.float32).contiguous()
-        # transposed FMM: targets x_s, sources x_t, charges w
+        # transposed FMM (fmmb_evaluate_transpose): targets x_s, sources x_t,
+        # charges w; the sign of the normal-derivative kernels is applied there
         adj = torch.zeros(op.nj, dtype=torch.float64, device=w.device)
         want_field = op.kernel == LAPLACE_G and ctx.needs[1]
         field = torch.zeros(3 * op.nj, dtype=torch.float64, device=w.device) if want_field else None
-        op.plan_t.evaluate(wd, adj, field, f64=True)
-        dq = (op.sign * adj).to(w.dtype)
+        op.plan.evaluate_transpose(wd, adj, field, f64=True)
+        dq = adj.to(w.dtype)
         dxt = dxs = None
         if op.kernel == LAPLACE_G:
             if ctx.needs[0]:

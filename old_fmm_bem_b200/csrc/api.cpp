@@ -194,6 +194,7 @@ int fmmb_plan_destroy(fmmb_plan* pl) {
   cudaDeviceSynchronize();
   for (auto& g : pl->gexec)
     if (g) cudaGraphExecDestroy(g);
+  if (pl->tplan) fmmb_plan_destroy(pl->tplan);
   if (pl->own_stream && pl->st.main) cudaStreamDestroy(pl->st.main);
   if (pl->st.side) cudaStreamDestroy(pl->st.side);
   if (pl->st.cap) cudaStreamDestroy(pl->st.cap);
@@ -215,6 +216,10 @@ int fmmb_set_stream(fmmb_plan* pl, void* stream) {
     if (pl->own_stream && pl->st.main) FMMB_CUDA(cudaStreamDestroy(pl->st.main));
     pl->st.main = (cudaStream_t)stream;
     pl->own_stream = false;
+    if (pl->tplan) {
+      const int rc = fmmb_set_stream(pl->tplan, stream);
+      if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+    }
   });
 }
 
@@ -230,6 +235,10 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
         cudaGraphExecDestroy(pl->gexec[w]);
         pl->gexec[w] = nullptr;
       }
+    }
+    if (pl->tplan) {  // its geometry is the old one
+      fmmb_plan_destroy(pl->tplan);
+      pl->tplan = nullptr;
     }
     FMMB_REQUIRE(tx && ty && tz && sx && sy && sz, FMMB_ERR_ARG, "null coordinates");
     FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNI || (tnx && tny && tnz), FMMB_ERR_ARG, "Gni needs target normals");
@@ -251,6 +260,15 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
                           to_device(sx, nj, st[6], s),  to_device(sy, nj, st[7], s),  to_device(sz, nj, st[8], s),
                           to_device(snx, nj, st[9], s), to_device(sny, nj, st[10], s), to_device(snz, nj, st[11], s)};
     build_tree(pl, ni, d[0], d[1], d[2], d[3], d[4], d[5], nj, d[6], d[7], d[8], d[9], d[10], d[11], bbox ? bb : nullptr);
+    // caller-order copy of the geometry for the transposed plan
+    pl->geo.alloc((size_t)6 * ni + 6 * (size_t)nj);
+    pl->geo_tn = d[3] && d[4] && d[5];
+    pl->geo_sn = d[9] && d[10] && d[11];
+    for (int k = 0; k < 12; k++) {
+      const size_t n = k < 6 ? ni : nj;
+      float* dst = pl->geo.get() + (k < 6 ? (size_t)k * ni : (size_t)6 * ni + (size_t)(k - 6) * nj);
+      if (d[k]) FMMB_CUDA(cudaMemcpyAsync(dst, d[k], n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
     // reference semantics: the M2L distance carries an absolute eps, so the
     // operator set depends on the level sizes (rebuilt when they change)
     if (pl->ref && (pl->ops.m2l_lmax != pl->lmax || pl->ops.m2l_rd != pl->bbox[3])) {
@@ -854,6 +872,107 @@ int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const fl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     FMMB_REQUIRE(*best >= 0, FMMB_ERR_NOMEM, "no octree depth in the range fits on the device");
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// The plan with targets and sources swapped (G -> G, Gni -> Gnj, Gnj -> Gni),
+// on the same root cube and stream, built on first use.
+fmmb_plan* transposed_plan(fmmb_plan* pl) {
+  if (pl->tplan) return pl->tplan;
+  FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+  fmmb_config c = pl->cfg;
+  c.kernel = pl->cfg.kernel == FMMB_LAPLACE_GNI ? FMMB_LAPLACE_GNJ
+             : pl->cfg.kernel == FMMB_LAPLACE_GNJ ? FMMB_LAPLACE_GNI : FMMB_LAPLACE_G;
+  fmmb_plan* t = nullptr;
+  int rc = fmmb_plan_create(&c, &t);
+  if (rc == FMMB_OK) rc = fmmb_set_stream(t, pl->st.main);
+  const int ni = pl->ni, nj = pl->nj;
+  const float* g = pl->geo.get();
+  const float* tg = g;                    // this plan's targets: the transposed sources
+  const float* sg = g + (size_t)6 * ni;   // this plan's sources: the transposed targets
+  const bool tn = c.kernel == FMMB_LAPLACE_GNI, sn = c.kernel == FMMB_LAPLACE_GNJ;
+  if (rc == FMMB_OK)
+    rc = fmmb_set_geometry(t, nj, sg, sg + nj, sg + 2 * (size_t)nj, tn ? sg + 3 * (size_t)nj : nullptr,
+                           tn ? sg + 4 * (size_t)nj : nullptr, tn ? sg + 5 * (size_t)nj : nullptr, ni, tg, tg + ni,
+                           tg + 2 * (size_t)ni, sn ? tg + 3 * (size_t)ni : nullptr, sn ? tg + 4 * (size_t)ni : nullptr,
+                           sn ? tg + 5 * (size_t)ni : nullptr, pl->bbox);
+  if (rc != FMMB_OK) {
+    const std::string msg = fmmb_last_error();
+    if (t) fmmb_plan_destroy(t);
+    throw Error{rc, "transposed plan: " + msg};
+  }
+  pl->tplan = t;
+  return t;
+}
+
+template <typename T>
+void negate(T* p, size_t n, cudaStream_t s) {
+  if (is_device_ptr(p)) {
+    launch_scale(p, n, T(-1), s);
+  } else {
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < n; i++) p[i] = -p[i];
+  }
+}
+
+template <typename T>
+int transpose_impl(fmmb_plan* pl, const float* w, T* out, T* grad) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && w && out, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G || grad == nullptr, FMMB_ERR_ARG,
+                 "the transposed normal-derivative kernels have no gradient output");
+    fmmb_plan* t = transposed_plan(pl);
+    const int rc = sizeof(T) == 4 ? fmmb_evaluate(t, w, (float*)out, (float*)grad)
+                                  : fmmb_evaluate_f64(t, w, (double*)out, (double*)grad);
+    if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+    if (pl->cfg.kernel != FMMB_LAPLACE_G) negate(out, (size_t)pl->nj * pl->cfg.nrhs, t->st.main);
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmmb_evaluate_transpose(fmmb_plan* pl, const float* w, float* out, float* grad) {
+  return transpose_impl<float>(pl, w, out, grad);
+}
+int fmmb_evaluate_transpose_f64(fmmb_plan* pl, const float* w, double* out, double* grad) {
+  return transpose_impl<double>(pl, w, out, grad);
+}
+
+int fmmb_position_grad(fmmb_plan* pl, const float* q, const float* w, double* dxt, double* dxs) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && q && w && (dxt || dxs), FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G, FMMB_ERR_ARG, "position gradients are for the Laplace G kernel");
+    FMMB_REQUIRE(pl->cfg.nrhs == 1, FMMB_ERR_ARG, "position gradients take one right-hand side");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+    const int ni = pl->ni, nj = pl->nj;
+    cudaStream_t m = pl->st.main;
+    // work space: pot[ni], field_t[3 ni], adj[nj], field_s[3 nj], out staging[3 ni + 3 nj]
+    pl->pg_tmp.alloc((size_t)4 * ni + 4 * (size_t)nj + 3 * (size_t)ni + 3 * (size_t)nj);
+    double* pot = pl->pg_tmp.get();
+    double* ft = pot + ni;
+    double* adj = ft + 3 * (size_t)ni;
+    double* fs = adj + nj;
+    double* stage = fs + 3 * (size_t)nj;
+    int rc = FMMB_OK;
+    if (dxt) rc = fmmb_evaluate_f64(pl, q, pot, ft);
+    if (rc == FMMB_OK && dxs) rc = fmmb_evaluate_transpose_f64(pl, w, adj, fs);
+    if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+    DevBuf<float> sw, sq;
+    const float* wd = to_device(w, ni, sw, m);
+    const float* qd = to_device(q, nj, sq, m);
+    double* ot = dxt ? (is_device_ptr(dxt) ? dxt : stage) : nullptr;
+    double* os = dxs ? (is_device_ptr(dxs) ? dxs : stage + 3 * (size_t)ni) : nullptr;
+    if (ot) launch_weight_field(ni, wd, ft, ot, m);   // dL/dx_t = w * grad(pot)(x_t)
+    if (os) launch_weight_field(nj, qd, fs, os, m);   // dL/dx_s = q * grad(psi)(x_s)
+    if (dxt && ot != dxt) FMMB_CUDA(cudaMemcpyAsync(dxt, ot, 3 * (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, m));
+    if (dxs && os != dxs) FMMB_CUDA(cudaMemcpyAsync(dxs, os, 3 * (size_t)nj * sizeof(double), cudaMemcpyDeviceToHost, m));
+    FMMB_CUDA(cudaStreamSynchronize(m));
   });
 }
 

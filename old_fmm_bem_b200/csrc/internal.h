@@ -164,6 +164,13 @@ struct fmmb_plan {
   // launch count of the capturing call.
   bool use_graph = true;
   bool capturing = false;
+  // transposed FMM (fmmb_evaluate_transpose, fmmb_position_grad): caller-order
+  // copies of the geometry [tx ty tz tnx tny tnz | sx sy sz snx sny snz] and the
+  // plan with targets and sources swapped, built on first use
+  fmmb::DevBuf<float> geo;
+  bool geo_tn = false, geo_sn = false;
+  fmmb_plan* tplan = nullptr;
+  fmmb::DevBuf<double> pg_tmp;                 // position-gradient work space
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   std::vector<std::pair<int, int>> gphase[2];
   int glaunches[2] = {0, 0};

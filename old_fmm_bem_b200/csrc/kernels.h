@@ -63,6 +63,10 @@ void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float
 namespace fmmb {
 // tensor-core translations (translate_tc.cu)
 int tc_tile();
+// p[i] *= s; out[k n + i] = w[i] * field[k n + i] (k = 0..2)
+void launch_scale(float* p, size_t n, float s, cudaStream_t st);
+void launch_scale(double* p, size_t n, double s, cudaStream_t st);
+void launch_weight_field(int n, const float* w, const double* field, double* out, cudaStream_t st);
 // FP64 box-pair translations (M2M, L2L): tiles of tp pairs of one operator
 struct PairArgs {
   int ntile, tp, K, atomic;

@@ -732,6 +732,36 @@ void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
   FMMB_CHECK_LAUNCH();
 }
 
+namespace {
+template <typename T>
+__global__ void scale_kernel(T* p, size_t n, T s) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] *= s;
+}
+__global__ void weight_field_kernel(int n, const float* __restrict__ w, const double* __restrict__ f,
+                                    double* __restrict__ out) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < 3 * (size_t)n) out[i] = (double)w[i % n] * f[i];
+}
+}  // namespace
+
+void launch_scale(float* p, size_t n, float s, cudaStream_t st) {
+  if (n == 0) return;
+  scale_kernel<float><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, s);
+  FMMB_CHECK_LAUNCH();
+}
+void launch_scale(double* p, size_t n, double s, cudaStream_t st) {
+  if (n == 0) return;
+  scale_kernel<double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, s);
+  FMMB_CHECK_LAUNCH();
+}
+void launch_weight_field(int n, const float* w, const double* field, double* out, cudaStream_t st) {
+  if (n <= 0) return;
+  const size_t t = 3 * (size_t)n;
+  weight_field_kernel<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(n, w, field, out);
+  FMMB_CHECK_LAUNCH();
+}
+
 void launch_direct_f64(int kernel, int i0, int i1, const int* inv_i, const float4* tpos, const float4* tnrm, int nj,
                        const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot, double* grad,
                        cudaStream_t st) {
