@@ -95,6 +95,24 @@ FMMB_API int fmmb_set_geometry(fmmb_plan* plan, int ni, const float* tx, const f
                       const float* sx, const float* sy, const float* sz, const float* snx,
                       const float* sny, const float* snz, const float* bbox);
 
+/* Many independent problems in one plan (a forest of octrees): problem b owns
+ * targets [t_off[b], t_off[b+1]) and sources [s_off[b], s_off[b+1]) of the
+ * concatenated arrays (t_off[0] = s_off[0] = 0; t_off[nprob] = ni and
+ * s_off[nprob] = nj are the totals).  Points of different problems never
+ * interact: the problem index sits above the Morton bits of every box key, so
+ * neighbour and interaction lists stay inside a problem, and each problem's
+ * result equals that of its own plan over the same root cube.  All problems
+ * share bbox (NULL: a cube enclosing all points) and lmax; 3*lmax +
+ * ceil(log2(nprob)) <= 30.  fmmb_evaluate then runs every problem in the
+ * same launches; q / pot keep the concatenated order (nrhs blocks of nj / ni).
+ * Offsets may be host or device arrays.  The reference runs one problem per
+ * fmm() call (bio/main.cxx:377-413); no counterpart. */
+FMMB_API int fmmb_set_geometry_batch(fmmb_plan* plan, int nprob, const int* t_off, const float* tx,
+                                     const float* ty, const float* tz, const float* tnx, const float* tny,
+                                     const float* tnz, const int* s_off, const float* sx, const float* sy,
+                                     const float* sz, const float* snx, const float* sny, const float* snz,
+                                     const float* bbox);
+
 /* One FMM matvec (replaces fmm(mi, mj, neq), fmm/fmm.cxx:29-152).
  * q: nrhs x nj charges (caller order).  pot: nrhs x ni potentials (overwritten,
  * unlike the reference's += into vi).  grad: nrhs x 3 x ni gradient for
@@ -126,6 +144,33 @@ FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w,
  * kernel/Gni_dir.cxx:6-21, kernel/Gnj_dir.cxx:6-21), FP64 arithmetic.  Uses
  * the geometry and the first right-hand side of q; targets [i0, i1). */
 FMMB_API int fmmb_direct_f64(fmmb_plan* plan, const float* q, int i0, int i1, double* pot, double* grad);
+
+/* GMRES for the boundary-integral systems of a plan whose targets are its
+ * sources (problem by problem):  A x = diag * x + K (weight .* x),  left
+ * preconditioned by y = precond * x.  This is the reference's PETSc shell
+ * solve (bio/main.cxx:27-53 mymatmult: weight = are/e1, diag =
+ * (e1+e2)/(2 e1 (e1-e2)); :55-70 mypcshell: precond = 1/diag; :377-413
+ * KSPSolve with KSPGMRES) moved onto the GPU, for nrhs x nprob independent
+ * systems at once: each iteration is one fmmb_evaluate of all of them. */
+typedef struct fmmb_gmres_config {
+  int restart;    /* Krylov vectors per cycle, 1..64 (PETSc's default 30) */
+  int max_iter;   /* iterations (matvecs after the initial residual) in all */
+  double rtol;    /* a system stops when its preconditioned residual norm falls to
+                     rtol times its initial one; 0 runs max_iter iterations */
+  double diag;    /* identity term of A */
+  double precond; /* scale of the preconditioner */
+} fmmb_gmres_config;
+
+/* Defaults: restart 30, max_iter 20, rtol 0, diag 0, precond 1. */
+FMMB_API int fmmb_gmres_config_init(fmmb_gmres_config* cfg);
+
+/* b: nrhs x n right-hand sides; x: nrhs x n initial guess, overwritten by the
+ * solution (FP64, host or device; n = the plan's point count).  weight: n
+ * floats or NULL (= 1).  iters: iterations done (may be NULL).  resid:
+ * nrhs x nprob relative preconditioned residual estimates ||r_k|| / ||r_0||
+ * per system (may be NULL). */
+FMMB_API int fmmb_gmres(fmmb_plan* plan, const fmmb_gmres_config* cfg, const float* weight, const double* b,
+                        double* x, int* iters, double* resid);
 
 /* Direct sum without a plan that allocates nothing (no cudaMalloc/cudaFree,
  * no allocating library routine).  It has no counterpart in the reference:

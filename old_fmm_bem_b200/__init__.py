@@ -32,7 +32,8 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_evaluate", "fmmb_evaluate_f64", "fmmb_direct_f64", "fmmb_get_tree_size", "fmmb_get_tree",
            "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
-           "fmmb_evaluate_transpose_f64", "fmmb_position_grad"]
+           "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
+           "fmmb_gmres"]
 
 
 def lib_path() -> str:
@@ -47,6 +48,11 @@ class _Config(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("p", ctypes.c_int), ("lmax", ctypes.c_int), ("precision", ctypes.c_int),
                 ("semantics", ctypes.c_int), ("eps2", ctypes.c_double), ("exclude_self", ctypes.c_int),
                 ("nrhs", ctypes.c_int)]
+
+
+class _GmresConfig(ctypes.Structure):
+    _fields_ = [("restart", ctypes.c_int), ("max_iter", ctypes.c_int), ("rtol", ctypes.c_double),
+                ("diag", ctypes.c_double), ("precond", ctypes.c_double)]
 
 
 _LIB = None
@@ -67,6 +73,9 @@ def load():
     lib.fmmb_plan_destroy.argtypes = [_vp]
     lib.fmmb_set_stream.argtypes = [_vp, _vp]
     lib.fmmb_set_geometry.argtypes = [_vp, ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + [_vp] * 6 + [_vp]
+    lib.fmmb_set_geometry_batch.argtypes = [_vp, ctypes.c_int, _vp] + [_vp] * 6 + [_vp] + [_vp] * 6 + [_vp]
+    lib.fmmb_gmres_config_init.argtypes = [ctypes.POINTER(_GmresConfig)]
+    lib.fmmb_gmres.argtypes = [_vp, ctypes.POINTER(_GmresConfig), _vp, _vp, _vp, _vp, _vp]
     lib.fmmb_evaluate.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_evaluate_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_direct_f64.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
@@ -176,7 +185,50 @@ class Plan:
         _check(load().fmmb_set_geometry(self._h, ni, t[0][0], t[1][0], t[2][0], tn[0][0], tn[1][0], tn[2][0], nj,
                                         s[0][0], s[1][0], s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0]))
         self.ni, self.nj = ni, nj
+        self.nprob = 1
         return self
+
+    def set_geometry_batch(self, t_off, targets, s_off, sources, target_normals=None, source_normals=None,
+                           bbox=None):
+        """Independent problems in one plan (fmmb_set_geometry_batch): problem b
+        owns targets[:, t_off[b]:t_off[b+1]] and sources[:, s_off[b]:s_off[b+1]];
+        t_off / s_off have nprob + 1 entries."""
+        to = np.ascontiguousarray(t_off, np.int32)
+        so = np.ascontiguousarray(s_off, np.int32)
+        assert len(to) == len(so) and len(to) >= 2
+        t = [_ptr(targets[k], np.float32) for k in range(3)]
+        s = [_ptr(sources[k], np.float32) for k in range(3)]
+        tn = [_ptr(target_normals[k], np.float32) for k in range(3)] if target_normals is not None else [(None, None)] * 3
+        sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
+        bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
+        self._follow_torch(*targets, *sources)
+        _check(load().fmmb_set_geometry_batch(self._h, len(to) - 1, to.ctypes.data, t[0][0], t[1][0], t[2][0],
+                                              tn[0][0], tn[1][0], tn[2][0], so.ctypes.data, s[0][0], s[1][0],
+                                              s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0]))
+        self.ni, self.nj = int(to[-1]), int(so[-1])
+        self.nprob = len(to) - 1
+        return self
+
+    def gmres(self, b, x=None, weight=None, *, diag=0.0, precond=1.0, restart=30, max_iter=20, rtol=0.0):
+        """Batched GMRES (fmmb_gmres) for  diag*x + K(weight .* x) = b  with
+        the left preconditioner precond*I, every (rhs, problem) system at once.
+        b, x: (nrhs * n,) float64 (numpy or torch CUDA).  Returns (x, iters,
+        resid (nrhs, nprob))."""
+        cfg = _GmresConfig()
+        load().fmmb_gmres_config_init(ctypes.byref(cfg))
+        cfg.restart, cfg.max_iter, cfg.rtol, cfg.diag, cfg.precond = restart, max_iter, rtol, diag, precond
+        n = self.ni * self.nrhs
+        if x is None:
+            x = np.zeros(n)
+        bp, bk = _ptr(b, np.float64)
+        xp, xk = _ptr(x, np.float64)
+        wp, wk = _ptr(weight, np.float32)
+        nprob = getattr(self, "nprob", 1)
+        resid = np.zeros(self.nrhs * nprob)
+        it = ctypes.c_int(0)
+        self._follow_torch(b, x, weight)
+        _check(load().fmmb_gmres(self._h, ctypes.byref(cfg), wp, bp, xp, ctypes.byref(it), resid.ctypes.data))
+        return xk, it.value, resid.reshape(self.nrhs, nprob)
 
     def evaluate(self, q, pot=None, grad=None, f64=False):
         """One matvec.  q: (nrhs*nj,) charges.  Returns (pot, grad) -- grad only

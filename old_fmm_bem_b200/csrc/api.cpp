@@ -223,12 +223,37 @@ int fmmb_set_stream(fmmb_plan* pl, void* stream) {
   });
 }
 
-int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
-                      const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
-                      const float* snx, const float* sny, const float* snz, const float* bbox) {
+}  // extern "C"
+
+namespace {
+
+// fmmb_set_geometry (nprob = 1, no offsets) and fmmb_set_geometry_batch
+// (nprob problems, host or device offsets toff / soff of nprob + 1 entries)
+int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, int ni, const float* tx, const float* ty,
+                  const float* tz, const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,
+                  const float* sy, const float* sz, const float* snx, const float* sny, const float* snz,
+                  const float* bbox) {
   return guarded([&] {
     FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
     FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
+    FMMB_REQUIRE(nprob >= 1 && nprob <= (1 << 20), FMMB_ERR_ARG, "number of problems must be in 1..2^20");
+    std::vector<int> to(nprob + 1), so(nprob + 1);
+    if (nprob == 1) {
+      to = {0, ni};
+      so = {0, nj};
+    } else {
+      FMMB_REQUIRE(toff && soff, FMMB_ERR_ARG, "null problem offsets");
+      for (int w = 0; w < 2; w++) {
+        const int* src = w ? soff : toff;
+        std::vector<int>& dst = w ? so : to;
+        if (is_device_ptr(src)) FMMB_CUDA(cudaMemcpy(dst.data(), src, (nprob + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+        else std::memcpy(dst.data(), src, (nprob + 1) * sizeof(int));
+      }
+      for (int b = 0; b < nprob; b++)
+        FMMB_REQUIRE(to[b] <= to[b + 1] && so[b] <= so[b + 1], FMMB_ERR_ARG, "problem offsets must not decrease");
+      FMMB_REQUIRE(to[0] == 0 && so[0] == 0 && to[nprob] == ni && so[nprob] == nj, FMMB_ERR_ARG,
+                   "problem offsets must run from 0 to the point counts");
+    }
     for (int w = 0; w < 2; w++) {  // captured evaluates refer to the old buffers
       if (pl->gexec[w]) {
         FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
@@ -259,6 +284,13 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
                           to_device(tnx, ni, st[3], s), to_device(tny, ni, st[4], s), to_device(tnz, ni, st[5], s),
                           to_device(sx, nj, st[6], s),  to_device(sy, nj, st[7], s),  to_device(sz, nj, st[8], s),
                           to_device(snx, nj, st[9], s), to_device(sny, nj, st[10], s), to_device(snz, nj, st[11], s)};
+    pl->nprob = nprob;
+    pl->prob_toff = to;
+    pl->prob_soff = so;
+    pl->d_prob_off.alloc(2 * (size_t)(nprob + 1));
+    FMMB_CUDA(cudaMemcpyAsync(pl->d_prob_off.get(), to.data(), (nprob + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    FMMB_CUDA(cudaMemcpyAsync(pl->d_prob_off.get() + nprob + 1, so.data(), (nprob + 1) * sizeof(int),
+                              cudaMemcpyHostToDevice, s));
     build_tree(pl, ni, d[0], d[1], d[2], d[3], d[4], d[5], nj, d[6], d[7], d[8], d[9], d[10], d[11], bbox ? bb : nullptr);
     // caller-order copy of the geometry for the transposed plan
     pl->geo.alloc((size_t)6 * ni + 6 * (size_t)nj);
@@ -501,6 +533,35 @@ int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, c
   });
 }
 
+}  // namespace
+
+extern "C" {
+
+int fmmb_set_geometry(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
+                      const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
+                      const float* snx, const float* sny, const float* snz, const float* bbox) {
+  return geometry_impl(pl, 1, nullptr, nullptr, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+}
+
+int fmmb_set_geometry_batch(fmmb_plan* pl, int nprob, const int* t_off, const float* tx, const float* ty,
+                            const float* tz, const float* tnx, const float* tny, const float* tnz, const int* s_off,
+                            const float* sx, const float* sy, const float* sz, const float* snx, const float* sny,
+                            const float* snz, const float* bbox) {
+  int ni = 0, nj = 0;
+  const int rc = guarded([&] {
+    FMMB_REQUIRE(pl && t_off && s_off, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(nprob >= 1, FMMB_ERR_ARG, "need at least one problem");
+    for (int w = 0; w < 2; w++) {
+      const int* src = (w ? s_off : t_off) + nprob;
+      int& dst = w ? nj : ni;
+      if (is_device_ptr(src)) FMMB_CUDA(cudaMemcpy(&dst, src, sizeof(int), cudaMemcpyDeviceToHost));
+      else dst = *src;
+    }
+  });
+  if (rc != FMMB_OK) return rc;
+  return geometry_impl(pl, nprob, t_off, s_off, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+}
+
 }  // extern "C"
 
 namespace {
@@ -586,12 +647,12 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   {
     PhaseTimer tm(pl, 1, m);
     if (pl->ref)  // the reference's spherical formulation, quirks included
-      launch_p2m(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(),
+      launch_p2m(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(),
                  qs, pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
     else if (!(pl->cfg.precision == FMMB_MIXED &&
-               launch_p2m_f32(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
+               launch_p2m_f32(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(),
                               pl->snrm.get(), qs, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m)))
-      launch_p2m_cart(ker, nleaf_j, p, K, pl->key_j.get() + pl->off_j[lmax], pl->leaf_j.get(), pl->spos.get(),
+      launch_p2m_cart(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(),
                       pl->snrm.get(), qs, pl->d_fac.get(), pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
   }
   FMMB_CUDA(time_mark(pl, pl->ev[3], m));
@@ -667,13 +728,13 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   {
     PhaseTimer tm(pl, 5, m);
     if (pl->ref)
-      launch_l2p(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
+      launch_l2p(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
                  pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
     else if (!(pl->cfg.precision == FMMB_MIXED &&
-               launch_l2p_f32(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(),
+               launch_l2p_f32(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
                               pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef,
                               pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m)))
-      launch_l2p_cart(ker, nleaf_i, p, K, pl->key_i.get() + pl->off_i[lmax], pl->leaf_i.get(), pl->tpos.get(),
+      launch_l2p_cart(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
                       pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K,
                       pot_far, g_far, pl->ni, m);
   }
@@ -896,10 +957,11 @@ fmmb_plan* transposed_plan(fmmb_plan* pl) {
   const float* sg = g + (size_t)6 * ni;   // this plan's sources: the transposed targets
   const bool tn = c.kernel == FMMB_LAPLACE_GNI, sn = c.kernel == FMMB_LAPLACE_GNJ;
   if (rc == FMMB_OK)
-    rc = fmmb_set_geometry(t, nj, sg, sg + nj, sg + 2 * (size_t)nj, tn ? sg + 3 * (size_t)nj : nullptr,
-                           tn ? sg + 4 * (size_t)nj : nullptr, tn ? sg + 5 * (size_t)nj : nullptr, ni, tg, tg + ni,
-                           tg + 2 * (size_t)ni, sn ? tg + 3 * (size_t)ni : nullptr, sn ? tg + 4 * (size_t)ni : nullptr,
-                           sn ? tg + 5 * (size_t)ni : nullptr, pl->bbox);
+    rc = geometry_impl(t, pl->nprob, pl->prob_soff.data(), pl->prob_toff.data(), nj, sg, sg + nj, sg + 2 * (size_t)nj,
+                       tn ? sg + 3 * (size_t)nj : nullptr, tn ? sg + 4 * (size_t)nj : nullptr,
+                       tn ? sg + 5 * (size_t)nj : nullptr, ni, tg, tg + ni, tg + 2 * (size_t)ni,
+                       sn ? tg + 3 * (size_t)ni : nullptr, sn ? tg + 4 * (size_t)ni : nullptr,
+                       sn ? tg + 5 * (size_t)ni : nullptr, pl->bbox);
   if (rc != FMMB_OK) {
     const std::string msg = fmmb_last_error();
     if (t) fmmb_plan_destroy(t);
@@ -988,8 +1050,29 @@ int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, 
     const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
     DevBuf<double> out;
     out.alloc((size_t)cnt * 4 + 1);
-    launch_direct_f64(pl->cfg.kernel, i0, i1, pl->inv_i.get(), pl->tpos.get(), pl->tnrm.get(), nj, pl->spos.get(),
-                      pl->snrm.get(), pl->qs.get(), make_sem(pl), out.get(), want_grad ? out.get() + cnt : nullptr, m);
+    if (pl->nprob == 1) {
+      launch_direct_f64(pl->cfg.kernel, i0, i1, pl->inv_i.get(), pl->tpos.get(), pl->tnrm.get(), nj, pl->spos.get(),
+                        pl->snrm.get(), pl->qs.get(), make_sem(pl), out.get(), want_grad ? out.get() + cnt : nullptr, m);
+    } else {
+      // one launch per problem over its own sources (sorted source positions
+      // of problem b are [soff[b], soff[b+1]) like the caller's), then the
+      // [pot | gx | gy | gz] blocks of each problem moved into place
+      DevBuf<double> tmp;
+      tmp.alloc((size_t)cnt * 4 + 1);
+      const std::vector<int>&to = pl->prob_toff, &so = pl->prob_soff;
+      for (int b = 0; b < pl->nprob; b++) {
+        const int a0 = std::max(i0, to[b]), a1 = std::min(i1, to[b + 1]);
+        if (a0 >= a1) continue;
+        const int mb = a1 - a0;
+        double* tb = tmp.get() + (size_t)4 * (a0 - i0);
+        launch_direct_f64(pl->cfg.kernel, a0, a1, pl->inv_i.get(), pl->tpos.get(), pl->tnrm.get(), so[b + 1] - so[b],
+                          pl->spos.get() + so[b], pl->snrm.get() + so[b], pl->qs.get() + so[b], make_sem(pl), tb,
+                          want_grad ? tb + mb : nullptr, m);
+        for (int c = 0; c < (want_grad ? 4 : 1); c++)
+          FMMB_CUDA(cudaMemcpyAsync(out.get() + (size_t)c * cnt + (a0 - i0), tb + (size_t)c * mb, mb * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, m));
+      }
+    }
     FMMB_CUDA(cudaMemcpyAsync(pot, out.get(), cnt * sizeof(double), is_device_ptr(pot) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, m));
     if (want_grad)
       FMMB_CUDA(cudaMemcpyAsync(grad, out.get() + cnt, 3 * (size_t)cnt * sizeof(double),

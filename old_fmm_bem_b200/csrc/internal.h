@@ -142,6 +142,13 @@ struct fmmb_plan {
   fmmb::DevBuf<int2> leaf_i, leaf_j;         // leaf (first, count) in sorted order
   fmmb::DevBuf<int> p2p_list;                // [nleaf_i][27] source leaf or -1
   fmmb::DevBuf<int> m2l_list;                // [tot_i][189] source box (within level) or -1
+  fmmb::DevBuf<int> leafkey_i, leafkey_j;    // leaf keys without the problem bits (box centres)
+  // independent problems in one plan (fmmb_set_geometry_batch): problem b owns
+  // targets [prob_toff[b], prob_toff[b+1]) and sources [prob_soff[b], ..),
+  // in caller and in sorted order alike; on the device [toff | soff]
+  int nprob = 1;
+  std::vector<int> prob_toff, prob_soff;
+  fmmb::DevBuf<int> d_prob_off;
   fmmb::DevBuf<int> child_start_j;           // for M2M: per source box at level l (<lmax): first child index, count
   fmmb::DevBuf<int> child_count_j;
 

@@ -13,6 +13,13 @@
 // 189 slots per target box for M2L, -1 where the source box is empty.  The
 // slot order is the reference's loop order, so dropping the -1 entries gives
 // the reference lists.
+//
+// Forest (many independent problems in one plan): the problem index of a
+// point sits above its 3*lmax Morton bits, so the sort groups the points by
+// problem, every box belongs to one problem (its key at level l is
+// (problem << 3l) | morton), and a neighbour or interaction-list lookup only
+// finds boxes of the same problem.  With one problem the keys are the
+// reference's.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -204,13 +211,31 @@ __device__ __forceinline__ int box_coord(float x, float xmin, double rb, int kl)
   return c;
 }
 
+// off[0..nprob]: first point of each problem (off[nprob] = n)
 __global__ void keys_kernel(int n, const float* x, const float* y, const float* z, float xmin, float ymin, float zmin,
-                            double rb, int lmax, int* key, int* idx) {
+                            double rb, int lmax, int nprob, const int* off, int* key, int* idx) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int kl = 1 << lmax;
-  key[i] = morton(box_coord(x[i], xmin, rb, kl), box_coord(y[i], ymin, rb, kl), box_coord(z[i], zmin, rb, kl), lmax);
+  int pid = 0;
+  if (nprob > 1) {  // last problem whose first point is <= i
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (off[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    pid = lo;
+  }
+  key[i] = (pid << (3 * lmax)) |
+           morton(box_coord(x[i], xmin, rb, kl), box_coord(y[i], ymin, rb, kl), box_coord(z[i], zmin, rb, kl), lmax);
   idx[i] = i;
+}
+
+// spatial part of the keys (problem bits removed)
+__global__ void mask_keys(int n, const int* key, int mask, int* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = key[i] & mask;
 }
 
 __global__ void gather_points(int n, const int* perm, const float* x, const float* y, const float* z, const float* nx,
@@ -282,7 +307,8 @@ __global__ void p2p_lists(int nleaf_i, const int* key_i, int nleaf_j, const int*
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nleaf_i) return;
   int ix, iy, iz;
-  demorton(key_i[b], ix, iy, iz);
+  const int smask = (1 << (3 * lev)) - 1, prob = key_i[b] & ~smask;
+  demorton(key_i[b] & smask, ix, iy, iz);
   const int kl = 1 << lev;
   int s = 0;
   for (int jx = ix - 1; jx <= ix + 1; jx++)
@@ -290,7 +316,7 @@ __global__ void p2p_lists(int nleaf_i, const int* key_i, int nleaf_j, const int*
       for (int jz = iz - 1; jz <= iz + 1; jz++) {
         int v = -1;
         if (jx >= 0 && jx < kl && jy >= 0 && jy < kl && jz >= 0 && jz < kl)
-          v = find_key(key_j, nleaf_j, morton(jx, jy, jz, lev));
+          v = find_key(key_j, nleaf_j, prob | morton(jx, jy, jz, lev));
         list[(size_t)b * kP2PSlots + s++] = v;
       }
 }
@@ -303,13 +329,15 @@ __global__ void m2l_lists(int nbox_i, const int* key_i, int nbox_j, const int* k
   if (t >= nbox_i * kM2LSlots) return;
   const int b = t / kM2LSlots, s = t % kM2LSlots;
   const int key = key_i[b];
+  const int smask = (1 << (3 * lev)) - 1, prob = key & ~smask;
   int ix, iy, iz;
-  demorton(key, ix, iy, iz);
+  demorton(key & smask, ix, iy, iz);
   const int code = slot_rel[(key & 7) * kM2LSlots + s];
   const int jx = ix - (code / 49 - 3), jy = iy - ((code / 7) % 7 - 3), jz = iz - (code % 7 - 3);
   const int kl = 1 << lev;
   int v = -1;
-  if (jx >= 0 && jx < kl && jy >= 0 && jy < kl && jz >= 0 && jz < kl) v = find_key(key_j, nbox_j, morton(jx, jy, jz, lev));
+  if (jx >= 0 && jx < kl && jy >= 0 && jy < kl && jz >= 0 && jz < kl)
+    v = find_key(key_j, nbox_j, prob | morton(jx, jy, jz, lev));
   list[t] = v;
 }
 
@@ -362,7 +390,14 @@ __global__ void gather_int(int n, const int* idx, const int* src, int* dst) {
 struct Side {
   const float *x, *y, *z, *nx, *ny, *nz;
   int n;
+  const int* off;  // device [nprob + 1] first point of each problem
 };
+
+int prob_bits(int nprob) {
+  int b = 0;
+  while ((1 << b) < nprob) b++;
+  return b;
+}
 
 // Builds keys, order, sorted points and all levels of one point set.
 void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
@@ -372,9 +407,9 @@ void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
   idx.alloc(n);
   const double rb = (double)((float)(1 << lmax) / pl->bbox[3]);  // kl/rd: float division, as the reference
   keys_kernel<<<blocks(n, 256), 256, 0, s>>>(n, sd.x, sd.y, sd.z, pl->bbox[0], pl->bbox[1], pl->bbox[2], rb, lmax,
-                                              key.get(), idx.get());
+                                              pl->nprob, sd.off, key.get(), idx.get());
   FMMB_CHECK_LAUNCH();
-  radix_sort(key.get(), idx.get(), n, 3 * lmax, s);
+  radix_sort(key.get(), idx.get(), n, 3 * lmax + prob_bits(pl->nprob), s);
   DevBuf<int>& perm = is_target ? pl->perm_i : pl->perm_j;
   DevBuf<float4>& pos = is_target ? pl->tpos : pl->spos;
   DevBuf<float4>& nrm = is_target ? pl->tnrm : pl->snrm;
@@ -442,6 +477,12 @@ void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
   leaf.alloc(nbox[lmax]);
   leaf_ranges<<<blocks(nbox[lmax], 256), 256, 0, s>>>(nbox[lmax], n, fstore[lmax].get(), leaf.get());
   FMMB_CHECK_LAUNCH();
+  // leaf keys without the problem bits (box centres of P2M / L2P)
+  DevBuf<int>& lk = is_target ? pl->leafkey_i : pl->leafkey_j;
+  lk.alloc(nbox[lmax]);
+  mask_keys<<<blocks(nbox[lmax], 256), 256, 0, s>>>(nbox[lmax], keys_all.get() + off[lmax], (1 << (3 * lmax)) - 1,
+                                                    lk.get());
+  FMMB_CHECK_LAUNCH();
   if (!is_target) {
     pl->child_start_j.alloc(tot);
     pl->child_count_j.alloc(tot);
@@ -485,6 +526,8 @@ void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const f
                 const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
                 const float* snx, const float* sny, const float* snz, const float* bbox_in) {
   cudaStream_t s = pl->st.main;
+  FMMB_REQUIRE(3 * pl->cfg.lmax + prob_bits(pl->nprob) <= 30, FMMB_ERR_CAPACITY,
+               "box keys: 3*lmax + ceil(log2(problems)) must stay within 30 bits");
   pl->ni = ni;
   pl->nj = nj;
   pl->lmax = pl->cfg.lmax;
@@ -537,8 +580,8 @@ void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const f
     pl->bbox[3] = rd;
   }
   FMMB_REQUIRE(pl->bbox[3] > 0, FMMB_ERR_ARG, "root box side must be positive");
-  build_side(pl, Side{tx, ty, tz, tnx, tny, tnz, ni}, true, s);
-  build_side(pl, Side{sx, sy, sz, snx, sny, snz, nj}, false, s);
+  build_side(pl, Side{tx, ty, tz, tnx, tny, tnz, ni, pl->d_prob_off.get()}, true, s);
+  build_side(pl, Side{sx, sy, sz, snx, sny, snz, nj, pl->d_prob_off.get() + pl->nprob + 1}, false, s);
 
   const int lmax = pl->lmax;
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];

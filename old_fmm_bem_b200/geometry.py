@@ -82,3 +82,57 @@ def bem_double_layer_problem(subdivisions: int = 6, seed: int = 0, rule: str = "
     dens = rng.uniform(-1.0, 1.0, len(f))
     q = (dens[panel] * w).astype(np.float32)
     return x, n, q
+
+
+def geodesic_sphere(freq: int, radius: float = 1.0):
+    """Class-I geodesic sphere of frequency `freq`: every icosahedron face split
+    into freq^2 triangles (20 * freq^2 in all, any size, unlike the 4^s steps
+    of `icosphere`), vertices projected on the sphere, outward orientation.
+    Edge vertices are not merged between faces: the BEM inputs need only the
+    triangles."""
+    v0, f0 = icosphere(0)
+    nu = int(freq)
+    assert nu >= 1
+    ij = np.array([(i, j) for i in range(nu + 1) for j in range(nu + 1 - i)])
+    loc = {(i, j): k for k, (i, j) in enumerate(ij)}
+    tri = []
+    for i in range(nu):
+        for j in range(nu - i):
+            tri.append((loc[i, j], loc[i + 1, j], loc[i, j + 1]))
+            if i + j <= nu - 2:
+                tri.append((loc[i + 1, j], loc[i + 1, j + 1], loc[i, j + 1]))
+    tri = np.array(tri, dtype=np.int64)
+    a, b, c = v0[f0[:, 0]], v0[f0[:, 1]], v0[f0[:, 2]]
+    u = ij[:, 0:1] / nu
+    w = ij[:, 1:2] / nu
+    pts = a[:, None, :] + u[None] * (b - a)[:, None, :] + w[None] * (c - a)[:, None, :]
+    pts /= np.linalg.norm(pts, axis=2, keepdims=True)
+    v = pts.reshape(-1, 3) * radius
+    f = (tri[None, :, :] + (np.arange(20) * len(ij))[:, None, None]).reshape(-1, 3)
+    n = np.cross(v[f[:, 1]] - v[f[:, 0]], v[f[:, 2]] - v[f[:, 0]])
+    flip = np.einsum("ij,ij->i", n, v[f].mean(axis=1)) < 0
+    f[flip] = f[flip][:, [0, 2, 1]]
+    return v, f
+
+
+# Dielectric constants of the reference's BEM solve (bio/parameters.h: e1 = 4,
+# e2 = 20) and the shell operator built from them (bio/main.cxx:43-48, 65)
+E1, E2 = 4.0, 20.0
+BEM_DIAG = (E1 + E2) / (2 * E1 * (E1 - E2))
+
+
+def bem_batch_problems(nprob: int = 64, tmin: int = 2000, tmax: int = 200000, seed: int = 0):
+    """Independent unit-sphere BEM problems with triangle counts log-uniform in
+    [tmin, tmax] (geodesic frequency round(sqrt(T / 20))), one point per
+    triangle at its centroid with outward unit normal and the panel area, as
+    the reference's BEM driver places them (bio/main.cxx:256-282).  Returns a
+    list of (x (3, n) float32, normals (3, n) float32, area (n,) float64)."""
+    rng = np.random.default_rng(seed)
+    t = np.exp(rng.uniform(np.log(tmin), np.log(tmax), nprob))
+    out = []
+    for T in t:
+        nu = max(1, int(round((T / 20.0) ** 0.5)))
+        v, f = geodesic_sphere(nu)
+        x, n, w, _ = quadrature_points(v, f, "centroid")
+        out.append((x, n, w))
+    return out

@@ -1,0 +1,96 @@
+"""Dense BEM operator and GMRES in numpy -- TEST INFRASTRUCTURE ONLY.
+
+The checker of fmmb_gmres.  The reference solves its boundary-integral system
+with PETSc KSP GMRES over a shell matrix (bio/main.cxx:27-70, 377-413); PETSc is
+not vendored with the reference and is absent here, and no reference test pins
+a solve, so GMRES parity is unpinned: this module restates the method from its
+definition (x_k minimises the preconditioned residual over x_0 plus the Krylov
+space of order k; Saad and Schultz, SIAM J. Sci. Stat. Comput. 7 (1986)), with
+modified Gram-Schmidt Arnoldi and a least-squares solve per cycle -- not the
+CGS2 + Givens form of the product -- and it is checked against
+numpy.linalg.solve.  The dense operator is the direct-sum kernel of
+kernel/Gni_dir.cxx:12-17 / kernel/Gnj_dir.cxx:12-17 (accurate semantics: no
+softening, zero-distance pairs skipped), checked against the oracle's C direct
+sum in tests/test_oracle_pin.py.
+
+Only tests/ and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+COEF = 0.25 / np.pi
+
+
+def kernel_matrix(x, kernel, nt=None, ns=None, xs=None):
+    """Dense FP64 matrix of the Laplace kernels between targets x (3, n) and
+    sources xs (3, m) (default x): G (kernel 0), Gni (1, target normals nt),
+    Gnj (2, source normals ns); zero-distance pairs give 0."""
+    x = np.asarray(x, np.float64)
+    xs = x if xs is None else np.asarray(xs, np.float64)
+    d = x[:, :, None] - xs[:, None, :]
+    r2 = np.einsum("kij,kij->ij", d, d)
+    zero = r2 == 0
+    r2[zero] = 1.0
+    rinv = 1.0 / np.sqrt(r2)
+    if kernel == 0:
+        k = COEF * rinv
+    elif kernel == 1:
+        k = COEF * np.einsum("kij,ki->ij", d, np.asarray(nt, np.float64)) * rinv ** 3
+    else:
+        k = COEF * np.einsum("kij,kj->ij", d, np.asarray(ns, np.float64)) * rinv ** 3
+    k[zero] = 0.0
+    return k
+
+
+def bem_matrix(x, normals, weight, kernel, diag):
+    """A = diag * I + K diag(weight) for targets = sources = x (the shell
+    matrix of bio/main.cxx:27-53 with K = Gni there)."""
+    K = kernel_matrix(x, kernel, nt=normals if kernel == 1 else None, ns=normals if kernel == 2 else None)
+    return diag * np.eye(len(weight)) + K * np.asarray(weight, np.float64)[None, :]
+
+
+def gmres(A, b, x0=None, *, precond=1.0, restart=30, max_iter=20, rtol=0.0):
+    """Left-preconditioned restarted GMRES (M^-1 = precond * I) for A x = b.
+    Returns (x, iterations, ||r_k|| / ||r_0|| of the preconditioned residual)."""
+    n = len(b)
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    it = 0
+    beta0 = None
+    rel = 0.0
+    while True:
+        r = precond * (b - A @ x)
+        beta = np.linalg.norm(r)
+        if beta0 is None:
+            beta0 = beta
+        if beta == 0.0 or beta <= rtol * beta0 or it >= max_iter:
+            rel = beta / beta0 if beta0 else 0.0
+            break
+        V = [r / beta]
+        H = np.zeros((restart + 1, restart))
+        k = 0
+        done = False
+        while k < restart and it < max_iter:
+            w = precond * (A @ V[k])
+            for i in range(k + 1):
+                H[i, k] = V[i] @ w
+                w = w - H[i, k] * V[i]
+            H[k + 1, k] = np.linalg.norm(w)
+            k += 1
+            it += 1
+            e1 = np.zeros(k + 1)
+            e1[0] = beta
+            y, *_ = np.linalg.lstsq(H[:k + 1, :k], e1, rcond=None)
+            res = np.linalg.norm(e1 - H[:k + 1, :k] @ y)
+            if H[k, k - 1] <= 1e-14 * np.linalg.norm(H[:k + 1, k - 1]) or res <= rtol * beta0:
+                done = True
+                break
+            V.append(w / H[k, k - 1])
+        e1 = np.zeros(k + 1)
+        e1[0] = beta
+        y, *_ = np.linalg.lstsq(H[:k + 1, :k], e1, rcond=None)
+        x = x + np.stack(V[:k], 1) @ y
+        rel = np.linalg.norm(e1 - H[:k + 1, :k] @ y) / beta0
+        if done or it >= max_iter:
+            break
+    return x, it, rel
