@@ -442,6 +442,86 @@ def run_c3(args):
                                                   res[f"p{p}_mixed"]["forward_backward_ms"] for p in (10, 12)}}))
 
 
+def run_c4(args):
+    """Batched BEM: 64 independent unit-sphere problems with triangle counts
+    log-uniform in [2k, 200k] (seeded), one point per triangle (centroid,
+    outward normal, panel area); for Gni and for Gnj the systems
+    diag x + K(area/e1 .* x) = b with 8 right-hand sides U[-1, 1] each, 20
+    GMRES iterations (fmmb_gmres, restart 30).  All 64 x 8 systems share the
+    launches of one forest plan (fmmb_set_geometry_batch), every right-hand
+    side replayed as a CUDA graph; one depth for the forest from
+    fmmb_autotune_lmax_batch.  p = 10, mixed precision."""
+    import torch
+    import old_fmm_bem_b200 as ob
+    from old_fmm_bem_b200 import geometry
+    probs = geometry.bem_batch_problems(64, seed=17)
+    off = np.cumsum([0] + [p[0].shape[1] for p in probs]).astype(np.int32)
+    x = np.ascontiguousarray(np.concatenate([p[0] for p in probs], axis=1))
+    nrm = np.ascontiguousarray(np.concatenate([p[1] for p in probs], axis=1))
+    weight = (np.concatenate([p[2] for p in probs]) / geometry.E1).astype(np.float32)
+    n, nrhs, iters = x.shape[1], 8, 20
+    bbox = (-1.0001, -1.0001, -1.0001, 2.0002)
+    xd, nd, wd = torch.from_numpy(x).cuda(), torch.from_numpy(nrm).cuda(), torch.from_numpy(weight).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    rng = np.random.default_rng(23)
+    b = torch.from_numpy(rng.uniform(-1, 1, nrhs * n)).cuda()
+    res = {}
+    total_ms = 0.0
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for name, kernel in (("gni", ob.LAPLACE_GNI), ("gnj", ob.LAPLACE_GNJ)):
+            tn, sn = (nd, None) if kernel == ob.LAPLACE_GNI else (None, nd)
+            kw = dict(kernel=kernel, p=P_ORDER, precision=ob.MIXED, semantics=ob.SEM_ACCURATE, exclude_self=True)
+            lmax, tune = ob.autotune_lmax_batch(off, xd, off, xd, target_normals=tn, source_normals=sn, bbox=bbox,
+                                                lmin=3, lmax=6, reps=1, nrhs=nrhs, **kw)
+            plan = ob.Plan(lmax=lmax, nrhs=nrhs, **kw)
+            plan.set_stream(stream)
+            t0 = time.perf_counter()
+            plan.set_geometry_batch(off, xd, off, xd, tn, sn, bbox=bbox)
+            torch.cuda.synchronize()
+            tree_s = time.perf_counter() - t0
+            X = torch.zeros(nrhs * n, dtype=torch.float64, device="cuda")
+            box = {}
+
+            def solve():
+                X.zero_()
+                box["out"] = plan.gmres(b, X, wd, diag=geometry.BEM_DIAG, precond=1 / geometry.BEM_DIAG, restart=30,
+                                        max_iter=iters)
+
+            ms = _timed(solve, stream, max(1, min(args.steps, 3)), max(3, min(args.warmup, 3)), flush)
+            _, it, resid = box["out"]
+            # one matvec against the per-problem FP64 direct sum (first right-hand side, 1024 targets of
+            # each of the four largest problems)
+            q1 = (weight * rng.uniform(-1, 1, n)).astype(np.float32)
+            q8 = np.tile(q1, nrhs)
+            pot, _ = plan.evaluate(q8, f64=True)
+            errs = []
+            for k in np.argsort(np.diff(off))[-4:]:
+                i0 = int(off[k])
+                i1 = min(int(off[k + 1]), i0 + 1024)
+                vd, _ = plan.direct(q8, i0, i1)
+                errs.append(float(np.linalg.norm(pot[i0:i1] - vd) / np.linalg.norm(vd)))
+            matvecs = iters + 1  # the initial residual and one per iteration
+            res[name] = {"lmax": lmax, "autotune_ms_per_matvec": tune, "tree_build_s": tree_s, "solve_ms": ms,
+                         "iterations": it, "matvecs": matvecs, "matvec_ms": ms / matvecs,
+                         "max_rel_resid": float(np.max(resid)), "median_rel_resid": float(np.median(resid)),
+                         "rel_err_vs_fp64_direct": float(np.sqrt(np.mean(np.square(errs)))),
+                         "gpu_launches_per_matvec": plan.stats()["launches"]}
+            total_ms += ms
+            plan.close()
+    pts = 2 * n * nrhs * (iters + 1)
+    print(json.dumps({"metric": "batched BEM GMRES: FMM matvec Mpts/s (64 unit-sphere problems, 8 RHS, Gni + Gnj)",
+                      "value": pts / (total_ms * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1,
+                      "steps": max(1, min(args.steps, 3)), "ms_per_step": total_ms, "dtype": "f32+tf32x3+f64",
+                      "data": "synthetic",
+                      "config": {"workload": f"64 geodesic unit spheres, {n} centroid points in all "
+                                             f"({int(np.diff(off).min())}..{int(np.diff(off).max())} per problem), "
+                                             "Gni and Gnj BEM systems (diag (e1+e2)/(2e1(e1-e2)), weights area/e1, "
+                                             "e1=4, e2=20), 8 RHS U[-1,1], 20 GMRES iterations, p=10 mixed; step = "
+                                             "both solves", "l2": "flushed between steps"},
+                      "results": res, "clocks": clk.summary()}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,9 +530,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m"],
+    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64"],
                     help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "
-                         "points; adjoint1m: forward + backward on 1,048,576 clustered points")
+                         "points; adjoint1m: forward + backward on 1,048,576 clustered points; batch64: GMRES on 64 "
+                         "BEM problems x 8 right-hand sides")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -468,6 +549,8 @@ def main():
         run_c1(args)
     elif args.config == "adjoint1m":
         run_c3(args)
+    elif args.config == "batch64":
+        run_c4(args)
     else:
         run_ours(args, rank, world)
     if world > 1 and args.impl == "ours":

@@ -207,6 +207,14 @@ FMMB_API int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx,
                                 const float* snz, const float* bbox, int lmin, int lmax_hi, int reps, int* best,
                                 float* ms_out);
 
+/* fmmb_autotune_lmax for a batch of independent problems
+ * (fmmb_set_geometry_batch's arguments): the one depth of the forest. */
+FMMB_API int fmmb_autotune_lmax_batch(const fmmb_config* cfg, int nprob, const int* t_off, const float* tx,
+                                      const float* ty, const float* tz, const float* tnx, const float* tny,
+                                      const float* tnz, const int* s_off, const float* sx, const float* sy,
+                                      const float* sz, const float* snx, const float* sny, const float* snz,
+                                      const float* bbox, int lmin, int lmax_hi, int reps, int* best, float* ms_out);
+
 /* ---- inspection (tests, tooling) ---- */
 
 /* Tree of the current geometry.  kind: 0 target permutation (sorted position

@@ -33,7 +33,7 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_get_expansion_size", "fmmb_get_expansions", "fmmb_get_timings", "fmmb_get_stats",
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
-           "fmmb_gmres"]
+           "fmmb_gmres", "fmmb_autotune_lmax_batch"]
 
 
 def lib_path() -> str:
@@ -83,6 +83,8 @@ def load():
     lib.fmmb_evaluate_transpose_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_position_grad.argtypes = [_vp, _vp, _vp, _vp, _vp]
     lib.fmmb_autotune_lmax.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
+        [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_autotune_lmax_batch.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, _vp] + [_vp] * 6 + [_vp] + \
         [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
     lib.fmmb_direct_static.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
         [_vp] * 6 + [_vp, _vp, _vp, _vp]
@@ -319,33 +321,57 @@ class Plan:
         return dict(zip(["ni", "nj", "leaves_i", "leaves_j", "p2p_pairs", "m2l_pairs", "lmax", "launches"], o.tolist()))
 
 
-def autotune_lmax(targets, sources, *, kernel=LAPLACE_G, target_normals=None, source_normals=None, p=8,
-                  precision=FP64, semantics=SEM_REFERENCE, eps2=0.0, exclude_self=False, bbox=None, lmin=0, lmax=0,
-                  reps=3):
-    """Fastest octree depth for this geometry (fmmb_autotune_lmax); returns
-    (best_lmax, {lmax: ms per evaluate})."""
+def _autotune(kernel, p, precision, semantics, eps2, exclude_self, nrhs, ni, nj, lmin, lmax, run):
     lib = load()
     cfg = _Config()
     lib.fmmb_config_init(ctypes.byref(cfg))
     cfg.kernel, cfg.p, cfg.precision, cfg.semantics = kernel, p, precision, semantics
-    cfg.eps2, cfg.exclude_self = eps2, int(exclude_self)
-    t = [_ptr(targets[k], np.float32) for k in range(3)]
-    s = [_ptr(sources[k], np.float32) for k in range(3)]
-    tn = [_ptr(target_normals[k], np.float32) for k in range(3)] if target_normals is not None else [(None, None)] * 3
-    sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
-    bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
-    ni, nj = len(targets[0]), len(sources[0])
+    cfg.eps2, cfg.exclude_self, cfg.nrhs = eps2, int(exclude_self), nrhs
     best = ctypes.c_int(-1)
     ms = np.zeros(16, np.float32)
-    _check(lib.fmmb_autotune_lmax(ctypes.byref(cfg), ni, t[0][0], t[1][0], t[2][0], tn[0][0], tn[1][0], tn[2][0], nj,
-                                  s[0][0], s[1][0], s[2][0], sn[0][0], sn[1][0], sn[2][0], bb[0], lmin, lmax, reps,
-                                  ctypes.byref(best), ms.ctypes.data))
+    _check(run(lib, cfg, best, ms))
     if lmin <= 0 or lmax <= 0:  # the library chose the range around its estimate
         l = 2
         while l < 10 and max(ni, nj) / 8.0 ** l > 64.0:
             l += 1
         lmin, lmax = max(2, l - 1), min(10, l + 2)
     return best.value, {l: float(ms[l - lmin]) for l in range(lmin, lmax + 1)}
+
+
+def _sets(targets, sources, target_normals, source_normals, bbox):
+    t = [_ptr(targets[k], np.float32) for k in range(3)]
+    s = [_ptr(sources[k], np.float32) for k in range(3)]
+    tn = [_ptr(target_normals[k], np.float32) for k in range(3)] if target_normals is not None else [(None, None)] * 3
+    sn = [_ptr(source_normals[k], np.float32) for k in range(3)] if source_normals is not None else [(None, None)] * 3
+    bb = _ptr(np.asarray(bbox, np.float32), np.float32) if bbox is not None else (None, None)
+    return [x[0] for x in t], [x[0] for x in tn], [x[0] for x in s], [x[0] for x in sn], bb[0], (t, s, tn, sn, bb)
+
+
+def autotune_lmax(targets, sources, *, kernel=LAPLACE_G, target_normals=None, source_normals=None, p=8,
+                  precision=FP64, semantics=SEM_REFERENCE, eps2=0.0, exclude_self=False, bbox=None, lmin=0, lmax=0,
+                  reps=3, nrhs=1):
+    """Fastest octree depth for this geometry (fmmb_autotune_lmax); returns
+    (best_lmax, {lmax: ms per evaluate})."""
+    t, tn, s, sn, bb, keep = _sets(targets, sources, target_normals, source_normals, bbox)
+    ni, nj = len(targets[0]), len(sources[0])
+    return _autotune(kernel, p, precision, semantics, eps2, exclude_self, nrhs, ni, nj, lmin, lmax,
+                     lambda lib, cfg, best, ms: lib.fmmb_autotune_lmax(
+                         ctypes.byref(cfg), ni, *t, *tn, nj, *s, *sn, bb, lmin, lmax, reps, ctypes.byref(best),
+                         ms.ctypes.data))
+
+
+def autotune_lmax_batch(t_off, targets, s_off, sources, *, kernel=LAPLACE_G, target_normals=None,
+                        source_normals=None, p=8, precision=FP64, semantics=SEM_REFERENCE, eps2=0.0,
+                        exclude_self=False, bbox=None, lmin=0, lmax=0, reps=3, nrhs=1):
+    """Fastest depth of a forest plan (fmmb_autotune_lmax_batch)."""
+    to = np.ascontiguousarray(t_off, np.int32)
+    so = np.ascontiguousarray(s_off, np.int32)
+    t, tn, s, sn, bb, keep = _sets(targets, sources, target_normals, source_normals, bbox)
+    ni, nj = int(to[-1]), int(so[-1])
+    return _autotune(kernel, p, precision, semantics, eps2, exclude_self, nrhs, ni, nj, lmin, lmax,
+                     lambda lib, cfg, best, ms: lib.fmmb_autotune_lmax_batch(
+                         ctypes.byref(cfg), len(to) - 1, to.ctypes.data, *t, *tn, so.ctypes.data, *s, *sn, bb, lmin,
+                         lmax, reps, ctypes.byref(best), ms.ctypes.data))
 
 
 def fmm(xi, yi, zi, gxi, gyi, gzi, xj, yj, zj, gxj, gyj, gzj, vj, neq, *, lmax, xmin, ymin, zmin, rd, p=8,

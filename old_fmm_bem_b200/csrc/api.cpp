@@ -830,10 +830,16 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
       if (want_grad && !grad_dev) gd = (T*)base;
     }
     for (int r = 0; r < nr; r++) {
-      if (nr == 1 && pl->use_graph)
+      if (pl->use_graph) {
+        // the graph reads the charges of the first block: move right-hand
+        // side r there once the previous one is consumed (stream order)
+        if (r > 0)
+          FMMB_CUDA(cudaMemcpyAsync(pl->qs.get(), pl->qs.get() + (size_t)r * nj, (size_t)nj * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, m));
         run_graph(pl, want_grad);
-      else
+      } else {
         run_one(pl, pl->qs.get() + (size_t)r * nj, want_grad);
+      }
       const double* pn = pl->pot_s.get();
       const double* gn = pl->grad_s.get();
       if (sizeof(T) == 4)
@@ -863,10 +869,15 @@ int fmmb_evaluate_f64(fmmb_plan* pl, const float* q, double* pot, double* grad) 
   return evaluate_impl<double>(pl, q, pot, grad);
 }
 
-int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
-                       const float* tnx, const float* tny, const float* tnz, int nj, const float* sx, const float* sy,
-                       const float* sz, const float* snx, const float* sny, const float* snz, const float* bbox,
-                       int lmin, int lmax_hi, int reps, int* best, float* ms_out) {
+}  // extern "C"
+
+namespace {
+
+// Times one evaluate per octree depth in [lmin, lmax_hi] on the geometry that
+// set_geo gives a fresh plan, and returns the fastest depth.
+template <typename SetGeo>
+int autotune_impl(const fmmb_config* cfg, int ni, int nj, int lmin, int lmax_hi, int reps, int* best, float* ms_out,
+                  SetGeo set_geo) {
   return guarded([&] {
     FMMB_REQUIRE(cfg && best, FMMB_ERR_ARG, "null argument");
     FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
@@ -901,8 +912,7 @@ int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const fl
       c.lmax = l;
       fmmb_plan* pl = nullptr;
       int rc = fmmb_plan_create(&c, &pl);
-      if (rc == FMMB_OK)
-        rc = fmmb_set_geometry(pl, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+      if (rc == FMMB_OK) rc = set_geo(pl);
       float ms = -1.f;
       if (rc == FMMB_OK) {
         float* g = cfg->kernel == FMMB_LAPLACE_G ? dgrad.get() : nullptr;
@@ -933,6 +943,41 @@ int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const fl
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     FMMB_REQUIRE(*best >= 0, FMMB_ERR_NOMEM, "no octree depth in the range fits on the device");
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                       const float* tnx, const float* tny, const float* tnz, int nj, const float* sx, const float* sy,
+                       const float* sz, const float* snx, const float* sny, const float* snz, const float* bbox,
+                       int lmin, int lmax_hi, int reps, int* best, float* ms_out) {
+  return autotune_impl(cfg, ni, nj, lmin, lmax_hi, reps, best, ms_out, [&](fmmb_plan* pl) {
+    return fmmb_set_geometry(pl, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+  });
+}
+
+int fmmb_autotune_lmax_batch(const fmmb_config* cfg, int nprob, const int* t_off, const float* tx, const float* ty,
+                             const float* tz, const float* tnx, const float* tny, const float* tnz, const int* s_off,
+                             const float* sx, const float* sy, const float* sz, const float* snx, const float* sny,
+                             const float* snz, const float* bbox, int lmin, int lmax_hi, int reps, int* best,
+                             float* ms_out) {
+  int ni = 0, nj = 0;
+  const int rc = guarded([&] {
+    FMMB_REQUIRE(t_off && s_off && nprob >= 1, FMMB_ERR_ARG, "null problem offsets");
+    for (int w = 0; w < 2; w++) {
+      const int* src = (w ? s_off : t_off) + nprob;
+      int& dst = w ? nj : ni;
+      if (is_device_ptr(src)) FMMB_CUDA(cudaMemcpy(&dst, src, sizeof(int), cudaMemcpyDeviceToHost));
+      else dst = *src;
+    }
+  });
+  if (rc != FMMB_OK) return rc;
+  return autotune_impl(cfg, ni, nj, lmin, lmax_hi, reps, best, ms_out, [&](fmmb_plan* pl) {
+    return fmmb_set_geometry_batch(pl, nprob, t_off, tx, ty, tz, tnx, tny, tnz, s_off, sx, sy, sz, snx, sny, snz,
+                                   bbox);
   });
 }
 

@@ -220,3 +220,22 @@ def test_autotune_lmax_picks_a_measured_depth(ob):
                                 bbox=(0, 0, 0, 1), lmin=2, lmax=4, reps=2)
     assert set(ms) == {2, 3, 4} and all(v > 0 for v in ms.values())
     assert best == min(ms, key=ms.get)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_many_right_hand_sides_equal_single_evaluates(precision, ob):
+    """nrhs = 3 in one evaluate (each right-hand side replayed through the
+    plan's CUDA graph) gives the three single evaluates, gradients included."""
+    t, tn, s, sn, q = make_points(12000, 110, "clustered")
+    rng = np.random.default_rng(111)
+    qs = rng.uniform(-1, 1, (3, s.shape[1])).astype(np.float32)
+    kw = dict(semantics=1, precision=precision, exclude_self=True)
+    pl = plan_for(ob, 0, 8, 4, t, tn, s, sn, nrhs=3, **kw)
+    v3, g3 = pl.evaluate(qs.ravel(), f64=True)
+    pl.close()
+    one = plan_for(ob, 0, 8, 4, t, tn, s, sn, **kw)
+    for r in range(3):
+        v, g = one.evaluate(qs[r], f64=True)
+        assert rel(v3[r * 12000:(r + 1) * 12000], v) < 1e-12
+        assert rel(g3.reshape(3, 3, -1)[r], g.reshape(3, -1)) < 1e-12
+    one.close()
