@@ -22,10 +22,11 @@ import os
 import numpy as np
 
 __all__ = ["Plan", "FMMError", "fmm", "G_dir", "Gni_dir", "Gnj_dir", "lib_path", "load",
-           "LAPLACE_G", "LAPLACE_GNI", "LAPLACE_GNJ", "FP64", "MIXED", "SEM_REFERENCE", "SEM_ACCURATE"]
+           "LAPLACE_G", "LAPLACE_GNI", "LAPLACE_GNJ", "HELMHOLTZ_G", "FP64", "MIXED", "SEM_REFERENCE", "SEM_ACCURATE"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LAPLACE_G, LAPLACE_GNI, LAPLACE_GNJ = 0, 1, 2
+HELMHOLTZ_G = 20
 FP64, MIXED = 0, 1
 SEM_REFERENCE, SEM_ACCURATE = 0, 1
 EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_set_stream", "fmmb_set_geometry",
@@ -47,7 +48,7 @@ class FMMError(RuntimeError):
 class _Config(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("p", ctypes.c_int), ("lmax", ctypes.c_int), ("precision", ctypes.c_int),
                 ("semantics", ctypes.c_int), ("eps2", ctypes.c_double), ("exclude_self", ctypes.c_int),
-                ("nrhs", ctypes.c_int)]
+                ("nrhs", ctypes.c_int), ("wavenumber", ctypes.c_double)]
 
 
 class _GmresConfig(ctypes.Structure):
@@ -126,12 +127,13 @@ class Plan:
     """One FMM configuration bound to a geometry (include/fmmb.h)."""
 
     def __init__(self, kernel=LAPLACE_G, p=8, lmax=3, precision=FP64, semantics=SEM_REFERENCE, eps2=0.0,
-                 exclude_self=False, nrhs=1):
+                 exclude_self=False, nrhs=1, wavenumber=0.0):
         lib = load()
         cfg = _Config()
         lib.fmmb_config_init(ctypes.byref(cfg))
         cfg.kernel, cfg.p, cfg.lmax, cfg.precision = kernel, p, lmax, precision
         cfg.semantics, cfg.eps2, cfg.exclude_self, cfg.nrhs = semantics, eps2, int(exclude_self), nrhs
+        cfg.wavenumber = wavenumber
         h = _vp()
         _check(lib.fmmb_plan_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -232,9 +234,40 @@ class Plan:
         _check(load().fmmb_gmres(self._h, ctypes.byref(cfg), wp, bp, xp, ctypes.byref(it), resid.ctypes.data))
         return xk, it.value, resid.reshape(self.nrhs, nprob)
 
+    def _complex_call(self, fn_name, q, n_out, out, f64):
+        """Helmholtz calls: complex q (numpy or torch complex64) and complex
+        outputs (numpy complex128 / complex64, or torch complex tensors), passed
+        to the library as interleaved (re, im) floats / doubles."""
+        rt = np.float64 if f64 else np.float32
+        if hasattr(q, "data_ptr"):
+            import torch
+            qr = torch.view_as_real(q.to(torch.complex64).contiguous()).contiguous()
+            qp = qr.data_ptr()
+        else:
+            qr = np.ascontiguousarray(q, np.complex64).view(np.float32)
+            qp = qr.ctypes.data
+        if out is None:
+            out = np.zeros(n_out, np.complex128 if f64 else np.complex64)
+        if hasattr(out, "data_ptr"):
+            import torch
+            want = torch.complex128 if f64 else torch.complex64
+            if out.dtype != want or not out.is_contiguous():
+                raise FMMError(f"expected a contiguous {want} tensor")
+            op_ = torch.view_as_real(out).data_ptr()
+        else:
+            if out.dtype != (np.complex128 if f64 else np.complex64) or not out.flags.c_contiguous:
+                raise FMMError("expected a contiguous complex output array")
+            op_ = out.ctypes.data
+        self._follow_torch(q, out)
+        _check(getattr(load(), fn_name)(self._h, qp, op_, None))
+        return out
+
     def evaluate(self, q, pot=None, grad=None, f64=False):
         """One matvec.  q: (nrhs*nj,) charges.  Returns (pot, grad) -- grad only
         for LAPLACE_G.  Outputs are numpy unless torch CUDA tensors are given."""
+        if self.kernel == HELMHOLTZ_G:  # complex charges -> complex potentials, no gradient
+            return self._complex_call("fmmb_evaluate_f64" if f64 else "fmmb_evaluate", q, self.ni * self.nrhs, pot,
+                                      f64), None
         dt = np.float64 if f64 else np.float32
         qp, qk = _ptr(q, np.float32)
         ni = self.ni * self.nrhs
@@ -252,6 +285,9 @@ class Plan:
     def evaluate_transpose(self, w, out=None, grad=None, f64=False):
         """Charge adjoint A^T w (fmmb_evaluate_transpose): w (nrhs*ni,) ->
         (out (nrhs*nj,), grad (3*nrhs*nj,) for LAPLACE_G or None)."""
+        if self.kernel == HELMHOLTZ_G:  # A^T w (no conjugation), complex
+            return self._complex_call("fmmb_evaluate_transpose_f64" if f64 else "fmmb_evaluate_transpose", w,
+                                      self.nj * self.nrhs, out, f64), None
         dt = np.float64 if f64 else np.float32
         wp, wk = _ptr(w, np.float32)
         nj = self.nj * self.nrhs
@@ -284,6 +320,11 @@ class Plan:
     def direct(self, q, i0=0, i1=None):
         """FP64 direct sum on the GPU for targets [i0, i1) (caller order)."""
         i1 = self.ni if i1 is None else i1
+        if self.kernel == HELMHOLTZ_G:  # complex charges, complex128 potentials
+            qr = np.ascontiguousarray(q, np.complex64).view(np.float32)
+            pot = np.zeros(i1 - i0, np.complex128)
+            _check(load().fmmb_direct_f64(self._h, qr.ctypes.data, i0, i1, pot.ctypes.data, None))
+            return pot, None
         qp, qk = _ptr(q, np.float32)
         pot = np.zeros(i1 - i0)
         grad = np.zeros(3 * (i1 - i0))

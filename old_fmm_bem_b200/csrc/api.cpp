@@ -134,8 +134,13 @@ int fmmb_config_init(fmmb_config* cfg) {
 int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
   return guarded([&] {
     FMMB_REQUIRE(cfg && out, FMMB_ERR_ARG, "null argument");
-    FMMB_REQUIRE(cfg->kernel == FMMB_LAPLACE_G || cfg->kernel == FMMB_LAPLACE_GNI || cfg->kernel == FMMB_LAPLACE_GNJ,
+    FMMB_REQUIRE(cfg->kernel == FMMB_LAPLACE_G || cfg->kernel == FMMB_LAPLACE_GNI || cfg->kernel == FMMB_LAPLACE_GNJ ||
+                     cfg->kernel == FMMB_HELMHOLTZ_G,
                  FMMB_ERR_ARG, "unknown kernel");
+    FMMB_REQUIRE(cfg->kernel != FMMB_HELMHOLTZ_G || (cfg->wavenumber > 0 && std::isfinite(cfg->wavenumber)),
+                 FMMB_ERR_ARG, "the Helmholtz kernel needs a finite wavenumber > 0");
+    FMMB_REQUIRE(cfg->kernel != FMMB_HELMHOLTZ_G || cfg->semantics == FMMB_SEM_ACCURATE, FMMB_ERR_ARG,
+                 "the Helmholtz kernel has no reference semantics: use FMMB_SEM_ACCURATE");
     FMMB_REQUIRE(cfg->p >= 1 && cfg->p <= 20, FMMB_ERR_ARG, "p must be in 1..20");
     FMMB_REQUIRE(cfg->lmax >= 2 && cfg->lmax <= 10, FMMB_ERR_ARG, "lmax must be in 2..10");
     FMMB_REQUIRE(cfg->precision == FMMB_FP64 || cfg->precision == FMMB_MIXED, FMMB_ERR_ARG, "unknown precision");
@@ -177,7 +182,7 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       *pl->h_err = 0;
       build_static_operators(pl->ops, pl->p, pl->ref);
       upload_static_ops(pl);
-      if (!pl->ref) {  // geometry-independent M2L set
+      if (!pl->ref && cfg->kernel != FMMB_HELMHOLTZ_G) {  // geometry-independent M2L set
         build_m2l_operators(pl->ops, 2, 1.0f);
         upload(pl->d_m2l, pl->ops.m2l, pl->st.main);
       }
@@ -300,6 +305,11 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       const size_t n = k < 6 ? ni : nj;
       float* dst = pl->geo.get() + (k < 6 ? (size_t)k * ni : (size_t)6 * ni + (size_t)(k - 6) * nj);
       if (d[k]) FMMB_CUDA(cudaMemcpyAsync(dst, d[k], n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
+    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // its own operators and jobs
+      helm_setup(pl);
+      pl->have_geometry = true;
+      return;
     }
     // reference semantics: the M2L distance carries an absolute eps, so the
     // operator set depends on the level sizes (rebuilt when they change)
@@ -600,8 +610,77 @@ struct PhaseTimer {
   }
 };
 
+// One right-hand side of the complex Helmholtz kernel: qs (sorted complex
+// charges) -> near / far sorted complex potentials.  P2P on the side stream;
+// P2M, M2M, M2L (all levels), L2L and L2P on the main stream, the dense
+// translations through the FP64 pair kernel.
+void run_one_helm(fmmb_plan* pl, const float* qs) {
+  const int K = pl->K, p = pl->p, lmax = pl->lmax;
+  const double k = pl->cfg.wavenumber;
+  cudaStream_t m = pl->st.main, side = pl->st.side;
+  double* pot_near = pl->pot_s.get();
+  double* pot_far = pl->pot_s.get() + 2 * (size_t)pl->ni;
+  const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
+  const double wleaf = (double)pl->bbox[3] / (double)(1 << lmax);
+  FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
+  FMMB_CUDA(cudaStreamWaitEvent(side, pl->st.fork, 0));
+  FMMB_CUDA(time_mark(pl, pl->ev[0], side));
+  {
+    PhaseTimer tm(pl, 0, side);
+    launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, (float)k, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(),
+                    pl->p2p_list.get(), pl->tpos.get(), pl->spos.get(), qs, pot_near, side);
+  }
+  FMMB_CUDA(time_mark(pl, pl->ev[1], side));
+  FMMB_CUDA(cudaEventRecord(pl->st.join, side));
+  FMMB_CUDA(time_mark(pl, pl->ev[2], m));
+  {
+    PhaseTimer tm(pl, 1, m);
+    launch_helm_p2m(nleaf_j, p, k, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), qs, pl->bbox, wleaf,
+                    pl->M.get() + (size_t)pl->off_j[lmax] * 2 * K, m);
+  }
+  FMMB_CUDA(time_mark(pl, pl->ev[3], m));
+  auto pairs_run = [&](const fmmb_plan::PairJob& job, double* xin, double* out, int atomic, int phase) {
+    if (job.ntile <= 0) return;
+    PhaseTimer tm(pl, phase, m);
+    PairArgs a{};
+    a.ntile = job.ntile;
+    a.tp = job.tp;
+    a.K = 2 * K;
+    a.atomic = atomic;
+    a.tile_op = job.tile_op.get();
+    a.tile_src = job.tile_src.get();
+    a.tile_dst = job.tile_dst.get();
+    a.opT = pl->d_hops.get();
+    a.ostride = (size_t)4 * K * K;
+    a.xin = xin;
+    a.out = out;
+    a.err = pl->d_err.get();
+    launch_translate_pairs_f64(a, m);
+  };
+  // parents are accumulated from their children, level by level
+  const size_t above = (size_t)(pl->tot_j - pl->nbox_j[lmax]) * 2 * K;
+  if (above) FMMB_CUDA(cudaMemsetAsync(pl->M.get() + (size_t)pl->off_j[lmax - 1] * 2 * K, 0, above * sizeof(double), m));
+  for (int lev = lmax - 1; lev >= 2; lev--) pairs_run(*pl->m2m_pairs[lev], pl->M.get(), pl->M.get(), 1, 2);
+  FMMB_CUDA(time_mark(pl, pl->ev[4], m));
+  FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * 2 * K * sizeof(double), m));
+  pairs_run(*pl->h_m2l, pl->M.get(), pl->L.get(), 1, 3);
+  for (int lev = 3; lev <= lmax; lev++) pairs_run(*pl->l2l_pairs[lev], pl->L.get(), pl->L.get(), 0, 4);
+  FMMB_CUDA(time_mark(pl, pl->ev[5], m));
+  {
+    PhaseTimer tm(pl, 5, m);
+    launch_helm_l2p(nleaf_i, p, k, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->bbox, wleaf,
+                    pl->L.get() + (size_t)pl->off_i[lmax] * 2 * K, pot_far, m);
+  }
+  FMMB_CUDA(time_mark(pl, pl->ev[6], m));
+  FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));
+}
+
 // Runs one right-hand side: qs (sorted, device) -> near/far sorted outputs.
 void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
+  if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {
+    run_one_helm(pl, qs);
+    return;
+  }
   const int K = pl->K, p = pl->p, lmax = pl->lmax, ker = pl->cfg.kernel;
   const Sem s = make_sem(pl);
   cudaStream_t m = pl->st.main, side = pl->st.side;
@@ -809,6 +888,37 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     pl->ev_phase.clear();
     pl->launches = 0;
     FMMB_CUDA(cudaEventRecord(pl->ev[7], m));
+    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // complex charges and potentials, interleaved
+      const float* qd = to_device(q, (size_t)2 * nj * nr, pl->stage_f, m);
+      launch_helm_gather(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
+      pl->launches++;
+      const bool pot_dev = is_device_ptr(pot);
+      T* pd = pot;
+      if (!pot_dev) {
+        pl->stage_out.alloc((size_t)2 * ni * nr * sizeof(T));
+        pd = (T*)pl->stage_out.get();
+      }
+      for (int r = 0; r < nr; r++) {
+        if (pl->use_graph) {
+          if (r > 0)
+            FMMB_CUDA(cudaMemcpyAsync(pl->qs.get(), pl->qs.get() + (size_t)2 * r * nj, (size_t)2 * nj * sizeof(float),
+                                      cudaMemcpyDeviceToDevice, m));
+          run_graph(pl, false);
+        } else {
+          run_one(pl, pl->qs.get() + (size_t)2 * r * nj, false);
+        }
+        launch_helm_finalize<T>(ni, pl->perm_i.get(), pl->pot_s.get(), pl->pot_s.get() + 2 * (size_t)ni,
+                                pd + (size_t)2 * r * ni, m);
+        pl->launches++;
+      }
+      FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
+      FMMB_CUDA(cudaMemcpyAsync(pl->h_err, pl->d_err.get(), sizeof(int), cudaMemcpyDeviceToHost, m));
+      if (!pot_dev) FMMB_CUDA(cudaMemcpyAsync(pot, pd, (size_t)2 * ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
+      if (!pot_dev || !is_device_ptr(q)) FMMB_CUDA(cudaStreamSynchronize(m));
+      pl->have_expansions = true;
+      pl->timings_valid = true;
+      return;
+    }
     const float* qd = to_device(q, (size_t)nj * nr, pl->stage_f, m);
     launch_gather_charges(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
     pl->launches++;
@@ -890,7 +1000,8 @@ int autotune_impl(const fmmb_config* cfg, int ni, int nj, int lmin, int lmax_hi,
     FMMB_REQUIRE(2 <= lmin && lmin <= lmax_hi && lmax_hi <= 10, FMMB_ERR_ARG, "lmax range must lie in [2, 10]");
     reps = std::max(1, reps);
     // random charges on the device (caller order), one FP64 output buffer
-    std::vector<float> hq((size_t)nj * std::max(1, cfg->nrhs));
+    const size_t cw = cfg->kernel == FMMB_HELMHOLTZ_G ? 2 : 1;  // complex: interleaved
+    std::vector<float> hq(cw * nj * std::max(1, cfg->nrhs));
     uint64_t st = 0x9E3779B97F4A7C15ull;
     for (auto& v : hq) {
       st = st * 6364136223846793005ull + 1442695040888963407ull;
@@ -900,7 +1011,7 @@ int autotune_impl(const fmmb_config* cfg, int ni, int nj, int lmin, int lmax_hi,
     dq.alloc(hq.size());
     FMMB_CUDA(cudaMemcpy(dq.get(), hq.data(), hq.size() * sizeof(float), cudaMemcpyHostToDevice));
     DevBuf<float> dpot, dgrad;
-    dpot.alloc((size_t)ni * std::max(1, cfg->nrhs));
+    dpot.alloc(cw * ni * std::max(1, cfg->nrhs));
     dgrad.alloc((size_t)3 * ni * std::max(1, cfg->nrhs));
     cudaEvent_t e0, e1;
     FMMB_CUDA(cudaEventCreate(&e0));
@@ -992,7 +1103,7 @@ fmmb_plan* transposed_plan(fmmb_plan* pl) {
   FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
   fmmb_config c = pl->cfg;
   c.kernel = pl->cfg.kernel == FMMB_LAPLACE_GNI ? FMMB_LAPLACE_GNJ
-             : pl->cfg.kernel == FMMB_LAPLACE_GNJ ? FMMB_LAPLACE_GNI : FMMB_LAPLACE_G;
+             : pl->cfg.kernel == FMMB_LAPLACE_GNJ ? FMMB_LAPLACE_GNI : pl->cfg.kernel;  // G, Helmholtz: symmetric
   fmmb_plan* t = nullptr;
   int rc = fmmb_plan_create(&c, &t);
   if (rc == FMMB_OK) rc = fmmb_set_stream(t, pl->st.main);
@@ -1031,12 +1142,13 @@ int transpose_impl(fmmb_plan* pl, const float* w, T* out, T* grad) {
   return guarded([&] {
     FMMB_REQUIRE(pl && w && out, FMMB_ERR_ARG, "null argument");
     FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G || grad == nullptr, FMMB_ERR_ARG,
-                 "the transposed normal-derivative kernels have no gradient output");
+                 "only the Laplace G transpose has a gradient output");
     fmmb_plan* t = transposed_plan(pl);
     const int rc = sizeof(T) == 4 ? fmmb_evaluate(t, w, (float*)out, (float*)grad)
                                   : fmmb_evaluate_f64(t, w, (double*)out, (double*)grad);
     if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
-    if (pl->cfg.kernel != FMMB_LAPLACE_G) negate(out, (size_t)pl->nj * pl->cfg.nrhs, t->st.main);
+    if (pl->cfg.kernel == FMMB_LAPLACE_GNI || pl->cfg.kernel == FMMB_LAPLACE_GNJ)
+      negate(out, (size_t)pl->nj * pl->cfg.nrhs, t->st.main);
   });
 }
 
@@ -1090,6 +1202,23 @@ int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, 
     FMMB_REQUIRE(0 <= i0 && i0 <= i1 && i1 <= pl->ni, FMMB_ERR_ARG, "target range out of bounds");
     cudaStream_t m = pl->st.main;
     const int nj = pl->nj, cnt = i1 - i0;
+    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // complex: pot holds 2 cnt doubles (re, im)
+      const float* qd = to_device(q, (size_t)2 * nj, pl->stage_f, m);
+      launch_helm_gather(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
+      DevBuf<double> out;
+      out.alloc((size_t)2 * cnt + 2);
+      const std::vector<int>&to = pl->prob_toff, &so = pl->prob_soff;
+      for (int b = 0; b < pl->nprob; b++) {
+        const int a0 = std::max(i0, to[b]), a1 = std::min(i1, to[b + 1]);
+        if (a0 >= a1) continue;
+        launch_helm_direct(a0, a1, pl->inv_i.get(), pl->tpos.get(), so[b + 1] - so[b], pl->spos.get() + so[b],
+                           pl->qs.get() + (size_t)2 * so[b], pl->cfg.wavenumber, out.get() + (size_t)2 * (a0 - i0), m);
+      }
+      FMMB_CUDA(cudaMemcpyAsync(pot, out.get(), (size_t)2 * cnt * sizeof(double),
+                                is_device_ptr(pot) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, m));
+      FMMB_CUDA(cudaStreamSynchronize(m));
+      return;
+    }
     const float* qd = to_device(q, nj, pl->stage_f, m);
     launch_gather_charges(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
     const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;

@@ -202,6 +202,12 @@ struct fmmb_plan {
     fmmb::DevBuf<int> tile_op, tile_src, tile_dst;
   };
   std::vector<std::unique_ptr<PairJob>> m2m_pairs, l2l_pairs;
+  // complex Helmholtz: dense operators in the real 2K x 2K form (transposed),
+  // [M2M child levels 3..lmax x 8 | L2L likewise | M2L levels 2..lmax x 316],
+  // and the M2L pairs of all levels
+  fmmb::DevBuf<double> d_hops;
+  int hop_m2m0 = 0, hop_l2l0 = 0, hop_m2l0 = 0;
+  std::unique_ptr<PairJob> h_m2l;
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging
   fmmb::DevBuf<double> stage_d;
@@ -219,6 +225,8 @@ struct fmmb_plan {
 };
 
 namespace fmmb {
+// complex Helmholtz operators, pair jobs and buffers (helmholtz_host.cpp)
+void helm_setup(fmmb_plan* pl);
 void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
                 const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
                 const float* snx, const float* sny, const float* snz, const float* bbox_in);

@@ -105,4 +105,27 @@ void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* i
 // K padded for the tensor-core operands (128, or a multiple of 32 up to tc_max_k())
 int tc_kpad(int K);
 int tc_max_k();
+
+// complex Helmholtz kernel (helmholtz.cu); complex values interleaved (re, im),
+// expansions [re(K) | im(K)] per box, K = (p+1)^2
+struct HelmOp {          // one translation operator to build
+  double dx, dy, dz;     // target centre - source centre
+  double rad;            // radius of the projection sphere around the target centre
+  int src_out, tgt_out;  // 1: outgoing (h_n) basis, 0: regular (j_n) basis
+};
+void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
+void launch_helm_p2p(bool f32, float k, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list,
+                     const float4* tpos, const float4* spos, const float* qs, double* pot, cudaStream_t st);
+// bbox: the plan's host copy {xmin, ymin, zmin, rd}
+void launch_helm_p2m(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* spos, const float* qs,
+                     const float* bbox, double w, double* M, cudaStream_t st);
+void launch_helm_l2p(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* tpos,
+                     const float* bbox, double w, const double* L, double* pot, cudaStream_t st);
+void launch_helm_direct(int i0, int i1, const int* inv_i, const float4* tpos, int nj, const float4* spos,
+                        const float* qs, double k, double* out, cudaStream_t st);
+template <typename T>
+void launch_helm_finalize(int n, const int* perm, const double* near, const double* far, T* out, cudaStream_t st);
+// operators in the real 2K x 2K form, transposed ([op][column][row], row stride 2K)
+void launch_helm_build_ops(int p, double k, int nops, const HelmOp* ops, const double* gl_x, const double* gl_w,
+                           const double* ybar_q, double* opT, cudaStream_t st);
 }  // namespace fmmb
