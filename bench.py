@@ -522,6 +522,87 @@ def run_c4(args):
                       "results": res, "clocks": clk.summary()}))
 
 
+
+def run_c5(args):
+    """Complex Helmholtz e^{ikr}/(4 pi r): 1,048,576 points uniform on the unit
+    sphere, complex charges with parts U[-1, 1], k = 5, p = 16; one step = the
+    matvec and its adjoint w.r.t. the charges (A^T w, the transposed plan);
+    mixed (FP32 complex P2P) and FP64 forms, octree depth from
+    fmmb_autotune_lmax for each; rel err of the potential against the FP64
+    complex direct sum (fmmb_direct_f64) on 1,024 targets."""
+    import torch
+    import old_fmm_bem_b200 as ob
+    from oracle import helmholtz_oracle as ho
+    n, k, p = 1 << 20, 5.0, 16
+    x, q = ho.sphere_points(n, 29)
+    w = ho.sphere_points(n, 31)[1]
+    bbox = (-1.0001, -1.0001, -1.0001, 2.0002)
+    xd = torch.from_numpy(x).cuda()
+    qd = torch.from_numpy(q).cuda()
+    wd = torch.from_numpy(w).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    steps = max(1, min(args.steps, 3))
+    res = {}
+    sel = np.sort(np.random.default_rng(3).choice(n, 1024, replace=False))
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for name, prec in (("mixed", ob.MIXED), ("fp64", ob.FP64)):
+            kw = dict(kernel=ob.HELMHOLTZ_G, p=p, precision=prec, semantics=ob.SEM_ACCURATE, exclude_self=True)
+            lmax, tune = _autotune_helm(ob, xd, bbox, kw, k)
+            plan = ob.Plan(lmax=lmax, wavenumber=k, **kw)
+            t0 = time.perf_counter()
+            plan.set_geometry(xd, xd, bbox=bbox)
+            torch.cuda.synchronize()
+            setup_s = time.perf_counter() - t0
+            pot = torch.zeros(n, dtype=torch.complex128, device="cuda")
+            adj = torch.zeros(n, dtype=torch.complex128, device="cuda")
+            plan.evaluate_transpose(wd, adj, f64=True)  # builds the transposed plan
+            t_f = _timed(lambda: plan.evaluate(qd, pot, f64=True), stream, steps, 2, flush)
+            t_fa = _timed(lambda: (plan.evaluate(qd, pot, f64=True), plan.evaluate_transpose(wd, adj, f64=True)),
+                          stream, steps, 2, flush)
+            # accuracy on 1,024 targets against the FP64 direct sum (a plan over those targets)
+            dp = ob.Plan(kernel=ob.HELMHOLTZ_G, p=4, lmax=2, semantics=ob.SEM_ACCURATE, exclude_self=True, wavenumber=k)
+            dp.set_geometry(np.ascontiguousarray(x[:, sel]), x, bbox=bbox)
+            vd, _ = dp.direct(q)
+            dp.close()
+            v = pot.cpu().numpy()[sel]
+            res[name] = {"lmax": lmax, "autotune_ms": tune, "setup_s": setup_s, "matvec_ms": t_f,
+                         "matvec_plus_adjoint_ms": t_fa, "phase_ms": plan.timings(),
+                         "rel_err_vs_fp64_direct": float(np.linalg.norm(v - vd) / np.linalg.norm(vd))}
+            plan.close()
+    m = res["mixed"]
+    print(json.dumps({"metric": "FMM matvec Mpts/s (complex Helmholtz G, 1,048,576 points on the unit sphere, k=5, "
+                                "p=16)",
+                      "value": n / (m["matvec_ms"] * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1, "steps": steps,
+                      "ms_per_step": m["matvec_ms"], "dtype": "c64 P2P + f64", "data": "synthetic",
+                      "config": {"workload": "complex Helmholtz e^{ikr}/(4 pi r), 1,048,576 points uniform on the unit "
+                                             "sphere, q with re/im U[-1,1], k=5 (kD=10), p=16; adjoint = A^T w",
+                                 "l2": "flushed between steps"},
+                      "results": res, "mixed_speedup_over_fp64": res["fp64"]["matvec_ms"] / m["matvec_ms"],
+                      "clocks": clk.summary()}))
+
+
+def _autotune_helm(ob, xd, bbox, kw, k):
+    """fmmb_autotune_lmax for the Helmholtz plan (depths 3..4: deeper trees
+    multiply the dense FP64 M2L work)."""
+    import ctypes
+    lib = ob.load()
+    cfg = ob._Config()
+    lib.fmmb_config_init(ctypes.byref(cfg))
+    cfg.kernel, cfg.p, cfg.precision, cfg.semantics = kw["kernel"], kw["p"], kw["precision"], kw["semantics"]
+    cfg.exclude_self, cfg.wavenumber = 1, k
+    best = ctypes.c_int(-1)
+    ms = np.zeros(2, np.float32)
+    bb = np.asarray(bbox, np.float32)
+    ptr = [xd[i].data_ptr() for i in range(3)]
+    n = xd.shape[1]
+    rc = lib.fmmb_autotune_lmax(ctypes.byref(cfg), n, *ptr, None, None, None, n, *ptr, None, None, None,
+                                bb.ctypes.data, 3, 4, 1, ctypes.byref(best), ms.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(lib.fmmb_last_error().decode())
+    return best.value, {l: float(ms[l - 3]) for l in range(3, 5)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -530,10 +611,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64"],
+    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64",
+                                                     "helmholtz1m"],
                     help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "
                          "points; adjoint1m: forward + backward on 1,048,576 clustered points; batch64: GMRES on 64 "
-                         "BEM problems x 8 right-hand sides")
+                         "BEM problems x 8 right-hand sides; helmholtz1m: complex Helmholtz, "
+                         "1,048,576 sphere points, k=5, p=16")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -551,6 +634,8 @@ def main():
         run_c3(args)
     elif args.config == "batch64":
         run_c4(args)
+    elif args.config == "helmholtz1m":
+        run_c5(args)
     else:
         run_ours(args, rank, world)
     if world > 1 and args.impl == "ours":
