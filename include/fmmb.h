@@ -150,6 +150,19 @@ FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w,
  * the geometry and the first right-hand side of q; targets [i0, i1). */
 FMMB_API int fmmb_direct_f64(fmmb_plan* plan, const float* q, int i0, int i1, double* pot, double* grad);
 
+/* The reference's batch near-field call p2pgpu_ (libgpu/gpufmm.cu:57-61) with
+ * its exact arguments and record format (host arrays; the GPU work is
+ * synchronous): targets xi..gzi in blocks of 128 (nvecd[1] blocks, gx.. the
+ * target normals), sources xj..vj (nvecd[3] of them, gx.. the source normals),
+ * nvecd[4] = neq 0/1/2, per block b: nvecd[b*nvecd[2] + 10] source ranges,
+ * range r = (first nvecd[b*nvecd[2] + 2r + 11], count nvecd[b*nvecd[2] + 2r + 12]).
+ * Overwrites vi, gxi, gyi, gzi of every packed target (gradient for neq 0,
+ * zeros otherwise) with the reference's arithmetic (eps = 1e-6 on r^2).
+ * compat/gpufmm_compat.cpp defines p2pgpu_ over it. */
+FMMB_API int fmmb_gpu_p2p(const int* nvecd, float* xi, float* yi, float* zi, float* gxi, float* gyi, float* gzi,
+                          float* vi, const float* xj, const float* yj, const float* zj, const float* gxj,
+                          const float* gyj, const float* gzj, const float* vj);
+
 /* GMRES for the boundary-integral systems of a plan whose targets are its
  * sources (problem by problem):  A x = diag * x + K (weight .* x),  left
  * preconditioned by y = precond * x.  This is the reference's PETSc shell

@@ -9,8 +9,9 @@
 // restated here), with two differences:
 //   * the expansion order `mp` comes from -DREF_MP=<p+1> so one build recipe
 //     produces a library per order (the reference fixes mp=9 at compile time);
-//   * ngpu is 0: only the CPU path is built, so alloc() skips the GPU staging
-//     buffers (reference fmm/alloc.cxx:85-118).
+//   * ngpu comes from -DREF_NGPU (default 0: the CPU path, alloc() skips the
+//     GPU staging buffers of fmm/alloc.cxx:85-118; 1 for the build whose
+//     near field goes through the reference's p2pgpu_ callers).
 // Nothing here computes anything on the FMM path.
 #ifndef ORACLE_REFSHIM_CONSTANTS_H
 #define ORACLE_REFSHIM_CONSTANTS_H
@@ -30,7 +31,10 @@
 #endif
 
 const int mp      = REF_MP;      // degrees n = 0..mp-1 (order p = mp-1)
-const int ngpu    = 0;           // CPU-only build
+#ifndef REF_NGPU
+#define REF_NGPU 0
+#endif
+const int ngpu    = REF_NGPU;    // 0: CPU-only build
 const int mprint  = 0;
 const int nwmax   = 50000;
 const int npmax   = 4194304;     // only sizes host staging; raised for 1M-point runs

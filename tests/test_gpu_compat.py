@@ -48,3 +48,28 @@ def test_reference_entry_points(path, driver, tmp_path, oracle):
         ref, _ = oracle.direct(d["t"], d["s"], d["q"], neq=neq, eps2=oracle.EPS_REF, exclude_self=False,
                                ref_pi=True, tn=d["tn"], sn=d["sn"])
         assert rel(got, ref) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("neq", [0, 1, 2])
+def test_reference_gpu_variant_through_p2pgpu(neq, oracle):
+    """The reference's own GPU-variant near-field host code (kernel/G_p2p_gpu.cxx,
+    Gni_p2p_gpu.cxx, Gnj_p2p_gpu.cxx: block packing into nvecd records) linked
+    to p2pgpu_ from compat/gpufmm_compat.cpp over libfmmb (oracle/Makefile,
+    _ref/libfmmref_gpup2p_mp9.so) reproduces the reference CPU fmm() at p = 8:
+    the P2P terms are the same FP32 arithmetic, summed per 128 sources in FP32
+    and then in FP64 instead of one float running sum, so 1e-6."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libfmmref_gpup2p_mp9.so")):
+        pytest.skip("reference p2pgpu_ build missing (oracle/Makefile gpup2p)")
+    rng = np.random.default_rng(40 + neq)
+    n = 20000
+    t = rng.random((3, n), dtype=np.float32)
+    s = rng.random((3, n), dtype=np.float32)
+    tn = rng.standard_normal((3, n)).astype(np.float32)
+    sn = rng.standard_normal((3, n)).astype(np.float32)
+    q = rng.uniform(-1, 1, n).astype(np.float32)
+    cpu = oracle.ref_fmm(t, s, q, neq=neq, p=8, lmax=3, tn=tn, sn=sn)
+    gpu = oracle.ref_fmm(t, s, q, neq=neq, p=8, lmax=3, tn=tn, sn=sn, gpu_p2p=True)
+    assert rel(gpu[0], cpu[0].astype(np.float64)) < 1e-6
+    if neq == 0:
+        assert rel(gpu[1], cpu[1].astype(np.float64)) < 1e-6
