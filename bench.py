@@ -472,8 +472,11 @@ def run_c4(args):
         for name, kernel in (("gni", ob.LAPLACE_GNI), ("gnj", ob.LAPLACE_GNJ)):
             tn, sn = (nd, None) if kernel == ob.LAPLACE_GNI else (None, nd)
             kw = dict(kernel=kernel, p=P_ORDER, precision=ob.MIXED, semantics=ob.SEM_ACCURATE, exclude_self=True)
-            lmax, tune = ob.autotune_lmax_batch(off, xd, off, xd, target_normals=tn, source_normals=sn, bbox=bbox,
-                                                lmin=3, lmax=6, reps=1, nrhs=nrhs, **kw)
+            if args.lmax:
+                lmax, tune = args.lmax, None
+            else:
+                lmax, tune = ob.autotune_lmax_batch(off, xd, off, xd, target_normals=tn, source_normals=sn,
+                                                    bbox=bbox, lmin=3, lmax=6, reps=1, nrhs=nrhs, **kw)
             plan = ob.Plan(lmax=lmax, nrhs=nrhs, **kw)
             plan.set_stream(stream)
             t0 = time.perf_counter()
@@ -548,7 +551,7 @@ def run_c5(args):
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         for name, prec in (("mixed", ob.MIXED), ("fp64", ob.FP64)):
             kw = dict(kernel=ob.HELMHOLTZ_G, p=p, precision=prec, semantics=ob.SEM_ACCURATE, exclude_self=True)
-            lmax, tune = _autotune_helm(ob, xd, bbox, kw, k)
+            lmax, tune = (args.lmax, None) if args.lmax else _autotune_helm(ob, xd, bbox, kw, k)
             plan = ob.Plan(lmax=lmax, wavenumber=k, **kw)
             t0 = time.perf_counter()
             plan.set_geometry(xd, xd, bbox=bbox)
@@ -611,6 +614,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--lmax", type=int, default=0,
+                    help="batch64 / helmholtz1m: this octree depth instead of the autotuner's")
     ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64",
                                                      "helmholtz1m"],
                     help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "

@@ -627,8 +627,9 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   FMMB_CUDA(time_mark(pl, pl->ev[0], side));
   {
     PhaseTimer tm(pl, 0, side);
-    launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, (float)k, nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(),
-                    pl->p2p_list.get(), pl->tpos.get(), pl->spos.get(), qs, pot_near, side);
+    launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, (float)k, pl->h_p2p_nwork, pl->h_p2p_work.get(),
+                    pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->spos.get(), qs,
+                    pot_near, side);
   }
   FMMB_CUDA(time_mark(pl, pl->ev[1], side));
   FMMB_CUDA(cudaEventRecord(pl->st.join, side));

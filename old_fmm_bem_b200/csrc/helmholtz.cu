@@ -288,73 +288,96 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const in
 }
 
 // ---------------------------------------------------------------- P2P
-// One block per target leaf (128 threads, one target each per pass), sources
-// of the 27 neighbour slots staged through shared memory in chunks of 128;
-// FP32 terms summed over 32 sources, then added in FP64 (F32 = true), or
-// everything in FP64.  Zero-distance pairs are skipped.
+// One block (128 threads) per work item = up to 256 targets of one leaf, two
+// per thread (one shared-memory read of a source serves both); the sources of
+// the leaf's 27 neighbour slots are staged through shared memory in chunks of
+// 128.  Work items split large leaves, so the launch is not bound by the
+// densest leaf.  Mixed form: FP32 terms (sincosf), summed over 32 sources,
+// then added in FP64; FP64 form: everything in FP64.  Zero-distance pairs
+// contribute nothing (their inverse distance is taken as 0).
 template <bool F32>
-__global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict__ leaf_i, const int2* __restrict__ leaf_j,
-                                                const int* __restrict__ list, const float4* __restrict__ tpos,
-                                                const float4* __restrict__ spos, const float2* __restrict__ q,
-                                                double2* __restrict__ pot) {
+__device__ __forceinline__ void helm_pair(float k, const float4 x, const float4 s, const float2 q, float& fr,
+                                          float& fi) {
+  const float dx = x.x - s.x, dy = x.y - s.y, dz = x.z - s.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  float sn, cs;
+  sincosf(k * (r2 * rinv), &sn, &cs);
+  fr += (q.x * cs - q.y * sn) * rinv;
+  fi += (q.x * sn + q.y * cs) * rinv;
+}
+__device__ __forceinline__ void helm_pair64(double k, const float4 x, const float4 s, const float2 q, double& ar,
+                                            double& ai) {
+  const double dx = (double)x.x - s.x, dy = (double)x.y - s.y, dz = (double)x.z - s.z;
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 == 0.0) return;
+  const double r = sqrt(r2);
+  double sn, cs;
+  sincos(k * r, &sn, &cs);
+  ar += (q.x * cs - q.y * sn) / r;
+  ai += (q.x * sn + q.y * cs) / r;
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict__ work, const int2* __restrict__ leaf_i,
+                                                const int2* __restrict__ leaf_j, const int* __restrict__ list,
+                                                const float4* __restrict__ tpos, const float4* __restrict__ spos,
+                                                const float2* __restrict__ q, double2* __restrict__ pot) {
   __shared__ float4 sp[128];
   __shared__ float2 sq[128];
-  const int b = blockIdx.x;
+  const int2 wk = work[blockIdx.x];
+  const int b = wk.x;
   const int2 li = leaf_i[b];
-  const double coef = 0.25 / M_PI;
-  for (int base = 0; base < li.y; base += 128) {
-    const int i = base + threadIdx.x;
-    const bool on = i < li.y;
-    const float4 xi = on ? tpos[li.x + i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    double ar = 0, ai = 0;
-    for (int s = 0; s < kP2PSlots; s++) {
-      const int jl = list[(size_t)b * kP2PSlots + s];
-      if (jl < 0) continue;
-      const int2 lj = leaf_j[jl];
-      for (int c0 = 0; c0 < lj.y; c0 += 128) {
-        __syncthreads();
-        if (c0 + threadIdx.x < lj.y) {
-          sp[threadIdx.x] = spos[lj.x + c0 + threadIdx.x];
-          sq[threadIdx.x] = q[lj.x + c0 + threadIdx.x];
-        }
-        __syncthreads();
-        const int nc = min(128, lj.y - c0);
-        if (!on) continue;
-        for (int r0 = 0; r0 < nc; r0 += 32) {
-          const int re = min(nc, r0 + 32);
-          if (F32) {
-            float fr = 0.f, fi = 0.f;
+  const int i0 = wk.y + threadIdx.x, i1 = i0 + 128;
+  const bool on0 = i0 < li.y, on1 = i1 < li.y;
+  const float4 x0 = on0 ? tpos[li.x + i0] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 x1 = on1 ? tpos[li.x + i1] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double ar0 = 0, ai0 = 0, ar1 = 0, ai1 = 0;
+  for (int sl = 0; sl < kP2PSlots; sl++) {
+    const int jl = list[(size_t)b * kP2PSlots + sl];
+    if (jl < 0) continue;
+    const int2 lj = leaf_j[jl];
+    for (int c0 = 0; c0 < lj.y; c0 += 128) {
+      __syncthreads();
+      if (c0 + threadIdx.x < lj.y) {
+        sp[threadIdx.x] = spos[lj.x + c0 + threadIdx.x];
+        sq[threadIdx.x] = q[lj.x + c0 + threadIdx.x];
+      }
+      __syncthreads();
+      const int nc = min(128, lj.y - c0);
+      if (!on0) continue;
+      for (int r0 = 0; r0 < nc; r0 += 32) {
+        const int re = min(nc, r0 + 32);
+        if (F32) {
+          float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
+          if (on1) {
             for (int jj = r0; jj < re; jj++) {
-              const float dx = xi.x - sp[jj].x, dy = xi.y - sp[jj].y, dz = xi.z - sp[jj].z;
-              const float r2 = dx * dx + dy * dy + dz * dz;
-              if (r2 == 0.f) continue;
-              const float rinv = rsqrtf(r2);
-              float sn, cs;
-              sincosf(k * (r2 * rinv), &sn, &cs);
+              const float4 sv = sp[jj];
               const float2 qq = sq[jj];
-              fr += (qq.x * cs - qq.y * sn) * rinv;
-              fi += (qq.x * sn + qq.y * cs) * rinv;
+              helm_pair<true>(k, x0, sv, qq, fr0, fi0);
+              helm_pair<true>(k, x1, sv, qq, fr1, fi1);
             }
-            ar += fr;
-            ai += fi;
           } else {
-            for (int jj = r0; jj < re; jj++) {
-              const double dx = (double)xi.x - sp[jj].x, dy = (double)xi.y - sp[jj].y, dz = (double)xi.z - sp[jj].z;
-              const double r2 = dx * dx + dy * dy + dz * dz;
-              if (r2 == 0.0) continue;
-              const double r = sqrt(r2);
-              double sn, cs;
-              sincos((double)k * r, &sn, &cs);
-              const float2 qq = sq[jj];
-              ar += (qq.x * cs - qq.y * sn) / r;
-              ai += (qq.x * sn + qq.y * cs) / r;
-            }
+            for (int jj = r0; jj < re; jj++) helm_pair<true>(k, x0, sp[jj], sq[jj], fr0, fi0);
+          }
+          ar0 += fr0;
+          ai0 += fi0;
+          ar1 += fr1;
+          ai1 += fi1;
+        } else {
+          for (int jj = r0; jj < re; jj++) {
+            const float4 sv = sp[jj];
+            const float2 qq = sq[jj];
+            helm_pair64((double)k, x0, sv, qq, ar0, ai0);
+            if (on1) helm_pair64((double)k, x1, sv, qq, ar1, ai1);
           }
         }
       }
     }
-    if (on) pot[li.x + i] = make_double2(coef * ar, coef * ai);
   }
+  const double coef = 0.25 / M_PI;
+  if (on0) pot[li.x + i0] = make_double2(coef * ar0, coef * ai0);
+  if (on1) pot[li.x + i1] = make_double2(coef * ar1, coef * ai1);
 }
 
 // ---------------------------------------------------------------- direct
@@ -515,13 +538,16 @@ void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float*
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_helm_p2p(bool f32, float k, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list,
-                     const float4* tpos, const float4* spos, const float* qs, double* pot, cudaStream_t st) {
-  if (nleaf <= 0) return;
+void launch_helm_p2p(bool f32, float k, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
+                     const int* list, const float4* tpos, const float4* spos, const float* qs, double* pot,
+                     cudaStream_t st) {
+  if (nwork <= 0) return;
   if (f32)
-    helm_p2p<true><<<nleaf, 128, 0, st>>>(k, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs, (double2*)pot);
+    helm_p2p<true><<<nwork, 128, 0, st>>>(k, work, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs,
+                                          (double2*)pot);
   else
-    helm_p2p<false><<<nleaf, 128, 0, st>>>(k, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs, (double2*)pot);
+    helm_p2p<false><<<nwork, 128, 0, st>>>(k, work, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs,
+                                           (double2*)pot);
   FMMB_CHECK_LAUNCH();
 }
 

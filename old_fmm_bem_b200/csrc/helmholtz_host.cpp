@@ -207,6 +207,16 @@ void helm_setup(fmmb_plan* pl) {
       }
     }
   pl->h_m2l = pair_job(m2l, 2 * K, nsm);
+  // P2P work items: every target leaf in pieces of 256 targets
+  {
+    const int nleaf = pl->nbox_i[lmax];
+    std::vector<int2> leaf(nleaf), work;
+    FMMB_CUDA(cudaMemcpy(leaf.data(), pl->leaf_i.get(), nleaf * sizeof(int2), cudaMemcpyDeviceToHost));
+    for (int b = 0; b < nleaf; b++)
+      for (int t = 0; t < leaf[b].y; t += 256) work.push_back(make_int2(b, t));
+    upload_vec(pl->h_p2p_work, work);
+    pl->h_p2p_nwork = (int)work.size();
+  }
   // inverse target permutation (caller -> sorted) for the direct sum
   {
     std::vector<int> perm(pl->ni), inv(pl->ni);

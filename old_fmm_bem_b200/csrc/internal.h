@@ -207,6 +207,8 @@ struct fmmb_plan {
   // and the M2L pairs of all levels
   fmmb::DevBuf<double> d_hops;
   int hop_m2m0 = 0, hop_l2l0 = 0, hop_m2l0 = 0;
+  fmmb::DevBuf<int2> h_p2p_work;  // P2P work items: (target leaf, first target), up to 256 targets each
+  int h_p2p_nwork = 0;
   std::unique_ptr<PairJob> h_m2l;
   fmmb::DevBuf<double> pot_s, grad_s;        // sorted outputs [ni], [3][ni]
   fmmb::DevBuf<float> stage_f;               // host<->device staging

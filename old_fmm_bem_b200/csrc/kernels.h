@@ -114,8 +114,10 @@ struct HelmOp {          // one translation operator to build
   int src_out, tgt_out;  // 1: outgoing (h_n) basis, 0: regular (j_n) basis
 };
 void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
-void launch_helm_p2p(bool f32, float k, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list,
-                     const float4* tpos, const float4* spos, const float* qs, double* pot, cudaStream_t st);
+// work: (target leaf, first target) per item of up to 256 targets
+void launch_helm_p2p(bool f32, float k, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
+                     const int* list, const float4* tpos, const float4* spos, const float* qs, double* pot,
+                     cudaStream_t st);
 // bbox: the plan's host copy {xmin, ymin, zmin, rd}
 void launch_helm_p2m(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* spos, const float* qs,
                      const float* bbox, double w, double* M, cudaStream_t st);
