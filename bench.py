@@ -40,7 +40,11 @@ METRIC = "FMM matvec Mpts/s (Laplace Gn double-layer BEM, 245,760 pts, p=10)"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 # DRAM bytes (read + write) of one launch on this workload, from the ncu
 # captures summarised in profiles/
-NCU_TRAFFIC = {"p2p_mixed": 13.41e6, "translate_tc": 175.89e6}  # bytes; profiles/p2p_mixed_bem245k_p10.md, profiles/translate_tc_m2l_bem245k_p10.md
+# DRAM bytes (read + write) per evaluate of the two dominant kernels, from one
+# ncu capture of this workload: P2P runs as two launches (7.03 MB read each, its
+# outputs stay in L2), the M2L as one; profiles/p2p_mixed_bem245k_p10.md,
+# profiles/translate_tc_m2l_bem245k_p10.md
+NCU_TRAFFIC = {"p2p_mixed": 2 * 7.026e6, "translate_tc": 170.88e6}
 
 
 def measured_peaks():
