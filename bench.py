@@ -590,8 +590,7 @@ def run_c5(args):
 
 
 def _autotune_helm(ob, xd, bbox, kw, k):
-    """fmmb_autotune_lmax for the Helmholtz plan (depths 3..4: deeper trees
-    multiply the dense FP64 M2L work)."""
+    """fmmb_autotune_lmax for the Helmholtz plan (depths 3..5)."""
     import ctypes
     lib = ob.load()
     cfg = ob._Config()
@@ -599,15 +598,15 @@ def _autotune_helm(ob, xd, bbox, kw, k):
     cfg.kernel, cfg.p, cfg.precision, cfg.semantics = kw["kernel"], kw["p"], kw["precision"], kw["semantics"]
     cfg.exclude_self, cfg.wavenumber = 1, k
     best = ctypes.c_int(-1)
-    ms = np.zeros(2, np.float32)
+    ms = np.zeros(3, np.float32)
     bb = np.asarray(bbox, np.float32)
     ptr = [xd[i].data_ptr() for i in range(3)]
     n = xd.shape[1]
     rc = lib.fmmb_autotune_lmax(ctypes.byref(cfg), n, *ptr, None, None, None, n, *ptr, None, None, None,
-                                bb.ctypes.data, 3, 4, 1, ctypes.byref(best), ms.ctypes.data)
+                                bb.ctypes.data, 3, 5, 1, ctypes.byref(best), ms.ctypes.data)
     if rc != 0:
         raise RuntimeError(lib.fmmb_last_error().decode())
-    return best.value, {l: float(ms[l - 3]) for l in range(3, 5)}
+    return best.value, {l: float(ms[l - 3]) for l in range(3, 6)}
 
 
 def main():

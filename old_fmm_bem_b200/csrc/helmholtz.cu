@@ -292,8 +292,9 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const in
 // per thread (one shared-memory read of a source serves both); the sources of
 // the leaf's 27 neighbour slots are staged through shared memory in chunks of
 // 128.  Work items split large leaves, so the launch is not bound by the
-// densest leaf.  Mixed form: FP32 terms (sincosf), summed over 32 sources,
-// then added in FP64; FP64 form: everything in FP64.  Zero-distance pairs
+// densest leaf.  Mixed form: FP32 terms (hardware sine / cosine of the
+// phase reduced to [-pi, pi]), summed over 32 sources, then added in FP64;
+// FP64 form: everything in FP64.  Zero-distance pairs
 // contribute nothing (their inverse distance is taken as 0).
 template <bool F32>
 __device__ __forceinline__ void helm_pair(float k, const float4 x, const float4 s, const float2 q, float& fr,
@@ -301,8 +302,12 @@ __device__ __forceinline__ void helm_pair(float k, const float4 x, const float4 
   const float dx = x.x - s.x, dy = x.y - s.y, dz = x.z - s.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  // phase k r reduced to [-pi, pi] (exact for k r < pi, the usual near-field
+  // range), then the hardware sine / cosine (absolute error ~4e-7 there)
+  const float ph = k * (r2 * rinv);
+  const float red = fmaf(-6.28318530717958647f, rintf(ph * 0.159154943091895336f), ph);
   float sn, cs;
-  sincosf(k * (r2 * rinv), &sn, &cs);
+  __sincosf(red, &sn, &cs);
   fr += (q.x * cs - q.y * sn) * rinv;
   fi += (q.x * sn + q.y * cs) * rinv;
 }
