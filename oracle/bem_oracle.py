@@ -94,3 +94,18 @@ def gmres(A, b, x0=None, *, precond=1.0, restart=30, max_iter=20, rtol=0.0):
         if done or it >= max_iter:
             break
     return x, it, rel
+
+
+def solvation_energy_dense(cen, nrm, area, x_atoms, q_atoms, e1=4.0, e2=20.0):
+    """The reference's BEM solvation pipeline (bio/main.cxx) with dense FP64
+    matrices and a direct solve: right-hand side -4 pi Gni(atoms -> centroids)
+    / e1, A = diag I + Gni diag(area / e1), reaction potential
+    G(centroids -> atoms) of x * area / e1, energy 0.5 * 332.112 * q . phi."""
+    diag = (e1 + e2) / (2 * e1 * (e1 - e2))
+    kni = kernel_matrix(cen, 1, nt=nrm, xs=x_atoms)
+    b = -4 * np.pi * (kni @ np.asarray(q_atoms, np.float64)) / e1
+    A = bem_matrix(cen, nrm, np.asarray(area) / e1, 1, diag)
+    x = np.linalg.solve(A, b)
+    kg = kernel_matrix(x_atoms, 0, xs=cen)
+    phi = kg @ (x * np.asarray(area) / e1)
+    return float(0.5 * 332.112 * np.dot(np.asarray(q_atoms, np.float64), phi)), x, phi
