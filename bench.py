@@ -383,12 +383,24 @@ def run_c1(args):
         ms = _timed(lambda: plan.evaluate(qd, pot), stream, args.steps, max(3, args.warmup), flush)
     pot64, _ = plan.evaluate(q, f64=True)
     err = rel_err_vs_direct(ob, ob.LAPLACE_G, x, x, q, pot64)
+    # the reference's own fmm() (oracle/_ref, p = 8, lmax = 3) on the same points, one core
+    cpu = None
+    if not args.no_cpu:
+        from oracle import pyoracle
+        if pyoracle.ref_available(8):
+            t0 = time.perf_counter()
+            pyoracle.ref_fmm(x, x, q, neq=0, p=8, lmax=3)
+            dt = time.perf_counter() - t0
+            cpu = {"value": x.shape[1] / dt / 1e6, "unit": "Mpts/s", "cores": 1, "kind": "reference",
+                   "sample": "reference fmm(ni,nj,0) at p=8, lmax=3 on the same 32,768 points (reference semantics, "
+                             "tree build included), one core"}
     print(json.dumps({"metric": "FMM matvec Mpts/s (Laplace G potential, 32,768 uniform points, p=8, FP64)",
                       "value": x.shape[1] / (ms * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1, "steps": args.steps,
                       "ms_per_step": ms, "dtype": "f64", "data": "synthetic",
                       "config": {"workload": "Laplace G, 32,768 points U[0,1]^3, q U[-1,1], p=8, lmax=3, FP64, "
                                              "self pairs excluded"},
-                      "rel_err_vs_fp64_direct": err, "phase_ms": plan.timings(), "clocks": clk.summary()}))
+                      "rel_err_vs_fp64_direct": err, "phase_ms": plan.timings(), "cpu_baseline": cpu,
+                      "clocks": clk.summary()}))
     plan.close()
 
 
