@@ -174,6 +174,7 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       FMMB_CUDA(cudaStreamCreateWithPriority(&pl->st.cap, cudaStreamNonBlocking, prio_high));
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.fork, cudaEventDisableTiming));
       FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.join, cudaEventDisableTiming));
+      FMMB_CUDA(cudaEventCreateWithFlags(&pl->st.near_done, cudaEventDisableTiming));
       for (auto& e : pl->ev) FMMB_CUDA(cudaEventCreate(&e));
       for (auto& e : pl->evp) FMMB_CUDA(cudaEventCreate(&e));
       pl->d_err.alloc(1);
@@ -205,6 +206,7 @@ int fmmb_plan_destroy(fmmb_plan* pl) {
   if (pl->st.cap) cudaStreamDestroy(pl->st.cap);
   if (pl->st.fork) cudaEventDestroy(pl->st.fork);
   if (pl->st.join) cudaEventDestroy(pl->st.join);
+  if (pl->st.near_done) cudaEventDestroy(pl->st.near_done);
   for (auto& e : pl->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : pl->evp)
@@ -259,7 +261,7 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       FMMB_REQUIRE(to[0] == 0 && so[0] == 0 && to[nprob] == ni && so[nprob] == nj, FMMB_ERR_ARG,
                    "problem offsets must run from 0 to the point counts");
     }
-    for (int w = 0; w < 2; w++) {  // captured evaluates refer to the old buffers
+    for (int w = 0; w < 4; w++) {  // captured evaluates refer to the old buffers
       if (pl->gexec[w]) {
         FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
         cudaGraphExecDestroy(pl->gexec[w]);
@@ -530,6 +532,18 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       pl->inv_i.alloc(ni);
       FMMB_CUDA(cudaMemcpy(pl->inv_i.get(), inv.data(), ni * sizeof(int), cudaMemcpyHostToDevice));
     }
+    // near-field work items of the many-right-hand-side pass: pieces of 128 targets
+    {
+      const int nleaf = pl->nbox_i[pl->lmax];
+      std::vector<int2> leaf(nleaf), work;
+      FMMB_CUDA(cudaMemcpy(leaf.data(), pl->leaf_i.get(), nleaf * sizeof(int2), cudaMemcpyDeviceToHost));
+      for (int b = 0; b < nleaf; b++)
+        for (int t = 0; t < leaf[b].y; t += 128) work.push_back(make_int2(b, t));
+      pl->m_p2p_work.alloc(work.size());
+      if (!work.empty())
+        FMMB_CUDA(cudaMemcpy(pl->m_p2p_work.get(), work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      pl->m_p2p_nwork = (int)work.size();
+    }
     // evaluation buffers
     const int nr = pl->cfg.nrhs;
     pl->qs.alloc((size_t)nj * nr);
@@ -695,6 +709,10 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   // launches that leave SMs idle), the second the downward tail (L2L / L2P);
   // the tensor-core M2L, which needs whole SMs, runs between them.
   auto near_field = [&](int l0, int l1, bool last) {
+    if (pl->far_only) {  // the near field of this evaluate runs elsewhere
+      if (last) FMMB_CUDA(cudaEventRecord(pl->st.join, m));
+      return;
+    }
     if (l1 <= l0) {
       if (last) FMMB_CUDA(cudaEventRecord(pl->st.join, side));
       return;
@@ -829,8 +847,9 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
 // on the main stream (which may be a legacy default stream, where capture is
 // not possible).  A graph that fails to instantiate turns graphs off for the
 // plan and runs the evaluate directly.
-void run_graph(fmmb_plan* pl, bool want_grad) {
-  const int w = want_grad ? 1 : 0;
+void run_graph(fmmb_plan* pl, bool want_grad, bool far_only = false) {
+  const int w = (want_grad ? 1 : 0) + (far_only ? 2 : 0);
+  const float* qin = far_only ? pl->qs_far.get() : pl->qs.get();
   cudaStream_t m = pl->st.main;
   if (!pl->gexec[w]) {
     cudaStream_t c = pl->st.cap;
@@ -838,11 +857,13 @@ void run_graph(fmmb_plan* pl, bool want_grad) {
     cudaGraph_t graph = nullptr;
     pl->st.main = c;
     pl->capturing = true;
+    pl->far_only = far_only;
     try {
-      run_one(pl, pl->qs.get(), want_grad);
+      run_one(pl, qin, want_grad);
     } catch (...) {
       pl->st.main = m;
       pl->capturing = false;
+      pl->far_only = false;
       cudaStreamEndCapture(c, &graph);
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
@@ -850,6 +871,7 @@ void run_graph(fmmb_plan* pl, bool want_grad) {
     }
     pl->st.main = m;
     pl->capturing = false;
+    pl->far_only = false;
     FMMB_CUDA(cudaStreamEndCapture(c, &graph));
     cudaGraphExec_t exec = nullptr;
     const cudaError_t e = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
@@ -859,7 +881,9 @@ void run_graph(fmmb_plan* pl, bool want_grad) {
       pl->use_graph = false;
       pl->ev_used = 0;
       pl->ev_phase.clear();
-      run_one(pl, pl->qs.get(), want_grad);
+      pl->far_only = far_only;
+      run_one(pl, qin, want_grad);
+      pl->far_only = false;
       return;
     }
     pl->gexec[w] = exec;
@@ -940,8 +964,29 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
       }
       if (want_grad && !grad_dev) gd = (T*)base;
     }
+    // several right-hand sides in the mixed form: the near field of all of
+    // them in one pass on the side stream (sources read once for every
+    // right-hand side), the far field of each through the far-field graph
+    const bool multi = nr > 1 && pl->cfg.precision == FMMB_MIXED && pl->use_graph;
+    if (multi) {
+      pl->near_all.alloc((size_t)nr * ni * (want_grad ? 4 : 1));
+      pl->qs_far.alloc(nj);
+      FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
+      FMMB_CUDA(cudaStreamWaitEvent(pl->st.side, pl->st.fork, 0));
+      pl->launches += launch_p2p_multi(pl->cfg.kernel, nr, pl->m_p2p_nwork, pl->m_p2p_work.get(), pl->leaf_i.get(),
+                                       pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
+                                       pl->spos.get(), pl->snrm.get(), pl->qs.get(), nj, make_sem(pl),
+                                       pl->near_all.get(), want_grad ? pl->near_all.get() + (size_t)nr * ni : nullptr,
+                                       ni, pl->st.side);
+      FMMB_CUDA(cudaEventRecord(pl->st.near_done, pl->st.side));
+    }
     for (int r = 0; r < nr; r++) {
-      if (pl->use_graph) {
+      if (multi) {
+        FMMB_CUDA(cudaMemcpyAsync(pl->qs_far.get(), pl->qs.get() + (size_t)r * nj, (size_t)nj * sizeof(float),
+                                  cudaMemcpyDeviceToDevice, m));
+        run_graph(pl, want_grad, true);
+        if (r == 0) FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.near_done, 0));
+      } else if (pl->use_graph) {
         // the graph reads the charges of the first block: move right-hand
         // side r there once the previous one is consumed (stream order)
         if (r > 0)
@@ -951,13 +996,16 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
       } else {
         run_one(pl, pl->qs.get() + (size_t)r * nj, want_grad);
       }
-      const double* pn = pl->pot_s.get();
-      const double* gn = pl->grad_s.get();
+      // near and far parts of right-hand side r
+      const double* pnear = multi ? pl->near_all.get() + (size_t)r * ni : pl->pot_s.get();
+      const double* gnear = multi ? pl->near_all.get() + (size_t)nr * ni + (size_t)3 * r * ni : pl->grad_s.get();
+      const double* pfar = pl->pot_s.get() + ni;
+      const double* gfar = pl->grad_s.get() + 3 * (size_t)ni;
       if (sizeof(T) == 4)
-        launch_finalize_f32(ni, pl->perm_i.get(), pn, pn + ni, want_grad ? gn : nullptr, want_grad ? gn + 3 * (size_t)ni : nullptr,
+        launch_finalize_f32(ni, pl->perm_i.get(), pnear, pfar, want_grad ? gnear : nullptr, want_grad ? gfar : nullptr,
                             (float*)(pd + (size_t)r * ni), want_grad ? (float*)(gd + (size_t)3 * r * ni) : nullptr, m);
       else
-        launch_finalize_f64(ni, pl->perm_i.get(), pn, pn + ni, want_grad ? gn : nullptr, want_grad ? gn + 3 * (size_t)ni : nullptr,
+        launch_finalize_f64(ni, pl->perm_i.get(), pnear, pfar, want_grad ? gnear : nullptr, want_grad ? gfar : nullptr,
                             (double*)(pd + (size_t)r * ni), want_grad ? (double*)(gd + (size_t)3 * r * ni) : nullptr, m);
       pl->launches++;
     }

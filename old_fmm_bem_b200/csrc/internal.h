@@ -98,6 +98,7 @@ struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
   cudaStream_t cap = nullptr;  // private stream the evaluate graphs are captured on
   cudaEvent_t fork = nullptr, join = nullptr;
+  cudaEvent_t near_done = nullptr;  // the all-right-hand-side near field finished
 };
 
 }  // namespace fmmb
@@ -178,9 +179,19 @@ struct fmmb_plan {
   bool geo_tn = false, geo_sn = false;
   fmmb_plan* tplan = nullptr;
   fmmb::DevBuf<double> pg_tmp;                 // position-gradient work space
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  std::vector<std::pair<int, int>> gphase[2];
-  int glaunches[2] = {0, 0};
+  // graphs [without / with gradient] x [whole evaluate / far field only]
+  cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<std::pair<int, int>> gphase[4];
+  int glaunches[4] = {0, 0, 0, 0};
+  // many right-hand sides (mixed form): the near field of all of them in one
+  // pass (p2p_multi.cu) into near_all ([nrhs][ni] potentials, then
+  // [nrhs][3][ni] gradients), the far field per right-hand side through the
+  // far-field-only graph, whose charges are qs_far
+  bool far_only = false;
+  fmmb::DevBuf<double> near_all;
+  fmmb::DevBuf<float> qs_far;
+  fmmb::DevBuf<int2> m_p2p_work;  // (target leaf, first target), up to 128 targets each
+  int m_p2p_nwork = 0;
   int opimg_sets = 0;
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots

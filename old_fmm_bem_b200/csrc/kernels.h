@@ -34,6 +34,13 @@ void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const
 void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
                      const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
                      double* pot, double* grad, int ni, cudaStream_t st);
+// mixed-form near field of nrhs right-hand sides in one pass (p2p_multi.cu):
+// qs [nrhs][nj] sorted charges, pot [nrhs][ni], grad [nrhs][3][ni] (G only,
+// may be null); work items (target leaf, first target) of up to 128 targets.
+// Returns the number of launches.
+int launch_p2p_multi(int kernel, int nrhs, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
+                     const int* list, const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm,
+                     const float* qs, int nj, const Sem& s, double* pot, double* grad, int ni, cudaStream_t st);
 // FP32 point-per-thread P2M for the mixed form (accurate semantics, p <= 11:
 // its 64 x K staging must fit 48 KB of shared memory); returns false outside
 // that range

@@ -224,8 +224,11 @@ def test_autotune_lmax_picks_a_measured_depth(ob):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_many_right_hand_sides_equal_single_evaluates(precision, ob):
-    """nrhs = 3 in one evaluate (each right-hand side replayed through the
-    plan's CUDA graph) gives the three single evaluates, gradients included."""
+    """nrhs = 3 in one evaluate gives the three single evaluates, gradients
+    included: FP64 form (each right-hand side replayed through the plan's CUDA
+    graph) to 1e-12; mixed form (the near field of all three in one pass,
+    p2p_multi.cu, summing FP32 terms over 128 sources instead of 32 before
+    the FP64 accumulation; the far field per right-hand side) to 1e-6."""
     t, tn, s, sn, q = make_points(12000, 110, "clustered")
     rng = np.random.default_rng(111)
     qs = rng.uniform(-1, 1, (3, s.shape[1])).astype(np.float32)
@@ -234,8 +237,24 @@ def test_many_right_hand_sides_equal_single_evaluates(precision, ob):
     v3, g3 = pl.evaluate(qs.ravel(), f64=True)
     pl.close()
     one = plan_for(ob, 0, 8, 4, t, tn, s, sn, **kw)
+    tol = 1e-12 if precision == 0 else 1e-6
     for r in range(3):
         v, g = one.evaluate(qs[r], f64=True)
-        assert rel(v3[r * 12000:(r + 1) * 12000], v) < 1e-12
-        assert rel(g3.reshape(3, 3, -1)[r], g.reshape(3, -1)) < 1e-12
+        assert rel(v3[r * 12000:(r + 1) * 12000], v) < tol
+        assert rel(g3.reshape(3, 3, -1)[r], g.reshape(3, -1)) < tol
     one.close()
+
+
+@pytest.mark.parametrize("neq", [0, 1, 2])
+def test_many_rhs_near_field_vs_direct(neq, ob, oracle):
+    """The all-right-hand-side near field (nrhs = 9: groups of 8 and 1) within
+    the FMM's accuracy of the FP64 direct sum for every right-hand side."""
+    t, tn, s, sn, q = make_points(8000, 120 + neq, "clustered")
+    rng = np.random.default_rng(121)
+    qs = rng.uniform(-1, 1, (9, 8000)).astype(np.float32)
+    pl = plan_for(ob, neq, 12, 3, t, tn, s, sn, nrhs=9, semantics=1, precision=1, exclude_self=True)
+    v, _ = pl.evaluate(qs.ravel(), f64=True)
+    pl.close()
+    for r in (0, 7, 8):
+        ref, _ = oracle.direct(t, s, qs[r], neq=neq, eps2=0.0, exclude_self=True, tn=tn, sn=sn, targets=(0, 1000))
+        assert rel(v[r * 8000:r * 8000 + 1000], ref) < 5e-6
