@@ -163,6 +163,33 @@ FMMB_API int fmmb_gpu_p2p(const int* nvecd, float* xi, float* yi, float* zi, flo
                           float* vi, const float* xj, const float* yj, const float* zj, const float* gxj,
                           const float* gyj, const float* gzj, const float* vj);
 
+/* The reference's batch P2M call p2mgpu_ (libgpu/gpufmm.cu:200-205): per
+ * block b (nvecd[1] blocks, stride nvecd[2]) the source leaf's Morton key
+ * nvecd[b*stride + 10] and its sources [nvecd[..+11], +nvecd[..+12]) of xj..vj
+ * (nvecd[3] in all), nvecd[4] = 0 (G) or 1 (Gn, source normals gxj..),
+ * nvecd[6] = mp (mp (mp+1) / 2 <= 64); rb the leaf side, xmin.. the root
+ * corner.  Writes the multipole coefficients M_n^m of block b, in the
+ * reference's normalisation, to brex/bimx[b*64 + n(n+1)/2 + m] (the other
+ * slots of the block zeroed).  The reference's float fac table is not read:
+ * the same table is built here.  compat/gpufmm_compat.cpp defines p2mgpu_. */
+FMMB_API int fmmb_gpu_p2m(const int* nvecd, const double* rb, const double* xmin, const double* ymin,
+                          const double* zmin, const float* xj, const float* yj, const float* zj, const float* gxj,
+                          const float* gyj, const float* gzj, const float* vj, float* brex, float* bimx);
+
+/* The reference's batch L2P call l2pgpu_ (libgpu/gpufmm.cu:481-486): blocks of
+ * 64 targets xi.. (gxi.. their normals for nvecd[4] = 1), per block the leaf
+ * key nvecd[b*stride + 10] and the offset nvecd[..+11] of its local
+ * coefficients in arex/aimx (mp (mp+1) / 2 of them, nvecd[3] in all).
+ * Overwrites vi (potential; for Gn -n.grad, the target-normal derivative) and
+ * gxi.. (the gradient for G, zeros for Gn) of every packed target.  The
+ * reference's Gn kernel stores its results at scrambled positions
+ * (libgpu/Gn_l2p.cu writes veck[tx], libgpu/kernel.cu reads veck[4*tx+i]);
+ * here every target gets its own value, as the reference's CPU Gn_l2p does.
+ * compat/gpufmm_compat.cpp defines l2pgpu_. */
+FMMB_API int fmmb_gpu_l2p(const int* nvecd, const double* rb, const double* xmin, const double* ymin,
+                          const double* zmin, const float* xi, const float* yi, const float* zi, float* gxi,
+                          float* gyi, float* gzi, float* vi, const float* arex, const float* aimx);
+
 /* GMRES for the boundary-integral systems of a plan whose targets are its
  * sources (problem by problem):  A x = diag * x + K (weight .* x),  left
  * preconditioned by y = precond * x.  This is the reference's PETSc shell

@@ -1,21 +1,21 @@
-// Link-time replacement of the reference's GPU library entry point for the
-// near field, p2pgpu_ (libgpu/gpufmm.cu:57-197), over libfmmb's
-// fmmb_gpu_p2p.
+// Link-time replacement of the reference's GPU library entry points p2pgpu_,
+// p2mgpu_ and l2pgpu_ (libgpu/gpufmm.cu:57, 200, 481) over libfmmb's
+// fmmb_gpu_p2p / fmmb_gpu_p2m / fmmb_gpu_l2p.
 //
 // The reference builds its GPU variant from the host-side kernel files
-// (kernel/G_p2p_gpu.cxx, Gni_p2p_gpu.cxx, Gnj_p2p_gpu.cxx: they pack targets
-// in blocks of 128 and source ranges in the record array nvecd) linked
+// (kernel/G_p2p_gpu.cxx, Gni_p2p_gpu.cxx, Gnj_p2p_gpu.cxx, G_p2m_gpu.cxx,
+// Gn_p2m_gpu.cxx, G_l2p_gpu.cxx, Gn_l2p_gpu.cxx: they pack targets and
+// sources in blocks and describe them in the record array nvecd) linked
 // against libgpu (test/Makefile:37-41, 75-76).  Linking this file and
-// libfmmb.so in place of libgpu's p2pgpu_ keeps those host files unchanged:
-// same symbol (C++ linkage, as libgpu/gpufmm.cu defines it), same arguments,
-// same record format, same outputs (vi, gxi, gyi, gzi of every packed target
-// overwritten: potential and gradient for neq 0, potential and zeros for
-// neq 1 and 2).  `op` (the caller's flop estimate) is not used.
+// libfmmb.so in place of libgpu keeps those host files unchanged: same
+// symbols (C++ linkage, as libgpu/gpufmm.cu defines them), same arguments,
+// same record formats, same outputs.  `op` (the caller's flop estimate) and
+// the `fac` table argument are not used (the library builds the same table).
 //
-// The expansion entry points p2mgpu_, m2lgpu_ and l2pgpu_ are not provided:
-// their float record formats feed the reference's 2010 kernels, whose M2L is
-// valid only for mp <= 5 (libgpu/var.h:2, libgpu/m2l.cu:69); a GPU far field
-// is reached through fmm() (fmm_compat.cpp) or the plan API instead.
+// m2lgpu_ (M2M / M2L / L2L on the GPU) is not provided: the reference's
+// kernel is valid only for mp <= 5 (libgpu/var.h:2, libgpu/m2l.cu:69); link
+// the CPU translation objects, or use fmm() (fmm_compat.cpp), whose far field
+// runs on the GPU.
 //
 // Errors: libgpu exits through CUDA_SAFE_CALL; so does this shim, after
 // printing fmmb_last_error().
@@ -30,6 +30,30 @@ void p2pgpu_(int nvecd[], double* op, float xi[], float yi[], float zi[], float 
   const int rc = fmmb_gpu_p2p(nvecd, xi, yi, zi, gxi, gyi, gzi, vi, xj, yj, zj, gxj, gyj, gzj, vj);
   if (rc != FMMB_OK) {
     std::fprintf(stderr, "p2pgpu_: %s\n", fmmb_last_error());
+    std::exit(EXIT_FAILURE);
+  }
+}
+
+void p2mgpu_(int nvecd[], double* op, double* rb, double* xmin, double* ymin, double* zmin, float xjg[], float yjg[],
+             float zjg[], float gxjg[], float gyjg[], float gzjg[], float vjg[], float brex[], float bimx[],
+             float fac[]) {
+  (void)op;
+  (void)fac;
+  const int rc = fmmb_gpu_p2m(nvecd, rb, xmin, ymin, zmin, xjg, yjg, zjg, gxjg, gyjg, gzjg, vjg, brex, bimx);
+  if (rc != FMMB_OK) {
+    std::fprintf(stderr, "p2mgpu_: %s\n", fmmb_last_error());
+    std::exit(EXIT_FAILURE);
+  }
+}
+
+void l2pgpu_(int nvecd[], double* op, double* rb, double* xmin, double* ymin, double* zmin, float xig[], float yig[],
+             float zig[], float gxig[], float gyig[], float gzig[], float vig[], float arex[], float aimx[],
+             float fac[]) {
+  (void)op;
+  (void)fac;
+  const int rc = fmmb_gpu_l2p(nvecd, rb, xmin, ymin, zmin, xig, yig, zig, gxig, gyig, gzig, vig, arex, aimx);
+  if (rc != FMMB_OK) {
+    std::fprintf(stderr, "l2pgpu_: %s\n", fmmb_last_error());
     std::exit(EXIT_FAILURE);
   }
 }
