@@ -176,6 +176,19 @@ FMMB_API int fmmb_gpu_p2m(const int* nvecd, const double* rb, const double* xmin
                           const double* zmin, const float* xj, const float* yj, const float* zj, const float* gxj,
                           const float* gyj, const float* gzj, const float* vj, float* brex, float* bimx);
 
+/* The reference's batch translation call m2lgpu_ (libgpu/gpufmm.cu:336-338):
+ * nvecd[4] = 0 (M2M), 1 (M2L), 2 (L2L), nvecd[6] = mp (mp (mp+1) / 2 <= 64);
+ * per block b (nvecd[1] blocks, stride nvecd[2]) nvecd[b*stride + 10] inputs,
+ * input r = (offset of its coefficients in brex/bimx nvecd[..+2r+11],
+ * relative-position code + 1 nvecd[..+2r+12]) with the codes of
+ * kernel/m2m_gpu.cxx, m2l_gpu.cxx, l2l_gpu.cxx; rb the side of the output
+ * boxes (parents for M2M, children for L2L).  Writes the sum over the block's
+ * inputs of the translated coefficients (reference normalisation) to
+ * arex/aimx[b*64 + n(n+1)/2 + m].  Reference semantics, every order (the
+ * reference's own kernel is valid for mp <= 5 only). */
+FMMB_API int fmmb_gpu_m2l(const int* nvecd, const double* rb, float* arex, float* aimx, const float* brex,
+                          const float* bimx);
+
 /* The reference's batch L2P call l2pgpu_ (libgpu/gpufmm.cu:481-486): blocks of
  * 64 targets xi.. (gxi.. their normals for nvecd[4] = 1), per block the leaf
  * key nvecd[b*stride + 10] and the offset nvecd[..+11] of its local

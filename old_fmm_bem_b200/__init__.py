@@ -35,7 +35,7 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
            "fmmb_gmres", "fmmb_autotune_lmax_batch", "fmmb_gpu_p2p",
-           "fmmb_gpu_p2m", "fmmb_gpu_l2p"]
+           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l"]
 
 
 def lib_path() -> str:
@@ -89,6 +89,7 @@ def load():
     lib.fmmb_gpu_p2p.argtypes = [_vp] * 15
     lib.fmmb_gpu_p2m.argtypes = [_vp] * 14
     lib.fmmb_gpu_l2p.argtypes = [_vp] * 14
+    lib.fmmb_gpu_m2l.argtypes = [_vp] * 6
     lib.fmmb_autotune_lmax_batch.argtypes = [ctypes.POINTER(_Config), ctypes.c_int, _vp] + [_vp] * 6 + [_vp] + \
         [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
     lib.fmmb_direct_static.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \

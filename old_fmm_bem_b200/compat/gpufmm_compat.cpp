@@ -1,21 +1,20 @@
 // Link-time replacement of the reference's GPU library entry points p2pgpu_,
-// p2mgpu_ and l2pgpu_ (libgpu/gpufmm.cu:57, 200, 481) over libfmmb's
-// fmmb_gpu_p2p / fmmb_gpu_p2m / fmmb_gpu_l2p.
+// p2mgpu_, m2lgpu_ and l2pgpu_ (libgpu/gpufmm.cu:57, 200, 336, 481) over
+// libfmmb's fmmb_gpu_p2p / _p2m / _m2l / _l2p.
 //
 // The reference builds its GPU variant from the host-side kernel files
 // (kernel/G_p2p_gpu.cxx, Gni_p2p_gpu.cxx, Gnj_p2p_gpu.cxx, G_p2m_gpu.cxx,
-// Gn_p2m_gpu.cxx, G_l2p_gpu.cxx, Gn_l2p_gpu.cxx: they pack targets and
-// sources in blocks and describe them in the record array nvecd) linked
-// against libgpu (test/Makefile:37-41, 75-76).  Linking this file and
-// libfmmb.so in place of libgpu keeps those host files unchanged: same
-// symbols (C++ linkage, as libgpu/gpufmm.cu defines them), same arguments,
-// same record formats, same outputs.  `op` (the caller's flop estimate) and
-// the `fac` table argument are not used (the library builds the same table).
-//
-// m2lgpu_ (M2M / M2L / L2L on the GPU) is not provided: the reference's
-// kernel is valid only for mp <= 5 (libgpu/var.h:2, libgpu/m2l.cu:69); link
-// the CPU translation objects, or use fmm() (fmm_compat.cpp), whose far field
-// runs on the GPU.
+// Gn_p2m_gpu.cxx, m2m_gpu.cxx, m2l_gpu.cxx, l2l_gpu.cxx, G_l2p_gpu.cxx,
+// Gn_l2p_gpu.cxx: they pack targets, sources and coefficients in blocks and
+// describe them in the record array nvecd) linked against libgpu
+// (test/Makefile:37-41, 75-76).  Linking this file and libfmmb.so in place of
+// libgpu keeps those host files unchanged: same symbols (C++ linkage, as
+// libgpu/gpufmm.cu defines them), same arguments, same record formats, same
+// outputs.  Not used: `op` (the caller's flop estimate) and the table
+// arguments (fac; ynm and the rotation tables dnm of m2lgpu_): the library
+// builds the same operators itself.  The reference's GPU translations are
+// valid only for mp <= 5 (libgpu/var.h:2, libgpu/m2l.cu:69); these are valid
+// for every mp with mp (mp+1) / 2 <= 64, the record block size.
 //
 // Errors: libgpu exits through CUDA_SAFE_CALL; so does this shim, after
 // printing fmmb_last_error().
@@ -54,6 +53,20 @@ void l2pgpu_(int nvecd[], double* op, double* rb, double* xmin, double* ymin, do
   const int rc = fmmb_gpu_l2p(nvecd, rb, xmin, ymin, zmin, xig, yig, zig, gxig, gyig, gzig, vig, arex, aimx);
   if (rc != FMMB_OK) {
     std::fprintf(stderr, "l2pgpu_: %s\n", fmmb_last_error());
+    std::exit(EXIT_FAILURE);
+  }
+}
+
+void m2lgpu_(int nvecd[], double* op, double* rb, float arex[], float aimx[], float brex[], float bimx[],
+             float ynmre[], float ynmim[], float dnmre[], float dnmim[]) {
+  (void)op;
+  (void)ynmre;
+  (void)ynmim;
+  (void)dnmre;
+  (void)dnmim;
+  const int rc = fmmb_gpu_m2l(nvecd, rb, arex, aimx, brex, bimx);
+  if (rc != FMMB_OK) {
+    std::fprintf(stderr, "m2lgpu_: %s\n", fmmb_last_error());
     std::exit(EXIT_FAILURE);
   }
 }

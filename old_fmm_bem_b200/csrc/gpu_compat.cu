@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -318,6 +319,210 @@ extern "C" int fmmb_gpu_l2p(const int* nvecd, const double* rb, const double* xm
       gxi[i] = neq == 0 ? (float)out[nt + i] : 0.f;
       gyi[i] = neq == 0 ? (float)out[2 * (size_t)nt + i] : 0.f;
       gzi[i] = neq == 0 ? (float)out[3 * (size_t)nt + i] : 0.f;
+    }
+  });
+}
+
+// ---------------------------------------------------------------- m2lgpu_
+// The reference's batch translation call (libgpu/gpufmm.cu:336-480 over
+// kernel/m2m_gpu.cxx, m2l_gpu.cxx, l2l_gpu.cxx): nvecd[4] = 0 M2M, 1 M2L,
+// 2 L2L; per block b the number of inputs nvecd[b*stride + 10] and per input
+// r the offset of its coefficients in brex/bimx (nvecd[..+2r+11]) and its
+// relative-position code + 1 (nvecd[..+2r+12]): the Morton encoding
+// (fmm/boxn1.cxx) of (4 - 2c) per axis for the child octant c of an M2M, of
+// (2c + 2) for an L2L, of (target - source + 3) for an M2L.  rb is the box
+// side of the parents (M2M), of both boxes (M2L), of the children (L2L).
+// Here the same dense operators as the plan path (reference semantics,
+// operators.cpp) are applied by the FP64 pair kernel to the inputs in the
+// scaled real-packed form, and the block sums are written back as the
+// reference's complex coefficients.
+namespace fmmb {
+namespace {
+
+struct TransTables {
+  DevBuf<double> m2m_t, l2l_t, m2l_t;  // transposed, [op][column][row], row stride even(K)
+  std::vector<int> rel_to_op;
+  float m2l_rb = -1.f;
+};
+
+std::vector<double> transpose_ops(const std::vector<double>& a, int K) {
+  const int KP = (K + 1) & ~1;
+  const size_t nop = a.size() / ((size_t)K * K), os = (size_t)K * KP;
+  std::vector<double> t(nop * os, 0.0);
+  for (size_t op = 0; op < nop; op++)
+    for (int r = 0; r < K; r++)
+      for (int c = 0; c < K; c++) t[op * os + (size_t)c * KP + r] = a[(op * K + r) * K + c];
+  return t;
+}
+
+TransTables& trans_tables(int p, double rb) {
+  static std::map<int, std::unique_ptr<TransTables>> cache;
+  auto& t = cache[p];
+  const int K = (p + 1) * (p + 1);
+  auto up = [&](DevBuf<double>& d, const std::vector<double>& h) {
+    d.alloc(h.size());
+    FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice));
+  };
+  if (!t) {
+    Operators ops;
+    build_static_operators(ops, p, true);
+    t.reset(new TransTables());
+    up(t->m2m_t, transpose_ops(ops.m2m, K));
+    up(t->l2l_t, transpose_ops(ops.l2l, K));
+    t->rel_to_op = ops.rel_to_op;
+  }
+  if (t->m2l_rb != (float)rb) {  // reference semantics: the M2L set depends on the box side
+    Operators ops;
+    build_static_operators(ops, p, true);
+    build_m2l_operators(ops, 2, (float)(4.0 * rb));  // level 2 of a root of side 4 rb has side rb
+    up(t->m2l_t, transpose_ops(ops.m2l, K));
+    t->m2l_rb = (float)rb;
+  }
+  return *t;
+}
+
+int morton3_decode(int code, int* c) {  // (x, y, z) of a 3-level key, bit order of fmm/boxn1.cxx
+  c[0] = c[1] = c[2] = 0;
+  for (int i = 0; i < 3; i++) {
+    c[1] |= ((code >> (3 * i)) & 1) << i;
+    c[0] |= ((code >> (3 * i + 1)) & 1) << i;
+    c[2] |= ((code >> (3 * i + 2)) & 1) << i;
+  }
+  return 0;
+}
+
+DevBuf<int> g_top, g_tsrc, g_tdst;
+DevBuf<double> g_in, g_tout;
+DevBuf<int> g_err;
+
+}  // namespace
+}  // namespace fmmb
+
+extern "C" int fmmb_gpu_m2l(const int* nvecd, const double* rb, float* arex, float* aimx, const float* brex,
+                            const float* bimx) {
+  return guarded_c([&] {
+    FMMB_REQUIRE(nvecd && rb && arex && aimx && brex && bimx, FMMB_ERR_ARG, "null argument");
+    const int nblock = nvecd[1], stride = nvecd[2], nin = nvecd[3], var = nvecd[4], mp = nvecd[6];
+    FMMB_REQUIRE(var >= 0 && var <= 2, FMMB_ERR_ARG, "m2lgpu_ takes nvecd[4] = 0 (M2M), 1 (M2L), 2 (L2L)");
+    FMMB_REQUIRE(mp >= 1 && mp * (mp + 1) / 2 <= kBlk1, FMMB_ERR_ARG, "m2lgpu_ takes mp (mp + 1) / 2 <= 64");
+    FMMB_REQUIRE(nblock >= 0 && stride >= 3 && nin >= 0 && *rb > 0, FMMB_ERR_ARG, "bad block records");
+    if (nblock == 0) return;
+    const int p = mp - 1, K = mp * mp, P = mp * (mp + 1) / 2;
+    TransTables& tt = trans_tables(p, *rb);
+    // input rows: one per distinct coefficient offset, scaled real-packed
+    const double r_in = var == 0 ? *rb / 2 : (var == 1 ? *rb : 2 * *rb);
+    std::map<int, int> row_of;
+    std::vector<double> in;
+    std::vector<std::array<int, 3>> pairs;  // {operator, input row, block}
+    for (int b = 0; b < nblock; b++) {
+      const int nr = nvecd[(size_t)b * stride + 10];
+      FMMB_REQUIRE(nr >= 0 && 2 * nr < stride, FMMB_ERR_ARG, "too many inputs for the record stride");
+      for (int r = 0; r < nr; r++) {
+        const int jb = nvecd[(size_t)b * stride + 2 * r + 11], code = nvecd[(size_t)b * stride + 2 * r + 12] - 1;
+        FMMB_REQUIRE(jb >= 0 && jb + P <= nin && code >= 0 && code < 512, FMMB_ERR_ARG, "bad input record");
+        int c[3];
+        morton3_decode(code, c);
+        int op;
+        if (var == 1) {
+          FMMB_REQUIRE(c[0] <= 6 && c[1] <= 6 && c[2] <= 6, FMMB_ERR_ARG, "M2L offset outside the 7^3 cube");
+          op = tt.rel_to_op[c[0] * 49 + c[1] * 7 + c[2]];
+          FMMB_REQUIRE(op >= 0, FMMB_ERR_ARG, "M2L between adjacent boxes");
+        } else {
+          int oc[3];
+          for (int d = 0; d < 3; d++) {
+            oc[d] = var == 0 ? (4 - c[d]) / 2 : (c[d] - 2) / 2;
+            FMMB_REQUIRE(oc[d] == 0 || oc[d] == 1, FMMB_ERR_ARG, "bad octant code");
+          }
+          op = (oc[0] << 1) | oc[1] | (oc[2] << 2);  // key bits: x 1, y 0, z 2
+        }
+        auto it = row_of.find(jb);
+        int row;
+        if (it == row_of.end()) {
+          row = (int)row_of.size();
+          row_of[jb] = row;
+          in.resize(in.size() + K);
+          double* v = &in[(size_t)row * K];
+          for (int n = 0; n <= p; n++) {
+            const double sc = var == 2 ? std::pow(r_in, n + 1) : 1.0 / std::pow(r_in, n);
+            v[n * n] = brex[jb + isym_h(n, 0)] * sc;
+            for (int m = 1; m <= n; m++) {
+              v[n * n + 2 * m - 1] = brex[jb + isym_h(n, m)] * sc;
+              v[n * n + 2 * m] = bimx[jb + isym_h(n, m)] * sc;
+            }
+          }
+        } else {
+          row = it->second;
+        }
+        pairs.push_back({op, row, b});
+      }
+    }
+    // tiles of same-operator pairs for the pair kernel
+    std::stable_sort(pairs.begin(), pairs.end(),
+                     [](const std::array<int, 3>& a, const std::array<int, 3>& b) { return a[0] < b[0]; });
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+    const int tp = pairs_f64_tile(K, (int)pairs.size(), nsm);
+    std::vector<int> top, tsrc, tdst;
+    for (size_t i = 0; i < pairs.size();) {
+      size_t j = i;
+      while (j < pairs.size() && pairs[j][0] == pairs[i][0]) j++;
+      for (size_t k = i; k < j; k += tp) {
+        top.push_back(pairs[i][0]);
+        for (int c = 0; c < tp; c++) {
+          tsrc.push_back(k + c < j ? pairs[k + c][1] : -1);
+          tdst.push_back(k + c < j ? pairs[k + c][2] : -1);
+        }
+      }
+      i = j;
+    }
+    auto upi = [&](DevBuf<int>& d, const std::vector<int>& h) {
+      d.alloc(std::max<size_t>(h.size(), 1));
+      if (!h.empty()) FMMB_CUDA(cudaMemcpy(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+    };
+    upi(g_top, top);
+    upi(g_tsrc, tsrc);
+    upi(g_tdst, tdst);
+    g_in.alloc(std::max<size_t>(in.size(), 1));
+    if (!in.empty()) FMMB_CUDA(cudaMemcpy(g_in.get(), in.data(), in.size() * sizeof(double), cudaMemcpyHostToDevice));
+    g_tout.alloc((size_t)nblock * K);
+    FMMB_CUDA(cudaMemset(g_tout.get(), 0, (size_t)nblock * K * sizeof(double)));
+    g_err.alloc(1);
+    FMMB_CUDA(cudaMemset(g_err.get(), 0, sizeof(int)));
+    prepare_translate_pairs_f64();
+    PairArgs a{};
+    a.ntile = (int)top.size();
+    a.tp = tp;
+    a.K = K;
+    a.atomic = 1;
+    a.tile_op = g_top.get();
+    a.tile_src = g_tsrc.get();
+    a.tile_dst = g_tdst.get();
+    a.opT = (var == 0 ? tt.m2m_t : var == 1 ? tt.m2l_t : tt.l2l_t).get();
+    a.ostride = (size_t)K * ((K + 1) & ~1);
+    a.xin = g_in.get();
+    a.out = g_tout.get();
+    a.err = g_err.get();
+    launch_translate_pairs_f64(a, cudaStreamLegacy);
+    std::vector<double> out((size_t)nblock * K);
+    FMMB_CUDA(cudaMemcpy(out.data(), g_tout.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    int err = 0;
+    FMMB_CUDA(cudaMemcpy(&err, g_err.get(), sizeof(int), cudaMemcpyDeviceToHost));
+    FMMB_REQUIRE(err == 0, FMMB_ERR_CUDA, "translation operator copy timed out");
+    // scaled outputs -> the reference's complex coefficients of each block
+    const double r_out = *rb;  // side of the output boxes: parents (M2M), the level (M2L), children (L2L)
+    for (int b = 0; b < nblock; b++) {
+      float* re = arex + (size_t)b * kBlk1;
+      float* im = aimx + (size_t)b * kBlk1;
+      for (int k = 0; k < kBlk1; k++) re[k] = im[k] = 0.f;
+      const double* v = &out[(size_t)b * K];
+      for (int n = 0; n <= p; n++) {
+        const double sc = var == 0 ? std::pow(r_out, n) : 1.0 / std::pow(r_out, n + 1);
+        re[isym_h(n, 0)] = (float)(v[n * n] * sc);
+        for (int m = 1; m <= n; m++) {
+          re[isym_h(n, m)] = (float)(v[n * n + 2 * m - 1] * sc);
+          im[isym_h(n, m)] = (float)(v[n * n + 2 * m] * sc);
+        }
+      }
     }
   });
 }

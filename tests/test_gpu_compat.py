@@ -53,15 +53,17 @@ def test_reference_entry_points(path, driver, tmp_path, oracle):
 @pytest.mark.gpu
 @pytest.mark.parametrize("neq", [0, 1, 2])
 def test_reference_gpu_variant_through_p2pgpu(neq, oracle):
-    """The reference's own GPU-variant host code for P2P, P2M and L2P
+    """The reference's own GPU-variant host code for every phase
     (kernel/G_p2p_gpu.cxx, Gni_p2p_gpu.cxx, Gnj_p2p_gpu.cxx, G_p2m_gpu.cxx,
-    Gn_p2m_gpu.cxx, G_l2p_gpu.cxx, Gn_l2p_gpu.cxx: block packing into nvecd
-    records) linked to p2pgpu_ / p2mgpu_ / l2pgpu_ from
-    compat/gpufmm_compat.cpp over libfmmb (oracle/Makefile,
-    _ref/libfmmref_gpup2p_mp9.so) reproduces the reference CPU fmm() at p = 8
-    to 1e-6: P2P terms in the same FP32 arithmetic (summed per 128 sources,
-    then in FP64), P2M / L2P in FP64 with the reference's conventions, their
-    float outputs rounded like the reference's."""
+    Gn_p2m_gpu.cxx, m2m_gpu.cxx, m2l_gpu.cxx, l2l_gpu.cxx, G_l2p_gpu.cxx,
+    Gn_l2p_gpu.cxx: block packing into nvecd records) linked to p2pgpu_ /
+    p2mgpu_ / m2lgpu_ / l2pgpu_ from compat/gpufmm_compat.cpp over libfmmb
+    (oracle/Makefile, _ref/libfmmref_gpup2p_mp9.so) reproduces the reference
+    CPU fmm() at p = 8 to 1e-6: P2P terms in the same FP32 arithmetic (summed
+    per 128 sources, then in FP64), the expansions in FP64 with the
+    reference's conventions, their float outputs rounded like the
+    reference's (the reference's own GPU translations are valid only up to
+    mp = 5)."""
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libfmmref_gpup2p_mp9.so")):
         pytest.skip("reference p2pgpu_ build missing (oracle/Makefile gpup2p)")
     rng = np.random.default_rng(40 + neq)
