@@ -304,6 +304,12 @@ FMMB_API int fmmb_get_timings(fmmb_plan* plan, float* ms7);
  * evaluate. */
 FMMB_API int fmmb_get_stats(fmmb_plan* plan, long long* out8);
 
+/* Wall times (ms) of the last fmmb_set_geometry: [0] the octree build on the
+ * GPU (keys, radix sort, levels, lists; it synchronises between levels),
+ * [1] the whole call (tree, interaction tiles and work lists built on the
+ * host, operator images, buffers). */
+FMMB_API int fmmb_get_setup_times(fmmb_plan* plan, double* ms2);
+
 FMMB_API const char* fmmb_last_error(void);
 
 #ifdef __cplusplus

@@ -35,7 +35,7 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
            "fmmb_gmres", "fmmb_autotune_lmax_batch", "fmmb_gpu_p2p",
-           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l"]
+           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times"]
 
 
 def lib_path() -> str:
@@ -102,6 +102,7 @@ def load():
     lib.fmmb_get_expansions.argtypes = [_vp, ctypes.c_int, _vp]
     lib.fmmb_get_timings.argtypes = [_vp, _vp]
     lib.fmmb_get_stats.argtypes = [_vp, _vp]
+    lib.fmmb_get_setup_times.argtypes = [_vp, _vp]
     lib.fmmb_last_error.restype = ctypes.c_char_p
     _LIB = lib
     return lib
@@ -360,6 +361,12 @@ class Plan:
         ms = np.zeros(7, np.float32)
         _check(load().fmmb_get_timings(self._h, ms.ctypes.data))
         return dict(zip(["p2p", "p2m", "m2m", "m2l", "l2l", "l2p", "total"], ms.tolist()))
+
+    def setup_times(self):
+        """(tree build ms, whole fmmb_set_geometry ms) of the current geometry."""
+        o = np.zeros(2)
+        _check(load().fmmb_get_setup_times(self._h, o.ctypes.data))
+        return float(o[0]), float(o[1])
 
     def stats(self):
         o = np.zeros(8, np.int64)

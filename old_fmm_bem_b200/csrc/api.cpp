@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -240,7 +241,8 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
                   const float* tz, const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,
                   const float* sy, const float* sz, const float* snx, const float* sny, const float* snz,
                   const float* bbox) {
-  return guarded([&] {
+  const auto t_setup = std::chrono::steady_clock::now();
+  const int rc = guarded([&] {
     FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
     FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
     FMMB_REQUIRE(nprob >= 1 && nprob <= (1 << 20), FMMB_ERR_ARG, "number of problems must be in 1..2^20");
@@ -298,7 +300,10 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     FMMB_CUDA(cudaMemcpyAsync(pl->d_prob_off.get(), to.data(), (nprob + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
     FMMB_CUDA(cudaMemcpyAsync(pl->d_prob_off.get() + nprob + 1, so.data(), (nprob + 1) * sizeof(int),
                               cudaMemcpyHostToDevice, s));
+    const auto t_tree = std::chrono::steady_clock::now();
     build_tree(pl, ni, d[0], d[1], d[2], d[3], d[4], d[5], nj, d[6], d[7], d[8], d[9], d[10], d[11], bbox ? bb : nullptr);
+    FMMB_CUDA(cudaStreamSynchronize(s));
+    pl->tree_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_tree).count();
     // caller-order copy of the geometry for the transposed plan
     pl->geo.alloc((size_t)6 * ni + 6 * (size_t)nj);
     pl->geo_tn = d[3] && d[4] && d[5];
@@ -555,6 +560,9 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     FMMB_CUDA(cudaStreamSynchronize(s));
     pl->have_geometry = true;
   });
+  if (rc == FMMB_OK && pl)
+    pl->setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_setup).count();
+  return rc;
 }
 
 }  // namespace
@@ -1435,6 +1443,15 @@ int fmmb_get_timings(fmmb_plan* pl, float* ms) {
     float tot = 0;
     FMMB_CUDA(cudaEventElapsedTime(&tot, pl->ev[7], pl->ev[6]));
     ms[6] = tot;
+  });
+}
+
+int fmmb_get_setup_times(fmmb_plan* pl, double* ms) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && ms, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "no geometry");
+    ms[0] = pl->tree_ms;
+    ms[1] = pl->setup_ms;
   });
 }
 

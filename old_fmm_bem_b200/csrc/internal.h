@@ -132,6 +132,7 @@ struct fmmb_plan {
   std::vector<int> off_i, off_j;    // offsets of each level in all-level arrays (lmax first)
   int tot_i = 0, tot_j = 0;
   long long p2p_pairs = 0, m2l_pairs = 0;
+  double tree_ms = 0, setup_ms = 0;  // wall time of the octree build and of the whole fmmb_set_geometry
 
   // sorted particles
   fmmb::DevBuf<int> perm_i, perm_j;          // sorted position -> caller index
