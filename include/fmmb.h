@@ -45,10 +45,12 @@ extern "C" {
 #define FMMB_LAPLACE_G 0    /* potential sum q/(4 pi r) and its gradient */
 #define FMMB_LAPLACE_GNI 1  /* target-normal derivative: sum q (r.n_i)/(4 pi r^3) */
 #define FMMB_LAPLACE_GNJ 2  /* source-normal (double layer): sum q (r.n_j)/(4 pi r^3) */
+#define FMMB_YUKAWA 10      /* the reference's neq 10 (kernel/Helmholtz_G_p2p.cxx:18-23): sum q
+                               (pi/2) e^{-l r}/(l r), l = cfg.wavenumber; real charges and
+                               potentials; no gradient; FMMB_SEM_ACCURATE only (no eps in r) */
 #define FMMB_HELMHOLTZ_G 20 /* complex sum q e^{ikr}/(4 pi r), k = cfg.wavenumber: charges and
                                potentials are complex, interleaved (re, im) floats; no gradient;
-                               FMMB_SEM_ACCURATE only.  The reference's neq 10 kernel is the
-                               real Yukawa kernel, a different one. */
+                               FMMB_SEM_ACCURATE only. */
 
 /* Precision of the evaluation. */
 #define FMMB_FP64 0   /* every phase in FP64 on the CUDA cores */
@@ -69,7 +71,7 @@ typedef struct {
   double eps2;      /* P2P softening added to r^2 (FMMB_SEM_ACCURATE only) */
   int exclude_self; /* skip pairs at zero distance (FMMB_SEM_ACCURATE only) */
   int nrhs;         /* right-hand sides per evaluate, >= 1 */
-  double wavenumber; /* k of FMMB_HELMHOLTZ_G (> 0); unused by the Laplace kernels */
+  double wavenumber; /* k of FMMB_HELMHOLTZ_G, lambda of FMMB_YUKAWA (> 0); unused otherwise */
 } fmmb_config;
 
 typedef struct fmmb_plan fmmb_plan;

@@ -22,10 +22,11 @@ import os
 import numpy as np
 
 __all__ = ["Plan", "FMMError", "fmm", "G_dir", "Gni_dir", "Gnj_dir", "lib_path", "load",
-           "LAPLACE_G", "LAPLACE_GNI", "LAPLACE_GNJ", "HELMHOLTZ_G", "FP64", "MIXED", "SEM_REFERENCE", "SEM_ACCURATE"]
+           "LAPLACE_G", "LAPLACE_GNI", "LAPLACE_GNJ", "YUKAWA", "HELMHOLTZ_G", "FP64", "MIXED", "SEM_REFERENCE", "SEM_ACCURATE"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LAPLACE_G, LAPLACE_GNI, LAPLACE_GNJ = 0, 1, 2
+YUKAWA = 10
 HELMHOLTZ_G = 20
 FP64, MIXED = 0, 1
 SEM_REFERENCE, SEM_ACCURATE = 0, 1

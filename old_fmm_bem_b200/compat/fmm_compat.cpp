@@ -36,6 +36,7 @@ extern float *xi, *yi, *zi, *gxi, *gyi, *gzi, *vi;
 extern float *xj, *yj, *zj, *gxj, *gyj, *gzj, *vj;
 extern int lmax;
 extern float xmin, ymin, zmin, rd;
+extern double lambda;  // Yukawa screening (include/constants.h:60)
 
 namespace {
 int g_order = 8;
@@ -47,16 +48,28 @@ bool report(int rc, const char* where) {
   return false;
 }
 
-// One plan per (kernel, order, depth, precision), rebuilt when they change.
+// The Yukawa kernel has no reference-semantics mode: its near field takes the
+// reference's conventions through the plan's eps2 (1e-6f added to r^2,
+// kernel/Helmholtz_G_p2p.cxx:21) and self pairs included; wavenumber = lambda.
+void yukawa_config(fmmb_config& cfg) {
+  cfg.semantics = FMMB_SEM_ACCURATE;
+  cfg.eps2 = (double)1e-6f;
+  cfg.exclude_self = 0;
+  cfg.wavenumber = lambda;
+}
+
+// One plan per (kernel, order, depth, precision, Yukawa lambda), rebuilt when they change.
 struct Cached {
   fmmb_plan* plan = nullptr;
   int kernel = -1, p = -1, lmax = -1, precision = -1;
+  double lam = 0;
 };
-Cached g_fmm[3];
+Cached g_fmm[4];  // neq 0, 1, 2, 10
 
 fmmb_plan* plan_for(int kernel, int levels) {
-  Cached& c = g_fmm[kernel];
-  if (c.plan && c.p == g_order && c.lmax == levels && c.precision == g_precision) return c.plan;
+  Cached& c = g_fmm[kernel == FMMB_YUKAWA ? 3 : kernel];
+  const double lam = kernel == FMMB_YUKAWA ? lambda : 0.0;
+  if (c.plan && c.p == g_order && c.lmax == levels && c.precision == g_precision && c.lam == lam) return c.plan;
   if (c.plan) fmmb_plan_destroy(c.plan);
   c.plan = nullptr;
   fmmb_config cfg;
@@ -66,11 +79,13 @@ fmmb_plan* plan_for(int kernel, int levels) {
   cfg.lmax = levels;
   cfg.precision = g_precision;
   cfg.semantics = FMMB_SEM_REFERENCE;
+  if (kernel == FMMB_YUKAWA) yukawa_config(cfg);
   if (!report(fmmb_plan_create(&cfg, &c.plan), "plan_create")) return nullptr;
   c.kernel = kernel;
   c.p = g_order;
   c.lmax = levels;
   c.precision = g_precision;
+  c.lam = lam;
   return c.plan;
 }
 
@@ -82,6 +97,7 @@ void direct(int neq, int n0, int n1, int n2, int n3) {
   cfg.kernel = neq;
   cfg.lmax = 2;
   cfg.semantics = FMMB_SEM_REFERENCE;
+  if (neq == FMMB_YUKAWA) yukawa_config(cfg);
   fmmb_plan* pl = nullptr;
   if (!report(fmmb_plan_create(&cfg, &pl), "plan_create")) return;
   if (report(fmmb_set_geometry(pl, ni, xi + n0, yi + n0, zi + n0, neq == 1 ? gxi + n0 : nullptr,
@@ -112,8 +128,8 @@ extern "C" void fmmb_compat_set_order(int p) { g_order = p; }
 extern "C" void fmmb_compat_set_precision(int precision) { g_precision = precision; }
 
 void fmm(int mi, int mj, int neq) {
-  if (neq != FMMB_LAPLACE_G && neq != FMMB_LAPLACE_GNI && neq != FMMB_LAPLACE_GNJ) {
-    std::fprintf(stderr, "fmmb: fmm(neq=%d) not supported (Laplace G/Gni/Gnj only)\n", neq);
+  if (neq != FMMB_LAPLACE_G && neq != FMMB_LAPLACE_GNI && neq != FMMB_LAPLACE_GNJ && neq != FMMB_YUKAWA) {
+    std::fprintf(stderr, "fmmb: fmm(neq=%d) not supported (0, 1, 2, 10)\n", neq);
     return;
   }
   fmmb_plan* pl = plan_for(neq, lmax);
@@ -135,9 +151,15 @@ void fmm(int mi, int mj, int neq) {
     delete[] grad;
   } else {
     report(fmmb_evaluate(pl, vj, vi, nullptr), "evaluate");
+    if (neq == FMMB_YUKAWA)  // the reference zeroes the gradient outputs for neq 10 (fmm/fmm.cxx:46-53)
+      for (int i = 0; i < mi; i++) gxi[i] = gyi[i] = gzi[i] = 0.f;
   }
 }
 
 void G_dir(int n0, int n1, int n2, int n3) { direct(FMMB_LAPLACE_G, n0, n1, n2, n3); }
 void Gni_dir(int n0, int n1, int n2, int n3) { direct(FMMB_LAPLACE_GNI, n0, n1, n2, n3); }
 void Gnj_dir(int n0, int n1, int n2, int n3) { direct(FMMB_LAPLACE_GNJ, n0, n1, n2, n3); }
+
+// kernel/Helmholtz_G_dir.cxx:6: the Yukawa direct sum on targets n0..n1 from
+// sources n2..n3 (inclusive), eps = 1e-6 on r^2, self pairs included
+void Helmholtz_G_dir(int n0, int n1, int n2, int n3) { direct(FMMB_YUKAWA, n0, n1, n2, n3); }

@@ -136,12 +136,12 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
   return guarded([&] {
     FMMB_REQUIRE(cfg && out, FMMB_ERR_ARG, "null argument");
     FMMB_REQUIRE(cfg->kernel == FMMB_LAPLACE_G || cfg->kernel == FMMB_LAPLACE_GNI || cfg->kernel == FMMB_LAPLACE_GNJ ||
-                     cfg->kernel == FMMB_HELMHOLTZ_G,
+                     helm_family(cfg->kernel),
                  FMMB_ERR_ARG, "unknown kernel");
-    FMMB_REQUIRE(cfg->kernel != FMMB_HELMHOLTZ_G || (cfg->wavenumber > 0 && std::isfinite(cfg->wavenumber)),
-                 FMMB_ERR_ARG, "the Helmholtz kernel needs a finite wavenumber > 0");
-    FMMB_REQUIRE(cfg->kernel != FMMB_HELMHOLTZ_G || cfg->semantics == FMMB_SEM_ACCURATE, FMMB_ERR_ARG,
-                 "the Helmholtz kernel has no reference semantics: use FMMB_SEM_ACCURATE");
+    FMMB_REQUIRE(!helm_family(cfg->kernel) || (cfg->wavenumber > 0 && std::isfinite(cfg->wavenumber)),
+                 FMMB_ERR_ARG, "the Helmholtz and Yukawa kernels need a finite wavenumber > 0");
+    FMMB_REQUIRE(!helm_family(cfg->kernel) || cfg->semantics == FMMB_SEM_ACCURATE, FMMB_ERR_ARG,
+                 "the Helmholtz and Yukawa kernels take FMMB_SEM_ACCURATE");
     FMMB_REQUIRE(cfg->p >= 1 && cfg->p <= 20, FMMB_ERR_ARG, "p must be in 1..20");
     FMMB_REQUIRE(cfg->lmax >= 2 && cfg->lmax <= 10, FMMB_ERR_ARG, "lmax must be in 2..10");
     FMMB_REQUIRE(cfg->precision == FMMB_FP64 || cfg->precision == FMMB_MIXED, FMMB_ERR_ARG, "unknown precision");
@@ -184,7 +184,7 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       *pl->h_err = 0;
       build_static_operators(pl->ops, pl->p, pl->ref);
       upload_static_ops(pl);
-      if (!pl->ref && cfg->kernel != FMMB_HELMHOLTZ_G) {  // geometry-independent M2L set
+      if (!pl->ref && !helm_family(cfg->kernel)) {  // geometry-independent M2L set
         build_m2l_operators(pl->ops, 2, 1.0f);
         upload(pl->d_m2l, pl->ops.m2l, pl->st.main);
       }
@@ -313,7 +313,7 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       float* dst = pl->geo.get() + (k < 6 ? (size_t)k * ni : (size_t)6 * ni + (size_t)(k - 6) * nj);
       if (d[k]) FMMB_CUDA(cudaMemcpyAsync(dst, d[k], n * sizeof(float), cudaMemcpyDeviceToDevice, s));
     }
-    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // its own operators and jobs
+    if (helm_family(pl->cfg.kernel)) {  // its own operators and jobs
       helm_setup(pl);
       pl->have_geometry = true;
       return;
@@ -639,6 +639,7 @@ struct PhaseTimer {
 void run_one_helm(fmmb_plan* pl, const float* qs) {
   const int K = pl->K, p = pl->p, lmax = pl->lmax;
   const double k = pl->cfg.wavenumber;
+  const bool yuk = pl->cfg.kernel == FMMB_YUKAWA;
   cudaStream_t m = pl->st.main, side = pl->st.side;
   double* pot_near = pl->pot_s.get();
   double* pot_far = pl->pot_s.get() + 2 * (size_t)pl->ni;
@@ -649,7 +650,8 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   FMMB_CUDA(time_mark(pl, pl->ev[0], side));
   {
     PhaseTimer tm(pl, 0, side);
-    launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, (float)k, pl->h_p2p_nwork, pl->h_p2p_work.get(),
+    launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, yuk, (float)k, (float)pl->cfg.eps2, pl->cfg.exclude_self != 0,
+                    pl->h_p2p_nwork, pl->h_p2p_work.get(),
                     pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->spos.get(), qs,
                     pot_near, side);
   }
@@ -658,7 +660,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   FMMB_CUDA(time_mark(pl, pl->ev[2], m));
   {
     PhaseTimer tm(pl, 1, m);
-    launch_helm_p2m(nleaf_j, p, k, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), qs, pl->bbox, wleaf,
+    launch_helm_p2m(nleaf_j, p, k, yuk, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), qs, pl->bbox, wleaf,
                     pl->M.get() + (size_t)pl->off_j[lmax] * 2 * K, m);
   }
   FMMB_CUDA(time_mark(pl, pl->ev[3], m));
@@ -691,7 +693,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);
-    launch_helm_l2p(nleaf_i, p, k, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->bbox, wleaf,
+    launch_helm_l2p(nleaf_i, p, k, yuk, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->bbox, wleaf,
                     pl->L.get() + (size_t)pl->off_i[lmax] * 2 * K, pot_far, m);
   }
   FMMB_CUDA(time_mark(pl, pl->ev[6], m));
@@ -700,7 +702,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
 
 // Runs one right-hand side: qs (sorted, device) -> near/far sorted outputs.
 void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
-  if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {
+  if (helm_family(pl->cfg.kernel)) {
     run_one_helm(pl, qs);
     return;
   }
@@ -921,14 +923,19 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     pl->ev_phase.clear();
     pl->launches = 0;
     FMMB_CUDA(cudaEventRecord(pl->ev[7], m));
-    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // complex charges and potentials, interleaved
-      const float* qd = to_device(q, (size_t)2 * nj * nr, pl->stage_f, m);
-      launch_helm_gather(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
+    if (helm_family(pl->cfg.kernel)) {
+      // Helmholtz: complex charges and potentials, interleaved; Yukawa: real
+      // ones, run through the same complex pipeline with zero imaginary parts
+      const bool yuk = pl->cfg.kernel == FMMB_YUKAWA;
+      const size_t cw = yuk ? 1 : 2;
+      const float* qd = to_device(q, cw * nj * nr, pl->stage_f, m);
+      if (yuk) launch_helm_gather_real(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
+      else launch_helm_gather(nj, nr, pl->perm_j.get(), qd, pl->qs.get(), m);
       pl->launches++;
       const bool pot_dev = is_device_ptr(pot);
       T* pd = pot;
       if (!pot_dev) {
-        pl->stage_out.alloc((size_t)2 * ni * nr * sizeof(T));
+        pl->stage_out.alloc(cw * ni * nr * sizeof(T));
         pd = (T*)pl->stage_out.get();
       }
       for (int r = 0; r < nr; r++) {
@@ -940,13 +947,17 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
         } else {
           run_one(pl, pl->qs.get() + (size_t)2 * r * nj, false);
         }
-        launch_helm_finalize<T>(ni, pl->perm_i.get(), pl->pot_s.get(), pl->pot_s.get() + 2 * (size_t)ni,
-                                pd + (size_t)2 * r * ni, m);
+        if (yuk)  // (pi/2) e^{-l r}/(l r) = (2 pi^2 / l) e^{-l r}/(4 pi r)
+          launch_helm_finalize_real<T>(ni, pl->perm_i.get(), pl->pot_s.get(), pl->pot_s.get() + 2 * (size_t)ni,
+                                       2.0 * M_PI * M_PI / pl->cfg.wavenumber, pd + (size_t)r * ni, m);
+        else
+          launch_helm_finalize<T>(ni, pl->perm_i.get(), pl->pot_s.get(), pl->pot_s.get() + 2 * (size_t)ni,
+                                  pd + (size_t)2 * r * ni, m);
         pl->launches++;
       }
       FMMB_CUDA(cudaEventRecord(pl->ev[6], m));
       FMMB_CUDA(cudaMemcpyAsync(pl->h_err, pl->d_err.get(), sizeof(int), cudaMemcpyDeviceToHost, m));
-      if (!pot_dev) FMMB_CUDA(cudaMemcpyAsync(pot, pd, (size_t)2 * ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
+      if (!pot_dev) FMMB_CUDA(cudaMemcpyAsync(pot, pd, cw * ni * nr * sizeof(T), cudaMemcpyDeviceToHost, m));
       if (!pot_dev || !is_device_ptr(q)) FMMB_CUDA(cudaStreamSynchronize(m));
       pl->have_expansions = true;
       pl->timings_valid = true;
@@ -1057,7 +1068,7 @@ int autotune_impl(const fmmb_config* cfg, int ni, int nj, int lmin, int lmax_hi,
     FMMB_REQUIRE(2 <= lmin && lmin <= lmax_hi && lmax_hi <= 10, FMMB_ERR_ARG, "lmax range must lie in [2, 10]");
     reps = std::max(1, reps);
     // random charges on the device (caller order), one FP64 output buffer
-    const size_t cw = cfg->kernel == FMMB_HELMHOLTZ_G ? 2 : 1;  // complex: interleaved
+    const size_t cw = cfg->kernel == FMMB_HELMHOLTZ_G ? 2 : 1;  // complex: interleaved (Yukawa is real)
     std::vector<float> hq(cw * nj * std::max(1, cfg->nrhs));
     uint64_t st = 0x9E3779B97F4A7C15ull;
     for (auto& v : hq) {
@@ -1259,9 +1270,11 @@ int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, 
     FMMB_REQUIRE(0 <= i0 && i0 <= i1 && i1 <= pl->ni, FMMB_ERR_ARG, "target range out of bounds");
     cudaStream_t m = pl->st.main;
     const int nj = pl->nj, cnt = i1 - i0;
-    if (pl->cfg.kernel == FMMB_HELMHOLTZ_G) {  // complex: pot holds 2 cnt doubles (re, im)
-      const float* qd = to_device(q, (size_t)2 * nj, pl->stage_f, m);
-      launch_helm_gather(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
+    if (helm_family(pl->cfg.kernel)) {  // Helmholtz: pot holds 2 cnt doubles (re, im); Yukawa: cnt
+      const bool yuk = pl->cfg.kernel == FMMB_YUKAWA;
+      const float* qd = to_device(q, (size_t)(yuk ? 1 : 2) * nj, pl->stage_f, m);
+      if (yuk) launch_helm_gather_real(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
+      else launch_helm_gather(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
       DevBuf<double> out;
       out.alloc((size_t)2 * cnt + 2);
       const std::vector<int>&to = pl->prob_toff, &so = pl->prob_soff;
@@ -1269,7 +1282,17 @@ int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, 
         const int a0 = std::max(i0, to[b]), a1 = std::min(i1, to[b + 1]);
         if (a0 >= a1) continue;
         launch_helm_direct(a0, a1, pl->inv_i.get(), pl->tpos.get(), so[b + 1] - so[b], pl->spos.get() + so[b],
-                           pl->qs.get() + (size_t)2 * so[b], pl->cfg.wavenumber, out.get() + (size_t)2 * (a0 - i0), m);
+                           pl->qs.get() + (size_t)2 * so[b], pl->cfg.wavenumber, yuk, pl->cfg.eps2,
+                           pl->cfg.exclude_self != 0, out.get() + (size_t)2 * (a0 - i0), m);
+      }
+      if (yuk) {
+        std::vector<double> h((size_t)2 * cnt);
+        FMMB_CUDA(cudaMemcpyAsync(h.data(), out.get(), h.size() * sizeof(double), cudaMemcpyDeviceToHost, m));
+        FMMB_CUDA(cudaStreamSynchronize(m));
+        std::vector<double> r(cnt);
+        for (int i = 0; i < cnt; i++) r[i] = 2.0 * M_PI * M_PI / pl->cfg.wavenumber * h[2 * (size_t)i];
+        FMMB_CUDA(cudaMemcpy(pot, r.data(), cnt * sizeof(double), cudaMemcpyDefault));
+        return;
       }
       FMMB_CUDA(cudaMemcpyAsync(pot, out.get(), (size_t)2 * cnt * sizeof(double),
                                 is_device_ptr(pot) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, m));

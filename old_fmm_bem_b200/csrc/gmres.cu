@@ -258,7 +258,7 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
     FMMB_REQUIRE(cfg->max_iter >= 0, FMMB_ERR_ARG, "max_iter must be >= 0");
     FMMB_REQUIRE(cfg->rtol >= 0 && std::isfinite(cfg->diag) && std::isfinite(cfg->precond), FMMB_ERR_ARG,
                  "rtol must be >= 0, diag and precond finite");
-    FMMB_REQUIRE(pl->cfg.kernel != FMMB_HELMHOLTZ_G, FMMB_ERR_ARG, "GMRES takes the real Laplace kernels");
+    FMMB_REQUIRE(!helm_family(pl->cfg.kernel), FMMB_ERR_ARG, "GMRES takes the Laplace kernels");
     FMMB_REQUIRE(pl->ni == pl->nj && pl->prob_toff == pl->prob_soff, FMMB_ERR_ARG,
                  "GMRES needs a square system: the targets are the sources, problem by problem");
     const int n = pl->ni, nrhs = pl->cfg.nrhs, nprob = pl->nprob, m = cfg->restart;

@@ -25,6 +25,14 @@
 // target radial function at the sphere's radius.  The operators are stored in
 // the real 2K x 2K form acting on [re | im] (transposed, row stride 2K) and
 // applied by the FP64 pair kernel of kernels_fp64.cu.
+//
+// The same code serves the Yukawa kernel (FMMB_YUKAWA, the reference's neq 10,
+// kernel/Helmholtz_G_p2p.cxx:18-23: (pi/2) e^{-lambda r} / (lambda r)) through
+//   e^{-l|x-y|} / (4 pi |x-y|) = (2l/pi) sum_n i_n(l|y|) k_n(l|x|) sum_m Y_n^m(x^) conj(Y_n^m(y^))
+// with the modified spherical Bessel functions i_n (Miller's backward
+// recurrence normalised by i_0 = sinh(x)/x) and k_n (k_0 = (pi/2) e^{-x}/x,
+// upward recurrence): real radial functions in place of j_n and h_n, the
+// factor 2l/pi in place of ik; the result is scaled by 2 pi^2 / l on output.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -84,6 +92,48 @@ __device__ void sph_y(int nmax, double x, double* y) {
   y[0] = -c / x;
   if (nmax >= 1) y[1] = -c / (x * x) - s / x;
   for (int n = 1; n < nmax; n++) y[n + 1] = (2 * n + 1) / x * y[n] - y[n - 1];
+}
+
+// i_n(x), n = 0..nmax, x >= 0: Miller's backward recurrence
+// i_{n-1} = i_{n+1} + (2n+1)/x i_n, normalised by i_0 = sinh(x)/x
+__device__ void sph_i(int nmax, double x, double* v) {
+  if (x < 1e-6) {  // x^n / (2n+1)!! (1 + x^2 / (2 (2n+3)))
+    double t = 1.0;
+    for (int n = 0; n <= nmax; n++) {
+      v[n] = t * (1.0 + x * x / (2.0 * (2 * n + 3)));
+      t *= x / (2 * n + 3);
+    }
+    return;
+  }
+  const int N = nmax + 24 + (int)x;
+  double ip1 = 0.0, in = 1e-250;
+  for (int n = N; n >= 1; n--) {
+    const double im1 = (2 * n + 1) / x * in + ip1;
+    ip1 = in;
+    in = im1;
+    if (n - 1 <= nmax) v[n - 1] = im1;
+    if (fabs(in) > 1e250) {
+      in *= 1e-250;
+      ip1 *= 1e-250;
+      for (int q = max(n - 1, 0); q <= nmax; q++) v[q] *= 1e-250;
+    }
+  }
+  const double sc = (sinh(x) / x) / v[0];
+  for (int n = 0; n <= nmax; n++) v[n] *= sc;
+}
+
+// k_n(x), n = 0..nmax, x > 0, normalised k_0 = (pi/2) e^{-x} / x (upward recurrence)
+__device__ void sph_k(int nmax, double x, double* v) {
+  const double e = 0.5 * M_PI * exp(-x);
+  v[0] = e / x;
+  if (nmax >= 1) v[1] = e * (1.0 / x + 1.0 / (x * x));
+  for (int n = 1; n < nmax; n++) v[n + 1] = v[n - 1] + (2 * n + 1) / x * v[n];
+}
+
+// regular radial functions: j_n (Helmholtz) or i_n (Yukawa)
+__device__ __forceinline__ void radial_reg(int yuk, int nmax, double x, double* v) {
+  if (yuk) sph_i(nmax, x, v);
+  else sph_j(nmax, x, v);
 }
 
 // direction of v: cos(theta), and e^{i phi} (1 on the axis)
@@ -156,7 +206,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 // One block (4 warps) per source leaf; a warp takes 32 points at a time, each
 // lane streams its point's terms over (m, n), warp sums go to shared FP64
 // accumulators; M = ik * sum.
-__global__ void __launch_bounds__(128) helm_p2m(int p, int K, double k, const int* __restrict__ keys,
+__global__ void __launch_bounds__(128) helm_p2m(int p, int K, double k, int yuk, const int* __restrict__ keys,
                                                 const int2* __restrict__ leaf, const float4* __restrict__ spos,
                                                 const float2* __restrict__ q, Corner bbox, double w,
                                                 double* __restrict__ M) {
@@ -185,7 +235,7 @@ __global__ void __launch_bounds__(128) helm_p2m(int p, int K, double k, const in
     const double r = sqrt(vx * vx + vy * vy + vz * vz);
     double ct, st, cp, sp;
     direction(vx, vy, vz, r, ct, st, cp, sp);
-    sph_j(p, k * r, jv);
+    radial_reg(yuk, p, k * r, jv);
     double ymm = 0.28209479177387814, er = 1.0, ei = 0.0;  // Ybar_m^m, e^{i m phi}
     for (int m = 0; m <= p; m++) {
       if (m > 0) {
@@ -226,14 +276,19 @@ __global__ void __launch_bounds__(128) helm_p2m(int p, int K, double k, const in
   __syncthreads();
   double* out = M + (size_t)b * 2 * K;
   for (int c = threadIdx.x; c < K; c += blockDim.x) {
-    out[c] = -k * acc[K + c];  // ik (a + ib) = -k b + i k a
-    out[K + c] = k * acc[c];
+    if (yuk) {  // (2 l / pi) (a + ib)
+      out[c] = 2.0 * k / M_PI * acc[c];
+      out[K + c] = 2.0 * k / M_PI * acc[K + c];
+    } else {  // ik (a + ib) = -k b + i k a
+      out[c] = -k * acc[K + c];
+      out[K + c] = k * acc[c];
+    }
   }
 }
 
 // ---------------------------------------------------------------- L2P
 // One block per target leaf, one thread per target: phi = sum L j_n(kr) Y_n^m.
-__global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const int* __restrict__ keys,
+__global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, int yuk, const int* __restrict__ keys,
                                                 const int2* __restrict__ leaf, const float4* __restrict__ tpos,
                                                 Corner bbox, double w, const double* __restrict__ L,
                                                 double2* __restrict__ pot) {
@@ -251,7 +306,7 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const in
     const double r = sqrt(vx * vx + vy * vy + vz * vz);
     double ct, st, cp, sp;
     direction(vx, vy, vz, r, ct, st, cp, sp);
-    sph_j(p, k * r, jv);
+    radial_reg(yuk, p, k * r, jv);
     double pr = 0, pi = 0;
     double ymm = 0.28209479177387814, er = 1.0, ei = 0.0;
     for (int m = 0; m <= p; m++) {
@@ -288,6 +343,8 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const in
 }
 
 // ---------------------------------------------------------------- P2P
+// Pairs at zero distance are skipped when the plan excludes them; eps2 (the
+// plan's softening) is added to r^2.
 // One block (128 threads) per work item = up to 256 targets of one leaf, two
 // per thread (one shared-memory read of a source serves both); the sources of
 // the leaf's 27 neighbour slots are staged through shared memory in chunks of
@@ -296,12 +353,18 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, const in
 // phase reduced to [-pi, pi]), summed over 32 sources, then added in FP64;
 // FP64 form: everything in FP64.  Zero-distance pairs
 // contribute nothing (their inverse distance is taken as 0).
-template <bool F32>
-__device__ __forceinline__ void helm_pair(float k, const float4 x, const float4 s, const float2 q, float& fr,
-                                          float& fi) {
+template <bool YUK>
+__device__ __forceinline__ void helm_pair(float k, float eps2, bool excl, const float4 x, const float4 s,
+                                          const float2 q, float& fr, float& fi) {
   const float dx = x.x - s.x, dy = x.y - s.y, dz = x.z - s.z;
-  const float r2 = dx * dx + dy * dy + dz * dz;
-  const float rinv = r2 > 0.f ? rsqrtf(r2) : 0.f;
+  const float d2 = dx * dx + dy * dy + dz * dz, r2 = d2 + eps2;
+  const float rinv = (excl && d2 == 0.f) || r2 == 0.f ? 0.f : rsqrtf(r2);
+  if (YUK) {  // real kernel e^{-l r} / r
+    const float e = __expf(-k * (r2 * rinv)) * rinv;
+    fr = fmaf(q.x, e, fr);
+    fi = fmaf(q.y, e, fi);
+    return;
+  }
   // phase k r reduced to [-pi, pi] (exact for k r < pi, the usual near-field
   // range), then the hardware sine / cosine (absolute error ~4e-7 there)
   const float ph = k * (r2 * rinv);
@@ -311,20 +374,28 @@ __device__ __forceinline__ void helm_pair(float k, const float4 x, const float4 
   fr += (q.x * cs - q.y * sn) * rinv;
   fi += (q.x * sn + q.y * cs) * rinv;
 }
-__device__ __forceinline__ void helm_pair64(double k, const float4 x, const float4 s, const float2 q, double& ar,
-                                            double& ai) {
+template <bool YUK>
+__device__ __forceinline__ void helm_pair64(double k, double eps2, bool excl, const float4 x, const float4 s,
+                                            const float2 q, double& ar, double& ai) {
   const double dx = (double)x.x - s.x, dy = (double)x.y - s.y, dz = (double)x.z - s.z;
-  const double r2 = dx * dx + dy * dy + dz * dz;
-  if (r2 == 0.0) return;
+  const double d2 = dx * dx + dy * dy + dz * dz, r2 = d2 + eps2;
+  if ((excl && d2 == 0.0) || r2 == 0.0) return;
   const double r = sqrt(r2);
+  if (YUK) {
+    const double e = exp(-k * r) / r;
+    ar += q.x * e;
+    ai += q.y * e;
+    return;
+  }
   double sn, cs;
   sincos(k * r, &sn, &cs);
   ar += (q.x * cs - q.y * sn) / r;
   ai += (q.x * sn + q.y * cs) / r;
 }
 
-template <bool F32>
-__global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict__ work, const int2* __restrict__ leaf_i,
+template <bool F32, bool YUK>
+__global__ void __launch_bounds__(128) helm_p2p(float k, float eps2, int excl, const int2* __restrict__ work,
+                                                const int2* __restrict__ leaf_i,
                                                 const int2* __restrict__ leaf_j, const int* __restrict__ list,
                                                 const float4* __restrict__ tpos, const float4* __restrict__ spos,
                                                 const float2* __restrict__ q, double2* __restrict__ pot) {
@@ -359,11 +430,11 @@ __global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict_
             for (int jj = r0; jj < re; jj++) {
               const float4 sv = sp[jj];
               const float2 qq = sq[jj];
-              helm_pair<true>(k, x0, sv, qq, fr0, fi0);
-              helm_pair<true>(k, x1, sv, qq, fr1, fi1);
+              helm_pair<YUK>(k, eps2, excl, x0, sv, qq, fr0, fi0);
+              helm_pair<YUK>(k, eps2, excl, x1, sv, qq, fr1, fi1);
             }
           } else {
-            for (int jj = r0; jj < re; jj++) helm_pair<true>(k, x0, sp[jj], sq[jj], fr0, fi0);
+            for (int jj = r0; jj < re; jj++) helm_pair<YUK>(k, eps2, excl, x0, sp[jj], sq[jj], fr0, fi0);
           }
           ar0 += fr0;
           ai0 += fi0;
@@ -373,8 +444,8 @@ __global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict_
           for (int jj = r0; jj < re; jj++) {
             const float4 sv = sp[jj];
             const float2 qq = sq[jj];
-            helm_pair64((double)k, x0, sv, qq, ar0, ai0);
-            if (on1) helm_pair64((double)k, x1, sv, qq, ar1, ai1);
+            helm_pair64<YUK>((double)k, (double)eps2, excl, x0, sv, qq, ar0, ai0);
+            if (on1) helm_pair64<YUK>((double)k, (double)eps2, excl, x1, sv, qq, ar1, ai1);
           }
         }
       }
@@ -389,7 +460,8 @@ __global__ void __launch_bounds__(128) helm_p2p(float k, const int2* __restrict_
 __global__ void __launch_bounds__(128) helm_direct(int i0, int i1, const int* __restrict__ inv_i,
                                                    const float4* __restrict__ tpos, int nj,
                                                    const float4* __restrict__ spos, const float2* __restrict__ q,
-                                                   double k, double2* __restrict__ out) {
+                                                   double k, int yuk, double eps2, int excl,
+                                                   double2* __restrict__ out) {
   __shared__ float4 sp[128];
   __shared__ float2 sq[128];
   const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
@@ -406,11 +478,16 @@ __global__ void __launch_bounds__(128) helm_direct(int i0, int i1, const int* __
     const int nl = min(128, nj - j0);
     for (int jj = 0; jj < nl; jj++) {
       const double dx = (double)xi.x - sp[jj].x, dy = (double)xi.y - sp[jj].y, dz = (double)xi.z - sp[jj].z;
-      const double r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 == 0.0) continue;
+      const double d2 = dx * dx + dy * dy + dz * dz, r2 = d2 + eps2;
+      if ((excl && d2 == 0.0) || r2 == 0.0) continue;
       const double r = sqrt(r2);
       double sn, cs;
-      sincos(k * r, &sn, &cs);
+      if (yuk) {
+        sn = 0.0;
+        cs = exp(-k * r);
+      } else {
+        sincos(k * r, &sn, &cs);
+      }
       ar += (sq[jj].x * cs - sq[jj].y * sn) / r;
       ai += (sq[jj].x * sn + sq[jj].y * cs) / r;
     }
@@ -423,7 +500,7 @@ __global__ void __launch_bounds__(128) helm_direct(int i0, int i1, const int* __
 // R_n(k|v|) Y_n^m(v^) at v = D + rad * s_q over the quadrature points s_q;
 // g[i][m'] = sum_j f[i][j] e^{-i m' phi_j} 2 pi / NP;
 // T[n'm'] = sum_i w_i g[i][m'] Ybar_n'^|m'|(x_i) / R'_n'(k rad).
-__global__ void __launch_bounds__(256) helm_build_ops(int p, int K, double k, const HelmOp* __restrict__ ops,
+__global__ void __launch_bounds__(256) helm_build_ops(int p, int K, double k, int yuk, const HelmOp* __restrict__ ops,
                                                       int NQ, int NP, const double* __restrict__ gl_x,
                                                       const double* __restrict__ gl_w,
                                                       const double* __restrict__ ybar_q,  // [NQ][P] Ybar at the nodes
@@ -458,19 +535,32 @@ __global__ void __launch_bounds__(256) helm_build_ops(int p, int K, double k, co
       er = tt;
     }
     if (m < 0) ei = -ei;
-    sph_j(n, k * r, rad);
-    double rr = rad[n], ri = 0.0;
-    if (op.src_out) {
-      sph_y(n, k * r, rad2);
-      ri = rad2[n];
+    double rr, ri = 0.0;
+    if (yuk) {  // k_n outgoing, i_n regular
+      if (op.src_out) sph_k(n, k * r, rad);
+      else sph_i(n, k * r, rad);
+      rr = rad[n];
+    } else {  // h_n = j_n + i y_n outgoing, j_n regular
+      sph_j(n, k * r, rad);
+      rr = rad[n];
+      if (op.src_out) {
+        sph_y(n, k * r, rad2);
+        ri = rad2[n];
+      }
     }
     // (rr + i ri) yb (er + i ei)
     f[t] = make_double2(yb * (rr * er - ri * ei), yb * (rr * ei + ri * er));
   }
   if (threadIdx.x == 0) {
-    sph_j(p, k * op.rad, rad);
-    if (op.tgt_out) sph_y(p, k * op.rad, rad2);
-    for (int l = 0; l <= p; l++) rt[l] = make_double2(rad[l], op.tgt_out ? rad2[l] : 0.0);
+    if (yuk) {
+      if (op.tgt_out) sph_k(p, k * op.rad, rad);
+      else sph_i(p, k * op.rad, rad);
+      for (int l = 0; l <= p; l++) rt[l] = make_double2(rad[l], 0.0);
+    } else {
+      sph_j(p, k * op.rad, rad);
+      if (op.tgt_out) sph_y(p, k * op.rad, rad2);
+      for (int l = 0; l <= p; l++) rt[l] = make_double2(rad[l], op.tgt_out ? rad2[l] : 0.0);
+    }
   }
   __syncthreads();
   // 2. azimuthal transform
@@ -522,6 +612,23 @@ __global__ void helm_gather(int n, int nrhs, const int* __restrict__ perm, const
   qs[t] = q[(size_t)r * n + perm[i]];
 }
 
+__global__ void helm_gather_real(int n, int nrhs, const int* __restrict__ perm, const float* __restrict__ q,
+                                 float2* __restrict__ qs) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)n * nrhs) return;
+  const int r = (int)(t / n), i = (int)(t % n);
+  qs[t] = make_float2(q[(size_t)r * n + perm[i]], 0.f);
+}
+
+// real part of near + far, scaled, to caller order (Yukawa)
+template <typename T>
+__global__ void helm_finalize_real(int n, const int* __restrict__ perm, const double2* __restrict__ near,
+                                   const double2* __restrict__ far, double scale, T* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[perm[i]] = (T)(scale * (near[i].x + (far ? far[i].x : 0.0)));
+}
+
 template <typename T>
 __global__ void helm_finalize(int n, const int* __restrict__ perm, const double2* __restrict__ near,
                               const double2* __restrict__ far, T* __restrict__ out) {
@@ -543,41 +650,67 @@ void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float*
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_helm_p2p(bool f32, float k, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
-                     const int* list, const float4* tpos, const float4* spos, const float* qs, double* pot,
-                     cudaStream_t st) {
+void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, int nwork, const int2* work,
+                     const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos, const float4* spos,
+                     const float* qs, double* pot, cudaStream_t st) {
   if (nwork <= 0) return;
-  if (f32)
-    helm_p2p<true><<<nwork, 128, 0, st>>>(k, work, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs,
-                                          (double2*)pot);
+  const float2* q2 = (const float2*)qs;
+  double2* p2 = (double2*)pot;
+  const int ex = excl ? 1 : 0;
+  if (f32 && !yuk)
+    helm_p2p<true, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+  else if (f32)
+    helm_p2p<true, true><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+  else if (!yuk)
+    helm_p2p<false, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   else
-    helm_p2p<false><<<nwork, 128, 0, st>>>(k, work, leaf_i, leaf_j, list, tpos, spos, (const float2*)qs,
-                                           (double2*)pot);
+    helm_p2p<false, true><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_helm_p2m(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* spos, const float* qs,
-                     const float* bbox, double w, double* M, cudaStream_t st) {
+void launch_helm_gather_real(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st) {
+  if (n <= 0) return;
+  helm_gather_real<<<nb((size_t)n * nrhs, 256), 256, 0, st>>>(n, nrhs, perm, q, (float2*)qs);
+  FMMB_CHECK_LAUNCH();
+}
+
+template <typename T>
+void launch_helm_finalize_real(int n, const int* perm, const double* near, const double* far, double scale, T* out,
+                               cudaStream_t st) {
+  if (n <= 0) return;
+  helm_finalize_real<T><<<nb(n, 256), 256, 0, st>>>(n, perm, (const double2*)near, (const double2*)far, scale, out);
+  FMMB_CHECK_LAUNCH();
+}
+template void launch_helm_finalize_real<float>(int, const int*, const double*, const double*, double, float*,
+                                               cudaStream_t);
+template void launch_helm_finalize_real<double>(int, const int*, const double*, const double*, double, double*,
+                                                cudaStream_t);
+
+void launch_helm_p2m(int nleaf, int p, double k, bool yuk, const int* keys, const int2* leaf, const float4* spos,
+                     const float* qs, const float* bbox, double w, double* M, cudaStream_t st) {
   if (nleaf <= 0) return;
   const int K = (p + 1) * (p + 1);
   const Corner c{bbox[0], bbox[1], bbox[2]};  // host array
-  helm_p2m<<<nleaf, 128, 2 * K * sizeof(double), st>>>(p, K, k, keys, leaf, spos, (const float2*)qs, c, w, M);
+  helm_p2m<<<nleaf, 128, 2 * K * sizeof(double), st>>>(p, K, k, yuk ? 1 : 0, keys, leaf, spos, (const float2*)qs, c,
+                                                        w, M);
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_helm_l2p(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* tpos,
+void launch_helm_l2p(int nleaf, int p, double k, bool yuk, const int* keys, const int2* leaf, const float4* tpos,
                      const float* bbox, double w, const double* L, double* pot, cudaStream_t st) {
   if (nleaf <= 0) return;
   const int K = (p + 1) * (p + 1);
   const Corner c{bbox[0], bbox[1], bbox[2]};  // host array
-  helm_l2p<<<nleaf, 128, 2 * K * sizeof(double), st>>>(p, K, k, keys, leaf, tpos, c, w, L, (double2*)pot);
+  helm_l2p<<<nleaf, 128, 2 * K * sizeof(double), st>>>(p, K, k, yuk ? 1 : 0, keys, leaf, tpos, c, w, L,
+                                                        (double2*)pot);
   FMMB_CHECK_LAUNCH();
 }
 
 void launch_helm_direct(int i0, int i1, const int* inv_i, const float4* tpos, int nj, const float4* spos,
-                        const float* qs, double k, double* out, cudaStream_t st) {
+                        const float* qs, double k, bool yuk, double eps2, bool excl, double* out, cudaStream_t st) {
   if (i1 <= i0) return;
-  helm_direct<<<nb(i1 - i0, 128), 128, 0, st>>>(i0, i1, inv_i, tpos, nj, spos, (const float2*)qs, k, (double2*)out);
+  helm_direct<<<nb(i1 - i0, 128), 128, 0, st>>>(i0, i1, inv_i, tpos, nj, spos, (const float2*)qs, k, yuk ? 1 : 0,
+                                                eps2, excl ? 1 : 0, (double2*)out);
   FMMB_CHECK_LAUNCH();
 }
 
@@ -595,8 +728,8 @@ size_t helm_build_smem(int p) {
   return ((size_t)NQ * NP + (size_t)NQ * (2 * p + 1) + (p + 1)) * sizeof(double2);
 }
 
-void launch_helm_build_ops(int p, double k, int nops, const HelmOp* ops, const double* gl_x, const double* gl_w,
-                           const double* ybar_q, double* opT, cudaStream_t st) {
+void launch_helm_build_ops(int p, double k, bool yuk, int nops, const HelmOp* ops, const double* gl_x,
+                           const double* gl_w, const double* ybar_q, double* opT, cudaStream_t st) {
   if (nops <= 0) return;
   const int K = (p + 1) * (p + 1), NQ = 2 * p + 8, NP = 2 * NQ;
   const size_t smem = helm_build_smem(p);
@@ -604,8 +737,8 @@ void launch_helm_build_ops(int p, double k, int nops, const HelmOp* ops, const d
   const size_t ostride = (size_t)4 * K * K;
   for (int o0 = 0; o0 < nops; o0 += 65535) {
     dim3 grid(K, std::min(65535, nops - o0));
-    helm_build_ops<<<grid, 256, smem, st>>>(p, K, k, ops + o0, NQ, NP, gl_x, gl_w, ybar_q, opT + (size_t)o0 * ostride,
-                                            ostride);
+    helm_build_ops<<<grid, 256, smem, st>>>(p, K, k, yuk ? 1 : 0, ops + o0, NQ, NP, gl_x, gl_w, ybar_q,
+                                            opT + (size_t)o0 * ostride, ostride);
     FMMB_CHECK_LAUNCH();
   }
 }

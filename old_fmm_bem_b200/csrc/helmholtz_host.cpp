@@ -124,7 +124,9 @@ void helm_setup(fmmb_plan* pl) {
     o[1] = ((oct & 1) - 0.5) * wc;         // key bit 0: y
     o[2] = (((oct >> 2) & 1) - 0.5) * wc;  // key bit 2: z
   };
-  const double rad_cap = 2.5 / k;  // keeps k * rad below the first zero of j_0
+  const bool yuk = pl->cfg.kernel == FMMB_YUKAWA;
+  // Helmholtz: keeps k * rad below the first zero of j_0 (i_n of Yukawa has no zeros)
+  const double rad_cap = yuk ? 1e300 : 2.5 / k;
   pl->hop_m2m0 = 0;
   for (int lc = 3; lc <= lmax; lc++)
     for (int oct = 0; oct < 8; oct++) {
@@ -162,7 +164,7 @@ void helm_setup(fmmb_plan* pl) {
     upload_vec(d_gw, gw);
     upload_vec(d_yb, yb);
     upload_vec(d_ops, ops);
-    launch_helm_build_ops(p, k, nops, d_ops.get(), d_gx.get(), d_gw.get(), d_yb.get(), pl->d_hops.get(), s);
+    launch_helm_build_ops(p, k, yuk, nops, d_ops.get(), d_gx.get(), d_gw.get(), d_yb.get(), pl->d_hops.get(), s);
     FMMB_CUDA(cudaStreamSynchronize(s));
   }
   // pair jobs (rows are indices into the all-level M / L arrays)

@@ -239,8 +239,10 @@ struct fmmb_plan {
 };
 
 namespace fmmb {
-// complex Helmholtz operators, pair jobs and buffers (helmholtz_host.cpp)
+// complex Helmholtz and Yukawa operators, pair jobs and buffers (helmholtz_host.cpp)
 void helm_setup(fmmb_plan* pl);
+// the kernels of the Helmholtz machinery (complex expansions, dense operators)
+inline bool helm_family(int kernel) { return kernel == FMMB_HELMHOLTZ_G || kernel == FMMB_YUKAWA; }
 void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const float* tz, const float* tnx,
                 const float* tny, const float* tnz, int nj, const float* sx, const float* sy, const float* sz,
                 const float* snx, const float* sny, const float* snz, const float* bbox_in);

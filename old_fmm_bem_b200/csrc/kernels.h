@@ -121,20 +121,25 @@ struct HelmOp {          // one translation operator to build
   int src_out, tgt_out;  // 1: outgoing (h_n) basis, 0: regular (j_n) basis
 };
 void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
-// work: (target leaf, first target) per item of up to 256 targets
-void launch_helm_p2p(bool f32, float k, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
-                     const int* list, const float4* tpos, const float4* spos, const float* qs, double* pot,
-                     cudaStream_t st);
+// work: (target leaf, first target) per item of up to 256 targets; yuk: the
+// Yukawa kernel (real e^{-k r}/(4 pi r), complex charges with zero imaginary parts)
+void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, int nwork, const int2* work,
+                     const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos, const float4* spos,
+                     const float* qs, double* pot, cudaStream_t st);
+void launch_helm_gather_real(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
+template <typename T>
+void launch_helm_finalize_real(int n, const int* perm, const double* near, const double* far, double scale, T* out,
+                               cudaStream_t st);
 // bbox: the plan's host copy {xmin, ymin, zmin, rd}
-void launch_helm_p2m(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* spos, const float* qs,
-                     const float* bbox, double w, double* M, cudaStream_t st);
-void launch_helm_l2p(int nleaf, int p, double k, const int* keys, const int2* leaf, const float4* tpos,
+void launch_helm_p2m(int nleaf, int p, double k, bool yuk, const int* keys, const int2* leaf, const float4* spos,
+                     const float* qs, const float* bbox, double w, double* M, cudaStream_t st);
+void launch_helm_l2p(int nleaf, int p, double k, bool yuk, const int* keys, const int2* leaf, const float4* tpos,
                      const float* bbox, double w, const double* L, double* pot, cudaStream_t st);
 void launch_helm_direct(int i0, int i1, const int* inv_i, const float4* tpos, int nj, const float4* spos,
-                        const float* qs, double k, double* out, cudaStream_t st);
+                        const float* qs, double k, bool yuk, double eps2, bool excl, double* out, cudaStream_t st);
 template <typename T>
 void launch_helm_finalize(int n, const int* perm, const double* near, const double* far, T* out, cudaStream_t st);
 // operators in the real 2K x 2K form, transposed ([op][column][row], row stride 2K)
-void launch_helm_build_ops(int p, double k, int nops, const HelmOp* ops, const double* gl_x, const double* gl_w,
-                           const double* ybar_q, double* opT, cudaStream_t st);
+void launch_helm_build_ops(int p, double k, bool yuk, int nops, const HelmOp* ops, const double* gl_x,
+                           const double* gl_w, const double* ybar_q, double* opT, cudaStream_t st);
 }  // namespace fmmb

@@ -175,6 +175,21 @@ def ref_fmm(t, s, q, *, neq=0, p=8, lmax=3, bbox=(0.0, 0.0, 0.0, 1.0), tn=None, 
     return v, (g if neq == 0 else None)
 
 
+def ref_direct(t, s, q, *, neq=0, p=8, lam=0.0, tn=None, sn=None):
+    """The reference's own direct sums (kernel/G_dir.cxx, Gni_dir.cxx,
+    Gnj_dir.cxx, Helmholtz_G_dir.cxx for neq 10 with screening lam), float32
+    outputs in caller order: (pot, grad or None)."""
+    lib = ref_lib(p)
+    t, tn, s, sn, q = _unpack(t, tn, s, sn, q)
+    ni, nj = t.shape[1], s.shape[1]
+    v = np.zeros(ni, np.float32)
+    g = np.zeros((3, ni), np.float32)
+    lib.ref_direct(ni, nj, neq, lam, _f(t[0]), _f(t[1]), _f(t[2]), _f(tn[0]), _f(tn[1]), _f(tn[2]),
+                   _f(s[0]), _f(s[1]), _f(s[2]), _f(sn[0]), _f(sn[1]), _f(sn[2]), _f(q),
+                   v.ctypes.data_as(_fp), g[0].ctypes.data_as(_fp), g[1].ctypes.data_as(_fp), g[2].ctypes.data_as(_fp))
+    return v, (g if neq == 0 else None)
+
+
 def ref_records(p):
     lib = ref_lib(p)
     out = {}

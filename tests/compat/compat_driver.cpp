@@ -1,9 +1,10 @@
 // Test driver for old_fmm_bem_b200/compat/fmm_compat.cpp, shaped like the
 // reference's test/test.cxx: it owns the global particle arrays, calls the
 // reference entry points fmm(ni, nj, neq) and G_dir/Gni_dir/Gnj_dir, and
-// writes the outputs.  Usage: compat_driver <dir> <n> <lmax> <p>
+// writes the outputs.  Usage: compat_driver <dir> <n> <lmax> <p> [lambda]
 //   reads  <dir>/in.bin  = t(3n) tn(3n) s(3n) sn(3n) q(n) float32
-//   writes <dir>/out.bin = v0(n) g0(3n) v1(n) v2(n) d0(n) d1(n) d2(n) float32
+//   writes <dir>/out.bin = v0(n) g0(3n) v1(n) v2(n) d0(n) d1(n) d2(n)
+//                          [v10(n) d10(n) with lambda: fmm(n, n, 10), Helmholtz_G_dir] float32
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -13,11 +14,13 @@ float *xi, *yi, *zi, *gxi, *gyi, *gzi, *vi;
 float *xj, *yj, *zj, *gxj, *gyj, *gzj, *vj;
 int lmax;
 float xmin, ymin, zmin, rd;
+double lambda;
 
 void fmm(int, int, int);
 void G_dir(int, int, int, int);
 void Gni_dir(int, int, int, int);
 void Gnj_dir(int, int, int, int);
+void Helmholtz_G_dir(int, int, int, int);
 extern "C" void fmmb_compat_set_order(int);
 
 int main(int argc, char** argv) {
@@ -70,6 +73,15 @@ int main(int argc, char** argv) {
   load(false);
   Gnj_dir(0, n - 1, 0, n - 1);
   out.insert(out.end(), vi, vi + n);
+  if (argc > 5) {  // Yukawa
+    lambda = std::atof(argv[5]);
+    load(false);
+    fmm(n, n, 10);
+    out.insert(out.end(), vi, vi + n);
+    load(false);
+    Helmholtz_G_dir(0, n - 1, 0, n - 1);
+    out.insert(out.end(), vi, vi + n);
+  }
   f = std::fopen((dir + "/out.bin").c_str(), "wb");
   if (!f) return 4;
   std::fwrite(out.data(), sizeof(float), out.size(), f);

@@ -78,3 +78,28 @@ def test_reference_gpu_variant_through_p2pgpu(neq, oracle):
     assert rel(gpu[0], cpu[0].astype(np.float64)) < 1e-6
     if neq == 0:
         assert rel(gpu[1], cpu[1].astype(np.float64)) < 1e-6
+
+
+@pytest.mark.gpu
+def test_yukawa_entry_points(driver, tmp_path, oracle):
+    """fmm(n, n, 10) and Helmholtz_G_dir through the compatibility shim against
+    the reference's own Yukawa direct sum (kernel/Helmholtz_G_dir.cxx, eps =
+    1e-6 on r^2, self pairs included; built from its sources).  The
+    reference's Yukawa FMM itself crashes in this container (the
+    kernel/multipoleh.cxx:10 overflow), so the direct sum is the reference
+    output compared against: the shim's direct sum to 1e-6 (float outputs),
+    its FMM at p = 12 to 1e-5 (truncation; the far field has no eps)."""
+    if not oracle.ref_available(8):
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(77)
+    n, lam = 6000, 3.0
+    t = rng.random((3, n), dtype=np.float32)
+    q = rng.uniform(-1, 1, n).astype(np.float32)
+    z = np.zeros((3, n), np.float32)
+    np.concatenate([t.ravel(), z.ravel(), t.ravel(), z.ravel(), q]).tofile(tmp_path / "in.bin")
+    subprocess.run([driver, str(tmp_path), str(n), "3", "12", str(lam)], check=True)
+    out = np.fromfile(tmp_path / "out.bin", np.float32)
+    v10, d10 = out[9 * n:10 * n], out[10 * n:11 * n]
+    ref, _ = oracle.ref_direct(t, t, q, neq=10, lam=lam)
+    assert rel(d10, ref.astype(np.float64)) < 1e-6
+    assert rel(v10, ref.astype(np.float64)) < 1e-5

@@ -117,3 +117,30 @@ def test_transpose_and_forest(ob):
     pf.close()
     assert rel(v[:6000], ho.direct(xt, xt, q[:6000], 5.0)) < 1e-6
     assert rel(v[6000:], ho.direct(xs, xs, q[6000:], 5.0)) < 1e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_yukawa_fmm_vs_direct(precision, ob):
+    """FMMB_YUKAWA (the reference's neq 10 kernel, (pi/2) e^{-l r}/(l r)) in
+    accurate semantics: GPU direct sum = numpy to 1e-12; FMM at p = 14 within
+    1e-6 (FP64) / 2e-6 (mixed), the error shrinking from p = 6 to 10 to 14."""
+    from oracle import helmholtz_oracle as ho
+    rng = np.random.default_rng(31)
+    x = rng.random((3, 20000), dtype=np.float32)
+    q = rng.uniform(-1, 1, 20000).astype(np.float32)
+    lam = 4.0
+    ref = ho.yukawa_direct(x[:, :1500], x, q, lam)
+    errs = {}
+    for p in (6, 10, 14):
+        pl = ob.Plan(kernel=ob.YUKAWA, p=p, lmax=4, precision=precision, semantics=1, exclude_self=True,
+                     wavenumber=lam)
+        pl.set_geometry(x, x, bbox=(0, 0, 0, 1))
+        v, g = pl.evaluate(q, f64=True)
+        assert g is None
+        if p == 14:
+            d, _ = pl.direct(q, 0, 1500)
+            assert rel(d, ref) < 1e-12
+        pl.close()
+        errs[p] = rel(v[:1500], ref)
+    assert errs[14] < (1e-6 if precision == 0 else 2e-6), errs
+    assert errs[6] > errs[10] > errs[14], errs
