@@ -34,9 +34,11 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
                                                 const float* __restrict__ qs, int nj, float eps2, int excl, double coef,
                                                 double* __restrict__ pot, double* __restrict__ grad, int ni) {
   constexpr int NC = KER == FMMB_LAPLACE_G ? 4 : 1;  // accumulated components per right-hand side
+  constexpr int RV = R % 4 == 0 ? R / 4 : 0;          // charges of a source as float4 vectors (R = 4, 8)
   __shared__ float4 sx[kT];
   __shared__ float4 sn[KER == FMMB_LAPLACE_GNJ ? kT : 1];
-  __shared__ float sq[R][kT];
+  __shared__ float4 sq4[RV > 0 ? kT : 1][RV > 0 ? RV : 1];
+  __shared__ float sq[RV > 0 ? 1 : R][kT];
   const int2 wk = work[blockIdx.x];
   const int b = wk.x;
   const int2 li = leaf_i[b];
@@ -59,8 +61,15 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
         const int j = lj.x + c0 + threadIdx.x;
         sx[threadIdx.x] = spos[j];
         if (KER == FMMB_LAPLACE_GNJ) sn[threadIdx.x] = snrm[j];
+        if (RV > 0) {
 #pragma unroll
-        for (int r = 0; r < R; r++) sq[r][threadIdx.x] = qs[(size_t)r * nj + j];
+          for (int v = 0; v < (RV > 0 ? RV : 1); v++)
+            sq4[threadIdx.x][v] = make_float4(qs[(size_t)(4 * v) * nj + j], qs[(size_t)(4 * v + 1) * nj + j],
+                                              qs[(size_t)(4 * v + 2) * nj + j], qs[(size_t)(4 * v + 3) * nj + j]);
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; r++) sq[r][threadIdx.x] = qs[(size_t)r * nj + j];
+        }
       }
       __syncthreads();
       if (!on) continue;
@@ -72,6 +81,20 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
         for (int c = 0; c < NC; c++) A[r][c] = 0.f;
 #pragma unroll 2
       for (int jj = 0; jj < nc; jj++) {
+        float qv[R];  // the source's charges, vector loads when R is a multiple of 4
+        if (RV > 0) {
+#pragma unroll
+          for (int v = 0; v < (RV > 0 ? RV : 1); v++) {
+            const float4 t4 = sq4[jj][v];
+            qv[4 * v] = t4.x;
+            qv[4 * v + 1] = t4.y;
+            qv[4 * v + 2] = t4.z;
+            qv[4 * v + 3] = t4.w;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; r++) qv[r] = sq[r][jj];
+        }
         const float4 xj = sx[jj];
         const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
@@ -81,7 +104,7 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
           const float r3 = rinv * rinv * rinv;
 #pragma unroll
           for (int r = 0; r < R; r++) {
-            const float q = sq[r][jj];
+            const float q = qv[r];
             const float qr3 = q * r3;
             A[r][0] = fmaf(q, rinv, A[r][0]);
             A[r][1] = fmaf(dx, qr3, A[r][1]);
@@ -97,7 +120,7 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
             kv = fmaf(dx, nj4.x, fmaf(dy, nj4.y, dz * nj4.z)) * (rinv * rinv * rinv);
           }
 #pragma unroll
-          for (int r = 0; r < R; r++) A[r][0] = fmaf(sq[r][jj], kv, A[r][0]);
+          for (int r = 0; r < R; r++) A[r][0] = fmaf(qv[r], kv, A[r][0]);
         }
       }
 #pragma unroll
