@@ -300,6 +300,12 @@ FMMB_API int fmmb_get_expansions(fmmb_plan* plan, int which, double* out);
  * [3] M2L, [4] L2L, [5] L2P, [6] whole evaluate (P2P overlaps the far field). */
 FMMB_API int fmmb_get_timings(fmmb_plan* plan, float* ms7);
 
+/* Overlap of the near field with the far field (default on).  With on = 0
+ * the near field runs on the plan's stream between the far-field phases, so
+ * that fmmb_get_timings gives each phase's time with the GPU to itself (the
+ * results are the same).  Captured evaluates are rebuilt. */
+FMMB_API int fmmb_set_overlap(fmmb_plan* plan, int on);
+
 /* Counts of the current geometry: [0] ni, [1] nj, [2] target leaves,
  * [3] source leaves, [4] P2P pairs (sum over near-field leaf pairs of
  * ni*nj), [5] M2L box pairs, [6] lmax, [7] kernel launches of the last

@@ -36,7 +36,7 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
            "fmmb_gmres", "fmmb_autotune_lmax_batch", "fmmb_gpu_p2p",
-           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times"]
+           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times", "fmmb_set_overlap"]
 
 
 def lib_path() -> str:
@@ -104,6 +104,7 @@ def load():
     lib.fmmb_get_timings.argtypes = [_vp, _vp]
     lib.fmmb_get_stats.argtypes = [_vp, _vp]
     lib.fmmb_get_setup_times.argtypes = [_vp, _vp]
+    lib.fmmb_set_overlap.argtypes = [_vp, ctypes.c_int]
     lib.fmmb_last_error.restype = ctypes.c_char_p
     _LIB = lib
     return lib
@@ -362,6 +363,12 @@ class Plan:
         ms = np.zeros(7, np.float32)
         _check(load().fmmb_get_timings(self._h, ms.ctypes.data))
         return dict(zip(["p2p", "p2m", "m2m", "m2l", "l2l", "l2p", "total"], ms.tolist()))
+
+    def set_overlap(self, on: bool):
+        """Overlap the near field with the far field (default).  Off: the
+        phases run one after another, so timings() gives each phase's time
+        with the GPU to itself; the results do not change."""
+        _check(load().fmmb_set_overlap(self._h, 1 if on else 0))
 
     def setup_times(self):
         """(tree build ms, whole fmmb_set_geometry ms) of the current geometry."""

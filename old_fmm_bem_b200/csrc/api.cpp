@@ -640,7 +640,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   const int K = pl->K, p = pl->p, lmax = pl->lmax;
   const double k = pl->cfg.wavenumber;
   const bool yuk = pl->cfg.kernel == FMMB_YUKAWA;
-  cudaStream_t m = pl->st.main, side = pl->st.side;
+  cudaStream_t m = pl->st.main, side = pl->serial ? m : pl->st.side;
   double* pot_near = pl->pot_s.get();
   double* pot_far = pl->pot_s.get() + 2 * (size_t)pl->ni;
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
@@ -708,7 +708,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   }
   const int K = pl->K, p = pl->p, lmax = pl->lmax, ker = pl->cfg.kernel;
   const Sem s = make_sem(pl);
-  cudaStream_t m = pl->st.main, side = pl->st.side;
+  cudaStream_t m = pl->st.main, side = pl->serial ? m : pl->st.side;
   double* pot_near = pl->pot_s.get();
   double* pot_far = pl->pot_s.get() + pl->ni;
   double* g_near = want_grad ? pl->grad_s.get() : nullptr;
@@ -990,14 +990,15 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     if (multi) {
       pl->near_all.alloc((size_t)nr * ni * (want_grad ? 4 : 1));
       pl->qs_far.alloc(nj);
+      cudaStream_t ns = pl->serial ? m : pl->st.side;
       FMMB_CUDA(cudaEventRecord(pl->st.fork, m));
-      FMMB_CUDA(cudaStreamWaitEvent(pl->st.side, pl->st.fork, 0));
+      FMMB_CUDA(cudaStreamWaitEvent(ns, pl->st.fork, 0));
       pl->launches += launch_p2p_multi(pl->cfg.kernel, nr, pl->m_p2p_nwork, pl->m_p2p_work.get(), pl->leaf_i.get(),
                                        pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->tnrm.get(),
                                        pl->spos.get(), pl->snrm.get(), pl->qs.get(), nj, make_sem(pl),
                                        pl->near_all.get(), want_grad ? pl->near_all.get() + (size_t)nr * ni : nullptr,
-                                       ni, pl->st.side);
-      FMMB_CUDA(cudaEventRecord(pl->st.near_done, pl->st.side));
+                                       ni, ns);
+      FMMB_CUDA(cudaEventRecord(pl->st.near_done, ns));
     }
     for (int r = 0; r < nr; r++) {
       if (multi) {
@@ -1466,6 +1467,21 @@ int fmmb_get_timings(fmmb_plan* pl, float* ms) {
     float tot = 0;
     FMMB_CUDA(cudaEventElapsedTime(&tot, pl->ev[7], pl->ev[6]));
     ms[6] = tot;
+  });
+}
+
+int fmmb_set_overlap(fmmb_plan* pl, int on) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl, FMMB_ERR_ARG, "null plan");
+    if (pl->serial == (on == 0)) return;
+    for (int w = 0; w < 4; w++) {  // captured with the other stream layout
+      if (pl->gexec[w]) {
+        FMMB_CUDA(cudaStreamSynchronize(pl->st.main));
+        cudaGraphExecDestroy(pl->gexec[w]);
+        pl->gexec[w] = nullptr;
+      }
+    }
+    pl->serial = on == 0;
   });
 }
 

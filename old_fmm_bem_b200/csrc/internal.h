@@ -189,6 +189,7 @@ struct fmmb_plan {
   // [nrhs][3][ni] gradients), the far field per right-hand side through the
   // far-field-only graph, whose charges are qs_far
   bool far_only = false;
+  bool serial = false;  // near field on the main stream (fmmb_set_overlap(0))
   fmmb::DevBuf<double> near_all;
   fmmb::DevBuf<float> qs_far;
   fmmb::DevBuf<int2> m_p2p_work;  // (target leaf, first target), up to 128 targets each

@@ -688,7 +688,10 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
 int pairs_f64_tile(int K, int npair, int nsm) {
   int tp = 32;
   while (tp > 8 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
-  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
+  // staged inputs: 48 KB, or up to 200 KB for operators too large to stage
+  // (K > 160: the operator streams from L2 and more pairs per tile reuse it)
+  const size_t cap = (size_t)K * ((K + 1) & ~1) * sizeof(double) > 160 * 1024 ? 200 * 1024 : 48 * 1024;
+  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > cap) tp /= 2;
   return tp;
 }
 
@@ -712,7 +715,7 @@ void prepare_tp() {
   FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPairsSmemMax));
   FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 48 * 1024));
+                                 (int)kPairsSmemMax));
 }
 }  // namespace
 

@@ -3,22 +3,35 @@
 // Same sums as the reference's P2P kernels (kernel/G_p2p.cxx:12-37,
 // kernel/Gni_p2p.cxx:12-28, kernel/Gnj_p2p.cxx:12-28) over the 27-slot
 // neighbour lists of the GPU tree.  Pair arithmetic is FP32 (hardware rsqrt);
-// each thread sums 32 sources at a time in FP32 and promotes every partial sum
-// into FP64 accumulators, so the accumulated rounding stays at the FP32 level
-// of one 32-term sum whatever the number of sources.
+// each lane sums up to 32 sources at a time in FP32 and promotes every
+// partial sum into FP64 accumulators, so the accumulated rounding stays at the
+// FP32 level of one 32-term sum whatever the number of sources.
 //
 // Layout: one block of 4 warps per target leaf.  The sources of all
-// neighbour leaves are staged once into shared memory as one list -- the
-// leaf's own source leaf first, padded to a multiple of 32 with far,
-// zero-charge points, then the other neighbours, padded likewise -- so that
-// every run of 32 sources needs no bounds check, and only runs of the own leaf
-// test for coincident points (points at zero distance share a leaf).  A pass
-// covers NT columns of 32 targets (NT = 1..4, as many as the leaf needs, so
-// a leaf of 53 targets fills 83% of its lanes); each lane holds the NT
-// targets of its column position, so one shared-memory read of a source
-// serves NT pairs; warp w takes runs w, w+4, ... and the four warps' FP64
-// partial sums are added through shared memory at the end of a pass.
+// neighbour leaves are staged into shared memory as one list -- the leaf's
+// own source leaf first, padded to a multiple of 32 with far, zero-charge
+// points, then the other neighbours, padded likewise -- so that no run of 32
+// sources needs a bounds check, and only the own leaf's runs test for
+// coincident points (points at zero distance share a leaf).  Warp 0 builds
+// the segment list with one lane per neighbour slot (ballot + scan), and the
+// staging issues four sources' loads per thread before storing any.
+//
+// A warp is 8 target lanes x 4 source streams: lane (g, s) = (lane % 8,
+// lane / 8) holds target g of each of its NT groups of 8 targets and takes
+// source pairs s, s + 4, s + 8, s + 12 of a run of 32 sources, so one
+// shared-memory read (four consecutive pairs per warp, one bank wavefront)
+// serves 2 NT pairs and a leaf occupies its lanes in steps of 8 targets
+// rather than 32 (leaves of a surface hold tens of points).  The pair
+// arithmetic uses the two-lane FP32 instructions (add / mul / fma .f32x2) on
+// the two sources of a pair: half the FP32 instructions of the scalar form,
+// the same values.  The warps form teams that share a tile of up
+// to 4 groups and split its runs: 1 team of 4 warps for leaves of up to 4
+// groups, 2 teams of 2 for up to 8, else 4 one-warp teams (with more rounds of
+// tiles for big leaves).  The 4 streams' FP64 sums of a target are added by
+// two shuffles, the warps of a team through shared memory.
 #include <cuda_runtime.h>
+
+#include <climits>
 
 #include "internal.h"
 #include "kernels.h"
@@ -28,10 +41,12 @@ namespace {
 
 constexpr int kThreads = 128;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxNT = 4;     // target columns of 32 per pass
-constexpr int kCap = 1024;    // staged sources per chunk (multiple of 32)
-constexpr int kSelfSlot = 13; // offset (0, 0, 0) in the 27-slot list
-constexpr float kFar = 1e18f; // padding sources: r^2 ~ 3e36 stays finite in FP32
+constexpr int kG = 8;          // targets of a group (lanes g = lane % 8)
+constexpr int kS = 32 / kG;    // source streams of a warp (s = lane / 8)
+constexpr int kMaxNT = 4;      // groups of a tile
+constexpr int kCap = 1024;     // staged sources per chunk (multiple of 32 * 4)
+constexpr int kSelfSlot = 13;  // offset (0, 0, 0) in the 27-slot list
+constexpr float kFar = 1e18f;  // padding sources: r^2 ~ 3e36 stays finite in FP32
 
 __device__ __forceinline__ int pad32(int n) { return (n + 31) & ~31; }
 
@@ -50,157 +65,173 @@ struct Acc {
   float p, fx, fy, fz;
 };
 
-// One run of 32 staged sources against the thread's NT targets.
-template <int KER, bool EXCL, int NT>
-__device__ __forceinline__ void run32(const float4* __restrict__ sp, const float4* __restrict__ sm, const float4* xt,
-                                      const float4* nt, float eps2, Acc<KER>* acc) {
-#pragma unroll 4
-  for (int k = 0; k < 32; k++) {
-    const float4 xj = sp[k];
-    float4 mj = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (KER == FMMB_LAPLACE_GNJ) mj = sm[k];
-#pragma unroll
-    for (int t = 0; t < NT; t++) {
-      const float4 xi = xt[t];
-      Acc<KER>& c = acc[t];
-      const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-      const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-      float rinv = rsqrt_ftz(r2);
-      if (EXCL) rinv = (r2 > 0.f) ? rinv : 0.f;
-      if (KER == FMMB_LAPLACE_G) {
-        const float qr = xj.w * rinv;
-        const float qr3 = qr * rinv * rinv;
-        c.p += qr;
-        c.fx = fmaf(dx, qr3, c.fx);
-        c.fy = fmaf(dy, qr3, c.fy);
-        c.fz = fmaf(dz, qr3, c.fz);
-      } else if (KER == FMMB_LAPLACE_GNI) {
-        const float4 nv = nt[t];
-        const float qr3 = xj.w * rinv * rinv * rinv;
-        c.p = fmaf(fmaf(dx, nv.x, fmaf(dy, nv.y, dz * nv.z)), qr3, c.p);
-      } else {
-        const float r3 = rinv * rinv * rinv;
-        c.p = fmaf(fmaf(dx, mj.x, fmaf(dy, mj.y, dz * mj.z)), r3, c.p);
-      }
-    }
-  }
+template <int KER>
+constexpr int ncomp() {
+  return KER == FMMB_LAPLACE_G ? 4 : 1;  // accumulated components
 }
 
-// Shared state of one block (one target leaf).
+// Negated positions of sources j, j + 1 (even j) of the staged list, packed
+// for the two-lane FP32 instructions: (-x_j, -x_j+1, -y_j, -y_j+1) and
+// (-z_j, -z_j+1); charges (q_j, q_j+1) (G, Gni) or q n (Gnj).  Pair values
+// are bit-identical to the scalar forms (x_i + (-x_j) = x_i - x_j, the same
+// operation order after it); each lane keeps two FP32 partial sums, over the
+// even and the odd sources.
 template <int KER>
 struct Smem {
-  static constexpr int NC = KER == FMMB_LAPLACE_G ? 4 : 1;  // accumulated components
-  float4 sp[kCap];                                          // x, y, z, q (Gnj: q unused)
-  float4 sm[KER == FMMB_LAPLACE_GNJ ? kCap : 1];            // q * n_j (Gnj)
-  double red[kWarps - 1][NC][kMaxNT * 32];
-  int2 seg[kP2PSlots];                                      // (first source, count), own leaf first
-  int nseg;
+  static constexpr int NC = ncomp<KER>();
+  static constexpr int NP = kCap / 2;
+  float4 A[NP];
+  float2 B[NP];
+  float2 Q[KER == FMMB_LAPLACE_GNJ ? 1 : NP];
+  float4 M[KER == FMMB_LAPLACE_GNJ ? NP : 1];   // (qn_x j, j+1, qn_y j, j+1)
+  float2 MZ[KER == FMMB_LAPLACE_GNJ ? NP : 1];  // (qn_z j, j+1)
+  double red[kWarps][kMaxNT][NC][kG];           // team partial sums
+  int2 seg[32];                                 // (first source, count), own leaf first
+  int vst[32];                                  // virtual start of each segment, then INT_MAX
 };
 
-// Stages virtual sources [c0, c1): far zero-charge points, then every
-// segment's part of the chunk.
-template <int KER>
-__device__ void stage(Smem<KER>& S, int c0, int c1, int self_end, const float4* __restrict__ spos,
-                      const float4* __restrict__ snrm, const float* __restrict__ qs) {
-  __syncthreads();
-  for (int e = threadIdx.x; e < c1 - c0; e += kThreads) {
-    S.sp[e] = make_float4(kFar, kFar, kFar, 0.f);
-    if (KER == FMMB_LAPLACE_GNJ) S.sm[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  __syncthreads();
-  int v0 = 0;  // virtual start of the segment
-  for (int s = 0; s < S.nseg; s++) {
-    const int2 sg = S.seg[s];
-    const int lo = max(v0, c0), hi = min(v0 + sg.y, c1);
-    for (int v = lo + (int)threadIdx.x; v < hi; v += kThreads) {
-      const int j = sg.x + (v - v0);
-      float4 x = spos[j];
-      const float q = qs[j];
-      x.w = q;
-      S.sp[v - c0] = x;
-      if (KER == FMMB_LAPLACE_GNJ) {
-        const float4 nj = snrm[j];
-        S.sm[v - c0] = make_float4(q * nj.x, q * nj.y, q * nj.z, 0.f);
+struct Tgt {
+  float2 x, y, z;     // the target's coordinates, duplicated in both lanes
+  float2 nx, ny, nz;  // Gni: its normal, duplicated
+};
+
+__device__ __forceinline__ float2 dup(float v) { return make_float2(v, v); }
+
+// The lane's 4 source pairs of one run of 32 (pairs pb, pb + 4, pb + 8,
+// pb + 12 of the chunk) against its NT targets.
+template <int KER, bool EXCL, int NT>
+__device__ __forceinline__ void run16(const Smem<KER>& S, int pb, const Tgt (&tg)[kMaxNT], float2 e2,
+                                      float2 (&acc)[NT][ncomp<KER>()]) {
+#pragma unroll (EXCL ? 1 : 4)
+  for (int u = 0; u < 4; u++) {
+    const int pi = pb + 4 * u;
+    const float4 a = S.A[pi];
+    const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w), sz = S.B[pi];
+    float2 q2 = make_float2(0.f, 0.f), mx = q2, my = q2, mz = q2;
+    if (KER == FMMB_LAPLACE_GNJ) {
+      const float4 m = S.M[pi];
+      mx = make_float2(m.x, m.y);
+      my = make_float2(m.z, m.w);
+      mz = S.MZ[pi];
+    } else {
+      q2 = S.Q[pi];
+    }
+#pragma unroll
+    for (int t = 0; t < NT; t++) {
+      const float2 dx = __fadd2_rn(tg[t].x, sx), dy = __fadd2_rn(tg[t].y, sy), dz = __fadd2_rn(tg[t].z, sz);
+      const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+      float2 ri = make_float2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+      if (EXCL) {
+        ri.x = r2.x > 0.f ? ri.x : 0.f;
+        ri.y = r2.y > 0.f ? ri.y : 0.f;
+      }
+      if (KER == FMMB_LAPLACE_G) {
+        const float2 qr = __fmul2_rn(q2, ri);
+        const float2 qr3 = __fmul2_rn(__fmul2_rn(qr, ri), ri);
+        acc[t][0] = __fadd2_rn(acc[t][0], qr);
+        acc[t][1] = __ffma2_rn(dx, qr3, acc[t][1]);
+        acc[t][2] = __ffma2_rn(dy, qr3, acc[t][2]);
+        acc[t][3] = __ffma2_rn(dz, qr3, acc[t][3]);
+      } else if (KER == FMMB_LAPLACE_GNI) {
+        const float2 qr3 = __fmul2_rn(__fmul2_rn(__fmul2_rn(q2, ri), ri), ri);
+        const float2 dot = __ffma2_rn(dx, tg[t].nx, __ffma2_rn(dy, tg[t].ny, __fmul2_rn(dz, tg[t].nz)));
+        acc[t][0] = __ffma2_rn(dot, qr3, acc[t][0]);
+      } else {
+        const float2 r3 = __fmul2_rn(__fmul2_rn(ri, ri), ri);
+        const float2 dot = __ffma2_rn(dx, mx, __ffma2_rn(dy, my, __fmul2_rn(dz, mz)));
+        acc[t][0] = __ffma2_rn(dot, r3, acc[t][0]);
       }
     }
-    v0 = (s == 0) ? self_end : v0 + sg.y;
   }
-  __syncthreads();
 }
 
-// One pass over target columns [t0, t0 + 32*NT) of the leaf.
-template <int KER, bool EXCL, int NT>
-__device__ void pass(Smem<KER>& S, int2 li, int t0, bool restage, int self_end, int vlen,
-                     const float4* __restrict__ tpos, const float4* __restrict__ tnrm,
-                     const float4* __restrict__ spos, const float4* __restrict__ snrm, const float* __restrict__ qs,
-                     float eps2, double coef, double* __restrict__ pot, double* __restrict__ grad, int ni) {
-  constexpr int NC = Smem<KER>::NC;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 xt[NT], nt[NT];
-  double P[NT][NC];
+// Stages virtual sources [c0, c1) of the list [own | pad | others | pad] as
+// packed pairs: each thread locates four sources (two pairs; binary search
+// over the segment starts), issues their loads, then stores them.
+template <int KER>
+__device__ __forceinline__ int locate(const Smem<KER>& S, int v, int c1) {
+  int sgi = 0;
 #pragma unroll
-  for (int t = 0; t < NT; t++) {
-    const int it = t0 + t * 32 + lane;
-    xt[t] = it < li.y ? tpos[li.x + it] : z4;
-    nt[t] = (KER == FMMB_LAPLACE_GNI && it < li.y) ? tnrm[li.x + it] : z4;
+  for (int st = 16; st > 0; st >>= 1)
+    if (S.vst[sgi + st] <= v) sgi += st;
+  const int2 sg = S.seg[sgi];
+  const int off = v - S.vst[sgi];
+  return (v < c1 && off < sg.y) ? sg.x + off : -1;
+}
+
+template <int KER>
+__device__ void stage(Smem<KER>& S, int c0, int c1, const float4* __restrict__ spos,
+                      const float4* __restrict__ snrm, const float* __restrict__ qs) {
+  __syncthreads();  // the previous chunk's readers are done
+  const int np = (c1 - c0) >> 1;
+  for (int pb = threadIdx.x; pb < np; pb += 2 * kThreads) {
+    int jj[4];
 #pragma unroll
-    for (int c = 0; c < NC; c++) P[t][c] = 0.0;
-  }
-  const int nchunk = (vlen + kCap - 1) / kCap;
-  for (int ch = 0; ch < nchunk; ch++) {
-    const int c0 = ch * kCap, c1 = min(vlen, c0 + kCap);
-    if (restage || nchunk > 1) stage<KER>(S, c0, c1, self_end, spos, snrm, qs);
-    // runs of 32 sources: warp w takes runs w, w + 4, ...
-    for (int r0 = c0 + warp * 32; r0 < c1; r0 += kWarps * 32) {
-      Acc<KER> acc[NT];
+    for (int u = 0; u < 4; u++) jj[u] = locate(S, c0 + 2 * (pb + (u >> 1) * kThreads) + (u & 1), c1);
+    float4 x[4], n[4];
+    float q[4];
 #pragma unroll
-      for (int t = 0; t < NT; t++) acc[t] = Acc<KER>{0.f, 0.f, 0.f, 0.f};
-      const float4* sp = S.sp + (r0 - c0);
-      const float4* sm = S.sm + (KER == FMMB_LAPLACE_GNJ ? r0 - c0 : 0);
-      if (EXCL && r0 < self_end)
-        run32<KER, true, NT>(sp, sm, xt, nt, eps2, acc);
-      else
-        run32<KER, false, NT>(sp, sm, xt, nt, eps2, acc);
+    for (int u = 0; u < 4; u++) {
+      x[u] = make_float4(kFar, kFar, kFar, 0.f);
+      n[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+      q[u] = 0.f;
+      if (jj[u] >= 0) {
+        x[u] = spos[jj[u]];
+        q[u] = qs[jj[u]];
+        if (KER == FMMB_LAPLACE_GNJ) n[u] = snrm[jj[u]];
+      }
+    }
 #pragma unroll
-      for (int t = 0; t < NT; t++) {
-        P[t][0] += (double)acc[t].p;
-        if (KER == FMMB_LAPLACE_G) {
-          P[t][1] += (double)acc[t].fx;
-          P[t][2] += (double)acc[t].fy;
-          P[t][3] += (double)acc[t].fz;
+    for (int h = 0; h < 2; h++) {
+      const int pi = pb + h * kThreads;
+      if (pi < np) {
+        const float4 x0 = x[2 * h], x1 = x[2 * h + 1];
+        const float q0 = q[2 * h], q1 = q[2 * h + 1];
+        S.A[pi] = make_float4(-x0.x, -x1.x, -x0.y, -x1.y);
+        S.B[pi] = make_float2(-x0.z, -x1.z);
+        if (KER == FMMB_LAPLACE_GNJ) {
+          const float4 n0 = n[2 * h], n1 = n[2 * h + 1];
+          S.M[pi] = make_float4(q0 * n0.x, q1 * n1.x, q0 * n0.y, q1 * n1.y);
+          S.MZ[pi] = make_float2(q0 * n0.z, q1 * n1.z);
+        } else {
+          S.Q[pi] = make_float2(q0, q1);
         }
       }
     }
   }
-  // add the warps' partial sums
-  if (warp > 0) {
+  __syncthreads();
+}
+
+// The team tile's runs of the chunk [c0, c1): runs k, k + m, ... (global run
+// index), the own leaf's runs (below self_end) with the coincident-point test.
+template <int KER, bool EXCL, int NT>
+__device__ __forceinline__ void tile_runs(const Smem<KER>& S, int c0, int c1, int self_end, int s, int k, int m,
+                                          const Tgt (&tg)[kMaxNT], float eps2, double (&P)[kMaxNT][ncomp<KER>()]) {
+  constexpr int NC = ncomp<KER>();
+  const float2 e2 = dup(eps2);
+  const int rend = c1 >> 5;
+  int r = (c0 >> 5) + k;  // c0 / 32 is a multiple of m
+  while (r < rend) {
+    float2 acc[NT][NC];
 #pragma unroll
     for (int t = 0; t < NT; t++)
 #pragma unroll
-      for (int c = 0; c < NC; c++) S.red[warp - 1][c][t * 32 + lane] = P[t][c];
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int t = 0; t < NT; t++) {
-#pragma unroll
-      for (int w = 0; w < kWarps - 1; w++)
-#pragma unroll
-        for (int c = 0; c < NC; c++) P[t][c] += S.red[w][c][t * 32 + lane];
-      const int it = t0 + t * 32 + lane;
-      if (it < li.y) {
-        const int i = li.x + it;
-        pot[i] = coef * P[t][0];
-        if (KER == FMMB_LAPLACE_G && grad) {
-          grad[i] = -coef * P[t][1];
-          grad[ni + i] = -coef * P[t][2];
-          grad[2 * (size_t)ni + i] = -coef * P[t][3];
-        }
-      }
+      for (int c = 0; c < NC; c++) acc[t][c] = make_float2(0.f, 0.f);
+    for (int i = 0; i < 4 && r < rend; i++, r += m) {
+      const int pb = ((r * 32 - c0) >> 1) + s;
+      if (EXCL && r * 32 < self_end)
+        run16<KER, true, NT>(S, pb, tg, e2, acc);
+      else
+        run16<KER, false, NT>(S, pb, tg, e2, acc);
     }
+#pragma unroll
+    for (int t = 0; t < NT; t++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        P[t][c] += (double)acc[t][c].x;
+        P[t][c] += (double)acc[t][c].y;
+      }
   }
-  __syncthreads();
 }
 
 template <int KER, bool EXCL>
@@ -210,40 +241,120 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ l
                                                       const float4* __restrict__ snrm, const float* __restrict__ qs,
                                                       float eps2, double coef, double* __restrict__ pot,
                                                       double* __restrict__ grad, int ni) {
+  constexpr int NC = ncomp<KER>();
   __shared__ Smem<KER> S;
   const int b = blockIdx.x;
   const int2 li = leaf_i[b];
-  if (threadIdx.x == 0) {
-    int n = 0;
-    const int self = list[(size_t)b * kP2PSlots + kSelfSlot];
-    S.seg[n++] = self >= 0 ? leaf_j[self] : make_int2(0, 0);
-    for (int s = 0; s < kP2PSlots; s++) {
-      const int jl = list[(size_t)b * kP2PSlots + s];
-      if (s != kSelfSlot && jl >= 0) S.seg[n++] = leaf_j[jl];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane & (kG - 1), s = lane / kG;
+  // segment list: lane l of warp 0 reads neighbour slot l; the own leaf goes
+  // first, the non-empty others after it in slot order
+  if (warp == 0) {
+    int2 sg = make_int2(0, 0);
+    if (lane < kP2PSlots) {
+      const int jl = list[(size_t)b * kP2PSlots + lane];
+      if (jl >= 0) sg = leaf_j[jl];
     }
-    S.nseg = n;
+    const int self_end = pad32(__shfl_sync(0xffffffffu, sg.y, kSelfSlot));
+    const bool oth = lane != kSelfSlot && sg.y > 0;
+    const unsigned mask = __ballot_sync(0xffffffffu, oth);
+    const int pos = 1 + __popc(mask & ((1u << lane) - 1u));
+    const int cnt = oth ? sg.y : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int nseg = 1 + __popc(mask);
+    if (lane == kSelfSlot) {
+      S.seg[0] = sg;
+      S.vst[0] = 0;
+    }
+    if (oth) {
+      S.seg[pos] = sg;
+      S.vst[pos] = self_end + incl - cnt;
+    }
+    if (lane >= nseg) S.vst[lane] = INT_MAX;
+    const int n_other = __shfl_sync(0xffffffffu, incl, 31);
+    if (lane == 0) S.seg[31] = make_int2(0, n_other);  // slot 31 is never a segment: it holds n_other
   }
   __syncthreads();
-  int n_other = 0;
-  for (int s = 1; s < S.nseg; s++) n_other += S.seg[s].y;
-  const int self_end = pad32(S.seg[0].y);                // virtual list: [own | pad | others | pad]
+  const int own = S.seg[0].y;
+  const int self_end = pad32(own);
+  const int n_other = S.seg[31].y;
   const int vlen = self_end + pad32(n_other);
-  for (int t0 = 0; t0 < li.y; t0 += kMaxNT * 32) {
-    const int nt = min(kMaxNT, (li.y - t0 + 31) / 32);
-    const bool restage = t0 == 0;
-    switch (nt) {
-      case 1:
-        pass<KER, EXCL, 1>(S, li, t0, restage, self_end, vlen, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
-        break;
-      case 2:
-        pass<KER, EXCL, 2>(S, li, t0, restage, self_end, vlen, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
-        break;
-      case 3:
-        pass<KER, EXCL, 3>(S, li, t0, restage, self_end, vlen, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
-        break;
-      default:
-        pass<KER, EXCL, 4>(S, li, t0, restage, self_end, vlen, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
-        break;
+  const int nchunk = (vlen + kCap - 1) / kCap;
+  // teams of m warps share a tile and split its runs
+  const int ng = (li.y + kG - 1) / kG;
+  const int m = ng <= kMaxNT ? 4 : ng <= 2 * kMaxNT ? 2 : 1;  // block-uniform
+  const int nteam = kWarps / m, team = warp / m, k = warp % m;
+  const int g0 = team * ng / nteam, g1 = (team + 1) * ng / nteam;
+  const int rounds = ((ng + nteam - 1) / nteam + kMaxNT - 1) / kMaxNT;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int tr = 0; tr < rounds; tr++) {
+    const int ga = g0 + tr * kMaxNT;
+    const int ntl = max(0, min(kMaxNT, g1 - ga));  // warp-uniform
+    Tgt tg[kMaxNT];
+    double P[kMaxNT][NC];
+#pragma unroll
+    for (int t = 0; t < kMaxNT; t++) {
+      const int it = (ga + t) * kG + g;
+      const bool on = t < ntl && it < li.y;
+      const float4 x = on ? tpos[li.x + it] : z4;
+      const float4 n = (KER == FMMB_LAPLACE_GNI && on) ? tnrm[li.x + it] : z4;
+      tg[t] = Tgt{dup(x.x), dup(x.y), dup(x.z), dup(n.x), dup(n.y), dup(n.z)};
+#pragma unroll
+      for (int c = 0; c < NC; c++) P[t][c] = 0.0;
+    }
+    for (int ch = 0; ch < nchunk; ch++) {
+      const int c0 = ch * kCap, c1 = min(vlen, c0 + kCap);
+      if (nchunk > 1 || tr == 0) stage<KER>(S, c0, c1, spos, snrm, qs);
+      switch (ntl) {
+        case 0: break;
+        case 1: tile_runs<KER, EXCL, 1>(S, c0, c1, self_end, s, k, m, tg, eps2, P); break;
+        case 2: tile_runs<KER, EXCL, 2>(S, c0, c1, self_end, s, k, m, tg, eps2, P); break;
+        case 3: tile_runs<KER, EXCL, 3>(S, c0, c1, self_end, s, k, m, tg, eps2, P); break;
+        default: tile_runs<KER, EXCL, 4>(S, c0, c1, self_end, s, k, m, tg, eps2, P); break;
+      }
+    }
+    // add the 4 streams' sums of each target (lanes g, g + 8, g + 16, g + 24)
+#pragma unroll
+    for (int t = 0; t < kMaxNT; t++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        P[t][c] += __shfl_xor_sync(0xffffffffu, P[t][c], 8);
+        P[t][c] += __shfl_xor_sync(0xffffffffu, P[t][c], 16);
+      }
+    if (m > 1) {  // block-uniform (rounds == 1): the team's warps through shared memory
+      if (s == 0 && k > 0) {
+#pragma unroll
+        for (int t = 0; t < kMaxNT; t++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) S.red[warp][t][c][g] = P[t][c];
+      }
+      __syncthreads();
+      if (k == 0 && s == 0) {
+        for (int w = 1; w < m; w++)
+#pragma unroll
+          for (int t = 0; t < kMaxNT; t++)
+#pragma unroll
+            for (int c = 0; c < NC; c++) P[t][c] += S.red[warp + w][t][c][g];
+      }
+    }
+    if (k == 0 && s == 0) {
+#pragma unroll
+      for (int t = 0; t < kMaxNT; t++) {
+        const int it = (ga + t) * kG + g;
+        if (t < ntl && it < li.y) {
+          const int i = li.x + it;
+          pot[i] = coef * P[t][0];
+          if (KER == FMMB_LAPLACE_G && grad) {
+            grad[i] = -coef * P[t][1];
+            grad[ni + i] = -coef * P[t][2];
+            grad[2 * (size_t)ni + i] = -coef * P[t][3];
+          }
+        }
+      }
     }
   }
 }

@@ -157,6 +157,38 @@ def test_mixed_matches_fp64(ob):
         assert rel(out[1][0], out[0][0]) < 1e-6
 
 
+@pytest.mark.parametrize("lmax", [2, 3])
+def test_mixed_near_field_large_leaves(lmax, ob):
+    """Leaves of hundreds of points: several rounds of target groups per warp
+    and source lists over many staged chunks (1e-6 vs FP64)."""
+    t, tn, s, sn, q = make_points(40000, 71 + lmax)
+    for neq in (0, 1, 2):
+        out = []
+        for prec in (0, 1):
+            pl = plan_for(ob, neq, 8, lmax, t, tn, s, sn, semantics=1, precision=prec, exclude_self=True)
+            out.append(pl.evaluate(q, f64=True))
+            pl.close()
+        assert rel(out[1][0], out[0][0]) < 1e-6
+        if neq == 0:
+            assert rel(out[1][1], out[0][1]) < 1e-6
+
+
+def test_serial_phases_give_the_same_results(ob):
+    t, tn, s, sn, q = make_points(20000, 75, "clustered")
+    for prec in (0, 1):
+        pl = plan_for(ob, 2, 10, 4, t, tn, s, sn, semantics=1, precision=prec, exclude_self=True)
+        a = pl.evaluate(q, f64=True)[0]
+        pl.set_overlap(False)
+        b = pl.evaluate(q, f64=True)[0]
+        ph = pl.timings()
+        pl.set_overlap(True)
+        c = pl.evaluate(q, f64=True)[0]
+        pl.close()
+        # the same sums (FP64 atomics in some translations: rounding order only)
+        assert rel(b, a) < 1e-13 and rel(c, a) < 1e-13
+        assert ph["p2p"] > 0 and ph["m2l"] > 0
+
+
 def test_host_and_device_pointers_agree(ob):
     torch = pytest.importorskip("torch")
     t, tn, s, sn, q = make_points(5000, 80)
