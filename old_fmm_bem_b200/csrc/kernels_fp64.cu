@@ -555,21 +555,38 @@ void launch_finalize_f64(int n, const int* perm, const double* pn, const double*
 
 namespace {
 
-// Box-pair translations on the FP64 CUDA cores (M2M, L2L): a block takes a
-// tile of TP pairs sharing one operator, stages their input expansions in
+// Box-pair translations (M2M, L2L, and every dense translation of the
+// Helmholtz-family kernels) in FP64: a tile holds up to 32 pairs sharing one
+// operator T, and  out[dst[p]][r] (+)= sum_c T[r][c] in[src[p]][c]  (added
+// atomically when an output row receives several pairs: M2M, M2L).  Two
+// kernels: operators that fit in shared memory are staged whole (one bulk
+// copy per block); larger ones run as grouped GEMMs on the FP64 tensor cores.
+constexpr int kGN = 32;  // pairs per tile (at most)
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+
+// Operators that fit in shared memory (K <= 160: the Laplace M2M / L2L up to
+// p = 11): a block takes a tile of TP pairs sharing one operator, stages their
+// input expansions in
 // shared memory (transposed, [coefficient][pair], row stride TP + 2) and forms
 // the outputs with a register tile per thread of 2 consecutive output rows x
 // J = TP / 4 pairs: per operator column c one 16-byte read of
 // T[c][2rp..2rp+1] and J/2 broadcast reads of the inputs feed 2J FMAs.
 // Thread t takes row pair t % 64 and pair group t / 64.  The transposed operator
 // (opT[op][c][r], row stride KP = K rounded up to even) is first brought into
-// shared memory with one bulk copy when it fits (STAGED), else read from
-// global memory.  Outputs are added (atomically when an output row receives
-// several pairs, M2M).
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
+// shared memory with one bulk copy (STAGED; the launcher takes this kernel
+// only when the operator fits).  Outputs are added (atomically when an output
+// row receives several pairs, M2M).
 template <int TP, bool STAGED>
 __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
   extern __shared__ __align__(16) double dsm[];
@@ -683,43 +700,148 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
   }
 }
 
+
+// Grouped GEMM on the FP64 tensor cores (mma.sync m8n8k4 .f64, 256 FMA per
+// warp instruction): a block of 8 warps computes 128 output rows x the
+// tile's 32 pairs, warp w rows 32 (w % 4) .. + 31 x pairs 16 (w / 4) .. + 15
+// (4 x 2 MMA tiles of 8 x 8, 16 FP64 accumulators per thread).  Operator
+// chunks of 16 columns and the inputs go through a 4-stage cp.async ring;
+// the shared-memory rows are padded (132 and 36 doubles) so that the
+// fragment reads of the four k-rows of an MMA fall in different banks.
+constexpr int kDM = 128, kDN = 32, kDK = 16, kDT = 256, kDS = 4;
+constexpr int kDAs = kDM + 4;  // operator chunk row stride (doubles)
+constexpr int kDXs = kDN + 4;  // input chunk row stride
+constexpr size_t kDSmem = kDS * (size_t)kDK * (kDAs + kDXs) * sizeof(double);  // 86 KB
+
+__device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kDT) pairs_dmma_f64(PairArgs P) {
+  extern __shared__ __align__(16) double dsm2[];
+  double* As = dsm2;                     // [kDS][kDK][kDAs]: operator T[r][c] at [c][r]
+  double* Xs = dsm2 + kDS * kDK * kDAs;  // [kDS][kDK][kDXs]: inputs x_p[c] at [c][p]
+  __shared__ int ssrc[kDN], sdst[kDN];
+  const int g = blockIdx.x, r0 = blockIdx.y * kDM, K = P.K, KP = (K + 1) & ~1, tp = P.tp;
+  const double* T = P.opT + (size_t)P.tile_op[g] * P.ostride;
+  if (threadIdx.x < kDN) {
+    const bool on = (int)threadIdx.x < tp;
+    ssrc[threadIdx.x] = on ? P.tile_src[(size_t)g * tp + threadIdx.x] : -1;
+    sdst[threadIdx.x] = on ? P.tile_dst[(size_t)g * tp + threadIdx.x] : -1;
+  }
+  __syncthreads();
+  auto issue = [&](int kc, int st) {
+    const int k0 = kc * kDK;
+#pragma unroll
+    for (int i = 0; i < kDK * kDM / 2 / kDT; i++) {  // operator: 16-byte pieces of 2 rows
+      const int e = (int)threadIdx.x + i * kDT;
+      const int c = e / (kDM / 2), rr = 2 * (e % (kDM / 2));
+      const int col = k0 + c, row = r0 + rr;
+      const bool ok = col < K && row < KP;
+      cp_async16(smem_addr(As + (st * kDK + c) * kDAs + rr), ok ? T + (size_t)col * KP + row : T, ok ? 16 : 0);
+    }
+#pragma unroll
+    for (int i = 0; i < kDK * kDN / kDT; i++) {  // inputs: 8 bytes each
+      const int e = (int)threadIdx.x + i * kDT;
+      const int pi = e % kDN, c = e / kDN;
+      const int sj = ssrc[pi], col = k0 + c;
+      const bool ok = sj >= 0 && col < K;
+      cp_async8(smem_addr(Xs + (st * kDK + c) * kDXs + pi), ok ? P.xin + (size_t)sj * K + col : P.xin, ok ? 8 : 0);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gq = lane >> 2, tq = lane & 3;             // MMA fragment coordinates
+  const int wr = 32 * (warp & 3), wp = 16 * (warp >> 2);  // the warp's rows and pairs in the block
+  double acc[4][2][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int nk = (K + kDK - 1) / kDK;
+#pragma unroll
+  for (int st = 0; st < kDS - 1; st++) {
+    if (st < nk)
+      issue(st, st);
+    else
+      asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  for (int kc = 0; kc < nk; kc++) {
+    if (kc + kDS - 1 < nk)
+      issue(kc + kDS - 1, (kc + kDS - 1) % kDS);
+    else
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group %0;" ::"n"(kDS - 1) : "memory");
+    __syncthreads();
+    const double* a = As + (kc % kDS) * kDK * kDAs + wr + gq;
+    const double* x = Xs + (kc % kDS) * kDK * kDXs + wp + gq;
+#pragma unroll
+    for (int k4 = 0; k4 < kDK; k4 += 4) {
+      const int kr = k4 + tq;  // the k-row of this lane's A column / B row
+      double af[4], bf[2];
+#pragma unroll
+      for (int i = 0; i < 4; i++) af[i] = a[kr * kDAs + 8 * i];
+#pragma unroll
+      for (int j = 0; j < 2; j++) bf[j] = x[kr * kDXs + 8 * j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++) dmma884(acc[i][j], af[i], bf[j]);
+    }
+    __syncthreads();  // the stage is refilled by the next iteration's copies
+  }
+  // accumulator (i, j): rows wr + 8 i + gq, pairs wp + 8 j + 2 tq + {0, 1}
+#pragma unroll
+  for (int j = 0; j < 2; j++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int d = sdst[wp + 8 * j + 2 * tq + h];
+      if (d < 0) continue;
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = r0 + wr + 8 * i + gq;
+        if (r >= K) continue;
+        double* o = P.out + (size_t)d * K + r;
+        if (P.atomic)
+          atomicAdd(o, acc[i][j][h]);
+        else
+          *o += acc[i][j][h];
+      }
+    }
+}
 }  // namespace
 
-int pairs_f64_tile(int K, int npair, int nsm) {
-  int tp = 32;
-  while (tp > 8 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
-  // staged inputs: 48 KB, or up to 200 KB for operators too large to stage
-  // (K > 160: the operator streams from L2 and more pairs per tile reuse it)
-  const size_t cap = (size_t)K * ((K + 1) & ~1) * sizeof(double) > 160 * 1024 ? 200 * 1024 : 48 * 1024;
-  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > cap) tp /= 2;
-  return tp;
-}
-
 namespace {
-size_t pairs_smem(int K, int tp, size_t ostride, bool staged) {
-  return (staged ? ostride * sizeof(double) : 0) + (size_t)K * (tp + 2) * sizeof(double);
-}
+size_t pairs_smem(int K, int tp, size_t ostride) { return ostride * sizeof(double) + (size_t)K * (tp + 2) * sizeof(double); }
 constexpr size_t kPairsSmemMax = 224 * 1024;  // below the 227 KB opt-in limit, which includes static shared memory
+bool staged_fits(int K) { return pairs_smem(K, 8, (size_t)K * ((K + 1) & ~1)) <= kPairsSmemMax && K <= 160; }
 
 template <int TP>
 void launch_tp(const PairArgs& a, cudaStream_t st) {
-  const bool staged = pairs_smem(a.K, TP, a.ostride, true) <= kPairsSmemMax;
-  if (staged)
-    translate_pairs_f64<TP, true><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride, true), st>>>(a);
-  else
-    translate_pairs_f64<TP, false><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride, false), st>>>(a);
+  translate_pairs_f64<TP, true><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride), st>>>(a);
 }
 
 template <int TP>
 void prepare_tp() {
   FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kPairsSmemMax));
-  FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kPairsSmemMax));
 }
 }  // namespace
 
+// Staged kernel (small K): tiles of 8-32 pairs, enough tiles for the SMs and
+// the inputs within 48 KB; tensor-core GEMM (larger K): 32 pairs.
+int pairs_f64_tile(int K, int npair, int nsm) {
+  if (!staged_fits(K)) return kGN;
+  int tp = 32;
+  while (tp > 8 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
+  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
+  return tp;
+}
+
 void prepare_translate_pairs_f64() {
+  FMMB_CUDA(cudaFuncSetAttribute(pairs_dmma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmem));
   prepare_tp<32>();
   prepare_tp<16>();
   prepare_tp<8>();
@@ -727,10 +849,16 @@ void prepare_translate_pairs_f64() {
 
 void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
   if (a.ntile <= 0) return;
-  switch (a.tp) {
-    case 32: launch_tp<32>(a, st); break;
-    case 16: launch_tp<16>(a, st); break;
-    default: launch_tp<8>(a, st); break;
+  FMMB_REQUIRE(a.tp >= 1 && a.tp <= kGN, FMMB_ERR_ARG, "pair tile larger than 32");
+  if (staged_fits(a.K) && (a.tp == 8 || a.tp == 16 || a.tp == 32)) {
+    switch (a.tp) {
+      case 32: launch_tp<32>(a, st); break;
+      case 16: launch_tp<16>(a, st); break;
+      default: launch_tp<8>(a, st); break;
+    }
+  } else {
+    const dim3 grid((unsigned)a.ntile, (unsigned)((a.K + kDM - 1) / kDM));
+    pairs_dmma_f64<<<grid, kDT, kDSmem, st>>>(a);
   }
   FMMB_CHECK_LAUNCH();
 }
