@@ -331,6 +331,24 @@ def run_ours(args, rank, world):
                 "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
                         f"execute 3 TF32 MMAs per product on 128x128 padded operators; peak = TF32 dense = half of "
                         f"{peak_kind} bf16"}
+    # whole matvec against the sum of its phases' roofline times: algorithmic
+    # work of each phase over the peak of the unit it runs on (P2P, P2M, L2P:
+    # FP32; M2L: TF32; M2M, L2L: FP64 at the nominal 37 TFLOP/s)
+    nb_i, nb_j = plan.tree(4), plan.tree(5)
+    fp64_peak = 37.0
+    ideal = {"p2p": 20.0 * st["p2p_pairs"] / fp32_peak,
+             "p2m": 2.0 * npts * K / fp32_peak,
+             "m2m": 2.0 * K * K * float(nb_j[3:LMAX + 1].sum()) / fp64_peak,
+             "m2l": 2.0 * K * K * st["m2l_pairs"] / tf32_peak,
+             "l2l": 2.0 * K * K * float(nb_i[3:LMAX + 1].sum()) / fp64_peak,
+             "l2p": 2.0 * npts * K / fp32_peak}
+    ideal = {k: v / 1e9 for k, v in ideal.items()}  # flops / (TFLOP/s) -> ms
+    matvec_roof = {"ideal_ms": ideal, "sum_ideal_ms": sum(ideal.values()), "step_ms": ms_step,
+                   "frac_of_step": sum(ideal.values()) / ms_step,
+                   "frac_per_phase_alone": {k: ideal[k] / float(phase_alone[i]) for i, k in enumerate(names)},
+                   "note": "algorithmic flops per phase (P2P 20 per pair, P2M/L2P 2(p+1)^2 per point, M2L/M2M/L2L "
+                           "2(p+1)^4 per box pair) over FP32 (nominal), TF32 (half the measured bf16) and FP64 "
+                           "(nominal 37) peaks"}
     dom = int(np.argmax(phase_alone[:6]))
     roof = roof_m2l if names[dom] == "m2l" else roof_p2p
     # CPU baseline: the reference's own fmm() on a bounded sample, one core
@@ -360,6 +378,7 @@ def run_ours(args, rank, world):
         "stats": st,
         "roofline": roof,
         "roofline_secondary": roof_p2p if roof is roof_m2l else roof_m2l,
+        "matvec_roofline": matvec_roof,
         "cpu_baseline": cpu,
         "e2e": {"value": world * npts / e2e_s / 1e6, "unit": "Mpts/s", "h2d_bytes_per_step": 4 * npts,
                 "d2h_bytes_per_step": 4 * npts},
