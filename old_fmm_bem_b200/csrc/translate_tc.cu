@@ -467,7 +467,7 @@ __global__ void split_tf32(int nbox, int K, int kpad, const double* __restrict__
 // out[rows[w]][0..K) += sum over e in [ptr[w], ptr[w+1]) of y[idx[e]][0..K)
 // (pair rows of ys floats), in FP64 and in list order (deterministic); one warp
 // per output row, lane l holding coefficients 128c + 4l .. 128c + 4l + 3 of
-// each 128-coefficient chunk c (K <= 256).
+// each 128-coefficient chunk c (K <= 256); for K <= 128 eight rows in flight.
 __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* __restrict__ ptr,
                              const int* __restrict__ idx, const float* __restrict__ y, int ys, int K,
                              double* __restrict__ out) {
@@ -478,6 +478,23 @@ __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* 
   double a[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   const int e0 = ptr[w], e1 = ptr[w + 1];
   int e = e0;
+  if (nch == 1) {  // K <= 128: one 512-byte read per pair row, 8 rows in flight
+    for (; e + 8 <= e1; e += 8) {
+      int r8[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) r8[u] = idx[e + u];
+      float4 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) v[u] = __ldg(reinterpret_cast<const float4*>(y + (size_t)r8[u] * ys) + lane);
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        a[0][0] += v[u].x;
+        a[0][1] += v[u].y;
+        a[0][2] += v[u].z;
+        a[0][3] += v[u].w;
+      }
+    }
+  }
   for (; e + 4 <= e1; e += 4) {
     float4 v[4][2];
 #pragma unroll
