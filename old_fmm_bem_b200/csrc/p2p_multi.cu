@@ -79,6 +79,12 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
       for (int r = 0; r < R; r++)
 #pragma unroll
         for (int c = 0; c < NC; c++) A[r][c] = 0.f;
+      // Gni / Gnj with 4 or 8 right-hand sides: the sums of right-hand sides
+      // 2h, 2h + 1 side by side for the two-lane FP32 FMA
+      constexpr bool PK = KER != FMMB_LAPLACE_G && RV > 0;
+      float2 A2[PK ? R / 2 : 1];
+#pragma unroll
+      for (int h = 0; h < (PK ? R / 2 : 1); h++) A2[h] = make_float2(0.f, 0.f);
 #pragma unroll 2
       for (int jj = 0; jj < nc; jj++) {
         float qv[R];  // the source's charges, vector loads when R is a multiple of 4
@@ -119,8 +125,22 @@ __global__ void __launch_bounds__(kT) p2p_multi(const int2* __restrict__ work, c
             const float4 nj4 = sn[jj];
             kv = fmaf(dx, nj4.x, fmaf(dy, nj4.y, dz * nj4.z)) * (rinv * rinv * rinv);
           }
+          if (PK) {
+            const float2 kv2 = make_float2(kv, kv);
 #pragma unroll
-          for (int r = 0; r < R; r++) A[r][0] = fmaf(qv[r], kv, A[r][0]);
+            for (int h = 0; h < (PK ? R / 2 : 1); h++)
+              A2[h] = __ffma2_rn(make_float2(qv[2 * h], qv[2 * h + 1]), kv2, A2[h]);
+          } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) A[r][0] = fmaf(qv[r], kv, A[r][0]);
+          }
+        }
+      }
+      if (PK) {
+#pragma unroll
+        for (int h = 0; h < (PK ? R / 2 : 1); h++) {
+          A[2 * h][0] = A2[h].x;
+          A[2 * h + 1][0] = A2[h].y;
         }
       }
 #pragma unroll
