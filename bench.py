@@ -391,8 +391,9 @@ def run_ours(args, rank, world):
 
 
 # ------------------------------------------------------------------ other configurations
-def _timed(step, stream, steps, warmup, flush):
-    """Mean CUDA-event time (ms) of `step` on `stream`, L2 flushed before each."""
+def _timed(step, stream, steps, warmup, flush, out=None):
+    """Mean CUDA-event time (ms) of `step` on `stream`, L2 flushed before each
+    (the per-step times are appended to `out` when given)."""
     import torch
     with torch.cuda.stream(stream):
         for _ in range(warmup):
@@ -408,6 +409,8 @@ def _timed(step, stream, steps, warmup, flush):
             b.record(stream)
             b.synchronize()
             ms.append(a.elapsed_time(b))
+    if out is not None:
+        out.extend(ms)
     return float(np.mean(ms))
 
 
@@ -565,7 +568,8 @@ def run_c4(args):
                 box["out"] = plan.gmres(b, X, wd, diag=geometry.BEM_DIAG, precond=1 / geometry.BEM_DIAG, restart=30,
                                         max_iter=iters)
 
-            ms = _timed(solve, stream, max(1, min(args.steps, 3)), max(3, min(args.warmup, 3)), flush)
+            per_step = []
+            ms = _timed(solve, stream, max(1, min(args.steps, 3)), max(3, min(args.warmup, 3)), flush, per_step)
             _, it, resid = box["out"]
             # one matvec against the per-problem FP64 direct sum (first right-hand side, 1024 targets of
             # each of the four largest problems)
@@ -580,6 +584,7 @@ def run_c4(args):
                 errs.append(float(np.linalg.norm(pot[i0:i1] - vd) / np.linalg.norm(vd)))
             matvecs = iters + 1  # the initial residual and one per iteration
             res[name] = {"lmax": lmax, "autotune_ms_per_matvec": tune, "tree_build_s": tree_s, "solve_ms": ms,
+                         "solve_ms_per_step": per_step,
                          "iterations": it, "matvecs": matvecs, "matvec_ms": ms / matvecs,
                          "max_rel_resid": float(np.max(resid)), "median_rel_resid": float(np.median(resid)),
                          "rel_err_vs_fp64_direct": float(np.sqrt(np.mean(np.square(errs)))),
