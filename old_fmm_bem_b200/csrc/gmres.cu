@@ -281,7 +281,7 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
       }
     sptr[nsys] = (int)csys.size();
     const int nch = (int)csys.size();
-    DevBuf<int> d_ci;
+    DevBuf<int>& d_ci = pl->gm_ci;  // workspaces kept by the plan (grown, never shrunk)
     d_ci.alloc(3 * (size_t)nch + nsys + 1 + 1);
     FMMB_CUDA(cudaMemcpyAsync(d_ci.get(), csys.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
     FMMB_CUDA(cudaMemcpyAsync(d_ci.get() + nch, cstart.data(), nch * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -292,14 +292,15 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
     int* d_count = d_ci.get() + 3 * nch + nsys + 1;
 
     // vectors: V[0..m], w, b, x, pot (FP64), q (FP32)
-    DevBuf<double> vec;
+    DevBuf<double>& vec = pl->gm_vec;
     vec.alloc((size_t)(m + 5) * L);
     double* V = vec.get();
     double* W = V + (size_t)(m + 1) * L;
     double* B = W + L;
     double* X = B + L;
     double* POT = X + L;
-    DevBuf<float> qbuf, wbuf;
+    DevBuf<float>& qbuf = pl->gm_q;
+    DevBuf<float>& wbuf = pl->gm_w;
     qbuf.alloc(L);
     const float* wt = nullptr;
     if (weight) {
@@ -316,7 +317,7 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
 
     // per-system state
     const int pst = m + 1;
-    DevBuf<double> sd;
+    DevBuf<double>& sd = pl->gm_sd;
     // H [(m+1) m], cs, sn [m], g, y, h1, h2 [m+1], beta0, inv, resid, nrm2 per
     // system, then the chunk partials
     sd.alloc((size_t)nsys * ((m + 1) * m + 2 * m + 4 * (m + 1) + 4) + (size_t)nch * pst);
@@ -334,7 +335,7 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
     S.resid = S.inv + nsys;
     double* nrm2 = S.resid + nsys;
     double* partial = nrm2 + nsys;
-    DevBuf<int> si;
+    DevBuf<int>& si = pl->gm_si;
     si.alloc(2 * (size_t)nsys);
     S.active = si.get();
     S.kact = si.get() + nsys;

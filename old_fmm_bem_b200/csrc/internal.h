@@ -190,6 +190,10 @@ struct fmmb_plan {
   // far-field-only graph, whose charges are qs_far
   bool far_only = false;
   bool serial = false;  // near field on the main stream (fmmb_set_overlap(0))
+  // fmmb_gmres workspaces (Krylov vectors, per-system state, chunk tables)
+  fmmb::DevBuf<int> gm_ci, gm_si;
+  fmmb::DevBuf<double> gm_vec, gm_sd;
+  fmmb::DevBuf<float> gm_q, gm_w;
   fmmb::DevBuf<double> near_all;
   fmmb::DevBuf<float> qs_far;
   fmmb::DevBuf<int2> m_p2p_work;  // (target leaf, first target), up to 128 targets each
