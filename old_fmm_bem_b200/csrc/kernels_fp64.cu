@@ -705,13 +705,14 @@ __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
 // warp instruction): a block of 8 warps computes 128 output rows x the
 // tile's 32 pairs, warp w rows 32 (w % 4) .. + 31 x pairs 16 (w / 4) .. + 15
 // (4 x 2 MMA tiles of 8 x 8, 16 FP64 accumulators per thread).  Operator
-// chunks of 16 columns and the inputs go through a 4-stage cp.async ring;
+// chunks of 8 columns and the inputs go through a 4-stage cp.async ring (43 KB:
+// three blocks per SM; 16-column chunks with one block fewer ran 10 % slower);
 // the shared-memory rows are padded (132 and 36 doubles) so that the
 // fragment reads of the four k-rows of an MMA fall in different banks.
-constexpr int kDM = 128, kDN = 32, kDK = 16, kDT = 256, kDS = 4;
+constexpr int kDM = 128, kDN = 32, kDK = 8, kDT = 256, kDS = 4;
 constexpr int kDAs = kDM + 4;  // operator chunk row stride (doubles)
 constexpr int kDXs = kDN + 4;  // input chunk row stride
-constexpr size_t kDSmem = kDS * (size_t)kDK * (kDAs + kDXs) * sizeof(double);  // 86 KB
+constexpr size_t kDSmem = kDS * (size_t)kDK * (kDAs + kDXs) * sizeof(double);  // 43 KB: 3 blocks per SM
 
 __device__ __forceinline__ void dmma884(double (&c)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
