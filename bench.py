@@ -605,6 +605,41 @@ def run_c4(args):
 
 
 
+def run_c4_matvec(args):
+    """The batched matvec of batch64 alone: the same 64 problems and forest
+    plan (Gni, p = 10, mixed, depth --lmax or 3) with 1 and with 8 right-hand
+    sides; CUDA-event time per evaluate (3 warm-up, 5 timed, L2 flushed)."""
+    import torch
+    import old_fmm_bem_b200 as ob
+    from old_fmm_bem_b200 import geometry
+    probs = geometry.bem_batch_problems(64, seed=17)
+    off = np.cumsum([0] + [p[0].shape[1] for p in probs]).astype(np.int32)
+    x = torch.from_numpy(np.ascontiguousarray(np.concatenate([p[0] for p in probs], axis=1))).cuda()
+    nrm = torch.from_numpy(np.ascontiguousarray(np.concatenate([p[1] for p in probs], axis=1))).cuda()
+    n = int(off[-1])
+    bbox = (-1.0001, -1.0001, -1.0001, 2.0002)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    lmax = args.lmax or 3
+    res = {}
+    for nrhs in (1, 8):
+        plan = ob.Plan(kernel=ob.LAPLACE_GNI, p=P_ORDER, lmax=lmax, nrhs=nrhs, precision=ob.MIXED,
+                       semantics=ob.SEM_ACCURATE, exclude_self=True)
+        plan.set_stream(stream)
+        plan.set_geometry_batch(off, x, off, x, nrm, None, bbox=bbox)
+        q = torch.from_numpy(np.random.default_rng(5).uniform(-1, 1, nrhs * n).astype(np.float32)).cuda()
+        pot = torch.zeros(nrhs * n, dtype=torch.float32, device="cuda")
+        ms = _timed(lambda: plan.evaluate(q, pot), stream, 5, 3, flush)
+        res[f"rhs{nrhs}"] = {"ms_per_evaluate": ms, "mpts_s": nrhs * n / (ms * 1e-3) / 1e6,
+                             "launches": plan.stats()["launches"]}
+        plan.close()
+    print(json.dumps({"metric": "batched BEM matvec Mpts/s (64 unit-sphere problems, Gni, p=10, 1 and 8 RHS)",
+                      "value": res["rhs8"]["mpts_s"], "unit": "Mpts/s", "n_gpus": 1, "steps": 5,
+                      "dtype": "f32+tf32x3+f64", "data": "synthetic",
+                      "config": {"workload": f"64 geodesic unit spheres, {n} centroids, Gni, depth {lmax}",
+                                 "l2": "flushed between steps"}, "results": res}))
+
+
 def run_c5(args):
     """Complex Helmholtz e^{ikr}/(4 pi r): 1,048,576 points uniform on the unit
     sphere, complex charges with parts U[-1, 1], k = 5, p = 16; one step = the
@@ -706,10 +741,11 @@ def main():
     ap.add_argument("--lmax", type=int, default=0,
                     help="batch64 / helmholtz1m: this octree depth instead of the autotuner's")
     ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64",
-                                                     "helmholtz1m"],
+                                                     "batch64_matvec", "helmholtz1m"],
                     help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "
                          "points; adjoint1m: forward + backward on 1,048,576 clustered points; batch64: GMRES on 64 "
-                         "BEM problems x 8 right-hand sides; helmholtz1m: complex Helmholtz, "
+                         "BEM problems x 8 right-hand sides; batch64_matvec: its matvec alone, 1 and 8 "
+                         "right-hand sides; helmholtz1m: complex Helmholtz, "
                          "1,048,576 sphere points, k=5, p=16")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -728,6 +764,8 @@ def main():
         run_c3(args)
     elif args.config == "batch64":
         run_c4(args)
+    elif args.config == "batch64_matvec":
+        run_c4_matvec(args)
     elif args.config == "helmholtz1m":
         run_c5(args)
     else:
