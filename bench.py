@@ -107,6 +107,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.sm), "source": "NVML, 2 ms polling"}
 
 
+def max_over_ranks(x, world):
+    """The largest of the ranks' values of x: an all-reduce MAX over the
+    process group (a device tensor with NCCL, a host tensor with gloo)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    dev = "cuda" if torch.distributed.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mpts_s(world, npts_per_rank, ms_step):
+    """Whole-job throughput: every rank's points over the slowest rank's time."""
+    return world * npts_per_rank / (ms_step * 1e-3) / 1e6
+
+
 def workload(seed):
     from old_fmm_bem_b200 import geometry
     return geometry.bem_double_layer_problem(SUBDIV, seed=seed)
@@ -273,10 +290,7 @@ def run_ours(args, rank, world):
             phase_alone += np.array(list(plan.timings().values()))
     phase_alone /= args.steps
     plan.set_overlap(True)
-    if world > 1:
-        t = torch.tensor([ms_step], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = max_over_ranks(ms_step, world)
 
     # end to end through the public API with host (pinned) buffers: the copy of
     # the charges in and of the potentials out are inside the timed call
@@ -290,10 +304,7 @@ def run_ours(args, rank, world):
         plan.evaluate(qh.numpy(), ph.numpy())
         e2e.append(time.perf_counter() - t0)
     e2e_s = float(np.median(e2e))
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world)
 
     if rank != 0:
         plan.close()
@@ -363,7 +374,7 @@ def run_ours(args, rank, world):
                                  "lmax 3), 2 runs, 1 core"}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"error": str(e)}
-    value = world * npts / (ms_step * 1e-3) / 1e6
+    value = job_mpts_s(world, npts, ms_step)
     line = {
         "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
