@@ -302,8 +302,10 @@ FMMB_API int fmmb_get_timings(fmmb_plan* plan, float* ms7);
 
 /* Overlap of the near field with the far field (default on).  With on = 0
  * the near field runs on the plan's stream between the far-field phases, so
- * that fmmb_get_timings gives each phase's time with the GPU to itself (the
- * results are the same).  Captured evaluates are rebuilt. */
+ * that fmmb_get_timings gives each phase's time with the GPU to itself, as the
+ * reference's per-routine timers do for its serial phases (tfmm[],
+ * fmm/alloc.cxx:121); the results are the same.  Captured evaluates are
+ * rebuilt. */
 FMMB_API int fmmb_set_overlap(fmmb_plan* plan, int on);
 
 /* Counts of the current geometry: [0] ni, [1] nj, [2] target leaves,
