@@ -1,20 +1,27 @@
 #!/usr/bin/env python
-"""Benchmark: Laplace double-layer (Gnj) BEM matvec, FMM on one B200 per rank.
+"""Benchmark: Laplace G FMM matvec + adjoint on one B200 per rank.
 
-Workload (one "step" = one FMM matvec over the whole surface):
-  icosphere of radius 1 subdivided 6 times (81,920 triangles), 3 Gauss points
-  per triangle (245,760 points), outward unit normals, panel densities
-  U[-1, 1] times the quadrature weights as charges; targets = the same points,
-  zero-distance pairs excluded; order p = 10, mixed precision.
-Metric: FMM matvec Mpts/s (targets per second of one matvec on a built tree).
+Headline workload (one "step" = one forward and one backward pass of the
+Laplace G FMM as a torch.autograd operator):
+  1,048,576 points from 32 Gaussian clusters (sigma 0.02) in the unit cube,
+  charges N(0,1), targets = sources (zero-distance pairs excluded), order
+  p = 12 -- the lowest order whose potential meets rel. err <= 1e-6 against
+  the FP64 direct sum on this point set -- mixed precision (FP32 near field,
+  TF32x3 tensor-core M2L, FP64 expansions).  The backward gives the
+  gradients of L = sum(w * pot) w.r.t. the charges (the transposed FMM) and
+  the positions (the forward's field and the transposed FMM's field).
+Metric: FMM matvec Mpts/s at rel err <= 1e-6 vs FP64 direct (points per
+second of forward + backward on a built tree); the same step in the plain FP64
+form is timed beside it (mixed_over_fp64, backward_over_forward).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--config adjoint1m|bem|uniform32k|batch64|batch64_matvec|helmholtz1m]
 
-Under torchrun each rank runs its own independent problem (a different
-density seed): the FMM of one surface does not shard, so N GPUs run N
-independent matvecs (weak scaling, no collective on the data path).  The
-reference arm (--impl reference) times the reference's own CPU fmm() (built
-from its sources into oracle/_ref) on the host cores.
+Under torchrun each rank runs its own independent problem (a different point
+seed): one FMM does not shard here, so N GPUs run N independent problems (weak
+scaling, no collective on the data path).  The reference arm (--impl
+reference) times the reference's own CPU fmm() (built from its sources into
+oracle/_ref) on the host cores.
 """
 from __future__ import annotations
 
@@ -33,17 +40,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+# C2: Laplace Gnj double-layer matvec on an icosphere (--config bem, and a
+# secondary key of the headline line)
 P_ORDER = 10
 SUBDIV = 6
 LMAX = 5
 METRIC = "FMM matvec Mpts/s (Laplace Gn double-layer BEM, 245,760 pts, p=10)"
+# C3, the headline: Laplace G forward + backward on clustered points
+C3_N = 1 << 20
+C3_P = 12
+C3_SEED = 13
+C3_METRIC = "FMM matvec Mpts/s at rel err <=1e-6 vs FP64 direct; mixed+adjoint vs plain FP64"
+# the reference arm's bounded sample: the C3 point set cut into 16 disjoint
+# slices of 65,536 points, each one reference forward + adjoint at depth 4
+# (the reference's fastest depth for this size, measured), one process per
+# core; then single runs at 1/4 N (depth 5) and 1/2 N (depth 6) for the fit
+C3_REF_SLICES = 16
+C3_REF_LMAX = {C3_N // 16: 4, C3_N // 4: 5, C3_N // 2: 6}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-# DRAM bytes (read + write) of one launch on this workload, from the ncu
-# captures summarised in profiles/
-# DRAM bytes (read + write) per evaluate of the two dominant kernels, from one
-# ncu capture of this workload: P2P runs as two launches (7.03 MB read each, its
-# outputs stay in L2), the M2L as one; profiles/p2p_mixed_bem245k_p10.md,
-# profiles/translate_tc_m2l_bem245k_p10.md
+# DRAM bytes (read + write) per evaluate of the two dominant kernels of the C2
+# workload, from one ncu capture of it: P2P runs as two launches (7.03 MB read
+# each, its outputs stay in L2), the M2L as one.
 NCU_TRAFFIC = {"p2p_mixed": 2 * 7.026e6, "translate_tc": 170.88e6}
 
 
@@ -156,7 +173,7 @@ def cpu_reference_time(workers, rep=1, pool=None):
     return max(r[0] for r in res), sum(r[1] for r in res)
 
 
-def run_reference(args, rank, world):
+def run_reference_c2(args, rank, world):
     if rank != 0:
         return
     from oracle import pyoracle
@@ -183,6 +200,110 @@ def run_reference(args, rank, world):
                        "points_per_process": 15360, "processes": cores},
             "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": cores, "kind": "reference",
                              "sample": "reference fmm(ni,nj,2) at p=10 on a 15,360-point icosphere, one per core"},
+            "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def gaussian_clusters(n, seed, nclusters=32, sigma=0.02):
+    """n points from nclusters Gaussian clusters (centres U[0.1, 0.9]^3, the
+    given sigma) clipped to [0, 1]^3, and charges N(0, 1).  The first m points
+    of a draw are a draw of m points of the same mixture (labels are iid)."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0.1, 0.9, (3, nclusters))
+    lab = rng.integers(0, nclusters, n)
+    x = np.clip(c[:, lab] + sigma * rng.standard_normal((3, n)), 0.0, 1.0).astype(np.float32)
+    return x, rng.standard_normal(n).astype(np.float32)
+
+
+def c3_problem(seed):
+    """The headline point set, charges and backward weights w = dL/dpot."""
+    x, q = gaussian_clusters(C3_N, seed)
+    w = np.random.default_rng(seed + 1000).standard_normal(C3_N).astype(np.float32)
+    return x, q, w
+
+
+def _ref_c3_worker(job):
+    """One reference forward + adjoint (fmm(ni,nj,0) with charges q, then with
+    weights w; the position gradient w*grad(pot) + q*grad(psi) assembled in
+    numpy) on points [a, b) of the C3 set.  Returns the seconds of the two
+    fmm() calls without their tree builds (tfmm[0..13]) and the point count."""
+    from oracle import pyoracle
+    a, b, lmax = job
+    x, q, w = c3_problem(C3_SEED)
+    x, q, w = np.ascontiguousarray(x[:, a:b]), q[a:b].copy(), w[a:b].copy()
+    el = 0.0
+    for charges in (q, w):
+        tm = np.zeros(100)
+        t0 = time.perf_counter()
+        v, g = pyoracle.ref_fmm(x, x, charges, neq=0, p=C3_P, lmax=lmax, bbox=(0, 0, 0, 1), timings=tm, perf=True)
+        el += time.perf_counter() - t0 - float(tm[0:14].sum())
+        if charges is q:
+            field = g
+    t0 = time.perf_counter()
+    _dx = w * field + q * g
+    el += time.perf_counter() - t0
+    return el, b - a
+
+
+def c3_reference_fit(pool):
+    """One-core seconds of the reference forward + adjoint at 1/16, 1/4 and
+    1/2 of the C3 points (run side by side, one process each), the linear fit
+    t = a + b N through them and its value at the full N."""
+    sizes = sorted(C3_REF_LMAX)
+    res = pool.map(_ref_c3_worker, [(0, n, C3_REF_LMAX[n]) for n in sizes])
+    secs = [r[0] for r in res]
+    b, a = np.polyfit(np.asarray(sizes, float), np.asarray(secs), 1)
+    t_full = a + b * C3_N
+    return {"points": sizes, "lmax": [C3_REF_LMAX[n] for n in sizes], "one_core_s": secs,
+            "fit": "t = a + b N (least squares)", "a_s": float(a), "b_s_per_point": float(b),
+            "full_n_one_core_s": float(t_full), "full_n_one_core_mpts_s": C3_N / t_full / 1e6}
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU fmm() on the headline workload, all host cores
+    (one process per core: the reference is serial).  A step runs every one of
+    the 16 disjoint 65,536-point slices of the C3 point set through a
+    reference forward + adjoint; after the timed steps, single runs at 1/4 and
+    1/2 of the points give a linear fit to the full set."""
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    if not pyoracle.ref_available(C3_P, perf=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference library (p=12, perf) not built"}))
+        return
+    cores = os.cpu_count() or 1
+    n_slice = C3_N // C3_REF_SLICES
+    jobs = [(k * n_slice, (k + 1) * n_slice, C3_REF_LMAX[n_slice]) for k in range(C3_REF_SLICES)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(cores, C3_REF_SLICES)) as pool:
+        pool.map(_ref_c3_worker, [(0, 4096, 2)] * min(cores, C3_REF_SLICES))  # load the library in every worker
+        for _ in range(args.warmup):
+            pool.map(_ref_c3_worker, [(0, 4096, 2)] * min(cores, C3_REF_SLICES))
+        walls, one_core = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_c3_worker, jobs)
+            walls.append(time.perf_counter() - t0)
+            one_core.extend(r[0] for r in res)
+        fit = c3_reference_fit(pool)
+    ms_step = 1e3 * float(np.mean(walls))
+    value = C3_N / (ms_step * 1e-3) / 1e6
+    procs = min(cores, C3_REF_SLICES)
+    line = {"impl": "reference", "metric": C3_METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "Laplace G forward + adjoint (charges and positions), 1,048,576 points from 32 "
+                                   "Gaussian clusters (sigma 0.02) in [0,1]^3, q N(0,1), p=12: reference CPU fmm(), "
+                                   "bounded sample = the point set cut into 16 disjoint slices of 65,536 points, one "
+                                   "forward + adjoint each (depth 4), one process per core",
+                       "points_per_step": C3_N, "slices": C3_REF_SLICES, "processes": procs,
+                       "build": "reference sources, g++ -O3 -march=x86-64-v3 (oracle/Makefile perf)"},
+            "one_core_s_per_slice": float(np.mean(one_core)),
+            "full_n_fit": fit,
+            "cpu_baseline": {"value": value, "unit": "Mpts/s", "cores": procs, "kind": "reference",
+                             "sample": "reference fmm() forward + adjoint on 16 disjoint 65,536-point slices of the "
+                                       "1,048,576-point C3 set per step, one process per core; full-N one-core time "
+                                       "from the linear fit in full_n_fit"},
             "e2e": {"value": value, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -228,7 +349,72 @@ def setup_line(plan, npts, ms_step):
 
 
 # ------------------------------------------------------------------ our arm
-def run_ours(args, rank, world):
+def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, traffic=None):
+    """Rooflines of the two dominant kernels, from their CUDA-event durations
+    in timed steps (phase timers on the launching streams; phase_alone = the
+    same steps with the near field run after the far field):
+      * p2p_mixed: 20 flops per algorithmic pair (Laplace G: differences 3,
+        r^2 6, rsqrt 1, r^-3 2, q r^-1 and q r^-3 2, potential 1, gradient 6;
+        Gni/Gnj: the normal dot in place of the gradient); bound by the FP32
+        pipes (peak 148 SMs x 128 lanes x 2 flops at the maximum SM clock);
+      * M2L (translate_tc + its pair-row reduction): 2 K^2 algorithmic flops
+        per box pair on the tensor cores; TF32 peak = half the measured dense
+        bf16;
+    and the whole matvec against the sum of its phases' roofline times
+    (algorithmic work of each phase over the peak of the unit it runs on: P2P,
+    P2M, L2P FP32; M2L TF32; M2M, L2L FP64 at the nominal 37 TFLOP/s).
+    traffic: DRAM bytes of one launch from an ncu capture, or None.
+    Returns (dominant, other, matvec)."""
+    st = plan.stats()
+    peaks, peak_kind = measured_peaks()
+    traffic = traffic or {}
+    names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
+    K = (p + 1) ** 2
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    p2p_ach = 20.0 * st["p2p_pairs"] / (phase_alone[0] * 1e-3) / 1e12
+    tf32_peak = peaks["bf16_tflops"] / 2
+    m2l_ach = 2.0 * K * K * st["m2l_pairs"] / (phase_alone[3] * 1e-3) / 1e12
+    roof_p2p = {"kernel": "p2p_mixed" if mixed else "p2p_f64", "bound": "fp32", "achieved": p2p_ach,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": p2p_ach / fp32_peak,
+                "traffic": traffic.get("p2p_mixed"), "ms": float(phase_alone[0]),
+                "ms_in_overlapped_step": float(phase[0]),
+                "note": f"20 flops per algorithmic pair ({st['p2p_pairs']} pairs); ms = the kernel's own launches "
+                        f"(near field not overlapped), summed per step; peak = nominal FP32 at "
+                        f"{sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)"}
+    roof_m2l = {"kernel": "translate_tc+reduce_pairs (M2L)" if mixed else "translate_f64 (M2L)", "bound": "tensor",
+                "achieved": m2l_ach, "peak": tf32_peak if mixed else None, "unit": "TFLOP/s",
+                "frac": (m2l_ach / tf32_peak) if mixed else None,
+                "traffic": traffic.get("translate_tc"), "ms": float(phase_alone[3]),
+                "ms_in_overlapped_step": float(phase[3]),
+                "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
+                        f"execute 3 TF32 MMAs per product on operators padded to 128-row blocks; peak = TF32 dense "
+                        f"= half of {peak_kind} bf16"}
+    nb_i, nb_j = plan.tree(4), plan.tree(5)
+    fp64_peak = 37.0
+    ideal = {"p2p": 20.0 * st["p2p_pairs"] / fp32_peak,
+             "p2m": 2.0 * npts * K / fp32_peak,
+             "m2m": 2.0 * K * K * float(nb_j[3:lmax + 1].sum()) / fp64_peak,
+             "m2l": 2.0 * K * K * st["m2l_pairs"] / tf32_peak,
+             "l2l": 2.0 * K * K * float(nb_i[3:lmax + 1].sum()) / fp64_peak,
+             "l2p": 2.0 * npts * K / fp32_peak}
+    ideal = {k: v / 1e9 for k, v in ideal.items()}  # flops / (TFLOP/s) -> ms
+    matvec_roof = {"ideal_ms": ideal, "sum_ideal_ms": sum(ideal.values()), "step_ms": ms_step,
+                   "frac_of_step": sum(ideal.values()) / ms_step,
+                   "frac_per_phase_alone": {k: ideal[k] / float(phase_alone[i]) for i, k in enumerate(names)},
+                   "note": "algorithmic flops per phase (P2P 20 per pair, P2M/L2P 2(p+1)^2 per point, M2L/M2M/L2L "
+                           "2(p+1)^4 per box pair) over FP32 (nominal), TF32 (half the measured bf16) and FP64 "
+                           "(nominal 37) peaks"}
+    dom = int(np.argmax(phase_alone[:6]))
+    if names[dom] == "m2l":
+        return roof_m2l, roof_p2p, matvec_roof
+    return roof_p2p, roof_m2l, matvec_roof
+
+
+def run_ours(args, rank, world, secondary=False):
+    """The C2 workload (--config bem): Laplace Gnj double-layer matvec on the
+    icosphere.  secondary: no CPU baseline, and a compact dict returned
+    instead of the printed line (the headline line carries it)."""
     import torch
     import old_fmm_bem_b200 as ob
 
@@ -312,59 +498,12 @@ def run_ours(args, rank, world):
     pot64, _ = plan.evaluate(q, f64=True)
     err = rel_err_vs_direct(ob, ob.LAPLACE_GNJ, x, x, q, pot64, n_s=n)
     st = plan.stats()
-    peaks, peak_kind = measured_peaks()
     names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
-    K = (P_ORDER + 1) ** 2
-    # Rooflines of the two dominant kernels, from their CUDA-event durations in
-    # the timed steps above (phase timers on the launching streams).
-    #  * p2p_mixed: 20 flops per algorithmic pair (3 sub, 3 fma for r^2, rsqrt,
-    #    r^-3, the normal dot and the accumulation); bound by the FP32 pipes
-    #    (peak 148 SMs x 128 lanes x 2 flops at the maximum SM clock).
-    #  * M2L (translate_tc + its pair-row reduction): 2 K^2 algorithmic flops per
-    #    box pair on the tensor cores; TF32 peak = half the measured dense bf16.
-    # traffic: DRAM bytes of one launch from ncu (profiles/*.md), or None.
-    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
-    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
-    p2p_ach = 20.0 * st["p2p_pairs"] / (phase_alone[0] * 1e-3) / 1e12
-    tf32_peak = peaks["bf16_tflops"] / 2
-    m2l_ach = 2.0 * K * K * st["m2l_pairs"] / (phase_alone[3] * 1e-3) / 1e12
-    roof_p2p = {"kernel": "p2p_mixed", "bound": "fp32", "achieved": p2p_ach, "peak": fp32_peak, "unit": "TFLOP/s",
-                "frac": p2p_ach / fp32_peak, "traffic": NCU_TRAFFIC.get("p2p_mixed"),
-                "ms": float(phase_alone[0]), "ms_in_overlapped_step": float(phase[0]),
-                "note": f"20 flops per algorithmic pair ({st['p2p_pairs']} pairs); ms = the kernel's own launches "
-                        f"(near field not overlapped), summed per step; peak = nominal FP32 at "
-                        f"{sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)"}
-    roof_m2l = {"kernel": "translate_tc+reduce_pairs (M2L)", "bound": "tensor", "achieved": m2l_ach,
-                "peak": tf32_peak if args.precision == "mixed" else None, "unit": "TFLOP/s",
-                "frac": (m2l_ach / tf32_peak) if args.precision == "mixed" else None,
-                "traffic": NCU_TRAFFIC.get("translate_tc"), "ms": float(phase_alone[3]),
-                "ms_in_overlapped_step": float(phase[3]),
-                "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
-                        f"execute 3 TF32 MMAs per product on 128x128 padded operators; peak = TF32 dense = half of "
-                        f"{peak_kind} bf16"}
-    # whole matvec against the sum of its phases' roofline times: algorithmic
-    # work of each phase over the peak of the unit it runs on (P2P, P2M, L2P:
-    # FP32; M2L: TF32; M2M, L2L: FP64 at the nominal 37 TFLOP/s)
-    nb_i, nb_j = plan.tree(4), plan.tree(5)
-    fp64_peak = 37.0
-    ideal = {"p2p": 20.0 * st["p2p_pairs"] / fp32_peak,
-             "p2m": 2.0 * npts * K / fp32_peak,
-             "m2m": 2.0 * K * K * float(nb_j[3:LMAX + 1].sum()) / fp64_peak,
-             "m2l": 2.0 * K * K * st["m2l_pairs"] / tf32_peak,
-             "l2l": 2.0 * K * K * float(nb_i[3:LMAX + 1].sum()) / fp64_peak,
-             "l2p": 2.0 * npts * K / fp32_peak}
-    ideal = {k: v / 1e9 for k, v in ideal.items()}  # flops / (TFLOP/s) -> ms
-    matvec_roof = {"ideal_ms": ideal, "sum_ideal_ms": sum(ideal.values()), "step_ms": ms_step,
-                   "frac_of_step": sum(ideal.values()) / ms_step,
-                   "frac_per_phase_alone": {k: ideal[k] / float(phase_alone[i]) for i, k in enumerate(names)},
-                   "note": "algorithmic flops per phase (P2P 20 per pair, P2M/L2P 2(p+1)^2 per point, M2L/M2M/L2L "
-                           "2(p+1)^4 per box pair) over FP32 (nominal), TF32 (half the measured bf16) and FP64 "
-                           "(nominal 37) peaks"}
-    dom = int(np.argmax(phase_alone[:6]))
-    roof = roof_m2l if names[dom] == "m2l" else roof_p2p
+    roof, roof2, matvec_roof = phase_rooflines(plan, P_ORDER, LMAX, npts, phase, phase_alone, ms_step,
+                                               args.precision == "mixed", NCU_TRAFFIC)
     # CPU baseline: the reference's own fmm() on a bounded sample, one core
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and not secondary:
         try:
             from oracle import pyoracle
             if pyoracle.ref_available(P_ORDER):
@@ -388,7 +527,7 @@ def run_ours(args, rank, world):
         "phase_ms_alone": dict(zip(names + ["total"], [float(v) for v in phase_alone])),
         "stats": st,
         "roofline": roof,
-        "roofline_secondary": roof_p2p if roof is roof_m2l else roof_m2l,
+        "roofline_secondary": roof2,
         "matvec_roofline": matvec_roof,
         "cpu_baseline": cpu,
         "e2e": {"value": world * npts / e2e_s / 1e6, "unit": "Mpts/s", "h2d_bytes_per_step": 4 * npts,
@@ -397,8 +536,12 @@ def run_ours(args, rank, world):
         "setup": setup_line(plan, npts, ms_step),
         "clocks": clk.summary(),
     }
-    print(json.dumps(line))
     plan.close()
+    if secondary:
+        return {k: line[k] for k in ("metric", "value", "unit", "ms_per_step", "dtype", "config",
+                                     "rel_err_vs_fp64_direct", "phase_ms", "phase_ms_alone", "stats", "roofline",
+                                     "roofline_secondary", "matvec_roofline", "e2e", "setup", "clocks")}
+    print(json.dumps(line))
 
 
 # ------------------------------------------------------------------ other configurations
@@ -428,14 +571,6 @@ def _timed(step, stream, steps, warmup, flush, out=None):
 def uniform_cube(n, seed):
     rng = np.random.default_rng(seed)
     return rng.random((3, n), dtype=np.float32), rng.uniform(-1, 1, n).astype(np.float32)
-
-
-def gaussian_clusters(n, seed, nclusters=32, sigma=0.02):
-    rng = np.random.default_rng(seed)
-    c = rng.uniform(0.1, 0.9, (3, nclusters))
-    lab = rng.integers(0, nclusters, n)
-    x = np.clip(c[:, lab] + sigma * rng.standard_normal((3, n)), 0.0, 1.0).astype(np.float32)
-    return x, rng.standard_normal(n).astype(np.float32)
 
 
 def run_c1(args):
@@ -476,58 +611,215 @@ def run_c1(args):
     plan.close()
 
 
-def run_c3(args):
-    """Adjoint: Laplace G as a torch.autograd operator, 1,048,576 points from 32
-    Gaussian clusters (sigma 0.02) in the unit cube, charges N(0,1); one step =
-    forward + backward (gradients w.r.t. charges and positions), mixed and FP64
-    forms, octree depth from the autotuner (fmmb_autotune_lmax) for each form.
-    p = 10 is the configuration's order; p = 12 is the lowest order whose
-    potential meets rel err <= 1e-6 here, measured alongside."""
+def run_headline(args, rank, world):
+    """The headline (C3): Laplace G as a torch.autograd operator on 1,048,576
+    clustered points, p = 12; one step = forward + backward (gradients w.r.t.
+    charges and positions of L = sum(w * pot)); mixed form timed over the
+    driver's steps, the plain FP64 form beside it; octree depth of each form
+    from fmmb_autotune_lmax.  Rank r runs its own point set (seed 13 + r)."""
     import torch
     import old_fmm_bem_b200 as ob
     from old_fmm_bem_b200.autograd import FMMOperator
-    x, q = gaussian_clusters(1 << 20, 13)
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    x, q, w = c3_problem(C3_SEED + rank)
     n = x.shape[1]
+    bbox = (0.0, 0.0, 0.0, 1.0)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    stream = torch.cuda.current_stream()
-    w = torch.randn(n, device="cuda", dtype=torch.float64, generator=torch.Generator("cuda").manual_seed(5))
+    stream = torch.cuda.Stream()
     xd = torch.from_numpy(x).cuda()
+    qd = torch.from_numpy(q).cuda()
+    wd = torch.from_numpy(w).cuda().to(torch.float64)
+    kw = dict(kernel=ob.LAPLACE_G, p=C3_P, semantics=ob.SEM_ACCURATE, exclude_self=True, bbox=bbox)
+
+    def make(prec):
+        lmax, tune = ob.autotune_lmax(xd, xd, precision=prec, reps=2, **kw)
+        X = xd.clone().requires_grad_(True)
+        Q = qd.to(torch.float64).requires_grad_(True)
+        op = FMMOperator(X, X, kernel=ob.LAPLACE_G, p=C3_P, lmax=lmax, precision=prec, bbox=bbox)
+        box = {}
+
+        def fwd():
+            box["pot"] = op(Q)
+
+        def fwd_bwd():
+            X.grad = None
+            Q.grad = None
+            (op(Q) * wd).sum().backward()
+
+        return op, X, Q, fwd, fwd_bwd, lmax, tune
+
     res = {}
-    for p in (10, 12):
-        for name, prec in (("mixed", ob.MIXED), ("fp64", ob.FP64)):
-            lmax, tune = ob.autotune_lmax(xd, xd, kernel=ob.LAPLACE_G, p=p, precision=prec, semantics=ob.SEM_ACCURATE,
-                                          exclude_self=True, bbox=(0, 0, 0, 1), reps=2)
-            X = xd.clone().requires_grad_(True)
-            Q = torch.from_numpy(q).cuda().to(torch.float64).requires_grad_(True)
-            op = FMMOperator(X, X, kernel=ob.LAPLACE_G, p=p, lmax=lmax, precision=prec, bbox=(0, 0, 0, 1))
-            box = {}
+    with ClockSampler(dev) as clk:
+        # mixed form: the driver's steps
+        op, X, Q, fwd, fwd_bwd, lmax, tune = make(ob.MIXED)
+        t_f = _timed(fwd, stream, max(3, args.steps // 2), max(3, args.warmup), flush)
+        per_step = []
+        t_fb = _timed(fwd_bwd, stream, args.steps, max(3, args.warmup), flush, per_step)
+        ph = np.array(list(op.plan.timings().values()))
+        launches = op.plan.stats()["launches"]
+    # each kernel's own duration: one evaluate with gradient, near field after
+    # the far field (phase timers, CUDA events on the launching streams)
+    op.plan.set_overlap(False)
+    ph_alone = np.zeros(7)
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            fwd()
+        for k in range(max(3, args.steps // 2)):
+            flush.fill_(float(k))
+            fwd()
+            stream.synchronize()
+            ph_alone += np.array(list(op.plan.timings().values()))
+    ph_alone /= max(3, args.steps // 2)
+    op.plan.set_overlap(True)
+    t_fb_job = max_over_ranks(t_fb, world)
 
-            def fwd():
-                box["pot"] = op(Q)
+    # end to end through the C ABI with pinned host buffers: charges and
+    # weights in, potential, charge gradient and position gradients out (the
+    # forward's field stays on the device for the backward)
+    plan = op.plan
+    qh = torch.from_numpy(q).pin_memory()
+    wh = torch.from_numpy(w).pin_memory()
+    f64h = [torch.zeros(k * n, dtype=torch.float64).pin_memory() for k in (1, 1, 3, 3)]
+    field_d = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+    e2e = []
+    with torch.cuda.stream(stream):
+        for k in range(max(3, args.steps // 2) + 2):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            plan.evaluate(qh.numpy(), f64h[0].numpy(), field_d, f64=True)
+            plan.adjoint(qh.numpy(), wh.numpy(), field_d, f64h[1].numpy(), f64h[2].numpy(), f64h[3].numpy(),
+                         want_dxs=True)
+            e2e.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(float(np.median(e2e[2:])), world)
 
-            def fwd_bwd():
-                X.grad = None
-                Q.grad = None
-                (op(Q) * w).sum().backward()
+    # plain FP64 form, same step
+    op64, X64, Q64, fwd64, fwd_bwd64, lmax64, tune64 = make(ob.FP64)
+    t_f64 = _timed(fwd64, stream, min(args.steps, 5), 2, flush)
+    t_fb64 = _timed(fwd_bwd64, stream, min(args.steps, 5), 2, flush)
 
-            t_f = _timed(fwd, stream, args.steps, max(3, args.warmup), flush)
-            t_fb = _timed(fwd_bwd, stream, args.steps, max(3, args.warmup), flush)
-            pot = box["pot"].detach().cpu().numpy()
-            field = op.plan.evaluate(q, f64=True)[1]
-            res[f"p{p}_{name}"] = {"lmax": lmax, "autotune_ms": tune, "forward_ms": t_f, "forward_backward_ms": t_fb,
-                                   "backward_over_forward": (t_fb - t_f) / t_f,
-                                   "rel_err_vs_fp64_direct": rel_err_vs_direct(ob, ob.LAPLACE_G, x, x, q, pot, field)}
-            op.close()
-    m = res["p10_mixed"]
-    print(json.dumps({"metric": "FMM matvec + adjoint Mpts/s (Laplace G, 1,048,576 clustered points, p=10)",
-                      "value": n / (m["forward_backward_ms"] * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1,
-                      "steps": args.steps, "dtype": "f32+tf32x3+f64", "data": "synthetic",
-                      "config": {"workload": "Laplace G, 1,048,576 points from 32 Gaussian clusters (sigma 0.02) in "
-                                             "[0,1]^3, q N(0,1), p=10 (and p=12); step = forward + backward (charges "
-                                             "and positions); lmax from fmmb_autotune_lmax"},
-                      "results": res,
-                      "mixed_speedup_over_fp64": {f"p{p}": res[f"p{p}_fp64"]["forward_backward_ms"] /
-                                                  res[f"p{p}_mixed"]["forward_backward_ms"] for p in (10, 12)}}))
+    # C2 (the Gnj BEM matvec on the icosphere) as a secondary key
+    c2 = run_ours(args, rank, world, secondary=True)
+
+    if rank != 0:
+        op.close()
+        op64.close()
+        return
+    # accuracy on 1,024 random points against FP64 direct sums: potential,
+    # field, charge gradient psi = A^T w and position gradient w grad(pot) +
+    # q grad(psi), for both forms
+    sel = np.sort(np.random.default_rng(7).choice(n, size=1024, replace=False))
+    pd = ob.Plan(kernel=ob.LAPLACE_G, p=4, lmax=2, precision=ob.FP64, semantics=ob.SEM_ACCURATE, exclude_self=True)
+    pd.set_geometry(np.ascontiguousarray(x[:, sel]), x)
+    vd, gd = pd.direct(q)
+    psid, gpsid = pd.direct(w)
+    pd.close()
+    dxd = w[sel] * gd + q[sel] * gpsid
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    errs = {}
+    for name, o in (("mixed", op), ("fp64", op64)):
+        pot, field = o.plan.evaluate(q, f64=True)
+        dq, dxt, dxs = o.plan.adjoint(q, w, field, want_dxs=True)
+        dx = (dxt + dxs).reshape(3, -1)[:, sel]
+        errs[name] = {"pot": rel(pot[sel], vd), "field": rel(field.reshape(3, -1)[:, sel], gd),
+                      "dq": rel(dq[sel], psid), "dx": rel(dx, dxd), "targets": 1024}
+    fd = c3_finite_differences(ob, x, q, w, lmax, ob.MIXED, args.fd)
+    st = op.plan.stats()
+    roof, roof2, matvec_roof = phase_rooflines(op.plan, C3_P, lmax, n, ph, ph_alone, t_f, True)
+    # CPU baseline: the reference's own forward + adjoint on one 65,536-point
+    # slice of this point set, one core
+    cpu = None
+    if not args.no_cpu:
+        try:
+            from oracle import pyoracle
+            if pyoracle.ref_available(C3_P, perf=True):
+                el, npt = _ref_c3_worker((0, C3_N // C3_REF_SLICES, C3_REF_LMAX[C3_N // C3_REF_SLICES]))
+                cpu = {"value": npt / el / 1e6, "unit": "Mpts/s", "cores": 1, "kind": "reference",
+                       "sample": "reference fmm() forward + adjoint (two fmm(ni,nj,0) calls, tree builds excluded) "
+                                 "at p=12, depth 4, on the first 65,536 points of this set, 1 core"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"error": str(e)}
+    setup = setup_line(op.plan, n, t_f)
+    op.close()
+    op64.close()
+    line = {
+        "metric": C3_METRIC, "value": job_mpts_s(world, n, t_fb_job), "unit": "Mpts/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fb_job, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+tf32x3+f64", "data": "synthetic",
+        "config": {"workload": "Laplace G FMM forward + backward (torch.autograd: gradients w.r.t. charges and "
+                               "positions of sum(w*pot)), 1,048,576 points from 32 Gaussian clusters (sigma 0.02) in "
+                               "[0,1]^3, q N(0,1), w N(0,1), p=12, mixed precision, self pairs excluded",
+                   "points": n, "p": C3_P, "lmax": lmax, "lmax_fp64": lmax64, "precision": "mixed",
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "rel_err_vs_fp64_direct": errs["mixed"],
+        "rel_err_fp64_form": errs["fp64"],
+        "finite_differences": fd,
+        "forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": (t_fb - t_f) / t_f,
+        "ms_per_step_each": per_step,
+        "fp64_form": {"lmax": lmax64, "forward_ms": t_f64, "forward_backward_ms": t_fb64,
+                      "backward_over_forward": (t_fb64 - t_f64) / t_f64, "autotune_ms": tune64},
+        "mixed_over_fp64": t_fb64 / t_fb,
+        "autotune_ms": tune,
+        "phase_ms": dict(zip(["p2p", "p2m", "m2m", "m2l", "l2l", "l2p", "total"], [float(v) for v in ph])),
+        "phase_ms_alone": dict(zip(["p2p", "p2m", "m2m", "m2l", "l2l", "l2p", "total"],
+                                   [float(v) for v in ph_alone])),
+        "stats": st,
+        "roofline": roof,
+        "roofline_secondary": roof2,
+        "matvec_roofline": matvec_roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * n / e2e_s / 1e6, "unit": "Mpts/s", "ms": 1e3 * e2e_s,
+                "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 64 * n,
+                "note": "fmmb_evaluate_f64 (q in; potential out, field kept on the device) + fmmb_adjoint_f64 "
+                        "(q, w in; dq, dL/dx_t, dL/dx_s out), pinned host buffers"},
+        "gpu_launches": (2 * launches + 2) * args.steps,
+        "setup": setup,
+        "c2_bem_gnj": c2,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line))
+
+
+def c3_finite_differences(ob, x, q, w, lmax, prec, ncoord, h=1e-4):
+    """Central differences of L = sum(w * pot) w.r.t. ncoord random
+    coordinates (step h; each side a fresh tree on the moved point set)
+    against the backward's position gradient, in the given form."""
+    if ncoord <= 0:
+        return None
+    rng = np.random.default_rng(11)
+    pts = rng.choice(x.shape[1], size=ncoord, replace=False)
+    dims = rng.integers(0, 3, ncoord)
+    plan = ob.Plan(kernel=ob.LAPLACE_G, p=C3_P, lmax=lmax, precision=prec, semantics=ob.SEM_ACCURATE,
+                   exclude_self=True)
+    bbox = (0.0, 0.0, 0.0, 1.0)
+    plan.set_geometry(x, x, bbox=bbox)
+    pot, field = plan.evaluate(q, f64=True)
+    _, dxt, dxs = plan.adjoint(q, w, field, want_dxs=True)
+    grad = (dxt + dxs).reshape(3, -1)
+    t0 = time.perf_counter()
+    fdv = np.zeros(ncoord)
+    xm = x.copy()
+    w64 = w.astype(np.float64)
+    for k, (i, d) in enumerate(zip(pts, dims)):
+        vals = []
+        for sgn in (1.0, -1.0):
+            xm[d, i] = np.float32(x[d, i] + sgn * h)
+            plan.set_geometry(xm, xm, bbox=bbox)
+            vals.append(float(w64 @ plan.evaluate(q, f64=True)[0]))
+        hh = float(np.float32(x[d, i] + h)) - float(np.float32(x[d, i] - h))  # the float32 step taken
+        xm[d, i] = x[d, i]
+        fdv[k] = (vals[0] - vals[1]) / hh
+    an = grad[dims, pts]
+    plan.close()
+    return {"coordinates": ncoord, "h": h, "rel_err": float(np.linalg.norm(fdv - an) / np.linalg.norm(an)),
+            "max_abs_rel": float(np.max(np.abs(fdv - an) / np.maximum(np.abs(an), 1e-30))),
+            "seconds": time.perf_counter() - t0,
+            "note": "central differences of sum(w * pot) over fresh trees, against the backward's dL/dx"}
 
 
 def run_c4(args):
@@ -751,10 +1043,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--lmax", type=int, default=0,
                     help="batch64 / helmholtz1m: this octree depth instead of the autotuner's")
-    ap.add_argument("--config", default="bem", choices=["bem", "uniform32k", "adjoint1m", "batch64",
-                                                     "batch64_matvec", "helmholtz1m"],
-                    help="bem: the headline Gnj BEM matvec (default); uniform32k: FP64 Laplace G on 32,768 uniform "
-                         "points; adjoint1m: forward + backward on 1,048,576 clustered points; batch64: GMRES on 64 "
+    ap.add_argument("--fd", type=int, default=64, help="adjoint1m: finite-difference coordinates (0: none)")
+    ap.add_argument("--config", default="adjoint1m", choices=["bem", "uniform32k", "adjoint1m", "batch64",
+                                                           "batch64_matvec", "helmholtz1m"],
+                    help="adjoint1m: the headline, Laplace G forward + backward on 1,048,576 clustered points, p=12 "
+                         "(default); bem: the Gnj BEM matvec on a 245,760-point icosphere; uniform32k: FP64 Laplace G "
+                         "on 32,768 uniform points; batch64: GMRES on 64 "
                          "BEM problems x 8 right-hand sides; batch64_matvec: its matvec alone, 1 and 8 "
                          "right-hand sides; helmholtz1m: complex Helmholtz, "
                          "1,048,576 sphere points, k=5, p=16")
@@ -768,11 +1062,14 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.impl == "reference":
-        run_reference(args, rank, world)
+        if args.config == "bem":
+            run_reference_c2(args, rank, world)
+        else:
+            run_reference(args, rank, world)
     elif args.config == "uniform32k":
         run_c1(args)
     elif args.config == "adjoint1m":
-        run_c3(args)
+        run_headline(args, rank, world)
     elif args.config == "batch64":
         run_c4(args)
     elif args.config == "batch64_matvec":
@@ -780,7 +1077,7 @@ def main():
     elif args.config == "helmholtz1m":
         run_c5(args)
     else:
-        run_ours(args, rank, world)
+        run_ours(args, rank, world)  # bem
     if world > 1 and args.impl == "ours":
         import torch
         torch.distributed.destroy_process_group()

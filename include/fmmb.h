@@ -146,6 +146,19 @@ FMMB_API int fmmb_evaluate_transpose_f64(fmmb_plan* plan, const float* w, double
  * one transposed matvec, both with gradient.  No reference counterpart. */
 FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w, double* dxt, double* dxs);
 
+/* The backward pass of one matvec pot = A q for L = sum_i w_i pot_i, given
+ * the forward's field: dq[nj] = A^T w (the transposed matvec, as
+ * fmmb_evaluate_transpose_f64), dxs[3 nj] = q * grad(psi)(x_s) with
+ * psi = A^T w, and dxt[3 ni] = w * field_t, field_t[3 ni] being the gradient
+ * output of the forward fmmb_evaluate_f64 with the same q.  Any of dq, dxs,
+ * dxt may be NULL (dxt needs field_t); position gradients are for the
+ * Laplace G kernel.  Costs one transposed matvec (with gradient when dxs is
+ * asked for); host or device pointers.  When the targets and sources were
+ * given as the same arrays the transposed matvec runs on this plan.  No
+ * reference counterpart (the reference has no adjoint). */
+FMMB_API int fmmb_adjoint_f64(fmmb_plan* plan, const float* q, const float* w, const double* field_t, double* dq,
+                              double* dxt, double* dxs);
+
 /* Direct O(ni*nj) sum on the GPU with the plan's kernel and semantics
  * (replaces G_dir/Gni_dir/Gnj_dir, kernel/G_dir.cxx:6-30,
  * kernel/Gni_dir.cxx:6-21, kernel/Gnj_dir.cxx:6-21), FP64 arithmetic.  Uses
@@ -238,15 +251,20 @@ FMMB_API int fmmb_gmres(fmmb_plan* plan, const fmmb_gmres_config* cfg, const flo
  * captured into a CUDA graph.  Same arithmetic as fmmb_direct_f64 (FP64, the
  * kernel, semantics, eps2 and exclude_self of cfg; the other fields are
  * ignored), float outputs pot[ni] and, for FMMB_LAPLACE_G, grad[3*ni] (may be
- * NULL).  Every pointer must be device (or managed) memory; work is queued on
- * `stream` (a cudaStream_t, NULL = the legacy default stream).
+ * NULL).  Every pointer must be device memory of the current device (or
+ * managed memory), else FMMB_ERR_ARG; work is queued on `stream` (a
+ * cudaStream_t, NULL = the legacy default stream).
  * The FP64 partial sums of its source split live in one static device array of
- * FMMB_STATIC_SCRATCH_BYTES per device: ncomp * ni must not exceed
+ * FMMB_STATIC_SCRATCH_BYTES per device, reserved on every device that loads
+ * this library's device code (at module load, whether or not this entry point
+ * is called): ncomp * ni must not exceed
  * FMMB_STATIC_SCRATCH_BYTES / 8 (ncomp = 4 for G with grad, else 1), larger
  * sizes return FMMB_ERR_CAPACITY.  All calls on a device share that array:
  * calls that overlap on the GPU race and must be ordered by the caller.  The
  * first call on a device (that device current) looks the array up with
- * cudaGetSymbolAddress; make it before any stream capture. */
+ * cudaGetSymbolAddress and keeps its address for the life of the process;
+ * make it before any stream capture, and do not reset the device
+ * (cudaDeviceReset) after it. */
 #define FMMB_STATIC_SCRATCH_BYTES (16u << 20)
 FMMB_API int fmmb_direct_static(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
                                 const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,

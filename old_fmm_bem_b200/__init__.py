@@ -36,7 +36,7 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
            "fmmb_gmres", "fmmb_autotune_lmax_batch", "fmmb_gpu_p2p",
-           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times", "fmmb_set_overlap"]
+           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times", "fmmb_set_overlap", "fmmb_adjoint_f64"]
 
 
 def lib_path() -> str:
@@ -85,6 +85,7 @@ def load():
     lib.fmmb_evaluate_transpose.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_evaluate_transpose_f64.argtypes = [_vp, _vp, _vp, _vp]
     lib.fmmb_position_grad.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    lib.fmmb_adjoint_f64.argtypes = [_vp] * 7
     lib.fmmb_autotune_lmax.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
         [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
     lib.fmmb_gpu_p2p.argtypes = [_vp] * 15
@@ -324,6 +325,26 @@ class Plan:
         self._follow_torch(q, w, dxt, dxs)
         _check(load().fmmb_position_grad(self._h, qp, wp, tp, sp))
         return tk.reshape(3, -1), sk.reshape(3, -1)
+
+    def adjoint(self, q, w, field_t=None, dq=None, dxt=None, dxs=None, *, want_dq=True, want_dxs=False):
+        """Backward pass of pot = A q for L = sum(w * pot) (fmmb_adjoint_f64):
+        dq = A^T w, dxs = q * grad(A^T w)(x_s) and, when the forward's field
+        field_t (3 * ni) is given, dxt = w * field_t.  FP64 outputs (numpy
+        unless torch CUDA tensors are given); returns (dq, dxt, dxs), None for
+        the ones not asked for."""
+        qp, qk = _ptr(q, np.float32) if q is not None else (None, None)
+        wp, wk = _ptr(w, np.float32)
+        fp, fk = _ptr(field_t, np.float64) if field_t is not None else (None, None)
+        if dq is None and want_dq:
+            dq = np.zeros(self.nj * self.nrhs)
+        if dxs is None and want_dxs:
+            dxs = np.zeros(3 * self.nj)
+        if dxt is None and field_t is not None:
+            dxt = np.zeros(3 * self.ni)
+        outs = [(_ptr(a, np.float64) if a is not None else (None, None)) for a in (dq, dxt, dxs)]
+        self._follow_torch(q, w, field_t, dq, dxt, dxs)
+        _check(load().fmmb_adjoint_f64(self._h, qp, wp, fp, outs[0][0], outs[1][0], outs[2][0]))
+        return tuple(o[1] for o in outs)
 
     def direct(self, q, i0=0, i1=None):
         """FP64 direct sum on the GPU for targets [i0, i1) (caller order)."""

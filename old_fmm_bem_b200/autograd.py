@@ -88,20 +88,23 @@ class FMMFunction(torch.autograd.Function):
         (qd,) = ctx.saved_tensors
         op = ctx.op
         wd = w.detach().to(torch.float32).contiguous()
-        # transposed FMM (fmmb_evaluate_transpose): targets x_s, sources x_t,
-        # charges w; the sign of the normal-derivative kernels is applied there
-        adj = torch.zeros(op.nj, dtype=torch.float64, device=w.device)
-        want_field = op.kernel == LAPLACE_G and ctx.needs[1]
-        field = torch.zeros(3 * op.nj, dtype=torch.float64, device=w.device) if want_field else None
-        op.plan.evaluate_transpose(wd, adj, field, f64=True)
-        dq = adj.to(w.dtype)
-        dxt = dxs = None
-        if op.kernel == LAPLACE_G:
-            if ctx.needs[0]:
-                dxt = (w.to(torch.float64) * ctx.field).to(w.dtype)
-            if ctx.needs[1]:
-                dxs = (qd.to(torch.float64) * field.view(3, op.nj)).to(w.dtype)
-        return dq, dxt, dxs, None
+        # one library call (fmmb_adjoint_f64): the transposed FMM (targets x_s,
+        # sources x_t, charges w; the sign of the normal-derivative kernels is
+        # applied there; on one point set the plan itself for G) and the
+        # weighting of the two fields
+        f64 = dict(dtype=torch.float64, device=w.device)
+        want_q = ctx.needs_input_grad[0]
+        want_xt = op.kernel == LAPLACE_G and ctx.needs[0]
+        want_xs = op.kernel == LAPLACE_G and ctx.needs[1]
+        dq = torch.empty(op.nj, **f64) if want_q else None
+        dxt = torch.empty(3 * op.ni, **f64) if want_xt else None
+        dxs = torch.empty(3 * op.nj, **f64) if want_xs else None
+        if want_q or want_xt or want_xs:
+            op.plan.adjoint(qd, wd, ctx.field.reshape(-1) if want_xt else None, dq, dxt, dxs,
+                            want_dq=want_q, want_dxs=want_xs)
+        return (dq.to(w.dtype) if dq is not None else None,
+                dxt.view(3, op.ni).to(w.dtype) if dxt is not None else None,
+                dxs.view(3, op.nj).to(w.dtype) if dxs is not None else None, None)
 
 
 def fmm_potential(x_t, x_s, q, *, kernel=LAPLACE_G, n_t=None, n_s=None, p=10, lmax=4, precision=MIXED,

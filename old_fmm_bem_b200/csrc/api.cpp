@@ -201,7 +201,7 @@ int fmmb_plan_destroy(fmmb_plan* pl) {
   cudaDeviceSynchronize();
   for (auto& g : pl->gexec)
     if (g) cudaGraphExecDestroy(g);
-  if (pl->tplan) fmmb_plan_destroy(pl->tplan);
+  if (pl->tplan && pl->tplan != pl) fmmb_plan_destroy(pl->tplan);
   if (pl->own_stream && pl->st.main) cudaStreamDestroy(pl->st.main);
   if (pl->st.side) cudaStreamDestroy(pl->st.side);
   if (pl->st.cap) cudaStreamDestroy(pl->st.cap);
@@ -224,7 +224,7 @@ int fmmb_set_stream(fmmb_plan* pl, void* stream) {
     if (pl->own_stream && pl->st.main) FMMB_CUDA(cudaStreamDestroy(pl->st.main));
     pl->st.main = (cudaStream_t)stream;
     pl->own_stream = false;
-    if (pl->tplan) {
+    if (pl->tplan && pl->tplan != pl) {
       const int rc = fmmb_set_stream(pl->tplan, stream);
       if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
     }
@@ -271,9 +271,12 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       }
     }
     if (pl->tplan) {  // its geometry is the old one
-      fmmb_plan_destroy(pl->tplan);
+      if (pl->tplan != pl) fmmb_plan_destroy(pl->tplan);
       pl->tplan = nullptr;
     }
+    // one set of points as both targets and sources (the same arrays): the
+    // transpose of a symmetric kernel is then this plan itself
+    pl->same_sets = nprob == 1 && ni == nj && tx == sx && ty == sy && tz == sz;
     FMMB_REQUIRE(tx && ty && tz && sx && sy && sz, FMMB_ERR_ARG, "null coordinates");
     FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNI || (tnx && tny && tnz), FMMB_ERR_ARG, "Gni needs target normals");
     FMMB_REQUIRE(pl->cfg.kernel != FMMB_LAPLACE_GNJ || (snx && sny && snz), FMMB_ERR_ARG, "Gnj needs source normals");
@@ -1170,6 +1173,10 @@ namespace {
 fmmb_plan* transposed_plan(fmmb_plan* pl) {
   if (pl->tplan) return pl->tplan;
   FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+  if (pl->same_sets && (pl->cfg.kernel == FMMB_LAPLACE_G || helm_family(pl->cfg.kernel))) {
+    pl->tplan = pl;  // G(x_i - x_j) = G(x_j - x_i) on one point set: A^T = A
+    return pl;
+  }
   fmmb_config c = pl->cfg;
   c.kernel = pl->cfg.kernel == FMMB_LAPLACE_GNI ? FMMB_LAPLACE_GNJ
              : pl->cfg.kernel == FMMB_LAPLACE_GNJ ? FMMB_LAPLACE_GNI : pl->cfg.kernel;  // G, Helmholtz: symmetric
@@ -1261,6 +1268,59 @@ int fmmb_position_grad(fmmb_plan* pl, const float* q, const float* w, double* dx
     if (dxt && ot != dxt) FMMB_CUDA(cudaMemcpyAsync(dxt, ot, 3 * (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, m));
     if (dxs && os != dxs) FMMB_CUDA(cudaMemcpyAsync(dxs, os, 3 * (size_t)nj * sizeof(double), cudaMemcpyDeviceToHost, m));
     FMMB_CUDA(cudaStreamSynchronize(m));
+  });
+}
+
+int fmmb_adjoint_f64(fmmb_plan* pl, const float* q, const float* w, const double* field_t, double* dq, double* dxt,
+                     double* dxs) {
+  return guarded([&] {
+    FMMB_REQUIRE(pl && w && (dq || dxt || dxs), FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE((!dxt && !dxs) || pl->cfg.kernel == FMMB_LAPLACE_G, FMMB_ERR_ARG,
+                 "position gradients are for the Laplace G kernel");
+    FMMB_REQUIRE(!dxt || field_t, FMMB_ERR_ARG, "dxt needs the forward field");
+    FMMB_REQUIRE(!dxs || q, FMMB_ERR_ARG, "dxs needs the charges");
+    FMMB_REQUIRE(pl->cfg.nrhs == 1 || (!dxt && !dxs), FMMB_ERR_ARG, "position gradients take one right-hand side");
+    FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
+    FMMB_REQUIRE(!helm_family(pl->cfg.kernel), FMMB_ERR_ARG, "the complex kernels use fmmb_evaluate_transpose");
+    const int ni = pl->ni, nj = pl->nj;
+    const size_t nadj = (size_t)nj * pl->cfg.nrhs;
+    cudaStream_t m = pl->st.main;
+    // plan-owned work space (allocated on first use): adj[nadj] | field_s[3 nj]
+    // | dxs[3 nj] | field_t[3 ni] | dxt[3 ni], and the staged charges / weights
+    pl->adj_tmp.alloc(nadj + 6 * (size_t)nj + 6 * (size_t)ni);
+    double* adj = pl->adj_tmp.get();
+    double* fs = adj + nadj;
+    double* os = fs + 3 * (size_t)nj;
+    double* ft = os + 3 * (size_t)nj;
+    double* ot = ft + 3 * (size_t)ni;
+    // w (ni nrhs) and q (nj) staged once when they are host arrays
+    const float* wd = to_device(w, (size_t)ni * pl->cfg.nrhs, pl->adj_ws, m);
+    if (dq || dxs) {
+      if (is_device_ptr(dq)) adj = dq;
+      const int rc = fmmb_evaluate_transpose_f64(pl, wd, adj, dxs ? fs : nullptr);
+      if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+      if (dq && adj != dq) FMMB_CUDA(cudaMemcpyAsync(dq, adj, nadj * sizeof(double), cudaMemcpyDeviceToHost, m));
+      if (dxs) {  // dL/dx_s = q * grad(psi)(x_s)
+        const float* qd = to_device(q, nj, pl->adj_qs, m);
+        if (is_device_ptr(dxs)) os = dxs;
+        launch_weight_field(nj, qd, fs, os, m);
+        if (os != dxs) FMMB_CUDA(cudaMemcpyAsync(dxs, os, 3 * (size_t)nj * sizeof(double), cudaMemcpyDeviceToHost, m));
+      }
+    }
+    if (dxt) {  // dL/dx_t = w * grad(pot)(x_t)
+      const double* fd = field_t;
+      if (!is_device_ptr(field_t)) {
+        FMMB_CUDA(cudaMemcpyAsync(ft, field_t, 3 * (size_t)ni * sizeof(double), cudaMemcpyHostToDevice, m));
+        fd = ft;
+      }
+      if (is_device_ptr(dxt)) ot = dxt;
+      launch_weight_field(ni, wd, fd, ot, m);
+      if (ot != dxt) FMMB_CUDA(cudaMemcpyAsync(dxt, ot, 3 * (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, m));
+    }
+    // host outputs are complete on return; device outputs are ordered on the plan's stream
+    if (!is_device_ptr(w) || (q && !is_device_ptr(q)) || (dq && !is_device_ptr(dq)) || (dxt && !is_device_ptr(dxt)) ||
+        (dxs && !is_device_ptr(dxs)) || (field_t && !is_device_ptr(field_t)))
+      FMMB_CUDA(cudaStreamSynchronize(m));
   });
 }
 

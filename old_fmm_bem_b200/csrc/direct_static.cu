@@ -55,13 +55,23 @@ double* scratch_for_current_device() {
   return g_scratch_ptr[dev];
 }
 
+// Device memory of the current device, or managed memory: the only memory
+// the kernels here may touch (another GPU's allocation would be a peer access
+// the caller never enabled, a fault instead of an argument error).
 bool on_device(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  if (a.type != cudaMemoryTypeDevice) return false;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.device == dev;
 }
 
 struct Soa {
@@ -189,7 +199,7 @@ extern "C" FMMB_API int fmmb_direct_static(const fmmb_config* cfg, int ni, const
                  "Gnj needs source normals");
     const void* dev_ptrs[] = {tx, ty, tz, pot, q, grad, tnx, tny, tnz, sx, sy, sz, snx, sny, snz};
     for (const void* p : dev_ptrs)
-      FMMB_REQUIRE(!p || on_device(p), FMMB_ERR_ARG, "fmmb_direct_static takes device (or managed) pointers only");
+      FMMB_REQUIRE(!p || on_device(p), FMMB_ERR_ARG, "fmmb_direct_static takes device memory of the current device (or managed memory) only");
 
     double* part = scratch_for_current_device();
     const bool ref = cfg->semantics == FMMB_SEM_REFERENCE;

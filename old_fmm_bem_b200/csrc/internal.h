@@ -178,8 +178,11 @@ struct fmmb_plan {
   // plan with targets and sources swapped, built on first use
   fmmb::DevBuf<float> geo;
   bool geo_tn = false, geo_sn = false;
-  fmmb_plan* tplan = nullptr;
+  bool same_sets = false;  // targets and sources given as the same arrays (one problem)
+  fmmb_plan* tplan = nullptr;  // == this plan for a symmetric kernel on one point set
   fmmb::DevBuf<double> pg_tmp;                 // position-gradient work space
+  fmmb::DevBuf<double> adj_tmp;                // fmmb_adjoint_f64 work space
+  fmmb::DevBuf<float> adj_qs, adj_ws;          // its staged charges and weights
   // graphs [without / with gradient] x [whole evaluate / far field only]
   cudaGraphExec_t gexec[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<std::pair<int, int>> gphase[4];

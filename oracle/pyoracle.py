@@ -69,10 +69,13 @@ def oracle_lib():
     return lib
 
 
-def ref_lib(p, gpu_p2p=False):
+def ref_lib(p, gpu_p2p=False, perf=False):
     """The reference library of order p; gpu_p2p: the p = 8 build whose near
-    field runs through the reference's p2pgpu_ callers into libfmmb."""
-    name = "libfmmref_gpup2p_mp9.so" if gpu_p2p else f"libfmmref_mp{p + 1}.so"
+    field runs through the reference's p2pgpu_ callers into libfmmb; perf: the
+    build made for timing (same sources, vectorising -march, oracle/Makefile
+    target perf)."""
+    name = "libfmmref_gpup2p_mp9.so" if gpu_p2p else (f"libfmmref_perf_mp{p + 1}.so" if perf else
+                                                       f"libfmmref_mp{p + 1}.so")
     if gpu_p2p:
         assert p == 8, "the p2pgpu_ build is made for mp = 9"
     lib = _load(os.path.join(HERE, "_ref", name))
@@ -85,8 +88,8 @@ def ref_lib(p, gpu_p2p=False):
     return lib
 
 
-def ref_available(p):
-    return os.path.exists(os.path.join(HERE, "_ref", f"libfmmref_mp{p + 1}.so"))
+def ref_available(p, perf=False):
+    return os.path.exists(os.path.join(HERE, "_ref", f"libfmmref_{'perf_' if perf else ''}mp{p + 1}.so"))
 
 
 def _unpack(t, tn, s, sn, q):
@@ -158,10 +161,10 @@ def direct(t, s, q, *, neq=0, eps2=0.0, exclude_self=True, ref_pi=False, tn=None
 
 
 def ref_fmm(t, s, q, *, neq=0, p=8, lmax=3, bbox=(0.0, 0.0, 0.0, 1.0), tn=None, sn=None, lam=0.0,
-            timings=None, gpu_p2p=False):
+            timings=None, gpu_p2p=False, perf=False):
     """The reference's own fmm() (built from its sources).  Returns float32
     (pot, grad) in caller order; the reference computes the gradient for neq 0."""
-    lib = ref_lib(p, gpu_p2p)
+    lib = ref_lib(p, gpu_p2p, perf)
     t, tn, s, sn, q = _unpack(t, tn, s, sn, q)
     ni, nj = t.shape[1], s.shape[1]
     v = np.zeros(ni, np.float32)

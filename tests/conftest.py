@@ -8,6 +8,18 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 
+def reference_root():
+    """The reference source tree: $REF_ROOT, else the default that the oracle
+    build recipe (oracle/Makefile, `REF_ROOT ?= ...`) compiles from."""
+    if os.environ.get("REF_ROOT"):
+        return os.environ["REF_ROOT"]
+    with open(os.path.join(ROOT, "oracle", "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF_ROOT") and "?=" in line:
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libfmmb.so")
 

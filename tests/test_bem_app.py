@@ -16,9 +16,10 @@ import os
 import numpy as np
 import pytest
 
+from conftest import reference_root
 from old_fmm_bem_b200 import bem, geometry
 
-REF_DATA = "/root/reference/bio/data"
+REF_DATA = os.path.join(reference_root(), "bio", "data")
 
 
 def test_msms_round_trip(tmp_path):

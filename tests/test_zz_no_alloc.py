@@ -125,3 +125,17 @@ def test_gni_and_oversize_rejected(ob):
     rc = lib.fmmb_direct_static(ctypes.byref(cfg), 8, hp, hp, hp, None, None, None, 8, hp, hp, hp, None, None, None,
                                 hp, hp, None, None)
     assert rc == -1 and b"device" in lib.fmmb_last_error()
+
+
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2, reason="needs two GPUs")
+def test_other_device_memory_rejected(ob):
+    """Memory of another GPU is refused before any GPU work: the kernels would
+    run on the current device and read it as a peer access nobody enabled."""
+    lib = ob.load()
+    cfg = _cfg(ob, 0, 1, 1)
+    other = torch.zeros(8, device="cuda:1")
+    op = other.data_ptr()
+    with torch.cuda.device(0):
+        rc = lib.fmmb_direct_static(ctypes.byref(cfg), 8, op, op, op, None, None, None, 8, op, op, op, None, None,
+                                    None, op, op, None, None)
+    assert rc == -1 and b"current device" in lib.fmmb_last_error()
