@@ -540,17 +540,47 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       pl->inv_i.alloc(ni);
       FMMB_CUDA(cudaMemcpy(pl->inv_i.get(), inv.data(), ni * sizeof(int), cudaMemcpyHostToDevice));
     }
-    // near-field work items of the many-right-hand-side pass: pieces of 128 targets
+    // near-field work items: pieces of up to 128 targets of a leaf.  The
+    // many-right-hand-side pass takes them in leaf order; the one-right-hand-
+    // side kernels heaviest first (targets x sources of the 27 neighbour
+    // leaves), dealt alternately to the two near-field launches of an
+    // evaluate, so that each launch starts with its longest blocks
     {
       const int nleaf = pl->nbox_i[pl->lmax];
-      std::vector<int2> leaf(nleaf), work;
+      std::vector<int2> leaf(nleaf), leafj(pl->nbox_j[pl->lmax]), work;
+      std::vector<int> plist((size_t)nleaf * kP2PSlots);
       FMMB_CUDA(cudaMemcpy(leaf.data(), pl->leaf_i.get(), nleaf * sizeof(int2), cudaMemcpyDeviceToHost));
-      for (int b = 0; b < nleaf; b++)
-        for (int t = 0; t < leaf[b].y; t += 128) work.push_back(make_int2(b, t));
+      FMMB_CUDA(cudaMemcpy(leafj.data(), pl->leaf_j.get(), leafj.size() * sizeof(int2), cudaMemcpyDeviceToHost));
+      FMMB_CUDA(cudaMemcpy(plist.data(), pl->p2p_list.get(), plist.size() * sizeof(int), cudaMemcpyDeviceToHost));
+      std::vector<std::pair<long long, int2>> items;
+      for (int b = 0; b < nleaf; b++) {
+        long long nsrc = 0;
+        for (int sl = 0; sl < kP2PSlots; sl++) {
+          const int jl = plist[(size_t)b * kP2PSlots + sl];
+          if (jl >= 0) nsrc += leafj[jl].y;
+        }
+        for (int t = 0; t < leaf[b].y; t += 128) {
+          work.push_back(make_int2(b, t));
+          items.push_back({(long long)std::min(128, leaf[b].y - t) * std::max(nsrc, 1LL), make_int2(b, t)});
+        }
+      }
       pl->m_p2p_work.alloc(work.size());
       if (!work.empty())
         FMMB_CUDA(cudaMemcpy(pl->m_p2p_work.get(), work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
       pl->m_p2p_nwork = (int)work.size();
+      std::stable_sort(items.begin(), items.end(),
+                       [](const std::pair<long long, int2>& x, const std::pair<long long, int2>& y) {
+                         return x.first > y.first;
+                       });
+      std::vector<int2> sorted;
+      sorted.reserve(items.size());
+      for (size_t k = 0; k < items.size(); k += 2) sorted.push_back(items[k].second);
+      pl->p2p_nwork0 = (int)sorted.size();
+      for (size_t k = 1; k < items.size(); k += 2) sorted.push_back(items[k].second);
+      pl->p2p_work.alloc(sorted.size());
+      if (!sorted.empty())
+        FMMB_CUDA(cudaMemcpy(pl->p2p_work.get(), sorted.data(), sorted.size() * sizeof(int2), cudaMemcpyHostToDevice));
+      pl->p2p_nwork = (int)sorted.size();
     }
     // evaluation buffers
     const int nr = pl->cfg.nrhs;
@@ -717,8 +747,8 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   double* g_near = want_grad ? pl->grad_s.get() : nullptr;
   double* g_far = want_grad ? pl->grad_s.get() + 3 * (size_t)pl->ni : nullptr;
   const int nleaf_i = pl->nbox_i[lmax], nleaf_j = pl->nbox_j[lmax];
-  // Near field on the low-priority side stream, in two halves of the target
-  // leaves: the first overlaps the upward pass (P2M / M2M, short dependent
+  // Near field on the low-priority side stream, in two halves of the work
+  // items: the first overlaps the upward pass (P2M / M2M, short dependent
   // launches that leave SMs idle), the second the downward tail (L2L / L2P);
   // the tensor-core M2L, which needs whole SMs, runs between them.
   auto near_field = [&](int l0, int l1, bool last) {
@@ -735,21 +765,20 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     if (l0 == 0) FMMB_CUDA(time_mark(pl, pl->ev[0], side));
     {
       PhaseTimer tm(pl, 0, side);
-      const int2* li = pl->leaf_i.get() + l0;
-      const int* lst = pl->p2p_list.get() + (size_t)l0 * kP2PSlots;
+      const int2* wk = pl->p2p_work.get() + l0;
       if (pl->cfg.precision == FMMB_MIXED)
-        launch_p2p_mixed(ker, l1 - l0, li, pl->leaf_j.get(), lst, pl->tpos.get(), pl->tnrm.get(), pl->spos.get(),
-                         pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+        launch_p2p_mixed(ker, l1 - l0, wk, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
+                         pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
       else
-        launch_p2p_f64(ker, l1 - l0, li, pl->leaf_j.get(), lst, pl->tpos.get(), pl->tnrm.get(), pl->spos.get(),
-                       pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
+        launch_p2p_f64(ker, l1 - l0, wk, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(),
+                       pl->tnrm.get(), pl->spos.get(), pl->snrm.get(), qs, s, pot_near, g_near, pl->ni, side);
     }
     if (last) {
       FMMB_CUDA(time_mark(pl, pl->ev[1], side));
       FMMB_CUDA(cudaEventRecord(pl->st.join, side));
     }
   };
-  const int p2p_split = nleaf_i / 2;
+  const int p2p_split = pl->p2p_nwork0;
   near_field(0, p2p_split, false);
 
   // far field on the main stream
@@ -832,7 +861,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
                            pl->L.get(), m);
     }
   }
-  near_field(p2p_split, nleaf_i, true);
+  near_field(p2p_split, pl->p2p_nwork, true);
   for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
     pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));

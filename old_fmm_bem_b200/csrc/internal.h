@@ -201,6 +201,10 @@ struct fmmb_plan {
   fmmb::DevBuf<float> qs_far;
   fmmb::DevBuf<int2> m_p2p_work;  // (target leaf, first target), up to 128 targets each
   int m_p2p_nwork = 0;
+  // the same items for the one-right-hand-side near field, heaviest first in
+  // each of its two launches: [0, p2p_nwork0) and [p2p_nwork0, p2p_nwork)
+  fmmb::DevBuf<int2> p2p_work;
+  int p2p_nwork = 0, p2p_nwork0 = 0;
   int opimg_sets = 0;
   float opimg_rd = 0;
   // tensor-core translation jobs: work items of 64 output boxes with their slots

@@ -19,12 +19,15 @@ struct Sem {
 __host__ __device__ __forceinline__ int ifull_d(int n, int m) { return n * n + n + m; }
 
 void launch_gather_charges(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
-void launch_p2p_f64(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
-                    const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot,
-                    double* grad, int ni, cudaStream_t st);
-void launch_p2p_mixed(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
-                      const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s,
-                      double* pot, double* grad, int ni, cudaStream_t st);
+// Near field of one right-hand side over work items (target leaf, first
+// target) of up to 128 targets of a leaf against its 27 neighbour slots
+// (list[leaf][27]); one block per item.
+void launch_p2p_f64(int kernel, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list,
+                    const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm, const float* qs,
+                    const Sem& s, double* pot, double* grad, int ni, cudaStream_t st);
+void launch_p2p_mixed(int kernel, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list,
+                      const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm, const float* qs,
+                      const Sem& s, double* pot, double* grad, int ni, cudaStream_t st);
 void launch_p2m(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos, const float4* snrm,
                 const float* qs, const double* fac, const Sem& s, const float* bbox, double rb, double* M, cudaStream_t st);
 // trig-free Cartesian P2M / L2P (accurate semantics), expansions_cart.cu

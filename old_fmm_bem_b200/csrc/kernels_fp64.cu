@@ -40,11 +40,13 @@ __global__ void gather_charges(int n, int nrhs, const int* perm, const float* q,
 
 // ---------------------------------------------------------------- P2P (FP64)
 // kernel/G_p2p.cxx:12-37, Gni_p2p.cxx:12-28, Gnj_p2p.cxx:12-28: one block per
-// target leaf, its 27 neighbour slots staged through shared memory.
+// work item (up to 128 targets of a target leaf), its 27 neighbour slots
+// staged through shared memory.
 constexpr int kP2PThreads = 128;
 
 template <int KER>
-__global__ void __launch_bounds__(kP2PThreads) p2p_f64(const int2* __restrict__ leaf_i, const int2* __restrict__ leaf_j,
+__global__ void __launch_bounds__(kP2PThreads) p2p_f64(const int2* __restrict__ work, const int2* __restrict__ leaf_i,
+                                                       const int2* __restrict__ leaf_j,
                                                        const int* __restrict__ list, const float4* __restrict__ tpos,
                                                        const float4* __restrict__ tnrm, const float4* __restrict__ spos,
                                                        const float4* __restrict__ snrm, const float* __restrict__ qs,
@@ -53,8 +55,11 @@ __global__ void __launch_bounds__(kP2PThreads) p2p_f64(const int2* __restrict__ 
   __shared__ float4 sp[kP2PThreads];
   __shared__ float4 sn[kP2PThreads];
   __shared__ float sq[kP2PThreads];
-  const int b = blockIdx.x;
-  const int2 li = leaf_i[b];
+  const int2 wk = work[blockIdx.x];
+  const int b = wk.x;
+  int2 li = leaf_i[b];
+  li.x += wk.y;
+  li.y = min(kP2PThreads, li.y - wk.y);
   for (int t0 = 0; t0 < li.y; t0 += kP2PThreads) {
     const int i = li.x + t0 + threadIdx.x;
     const bool act = (t0 + threadIdx.x) < li.y;
@@ -495,16 +500,19 @@ void launch_gather_charges(int n, int nrhs, const int* perm, const float* q, flo
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_p2p_f64(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
-                    const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s, double* pot,
-                    double* grad, int ni, cudaStream_t st) {
-  if (nleaf <= 0) return;
+void launch_p2p_f64(int kernel, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list,
+                    const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm, const float* qs,
+                    const Sem& s, double* pot, double* grad, int ni, cudaStream_t st) {
+  if (nwork <= 0) return;
   if (kernel == FMMB_LAPLACE_G)
-    p2p_f64<FMMB_LAPLACE_G><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+    p2p_f64<FMMB_LAPLACE_G><<<nwork, kP2PThreads, 0, st>>>(work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s,
+                                                           pot, grad, ni);
   else if (kernel == FMMB_LAPLACE_GNI)
-    p2p_f64<FMMB_LAPLACE_GNI><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+    p2p_f64<FMMB_LAPLACE_GNI><<<nwork, kP2PThreads, 0, st>>>(work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s,
+                                                             pot, grad, ni);
   else
-    p2p_f64<FMMB_LAPLACE_GNJ><<<nleaf, kP2PThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s, pot, grad, ni);
+    p2p_f64<FMMB_LAPLACE_GNJ><<<nwork, kP2PThreads, 0, st>>>(work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, s,
+                                                             pot, grad, ni);
   FMMB_CHECK_LAUNCH();
 }
 

@@ -7,7 +7,10 @@
 // partial sum into FP64 accumulators, so the accumulated rounding stays at the
 // FP32 level of one 32-term sum whatever the number of sources.
 //
-// Layout: one block of 4 warps per target leaf.  The sources of all
+// Layout: one block of 4 warps per work item, up to 128 targets of one
+// target leaf (a leaf of more targets is several items, so that the dense
+// leaves of clustered points spread over many SMs; the items come heaviest
+// first).  The sources of all
 // neighbour leaves are staged into shared memory as one list -- the leaf's
 // own source leaf first, padded to a multiple of 32 with far, zero-charge
 // points, then the other neighbours, padded likewise -- so that no run of 32
@@ -235,7 +238,8 @@ __device__ __forceinline__ void tile_runs(const Smem<KER>& S, int c0, int c1, in
 }
 
 template <int KER, bool EXCL>
-__global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ leaf_i, const int2* __restrict__ leaf_j,
+__global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ work, const int2* __restrict__ leaf_i,
+                                                      const int2* __restrict__ leaf_j,
                                                       const int* __restrict__ list, const float4* __restrict__ tpos,
                                                       const float4* __restrict__ tnrm, const float4* __restrict__ spos,
                                                       const float4* __restrict__ snrm, const float* __restrict__ qs,
@@ -243,8 +247,11 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ l
                                                       double* __restrict__ grad, int ni) {
   constexpr int NC = ncomp<KER>();
   __shared__ Smem<KER> S;
-  const int b = blockIdx.x;
-  const int2 li = leaf_i[b];
+  const int2 wk = work[blockIdx.x];
+  const int b = wk.x;  // target leaf; this item's targets: [li.x, li.x + li.y)
+  int2 li = leaf_i[b];
+  li.x += wk.y;
+  li.y = min(kThreads, li.y - wk.y);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane & (kG - 1), s = lane / kG;
   // segment list: lane l of warp 0 reads neighbour slot l; the own leaf goes
   // first, the non-empty others after it in slot order
@@ -360,29 +367,34 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ l
 }
 
 template <int KER>
-void launch_k(int nleaf, bool excl, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
-              const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, float eps2, double coef,
-              double* pot, double* grad, int ni, cudaStream_t st) {
+void launch_k(int nwork, bool excl, const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list,
+              const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm, const float* qs,
+              float eps2, double coef, double* pot, double* grad, int ni, cudaStream_t st) {
   if (excl)
-    p2p_mixed<KER, true><<<nleaf, kThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
+    p2p_mixed<KER, true><<<nwork, kThreads, 0, st>>>(work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2,
+                                                     coef, pot, grad, ni);
   else
-    p2p_mixed<KER, false><<<nleaf, kThreads, 0, st>>>(leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, coef, pot, grad, ni);
+    p2p_mixed<KER, false><<<nwork, kThreads, 0, st>>>(work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2,
+                                                      coef, pot, grad, ni);
 }
 
 }  // namespace
 
-void launch_p2p_mixed(int kernel, int nleaf, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
-                      const float4* tnrm, const float4* spos, const float4* snrm, const float* qs, const Sem& s,
-                      double* pot, double* grad, int ni, cudaStream_t st) {
-  if (nleaf <= 0) return;
+void launch_p2p_mixed(int kernel, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list,
+                      const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm, const float* qs,
+                      const Sem& s, double* pot, double* grad, int ni, cudaStream_t st) {
+  if (nwork <= 0) return;
   const float eps2 = (float)s.eps2;
   const bool excl = s.excl_self != 0;
   if (kernel == FMMB_LAPLACE_G)
-    launch_k<FMMB_LAPLACE_G>(nleaf, excl, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot, grad, ni, st);
+    launch_k<FMMB_LAPLACE_G>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot,
+                             grad, ni, st);
   else if (kernel == FMMB_LAPLACE_GNI)
-    launch_k<FMMB_LAPLACE_GNI>(nleaf, excl, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot, grad, ni, st);
+    launch_k<FMMB_LAPLACE_GNI>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot,
+                               grad, ni, st);
   else
-    launch_k<FMMB_LAPLACE_GNJ>(nleaf, excl, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot, grad, ni, st);
+    launch_k<FMMB_LAPLACE_GNJ>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot,
+                               grad, ni, st);
   FMMB_CHECK_LAUNCH();
 }
 
