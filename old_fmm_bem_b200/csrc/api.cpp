@@ -444,13 +444,19 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     // tensor-core M2L (mixed precision, K <= tc_max_k()): operator images (one
     // per operator and block of 128 output rows), the TF32 split of M, and
     // the work items over the pair tiles of all levels
-    pl->use_tc = pl->cfg.precision == FMMB_MIXED && pl->K <= tc_max_k();
+    // M2L on the tensor cores in the mixed form: FP16x3 for K <= h16_max_k()
+    // (p <= 12), TF32x3 above
+    const bool mixed = pl->cfg.precision == FMMB_MIXED;
+    pl->use_h16 = mixed && pl->K <= h16_max_k();
+    pl->use_tc = mixed && !pl->use_h16 && pl->K <= tc_max_k();
     init_fac32();
     prepare_translate_pairs_f64();
     if (pl->use_tc) prepare_translate_tc();
-    if (pl->use_tc) {
-      const int K = pl->K, kpad = tc_kpad(K), nrb = (K + 127) / 128;
-      if (pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd || pl->d_img_m2l.get() == nullptr) {
+    if (pl->use_h16) prepare_translate_h16();
+    if (pl->use_tc || pl->use_h16) {
+      const int K = pl->K, kpad = tc_kpad(K), nrb = pl->use_h16 ? 1 : (K + 127) / 128;
+      const bool stale = pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd;
+      if (pl->use_tc && (stale || pl->d_img_m2l.get() == nullptr)) {
         std::vector<float> img;
         build_tc_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, kpad, img);
         pl->d_img_m2l.alloc(img.size());
@@ -458,7 +464,19 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
         pl->opimg_sets = pl->ops.m2l_sets;
         pl->opimg_rd = pl->ops.m2l_rd;
       }
-      pl->Mtf.alloc((size_t)pl->tot_j * 2 * kpad);
+      if (pl->use_h16 && (stale || pl->d_img_h16.get() == nullptr)) {
+        std::vector<unsigned char> img;
+        build_h16_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, h16_n(K), h16_kpad(K), h16_img_bytes(K), img);
+        pl->d_img_h16.alloc(img.size());
+        FMMB_CUDA(cudaMemcpy(pl->d_img_h16.get(), img.data(), img.size(), cudaMemcpyHostToDevice));
+        pl->opimg_sets = pl->ops.m2l_sets;
+        pl->opimg_rd = pl->ops.m2l_rd;
+      }
+      if (pl->use_tc) pl->Mtf.alloc((size_t)pl->tot_j * 2 * kpad);
+      if (pl->use_h16) {
+        pl->Xh.alloc((size_t)pl->tot_j * 2 * h16_kpad(K));
+        pl->xexp.alloc(pl->tot_j);
+      }
       const int TT = tc_tile();
       auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
         d.alloc(h.size());
@@ -511,7 +529,7 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
         up(job.red_rows, rows);
         up(job.red_ptr, ptr);
         up(job.red_idx, idx);
-        job.ys = 128 * nrb;
+        job.ys = pl->use_h16 ? (K + 3) / 4 * 4 : 128 * nrb;
         pl->tc_y.alloc((size_t)ntile * TT * job.ys);
       };
       // M2L, all levels in one job: operator = set(level)*316 + relative position
@@ -844,12 +862,35 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
   for (int lev = lmax - 1; lev >= 2; lev--)  // parents at lev from their children (several per parent)
     pairs_run(*pl->m2m_pairs[lev], pl->d_m2m_t.get(), pl->M.get(), pl->M.get(), 1, 2);
   if (pl->use_tc) split(pl->M.get(), pl->Mtf.get(), 0, pl->tot_j, 2);  // every level, for the M2L
+  if (pl->use_h16) {
+    PhaseTimer tm(pl, 2, m);
+    launch_split_h16(pl->tot_j, K, pl->M.get(), pl->Xh.get(), pl->xexp.get(), m);
+  }
   FMMB_CUDA(time_mark(pl, pl->ev[4], m));
   // downward pass: M2L of every level into zeroed locals, then each level
   // adds its parent's translated local (L2L), top down
   FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * K * sizeof(double), m));
   if (pl->use_tc) {
     tc_run(pl->tc_m2l, pl->d_img_m2l.get(), pl->Mtf.get(), pl->L.get(), 3);
+  } else if (pl->use_h16) {
+    PhaseTimer tm(pl, 3, m);
+    const fmmb_plan::TcJob& job = pl->tc_m2l;
+    H16JobArgs a{};
+    a.ntile = job.ntile;
+    a.K = K;
+    a.ys = job.ys;
+    a.tile_op = job.tile_op.get();
+    a.tile_src = job.tile_src.get();
+    a.tile_y = reinterpret_cast<const int2*>(job.tile_y.get());
+    a.opimg = pl->d_img_h16.get();
+    a.xin = pl->Xh.get();
+    a.xexp = pl->xexp.get();
+    a.y = pl->tc_y.get();
+    a.err = pl->d_err.get();
+    launch_translate_h16(a, pl->nsm, m);
+    launch_reduce_pairs(job.nred, job.red_rows.get(), job.red_ptr.get(), job.red_idx.get(), pl->tc_y.get(), job.ys, K,
+                        pl->L.get(), m);
+    pl->launches++;
   } else {
     const size_t opsz = (size_t)316 * K * K;
     for (int lev = 2; lev <= lmax; lev++) {

@@ -232,6 +232,7 @@ void helm_setup(fmmb_plan* pl) {
   pl->L.alloc((size_t)pl->tot_i * 2 * K);
   pl->pot_s.alloc((size_t)4 * pl->ni);  // near, far (complex)
   pl->use_tc = false;
+  pl->use_h16 = false;
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 

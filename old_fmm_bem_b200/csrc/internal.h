@@ -93,6 +93,9 @@ void build_static_operators(Operators& ops, int p, bool ref_semantics);
 void build_m2l_operators(Operators& ops, int lmax, float rd);
 // TF32 hi/lo images of nmat K x K operators in the tensor-core operand layout
 void build_tc_images(const std::vector<double>& mats, int nmat, int K, int kpad, std::vector<float>& img);
+// FP16 hi/lo images (row-scaled) for the FP16x3 M2L, img_bytes each
+void build_h16_images(const std::vector<double>& mats, int nmat, int K, int n, int kpad, size_t img_bytes,
+                      std::vector<unsigned char>& img);
 
 struct Stream2 {
   cudaStream_t main = nullptr, side = nullptr;
@@ -166,7 +169,11 @@ struct fmmb_plan {
   fmmb::DevBuf<float> Mtf;                   // [tot_j][2][tc_kpad(K)] TF32 hi/lo split of M (mixed, M2L input)
   fmmb::DevBuf<int> d_err;                   // device error code of the tensor-core kernels
   int* h_err = nullptr;                      // pinned copy, checked by the next call
-  bool use_tc = false;                       // M2L on the tensor cores (mixed, K <= 128)
+  bool use_tc = false;                       // M2L on the tensor cores in TF32x3 (mixed, h16_max_k() < K <= 256)
+  bool use_h16 = false;                      // M2L on the tensor cores in FP16x3 (mixed, K <= h16_max_k())
+  fmmb::DevBuf<unsigned char> d_img_h16;     // [sets*316] FP16 operator images
+  fmmb::DevBuf<unsigned short> Xh;           // [tot_j][2][h16_kpad(K)] scaled FP16 hi/lo split of M
+  fmmb::DevBuf<int> xexp;                    // [tot_j] its exponents
   // The plan-internal part of a one-right-hand-side evaluate (sorted charges ->
   // sorted outputs, plan-owned buffers only) captured once per geometry as a
   // CUDA graph, without / with gradient, with the phase-timer records and the

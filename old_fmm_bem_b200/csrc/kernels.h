@@ -112,6 +112,28 @@ void launch_translate_tc(const TcJobArgs& a, int nsm, cudaStream_t st);
 // out[rows[w]] += sum of the pair rows y[idx[ptr[w]..ptr[w+1])] (rows of ys floats; FP64, list order)
 void launch_reduce_pairs(int nrow, const int* rows, const int* ptr, const int* idx, const float* y, int ys, int K,
                          double* out, cudaStream_t st);
+// FP16x3 tensor-core M2L (translate_h16.cu), K <= h16_max_k(): operators of
+// h16_n(K) output rows (K rounded up to 16), inputs split as [rows][2][h16_kpad(K)]
+// FP16 (hi, lo) with a power-of-two exponent per row, pair rows of ys floats
+struct H16JobArgs {
+  int ntile, K, ys;
+  const int* tile_op;           // [ntile] operator per tile (sorted)
+  const int* tile_src;          // [ntile][128] input rows (-1 = empty)
+  const int2* tile_y;           // [ntile] (first pair row of y, 0)
+  const void* opimg;            // operator images of h16_img_bytes(K) each
+  const void* xin;              // FP16 split of the inputs
+  const int* xexp;              // per input row: its scaling exponent
+  float* y;
+  int* err;
+};
+int h16_max_k();
+int h16_n(int K);
+int h16_kpad(int K);
+size_t h16_img_bytes(int K);
+// once per device, before any launch (and outside stream capture)
+void prepare_translate_h16();
+void launch_translate_h16(const H16JobArgs& a, int nsm, cudaStream_t st);
+void launch_split_h16(int nbox, int K, const double* M, void* xh, int* xexp, cudaStream_t st);
 // K padded for the tensor-core operands (128, or a multiple of 32 up to tc_max_k())
 int tc_kpad(int K);
 int tc_max_k();

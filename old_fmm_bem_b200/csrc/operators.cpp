@@ -20,6 +20,7 @@
 // relative position in box units -- except in reference semantics, where the
 // reference adds eps=1e-6 to the M2L distance in absolute units
 // (kernel/m2l.cxx:54), so one M2L set per level is built.
+#include <cuda_fp16.h>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -368,6 +369,45 @@ void build_tc_images(const std::vector<double>& mats, int nmat, int K, int kpad,
         }
       }
     }
+  });
+}
+
+// Translation operators for the FP16x3 tensor-core M2L (translate_h16.cu),
+// one image of img_bytes per operator:
+//  * the operator scaled by 2^-f so that its largest |entry| lies in
+//    [2^14, 2^15), just below the FP16 maximum; hi = FP16 rounding of the
+//    scaled entry, lo = FP16 rounding of the remainder;
+//  * hi then lo as kpad / 64 K-blocks each of n rows (n = K rounded up to 16)
+//    of 128 bytes, 16-byte chunk c of row r stored at chunk c ^ (r & 7)
+//    (K-major SWIZZLE_128B, the kernel's B operand), zero padded;
+//  * then the factor 2^f as a float, padded to 16 bytes.
+void build_h16_images(const std::vector<double>& mats, int nmat, int K, int n, int kpad, size_t img_bytes,
+                      std::vector<unsigned char>& img) {
+  const int nkb = kpad / 64;
+  const size_t kb_bytes = (size_t)n * 128;
+  img.assign((size_t)nmat * img_bytes, 0);
+  parallel_for(nmat, [&](int w) {
+    const double* T = &mats[(size_t)w * K * K];
+    unsigned char* base = &img[(size_t)w * img_bytes];
+    double mx = 0.0;
+    for (size_t i = 0; i < (size_t)K * K; i++) mx = std::max(mx, std::fabs(T[i]));
+    int f = 0;
+    if (mx > 0.0) {
+      std::frexp(mx, &f);  // mx = g 2^f, g in [0.5, 1)
+      f -= 15;
+    }
+    const float scale = std::ldexp(1.0f, f);
+    std::memcpy(base + 2 * nkb * kb_bytes, &scale, 4);
+    for (int r = 0; r < K; r++)
+      for (int c = 0; c < K; c++) {
+        const double v = std::ldexp(T[(size_t)r * K + c], -f);
+        const __half hi = __double2half(v);
+        const __half lo = __double2half(v - (double)__half2float(hi));
+        const int kb = c / 64, j = c % 64;
+        const size_t off = (size_t)r * 128 + (size_t)((((j >> 3) ^ (r & 7)) << 4) + (j & 7) * 2);
+        std::memcpy(base + (size_t)kb * kb_bytes + off, &hi, 2);
+        std::memcpy(base + (size_t)(nkb + kb) * kb_bytes + off, &lo, 2);
+      }
   });
 }
 

@@ -465,9 +465,10 @@ __global__ void split_tf32(int nbox, int K, int kpad, const double* __restrict__
 }
 
 // out[rows[w]][0..K) += sum over e in [ptr[w], ptr[w+1]) of y[idx[e]][0..K)
-// (pair rows of ys floats), in FP64 and in list order (deterministic); one warp
-// per output row, lane l holding coefficients 128c + 4l .. 128c + 4l + 3 of
-// each 128-coefficient chunk c (K <= 256); for K <= 128 eight rows in flight.
+// (pair rows of ys floats, ys >= K a multiple of 4), in FP64 and in list
+// order (deterministic); one warp per output row, lane l holding coefficients
+// 128c + 4l .. 128c + 4l + 3 of each 128-coefficient chunk c (K <= 256), the
+// lanes past the row reading nothing; for K <= 128 eight rows in flight.
 __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* __restrict__ ptr,
                              const int* __restrict__ idx, const float* __restrict__ y, int ys, int K,
                              double* __restrict__ out) {
@@ -477,15 +478,17 @@ __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* 
   const int nch = (K + 127) / 128;
   double a[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
   const int e0 = ptr[w], e1 = ptr[w + 1];
+  const bool live0 = 4 * lane < ys, live1 = nch > 1 && 128 + 4 * lane < ys;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   int e = e0;
-  if (nch == 1) {  // K <= 128: one 512-byte read per pair row, 8 rows in flight
+  if (nch == 1) {  // K <= 128: one read of up to 512 bytes per pair row, 8 rows in flight
     for (; e + 8 <= e1; e += 8) {
       int r8[8];
 #pragma unroll
       for (int u = 0; u < 8; u++) r8[u] = idx[e + u];
       float4 v[8];
 #pragma unroll
-      for (int u = 0; u < 8; u++) v[u] = __ldg(reinterpret_cast<const float4*>(y + (size_t)r8[u] * ys) + lane);
+      for (int u = 0; u < 8; u++) v[u] = live0 ? __ldcs(reinterpret_cast<const float4*>(y + (size_t)r8[u] * ys) + lane) : z4;
 #pragma unroll
       for (int u = 0; u < 8; u++) {
         a[0][0] += v[u].x;
@@ -500,8 +503,8 @@ __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* 
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const float4* yr = reinterpret_cast<const float4*>(y + (size_t)idx[e + u] * ys);
-      v[u][0] = __ldg(yr + lane);
-      v[u][1] = nch > 1 ? __ldg(yr + 32 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+      v[u][0] = live0 ? __ldcs(yr + lane) : z4;
+      v[u][1] = live1 ? __ldcs(yr + 32 + lane) : z4;
     }
 #pragma unroll
     for (int u = 0; u < 4; u++)
@@ -517,8 +520,8 @@ __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* 
     const float4* yr = reinterpret_cast<const float4*>(y + (size_t)idx[e] * ys);
 #pragma unroll
     for (int c = 0; c < 2; c++) {
-      if (c >= nch) break;
-      const float4 v = __ldg(yr + 32 * c + lane);
+      if (c >= nch || !(c ? live1 : live0)) break;
+      const float4 v = __ldcs(yr + 32 * c + lane);
       a[c][0] += v.x;
       a[c][1] += v.y;
       a[c][2] += v.z;
