@@ -656,7 +656,9 @@ def run_headline(args, rank, world):
         op, X, Q, fwd, fwd_bwd, lmax, tune = make(ob.MIXED)
         t_f = _timed(fwd, stream, max(3, args.steps // 2), max(3, args.warmup), flush)
         per_step = []
+        torch.cuda.nvtx.range_push("timed")  # the timed steps, for a profiler's launch list
         t_fb = _timed(fwd_bwd, stream, args.steps, max(3, args.warmup), flush, per_step)
+        torch.cuda.nvtx.range_pop()
         ph = np.array(list(op.plan.timings().values()))
         launches = op.plan.stats()["launches"]
     # each kernel's own duration: one evaluate with gradient, near field after
@@ -788,12 +790,22 @@ def run_headline(args, rank, world):
 def c3_finite_differences(ob, x, q, w, lmax, prec, ncoord, h=1e-4):
     """Central differences of L = sum(w * pot) w.r.t. ncoord random
     coordinates (step h; each side a fresh tree on the moved point set)
-    against the backward's position gradient, in the given form."""
+    against the backward's position gradient, in the given form.  The
+    coordinates are drawn among points with no neighbour closer than 30 h
+    (the difference quotient's O(h^2 / r^2) truncation stays below 1e-3)."""
     if ncoord <= 0:
         return None
     rng = np.random.default_rng(11)
-    pts = rng.choice(x.shape[1], size=ncoord, replace=False)
-    dims = rng.integers(0, 3, ncoord)
+    x64 = x.astype(np.float64)
+    pts, dims = [], []
+    while len(pts) < ncoord:
+        i = int(rng.integers(0, x.shape[1]))
+        r2 = ((x64 - x64[:, i:i + 1]) ** 2).sum(0)
+        r2[i] = np.inf
+        if r2.min() >= (30 * h) ** 2 and i not in pts:
+            pts.append(i)
+            dims.append(int(rng.integers(0, 3)))
+    pts, dims = np.array(pts), np.array(dims)
     plan = ob.Plan(kernel=ob.LAPLACE_G, p=C3_P, lmax=lmax, precision=prec, semantics=ob.SEM_ACCURATE,
                    exclude_self=True)
     bbox = (0.0, 0.0, 0.0, 1.0)
@@ -819,7 +831,8 @@ def c3_finite_differences(ob, x, q, w, lmax, prec, ncoord, h=1e-4):
     return {"coordinates": ncoord, "h": h, "rel_err": float(np.linalg.norm(fdv - an) / np.linalg.norm(an)),
             "max_abs_rel": float(np.max(np.abs(fdv - an) / np.maximum(np.abs(an), 1e-30))),
             "seconds": time.perf_counter() - t0,
-            "note": "central differences of sum(w * pot) over fresh trees, against the backward's dL/dx"}
+            "note": "central differences of sum(w * pot) over fresh trees, against the backward's dL/dx; points "
+                    "with no neighbour closer than 30 h"}
 
 
 def run_c4(args):

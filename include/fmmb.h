@@ -122,8 +122,11 @@ FMMB_API int fmmb_set_geometry_batch(fmmb_plan* plan, int nprob, const int* t_of
 
 /* One FMM matvec (replaces fmm(mi, mj, neq), fmm/fmm.cxx:29-152).
  * q: nrhs x nj charges (caller order).  pot: nrhs x ni potentials (overwritten,
- * unlike the reference's += into vi).  grad: nrhs x 3 x ni gradient for
- * FMMB_LAPLACE_G, may be NULL; ignored for the other kernels. */
+ * unlike the reference's += into vi).  grad (may be NULL): nrhs x 3 x ni
+ * gradient of the potential w.r.t. the target position -- the field for
+ * FMMB_LAPLACE_G; for FMMB_LAPLACE_GNI / FMMB_LAPLACE_GNJ the normals are held
+ * fixed (accurate semantics only, FMMB_ERR_ARG otherwise); ignored for the
+ * complex kernels. */
 FMMB_API int fmmb_evaluate(fmmb_plan* plan, const float* q, float* pot, float* grad);
 /* Same with FP64 outputs. */
 FMMB_API int fmmb_evaluate_f64(fmmb_plan* plan, const float* q, double* pot, double* grad);
@@ -132,18 +135,21 @@ FMMB_API int fmmb_evaluate_f64(fmmb_plan* plan, const float* q, double* pot, dou
  * blocks), A being this plan's FMM.  G is symmetric, so A^T is the G-FMM from
  * the targets to the sources; for the normal-derivative kernels
  * d/dx_j G = -d/dx_i G gives Gni^T = -Gnj and Gnj^T = -Gni with the point
- * sets swapped.  grad[3 nj] (Laplace G only, may be NULL) receives the
- * gradient of A^T w at the sources.  The transposed plan (same root cube,
+ * sets swapped.  grad[3 nj] (Laplace kernels, may be NULL) receives the
+ * gradient of A^T w w.r.t. the source position (normals fixed).  For G on
+ * one point set given as the same arrays the transposed plan is this plan;
+ * otherwise the transposed plan (same root cube,
  * same settings) is built on the first call after fmmb_set_geometry.  No
  * counterpart in the reference (its fmm() has no adjoint). */
 FMMB_API int fmmb_evaluate_transpose(fmmb_plan* plan, const float* w, float* out, float* grad);
 FMMB_API int fmmb_evaluate_transpose_f64(fmmb_plan* plan, const float* w, double* out, double* grad);
 
-/* Position gradients of L = sum_i w_i pot_i for the Laplace G kernel, one
- * right-hand side: dxt[3 ni] = w * grad(pot)(x_t) and dxs[3 nj] =
- * q * grad(psi)(x_s), psi = A^T w (either output may be NULL; when targets and
- * sources are the same points the caller adds the two).  Costs one matvec and
- * one transposed matvec, both with gradient.  No reference counterpart. */
+/* Position gradients of L = sum_i w_i pot_i for the Laplace kernels (normals
+ * held fixed; Gni / Gnj in accurate semantics), one right-hand side:
+ * dxt[3 ni] = w * grad_t(pot) and dxs[3 nj] = q * grad_s(psi), psi = A^T w
+ * (either output may be NULL; when targets and sources are the same points
+ * the caller adds the two).  Costs one matvec and one transposed matvec, both
+ * with gradient.  No reference counterpart. */
 FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w, double* dxt, double* dxs);
 
 /* The backward pass of one matvec pot = A q for L = sum_i w_i pot_i, given
@@ -151,8 +157,8 @@ FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w,
  * fmmb_evaluate_transpose_f64), dxs[3 nj] = q * grad(psi)(x_s) with
  * psi = A^T w, and dxt[3 ni] = w * field_t, field_t[3 ni] being the gradient
  * output of the forward fmmb_evaluate_f64 with the same q.  Any of dq, dxs,
- * dxt may be NULL (dxt needs field_t); position gradients are for the
- * Laplace G kernel.  Costs one transposed matvec (with gradient when dxs is
+ * dxt may be NULL (dxt needs field_t); position gradients of Gni / Gnj need
+ * accurate semantics.  Costs one transposed matvec (with gradient when dxs is
  * asked for); host or device pointers.  When the targets and sources were
  * given as the same arrays the transposed matvec runs on this plan.  No
  * reference counterpart (the reference has no adjoint). */
@@ -162,7 +168,9 @@ FMMB_API int fmmb_adjoint_f64(fmmb_plan* plan, const float* q, const float* w, c
 /* Direct O(ni*nj) sum on the GPU with the plan's kernel and semantics
  * (replaces G_dir/Gni_dir/Gnj_dir, kernel/G_dir.cxx:6-30,
  * kernel/Gni_dir.cxx:6-21, kernel/Gnj_dir.cxx:6-21), FP64 arithmetic.  Uses
- * the geometry and the first right-hand side of q; targets [i0, i1). */
+ * the geometry and the first right-hand side of q; targets [i0, i1).  grad
+ * (may be NULL): 3 x (i1 - i0), the gradient w.r.t. the target position
+ * (normals fixed), for every Laplace kernel. */
 FMMB_API int fmmb_direct_f64(fmmb_plan* plan, const float* q, int i0, int i1, double* pot, double* grad);
 
 /* The reference's batch near-field call p2pgpu_ (libgpu/gpufmm.cu:57-61) with
@@ -239,9 +247,11 @@ FMMB_API int fmmb_gmres_config_init(fmmb_gmres_config* cfg);
 
 /* b: nrhs x n right-hand sides; x: nrhs x n initial guess, overwritten by the
  * solution (FP64, host or device; n = the plan's point count).  weight: n
- * floats or NULL (= 1).  iters: iterations done (may be NULL).  resid:
- * nrhs x nprob relative preconditioned residual estimates ||r_k|| / ||r_0||
- * per system (may be NULL). */
+ * floats or NULL (= 1).  iters: iterations done (may be NULL).  resid (may be
+ * NULL): nrhs x nprob relative preconditioned residuals of the returned x per
+ * system, ||precond (b - A x)|| / ||precond (b - A x0)||, computed with one
+ * more matvec at exit (A being this plan's FMM; the rtol test during the
+ * iterations uses the Givens estimate). */
 FMMB_API int fmmb_gmres(fmmb_plan* plan, const fmmb_gmres_config* cfg, const float* weight, const double* b,
                         double* x, int* iters, double* resid);
 

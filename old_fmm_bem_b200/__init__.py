@@ -272,8 +272,11 @@ class Plan:
         return out
 
     def evaluate(self, q, pot=None, grad=None, f64=False):
-        """One matvec.  q: (nrhs*nj,) charges.  Returns (pot, grad) -- grad only
-        for LAPLACE_G.  Outputs are numpy unless torch CUDA tensors are given."""
+        """One matvec.  q: (nrhs*nj,) charges.  Returns (pot, grad): grad is the
+        gradient of the potential w.r.t. the target position (3 blocks of
+        nrhs*ni), computed for LAPLACE_G always and for LAPLACE_GNI /
+        LAPLACE_GNJ (normals held fixed, accurate semantics) when a grad array
+        is given.  Outputs are numpy unless torch CUDA tensors are given."""
         if self.kernel == HELMHOLTZ_G:  # complex charges -> complex potentials, no gradient
             return self._complex_call("fmmb_evaluate_f64" if f64 else "fmmb_evaluate", q, self.ni * self.nrhs, pot,
                                       f64), None
@@ -285,7 +288,7 @@ class Plan:
         if grad is None and self.kernel == LAPLACE_G:
             grad = np.zeros(3 * ni, dt)
         pp, pk = _ptr(pot, dt)
-        gp, gk = _ptr(grad, dt) if self.kernel == LAPLACE_G else (None, None)
+        gp, gk = _ptr(grad, dt)
         fn = load().fmmb_evaluate_f64 if f64 else load().fmmb_evaluate
         self._follow_torch(q, pot, grad)
         _check(fn(self._h, qp, pp, gp))
@@ -293,7 +296,9 @@ class Plan:
 
     def evaluate_transpose(self, w, out=None, grad=None, f64=False):
         """Charge adjoint A^T w (fmmb_evaluate_transpose): w (nrhs*ni,) ->
-        (out (nrhs*nj,), grad (3*nrhs*nj,) for LAPLACE_G or None)."""
+        (out (nrhs*nj,), grad (3*nrhs*nj,): the gradient of A^T w w.r.t. the
+        source position, for LAPLACE_G always, for the normal-derivative kernels
+        when grad is given; else None)."""
         if self.kernel == HELMHOLTZ_G:  # A^T w (no conjugation), complex
             return self._complex_call("fmmb_evaluate_transpose_f64" if f64 else "fmmb_evaluate_transpose", w,
                                       self.nj * self.nrhs, out, f64), None
@@ -305,15 +310,15 @@ class Plan:
         if grad is None and self.kernel == LAPLACE_G:
             grad = np.zeros(3 * nj, dt)
         op_, ok = _ptr(out, dt)
-        gp, gk = _ptr(grad, dt) if self.kernel == LAPLACE_G else (None, None)
+        gp, gk = _ptr(grad, dt)
         fn = load().fmmb_evaluate_transpose_f64 if f64 else load().fmmb_evaluate_transpose
         self._follow_torch(w, out, grad)
         _check(fn(self._h, wp, op_, gp))
         return ok, gk
 
     def position_grad(self, q, w, dxt=None, dxs=None):
-        """Laplace G position gradients of sum(w * pot) (fmmb_position_grad):
-        returns (dxt (3, ni), dxs (3, nj)) in FP64."""
+        """Position gradients of sum(w * pot) (fmmb_position_grad; Laplace
+        kernels, normals held fixed): returns (dxt (3, ni), dxs (3, nj)) in FP64."""
         qp, qk = _ptr(q, np.float32)
         wp, wk = _ptr(w, np.float32)
         if dxt is None:
@@ -347,7 +352,9 @@ class Plan:
         return tuple(o[1] for o in outs)
 
     def direct(self, q, i0=0, i1=None):
-        """FP64 direct sum on the GPU for targets [i0, i1) (caller order)."""
+        """FP64 direct sum on the GPU for targets [i0, i1) (caller order):
+        (pot, grad (3, i1 - i0)), grad = the gradient w.r.t. the target
+        position (normals held fixed)."""
         i1 = self.ni if i1 is None else i1
         if self.kernel == HELMHOLTZ_G:  # complex charges, complex128 potentials
             qr = np.ascontiguousarray(q, np.complex64).view(np.float32)
@@ -358,9 +365,8 @@ class Plan:
         pot = np.zeros(i1 - i0)
         grad = np.zeros(3 * (i1 - i0))
         self._follow_torch(q)
-        _check(load().fmmb_direct_f64(self._h, qp, i0, i1, pot.ctypes.data,
-                                      grad.ctypes.data if self.kernel == LAPLACE_G else None))
-        return pot, (grad.reshape(3, -1) if self.kernel == LAPLACE_G else None)
+        _check(load().fmmb_direct_f64(self._h, qp, i0, i1, pot.ctypes.data, grad.ctypes.data))
+        return pot, grad.reshape(3, -1)
 
     def tree(self, kind):
         lib = load()

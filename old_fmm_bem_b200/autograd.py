@@ -12,14 +12,14 @@ backward, for L = sum_i w_i pot_i with w = dL/dpot:
     Gni (target normals):   A^T w = -Gnj-FMM(targets = x_s, sources = x_t with normals n_t)
     Gnj (source normals):   A^T w = -Gni-FMM(targets = x_s with normals n_s, sources = x_t)
   since d/dx_j G(x_i - x_j) = -d/dx_i G(x_i - x_j).
-* positions (Laplace G): dL/dx_t = w * grad(pot)(x_t) (the forward FMM's field) and
-  dL/dx_s = q * grad(psi)(x_s) with psi = G-FMM(targets x_s, sources x_t,
-  charges w) -- the same transposed FMM as the charge adjoint, with its field.
-  So a backward costs one FMM with gradient.  When x_t and x_s are the same
-  tensor autograd adds the two contributions.
-  (Position gradients of the normal-derivative kernels need second
-  derivatives of the kernel and are not provided: their positions must not
-  require grad.)
+* positions: dL/dx_t = w * grad_t(A q) and dL/dx_s = q * grad_t(A^T w), grad_t
+  the gradient of a matvec's output w.r.t. its target position with the
+  normals held fixed: for G the field; for Gnj the field of the double layer;
+  for Gni -H n, H the Hessian of the single-layer potential (the transposed
+  matvec swaps the two).  The forward computes grad_t(A q) with the
+  potential, the backward one transposed FMM with its gradient (the charge
+  adjoint comes with it).  When x_t and x_s are the same tensor autograd adds
+  the two contributions.  Normals are constants (no gradient flows to them).
 
 An FMMOperator builds the plan (and, through fmmb_evaluate_transpose, its
 transposed plan) once; every call reuses the trees, so the geometry
@@ -59,8 +59,8 @@ class FMMOperator:
 
     def __call__(self, q):
         """Potential at the targets (FP64 accumulation, returned in q's dtype);
-        differentiable w.r.t. q and, for Laplace G, the position tensors given
-        at construction."""
+        differentiable w.r.t. q and the position tensors given at construction
+        (for Gni / Gnj in accurate semantics)."""
         return FMMFunction.apply(q, self.x_t, self.x_s, self)
 
     def close(self):
@@ -70,11 +70,9 @@ class FMMOperator:
 class FMMFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q, x_t, x_s, op):
-        if op.kernel != LAPLACE_G and (x_t.requires_grad or x_s.requires_grad):
-            raise ValueError("position gradients are provided for the Laplace G kernel only")
         qd = q.detach().to(torch.float32).contiguous()
         pot = torch.zeros(op.ni, dtype=torch.float64, device=q.device)
-        want_field = op.kernel == LAPLACE_G and x_t.requires_grad
+        want_field = x_t.requires_grad
         grad = torch.zeros(3 * op.ni, dtype=torch.float64, device=q.device) if want_field else None
         op.plan.evaluate(qd, pot, grad, f64=True)
         ctx.op = op
@@ -94,8 +92,7 @@ class FMMFunction(torch.autograd.Function):
         # weighting of the two fields
         f64 = dict(dtype=torch.float64, device=w.device)
         want_q = ctx.needs_input_grad[0]
-        want_xt = op.kernel == LAPLACE_G and ctx.needs[0]
-        want_xs = op.kernel == LAPLACE_G and ctx.needs[1]
+        want_xt, want_xs = ctx.needs
         dq = torch.empty(op.nj, **f64) if want_q else None
         dxt = torch.empty(3 * op.ni, **f64) if want_xt else None
         dxs = torch.empty(3 * op.nj, **f64) if want_xs else None
@@ -111,8 +108,7 @@ def fmm_potential(x_t, x_s, q, *, kernel=LAPLACE_G, n_t=None, n_s=None, p=10, lm
                   semantics=SEM_ACCURATE, eps2=0.0, exclude_self=True, bbox=None):
     """Differentiable FMM potential at targets x_t (3, ni) of charges q (nj,)
     at sources x_s (3, nj), all CUDA tensors (builds the trees for this call;
-    use FMMOperator to reuse them).  Gradients flow to q (all kernels) and to
-    x_t / x_s (Laplace G)."""
+    use FMMOperator to reuse them).  Gradients flow to q and to x_t / x_s."""
     op = FMMOperator(x_t, x_s, kernel=kernel, n_t=n_t, n_s=n_s, p=p, lmax=lmax, precision=precision,
                      semantics=semantics, eps2=eps2, exclude_self=exclude_self, bbox=bbox)
     return op(q)

@@ -911,13 +911,17 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     if (pl->ref)
       launch_l2p(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
                  pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
-    else if (!(pl->cfg.precision == FMMB_MIXED &&
+    else if (!(pl->cfg.precision == FMMB_MIXED && (ker == FMMB_LAPLACE_G || !want_grad) &&
                launch_l2p_f32(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
                               pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef,
                               pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m)))
       launch_l2p_cart(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
                       pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K,
-                      pot_far, g_far, pl->ni, m);
+                      pot_far, ker == FMMB_LAPLACE_GNI ? nullptr : g_far, pl->ni, m);
+    if (want_grad && ker == FMMB_LAPLACE_GNI && !pl->ref)  // its gradient needs the Hessian of the local expansion
+      launch_l2p_hess_gni(nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
+                          pl->d_fac.get(), pl->bbox, rb_leaf, s.coef, pl->L.get() + (size_t)pl->off_i[lmax] * K, g_far,
+                          pl->ni, m);
   }
   FMMB_CUDA(time_mark(pl, pl->ev[6], m));
   FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.join, 0));
@@ -985,7 +989,12 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
     cudaStream_t m = pl->st.main;
     const int ni = pl->ni, nj = pl->nj, nr = pl->cfg.nrhs;
-    const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
+    // gradient output: G, and the normal-derivative kernels in accurate
+    // semantics (the gradient w.r.t. the target position, normals fixed)
+    const bool gn = pl->cfg.kernel == FMMB_LAPLACE_GNI || pl->cfg.kernel == FMMB_LAPLACE_GNJ;
+    FMMB_REQUIRE(!(grad && gn && pl->ref), FMMB_ERR_ARG,
+                 "gradients of the normal-derivative kernels need FMMB_SEM_ACCURATE");
+    const bool want_grad = grad && (pl->cfg.kernel == FMMB_LAPLACE_G || gn);
     if (*pl->h_err) {  // reported by the tensor-core kernel of an earlier call
       const int e = *pl->h_err;
       *pl->h_err = 0;
@@ -1059,7 +1068,7 @@ int evaluate_impl(fmmb_plan* pl, const float* q, T* pot, T* grad) {
     // several right-hand sides in the mixed form: the near field of all of
     // them in one pass on the side stream (sources read once for every
     // right-hand side), the far field of each through the far-field graph
-    const bool multi = nr > 1 && pl->cfg.precision == FMMB_MIXED && pl->use_graph;
+    const bool multi = nr > 1 && pl->cfg.precision == FMMB_MIXED && pl->use_graph && !(want_grad && gn);
     if (multi) {
       pl->near_all.alloc((size_t)nr * ni * (want_grad ? 4 : 1));
       pl->qs_far.alloc(nj);
@@ -1287,14 +1296,16 @@ template <typename T>
 int transpose_impl(fmmb_plan* pl, const float* w, T* out, T* grad) {
   return guarded([&] {
     FMMB_REQUIRE(pl && w && out, FMMB_ERR_ARG, "null argument");
-    FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G || grad == nullptr, FMMB_ERR_ARG,
-                 "only the Laplace G transpose has a gradient output");
+    FMMB_REQUIRE(!helm_family(pl->cfg.kernel) || grad == nullptr, FMMB_ERR_ARG,
+                 "the complex kernels' transpose has no gradient output");
     fmmb_plan* t = transposed_plan(pl);
     const int rc = sizeof(T) == 4 ? fmmb_evaluate(t, w, (float*)out, (float*)grad)
                                   : fmmb_evaluate_f64(t, w, (double*)out, (double*)grad);
     if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
-    if (pl->cfg.kernel == FMMB_LAPLACE_GNI || pl->cfg.kernel == FMMB_LAPLACE_GNJ)
+    if (pl->cfg.kernel == FMMB_LAPLACE_GNI || pl->cfg.kernel == FMMB_LAPLACE_GNJ) {  // A^T = -(swapped plan)
       negate(out, (size_t)pl->nj * pl->cfg.nrhs, t->st.main);
+      if (grad) negate(grad, (size_t)3 * pl->nj * pl->cfg.nrhs, t->st.main);
+    }
   });
 }
 
@@ -1312,7 +1323,9 @@ int fmmb_evaluate_transpose_f64(fmmb_plan* pl, const float* w, double* out, doub
 int fmmb_position_grad(fmmb_plan* pl, const float* q, const float* w, double* dxt, double* dxs) {
   return guarded([&] {
     FMMB_REQUIRE(pl && q && w && (dxt || dxs), FMMB_ERR_ARG, "null argument");
-    FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G, FMMB_ERR_ARG, "position gradients are for the Laplace G kernel");
+    FMMB_REQUIRE(!helm_family(pl->cfg.kernel), FMMB_ERR_ARG, "position gradients are for the Laplace kernels");
+    FMMB_REQUIRE(pl->cfg.kernel == FMMB_LAPLACE_G || !pl->ref, FMMB_ERR_ARG,
+                 "position gradients of the normal-derivative kernels need FMMB_SEM_ACCURATE");
     FMMB_REQUIRE(pl->cfg.nrhs == 1, FMMB_ERR_ARG, "position gradients take one right-hand side");
     FMMB_REQUIRE(pl->have_geometry, FMMB_ERR_STATE, "fmmb_set_geometry must come first");
     const int ni = pl->ni, nj = pl->nj;
@@ -1345,8 +1358,8 @@ int fmmb_adjoint_f64(fmmb_plan* pl, const float* q, const float* w, const double
                      double* dxs) {
   return guarded([&] {
     FMMB_REQUIRE(pl && w && (dq || dxt || dxs), FMMB_ERR_ARG, "null argument");
-    FMMB_REQUIRE((!dxt && !dxs) || pl->cfg.kernel == FMMB_LAPLACE_G, FMMB_ERR_ARG,
-                 "position gradients are for the Laplace G kernel");
+    FMMB_REQUIRE((!dxt && !dxs) || pl->cfg.kernel == FMMB_LAPLACE_G || !pl->ref, FMMB_ERR_ARG,
+                 "position gradients of the normal-derivative kernels need FMMB_SEM_ACCURATE");
     FMMB_REQUIRE(!dxt || field_t, FMMB_ERR_ARG, "dxt needs the forward field");
     FMMB_REQUIRE(!dxs || q, FMMB_ERR_ARG, "dxs needs the charges");
     FMMB_REQUIRE(pl->cfg.nrhs == 1 || (!dxt && !dxs), FMMB_ERR_ARG, "position gradients take one right-hand side");
@@ -1432,7 +1445,7 @@ int fmmb_direct_f64(fmmb_plan* pl, const float* q, int i0, int i1, double* pot, 
     }
     const float* qd = to_device(q, nj, pl->stage_f, m);
     launch_gather_charges(nj, 1, pl->perm_j.get(), qd, pl->qs.get(), m);
-    const bool want_grad = grad && pl->cfg.kernel == FMMB_LAPLACE_G;
+    const bool want_grad = grad != nullptr;  // every Laplace kernel (w.r.t. the target position, normals fixed)
     DevBuf<double> out;
     out.alloc((size_t)cnt * 4 + 1);
     if (pl->nprob == 1) {

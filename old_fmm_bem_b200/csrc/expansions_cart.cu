@@ -395,12 +395,159 @@ __global__ void __launch_bounds__(kL2PThreads) l2p_cart(int p, int K, const int*
       pot[i] = -c2 * ((double)nv.x * gx + (double)nv.y * gy + (double)nv.z * gz);
     } else {
       pot[i] = c1 * F;
-      if (KER == FMMB_LAPLACE_G && grad) {
+      if (grad) {  // G and Gnj: the local expansion is the potential itself
         grad[i] = c2 * gx;
         grad[ni + i] = c2 * gy;
         grad[2 * ni + i] = c2 * gz;
       }
     }
+  }
+}
+
+// ------------------------------------------------------------------ L2P, Hessian
+// The gradient w.r.t. the target position of the far-field Gni potential
+// -(1/4pi) n . grad(phi) (normal held fixed): -(1/4pi) H n, H the Hessian of
+// the local expansion.  One block (64 threads) per target leaf.  With F the
+// real potential of L in scaled coordinates written over all orders,
+// F = sum_{n, |m| <= n} b_n^m S_n^m (b_n^m = fac(n,m) L_n^m for m >= 0,
+// b_n^{-m} = (-1)^m (n+m)!/(n-m)! conj(b_n^m)), the ladder identities give its
+// derivatives as expansions of one degree less:
+//   d/dx F: c_{n-1}^k = (b_n^{k-1} - (n+k+1)(n+k) b_n^{k+1}) / 2
+//   d/dy F: c_{n-1}^k = (b_n^{k-1} + (n+k+1)(n+k) b_n^{k+1}) / (2i)
+//   d/dz F: c_{n-1}^k = (n+k) b_n^k
+// i.e. local expansions L^D = c / fac of the same form (real potentials); the
+// gradient of each, evaluated like l2p_cart's, is one row of H.
+constexpr int kL2PHThreads = 64;
+
+__global__ void __launch_bounds__(kL2PHThreads) l2p_hess_gni(int p, int K, const int* __restrict__ keys,
+                                                             const int2* __restrict__ leaf,
+                                                             const float4* __restrict__ tpos,
+                                                             const float4* __restrict__ tnrm,
+                                                             const double* __restrict__ fac, float xmin, float ymin,
+                                                             float zmin, double rb, double coef,
+                                                             const double* __restrict__ L, double* __restrict__ grad,
+                                                             int ni) {
+  extern __shared__ double sm[];
+  const int P = (p + 1) * (p + 2) / 2;
+  cplx* Ld = reinterpret_cast<cplx*>(sm);  // [3][P] derivative expansions (m >= 0)
+  cplx* Cz = Ld + 3 * P;                   // [3][P] their gradient coefficient sets
+  cplx* Cp = Cz + 3 * P;
+  cplx* Cm = Cp + 3 * P;
+  double* Cs = reinterpret_cast<double*>(Cm + 3 * P);  // [3][p+1]
+  const int b = blockIdx.x;
+  const double* Lb = L + (size_t)b * K;
+  auto bnm = [&](int n, int m) -> cplx {  // b_n^m for -1 <= m
+    if (n < 0 || m > n || n > p) return {0.0, 0.0};
+    if (m == -1) {
+      if (n < 1) return {0.0, 0.0};
+      const double f = fac[ifull_d(n, 1)];
+      return {-(double)n * (n + 1) * f * Lb[n * n + 1], (double)n * (n + 1) * f * Lb[n * n + 2]};
+    }
+    if (m == 0) return {fac[ifull_d(n, 0)] * Lb[n * n], 0.0};
+    const double f = fac[ifull_d(n, m)];
+    return {f * Lb[n * n + 2 * m - 1], f * Lb[n * n + 2 * m]};
+  };
+  for (int idx = threadIdx.x; idx < P; idx += blockDim.x) {
+    int n1 = 0;
+    while ((n1 + 1) * (n1 + 2) / 2 <= idx) n1++;
+    const int k = idx - n1 * (n1 + 1) / 2;  // degree n1 = n - 1, order k
+    cplx cx = {0.0, 0.0}, cy = {0.0, 0.0}, cz = {0.0, 0.0};
+    if (n1 < p) {
+      const int n = n1 + 1;
+      const cplx lo = bnm(n, k - 1), hi = bnm(n, k + 1), mid = bnm(n, k);
+      const double a = (double)(n + k + 1) * (double)(n + k);
+      cx = {0.5 * (lo.re - a * hi.re), 0.5 * (lo.im - a * hi.im)};
+      const cplx t = {lo.re + a * hi.re, lo.im + a * hi.im};
+      cy = {0.5 * t.im, -0.5 * t.re};  // t / (2i)
+      cz = {(n + k) * mid.re, (n + k) * mid.im};
+    }
+    const double inv = 1.0 / fac[ifull_d(n1, k)];
+    Ld[idx] = cscale(cx, inv);
+    Ld[P + idx] = cscale(cy, inv);
+    Ld[2 * P + idx] = cscale(cz, inv);
+    if (k == 0) {  // real by construction; drop the rounding residue
+      Ld[idx].im = Ld[P + idx].im = Ld[2 * P + idx].im = 0.0;
+    }
+  }
+  __syncthreads();
+  // gradient coefficient sets of each derivative expansion (as l2p_cart's of L)
+  for (int e = threadIdx.x; e < 3 * P; e += blockDim.x) {
+    const int d = e / P, idx = e % P;
+    const cplx* Lx = Ld + d * P;
+    auto Lnm = [&](int n, int m) -> cplx { return Lx[n * (n + 1) / 2 + m]; };
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= idx) n++;
+    const int m = idx - n * (n + 1) / 2;
+    const double wm = m ? 2.0 : 1.0;
+    if (n < p) {
+      Cz[e] = cscale(Lnm(n + 1, m), wm * fac[ifull_d(n + 1, m)] * (n + 1 + m));
+      Cp[e] = (m >= 1) ? cscale(Lnm(n + 1, m - 1), (m - 1 ? 2.0 : 1.0) * fac[ifull_d(n + 1, m - 1)]) : cplx{0.0, 0.0};
+      Cm[e] = (m + 1 <= n + 1) ? cscale(Lnm(n + 1, m + 1), -2.0 * fac[ifull_d(n + 1, m + 1)] * (double)(n + m + 2) *
+                                                                (double)(n + m + 1))
+                               : cplx{0.0, 0.0};
+    } else {
+      Cz[e] = Cp[e] = Cm[e] = cplx{0.0, 0.0};
+    }
+  }
+  for (int e = threadIdx.x; e < 3 * (p + 1); e += blockDim.x) {
+    const int d = e / (p + 1), n = e % (p + 1);
+    Cs[e] = (n < p) ? fac[ifull_d(n + 1, 0)] * Ld[d * P + (n + 1) * (n + 2) / 2].re : 0.0;
+  }
+  __syncthreads();
+  double xc, yc, zc;
+  box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
+  const int2 lf = leaf[b];
+  const double inv_rb = 1.0 / rb;
+  for (int ii = threadIdx.x; ii < lf.y; ii += blockDim.x) {
+    const int i = lf.x + ii;
+    const float4 xt = tpos[i];
+    const double x = ((double)xt.x - xc) * inv_rb, y = ((double)xt.y - yc) * inv_rb, z = ((double)xt.z - zc) * inv_rb;
+    const double r2 = x * x + y * y + z * z;
+    double dzr[3] = {0, 0, 0}, dpr[3] = {0, 0, 0}, dpi[3] = {0, 0, 0}, dmr[3] = {0, 0, 0}, dmi[3] = {0, 0, 0};
+    cplx smm = {1.0, 0.0};
+    for (int m = 0; m <= p; m++) {
+      if (m > 0) smm = cscale(cmul(smm, cplx{x, y}), -(2.0 * m - 1.0));
+      cplx s1 = {0.0, 0.0}, s2 = {0.0, 0.0};
+      for (int n = m; n < p; n++) {  // the derivative expansions stop at degree p - 1
+        cplx sn;
+        if (n == m) sn = smm;
+        else if (n == m + 1) sn = cscale(s1, (2.0 * m + 1.0) * z);
+        else {
+          const double inv = c_inv[n - m];
+          const double a = (2.0 * n - 1.0) * z * inv, c = (n + m - 1.0) * r2 * inv;
+          sn = {a * s1.re - c * s2.re, a * s1.im - c * s2.im};
+        }
+        const int idx = n * (n + 1) / 2 + m;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+          const cplx cz = Cz[d * P + idx], cp = Cp[d * P + idx], cmm = Cm[d * P + idx];
+          dzr[d] += cz.re * sn.re - cz.im * sn.im;
+          dpr[d] += cp.re * sn.re - cp.im * sn.im;
+          dpi[d] += cp.re * sn.im + cp.im * sn.re;
+          dmr[d] += cmm.re * sn.re - cmm.im * sn.im;
+          dmi[d] += cmm.re * sn.im + cmm.im * sn.re;
+          if (m == 1) {
+            dmr[d] += Cs[d * (p + 1) + n] * sn.re;
+            dmi[d] -= Cs[d * (p + 1) + n] * sn.im;
+          }
+        }
+        s2 = s1;
+        s1 = sn;
+      }
+    }
+    const float4 nv = tnrm[i];
+    const double nn[3] = {(double)nv.x, (double)nv.y, (double)nv.z};
+    double hn[3] = {0, 0, 0};  // H n in scaled coordinates (H symmetric: row d of H is grad(d/dd F))
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      hn[0] += nn[d] * 0.5 * (dpr[d] + dmr[d]);
+      hn[1] += nn[d] * 0.5 * (dpi[d] - dmi[d]);
+      hn[2] += nn[d] * dzr[d];
+    }
+    const double c3 = -coef * inv_rb * inv_rb * inv_rb;
+    grad[i] = c3 * hn[0];
+    grad[ni + i] = c3 * hn[1];
+    grad[2 * ni + i] = c3 * hn[2];
   }
 }
 
@@ -636,6 +783,17 @@ void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const
     l2p_cart<FMMB_LAPLACE_GNI><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
   else
     l2p_cart<FMMB_LAPLACE_GNJ><<<nleaf, kL2PThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+  FMMB_CHECK_LAUNCH();
+}
+
+void launch_l2p_hess_gni(int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                         const float4* tnrm, const double* fac, const float* bbox, double rb, double coef,
+                         const double* L, double* grad, int ni, cudaStream_t st) {
+  if (nleaf <= 0) return;
+  const int P = (p + 1) * (p + 2) / 2;
+  const size_t sm = (size_t)12 * P * sizeof(cplx) + 3 * (p + 1) * sizeof(double);
+  l2p_hess_gni<<<nleaf, kL2PHThreads, sm, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef,
+                                                L, grad, ni);
   FMMB_CHECK_LAUNCH();
 }
 

@@ -406,11 +406,16 @@ int fmmb_gmres(fmmb_plan* pl, const fmmb_gmres_config* cfg, const float* weight,
       if (stop || it >= cfg->max_iter) break;
     }
     if (resid_out) {
+      // the residual of the returned iterate itself, ||d (b - A x)||, by one
+      // more matvec (the Givens estimate |g| keeps falling below what the
+      // matvec's own rounding lets A x reach, in the mixed form by orders)
+      matvec(X, nullptr, 1, V);
+      dots(V, 1, V, nrm2, 1);
       std::vector<double> r(nsys), b0(nsys);
-      FMMB_CUDA(cudaMemcpyAsync(r.data(), S.resid, nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
+      FMMB_CUDA(cudaMemcpyAsync(r.data(), nrm2, nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
       FMMB_CUDA(cudaMemcpyAsync(b0.data(), S.beta0, nsys * sizeof(double), cudaMemcpyDeviceToHost, st));
       FMMB_CUDA(cudaStreamSynchronize(st));
-      for (int k = 0; k < nsys; k++) r[k] = b0[k] > 0 ? r[k] / b0[k] : 0.0;
+      for (int k = 0; k < nsys; k++) r[k] = b0[k] > 0 ? std::sqrt(std::max(r[k], 0.0)) / b0[k] : 0.0;
       if (is_dev(resid_out)) FMMB_CUDA(cudaMemcpy(resid_out, r.data(), nsys * sizeof(double), cudaMemcpyHostToDevice));
       else std::memcpy(resid_out, r.data(), nsys * sizeof(double));
     }

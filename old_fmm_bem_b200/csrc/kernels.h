@@ -37,6 +37,11 @@ void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const
 void launch_l2p_cart(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
                      const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
                      double* pot, double* grad, int ni, cudaStream_t st);
+// far-field gradient of the Gni potential w.r.t. the target position
+// (normal fixed), -(1/4pi) H n from the local expansions (accurate semantics)
+void launch_l2p_hess_gni(int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
+                         const float4* tnrm, const double* fac, const float* bbox, double rb, double coef,
+                         const double* L, double* grad, int ni, cudaStream_t st);
 // mixed-form near field of nrhs right-hand sides in one pass (p2p_multi.cu):
 // qs [nrhs][nj] sorted charges, pot [nrhs][ni], grad [nrhs][3][ni] (G only,
 // may be null); work items (target leaf, first target) of up to 128 targets.

@@ -102,18 +102,35 @@ __global__ void __launch_bounds__(kP2PThreads) p2p_f64(const int2* __restrict__ 
             fx -= dx * qr3;
             fy -= dy * qr3;
             fz -= dz * qr3;
-          } else if (KER == FMMB_LAPLACE_GNI) {
-            p += (dx * (double)ni4.x + dy * (double)ni4.y + dz * (double)ni4.z) * qr * rinv * rinv;
           } else {
-            const float4 nj = sn[jj];
-            p += (dx * (double)nj.x + dy * (double)nj.y + dz * (double)nj.z) * qr * rinv * rinv;
+            // Gni: n = the target's normal; Gnj: the source's.  With a gradient
+            // (accurate semantics): d/dx_i of q (d.n) / r^3 = q n / r^3 - 3 q (d.n) d / r^5
+            double nx, ny, nz;
+            if (KER == FMMB_LAPLACE_GNI) {
+              nx = ni4.x;
+              ny = ni4.y;
+              nz = ni4.z;
+            } else {
+              const float4 nj = sn[jj];
+              nx = nj.x;
+              ny = nj.y;
+              nz = nj.z;
+            }
+            const double qr3 = qr * rinv * rinv, dot = dx * nx + dy * ny + dz * nz;
+            p += dot * qr * rinv * rinv;  // the potential's operation order as without the gradient
+            if (grad) {
+              const double c = -3.0 * dot * qr3 * rinv * rinv;
+              fx += qr3 * nx + c * dx;
+              fy += qr3 * ny + c * dy;
+              fz += qr3 * nz + c * dz;
+            }
           }
         }
       }
     }
     if (act) {
       pot[i] = p;
-      if (KER == FMMB_LAPLACE_G && grad) {
+      if (grad) {
         grad[i] = fx;
         grad[ni + i] = fy;
         grad[2 * ni + i] = fz;
@@ -473,17 +490,28 @@ __global__ void __launch_bounds__(128) direct_f64(int i0, int i1, const int* __r
         fx -= dx * qr3;
         fy -= dy * qr3;
         fz -= dz * qr3;
-      } else if (KER == FMMB_LAPLACE_GNI) {
-        p += (dx * nv.x + dy * nv.y + dz * nv.z) * qr * rinv * rinv;
       } else {
-        const float4 nj4 = sn[jj];
-        p += (dx * nj4.x + dy * nj4.y + dz * nj4.z) * qr * rinv * rinv;
+        // Gni: the target's normal, Gnj: the source's; gradient w.r.t. the
+        // target position with the normal fixed: q n / r^3 - 3 q (d.n) d / r^5
+        double nx = nv.x, ny = nv.y, nz = nv.z;
+        if (KER == FMMB_LAPLACE_GNJ) {
+          const float4 nj4 = sn[jj];
+          nx = nj4.x;
+          ny = nj4.y;
+          nz = nj4.z;
+        }
+        const double qr3 = qr * rinv * rinv, dot = dx * nx + dy * ny + dz * nz;
+        p += dot * qr * rinv * rinv;  // the potential's operation order as without the gradient
+        const double c = -3.0 * dot * qr3 * rinv * rinv;
+        fx += qr3 * nx + c * dx;
+        fy += qr3 * ny + c * dy;
+        fz += qr3 * nz + c * dz;
       }
     }
   }
   if (act) {
     pot[i - i0] = p;
-    if (KER == FMMB_LAPLACE_G && grad) {
+    if (grad) {
       const int m = i1 - i0;
       grad[i - i0] = fx;
       grad[m + i - i0] = fy;

@@ -68,9 +68,16 @@ struct Acc {
   float p, fx, fy, fz;
 };
 
+// Kernel selector of the templates: a Laplace kernel, plus kWithGrad for the
+// normal-derivative kernels with the gradient of the potential w.r.t. the
+// target position (normals held fixed) as well.
+constexpr int kWithGrad = 16;
+constexpr int base(int KER) { return KER & (kWithGrad - 1); }
+constexpr bool with_grad(int KER) { return KER == FMMB_LAPLACE_G || (KER & kWithGrad) != 0; }
+
 template <int KER>
 constexpr int ncomp() {
-  return KER == FMMB_LAPLACE_G ? 4 : 1;  // accumulated components
+  return with_grad(KER) ? 4 : 1;  // accumulated components: potential (and gradient)
 }
 
 // Negated positions of sources j, j + 1 (even j) of the staged list, packed
@@ -85,9 +92,9 @@ struct Smem {
   static constexpr int NP = kCap / 2;
   float4 A[NP];
   float2 B[NP];
-  float2 Q[KER == FMMB_LAPLACE_GNJ ? 1 : NP];
-  float4 M[KER == FMMB_LAPLACE_GNJ ? NP : 1];   // (qn_x j, j+1, qn_y j, j+1)
-  float2 MZ[KER == FMMB_LAPLACE_GNJ ? NP : 1];  // (qn_z j, j+1)
+  float2 Q[base(KER) == FMMB_LAPLACE_GNJ ? 1 : NP];
+  float4 M[base(KER) == FMMB_LAPLACE_GNJ ? NP : 1];   // (qn_x j, j+1, qn_y j, j+1)
+  float2 MZ[base(KER) == FMMB_LAPLACE_GNJ ? NP : 1];  // (qn_z j, j+1)
   double red[kWarps][kMaxNT][NC][kG];           // team partial sums
   int2 seg[32];                                 // (first source, count), own leaf first
   int vst[32];                                  // virtual start of each segment, then INT_MAX
@@ -111,7 +118,7 @@ __device__ __forceinline__ void run16(const Smem<KER>& S, int pb, const Tgt (&tg
     const float4 a = S.A[pi];
     const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w), sz = S.B[pi];
     float2 q2 = make_float2(0.f, 0.f), mx = q2, my = q2, mz = q2;
-    if (KER == FMMB_LAPLACE_GNJ) {
+    if (base(KER) == FMMB_LAPLACE_GNJ) {
       const float4 m = S.M[pi];
       mx = make_float2(m.x, m.y);
       my = make_float2(m.z, m.w);
@@ -135,14 +142,26 @@ __device__ __forceinline__ void run16(const Smem<KER>& S, int pb, const Tgt (&tg
         acc[t][1] = __ffma2_rn(dx, qr3, acc[t][1]);
         acc[t][2] = __ffma2_rn(dy, qr3, acc[t][2]);
         acc[t][3] = __ffma2_rn(dz, qr3, acc[t][3]);
-      } else if (KER == FMMB_LAPLACE_GNI) {
+      } else if (base(KER) == FMMB_LAPLACE_GNI) {
         const float2 qr3 = __fmul2_rn(__fmul2_rn(__fmul2_rn(q2, ri), ri), ri);
         const float2 dot = __ffma2_rn(dx, tg[t].nx, __ffma2_rn(dy, tg[t].ny, __fmul2_rn(dz, tg[t].nz)));
         acc[t][0] = __ffma2_rn(dot, qr3, acc[t][0]);
+        if (with_grad(KER)) {  // d/dx_i of (d.n_i) q / r^3 = q n_i / r^3 - 3 (d.n_i) q d / r^5
+          const float2 c = __fmul2_rn(__fmul2_rn(dot, qr3), __fmul2_rn(__fmul2_rn(ri, ri), dup(-3.f)));
+          acc[t][1] = __ffma2_rn(qr3, tg[t].nx, __ffma2_rn(c, dx, acc[t][1]));
+          acc[t][2] = __ffma2_rn(qr3, tg[t].ny, __ffma2_rn(c, dy, acc[t][2]));
+          acc[t][3] = __ffma2_rn(qr3, tg[t].nz, __ffma2_rn(c, dz, acc[t][3]));
+        }
       } else {
         const float2 r3 = __fmul2_rn(__fmul2_rn(ri, ri), ri);
         const float2 dot = __ffma2_rn(dx, mx, __ffma2_rn(dy, my, __fmul2_rn(dz, mz)));
         acc[t][0] = __ffma2_rn(dot, r3, acc[t][0]);
+        if (with_grad(KER)) {  // d/dx_i of (d.m) / r^3 = m / r^3 - 3 (d.m) d / r^5, m = q n_j
+          const float2 c = __fmul2_rn(__fmul2_rn(dot, r3), __fmul2_rn(__fmul2_rn(ri, ri), dup(-3.f)));
+          acc[t][1] = __ffma2_rn(mx, r3, __ffma2_rn(c, dx, acc[t][1]));
+          acc[t][2] = __ffma2_rn(my, r3, __ffma2_rn(c, dy, acc[t][2]));
+          acc[t][3] = __ffma2_rn(mz, r3, __ffma2_rn(c, dz, acc[t][3]));
+        }
       }
     }
   }
@@ -181,7 +200,7 @@ __device__ void stage(Smem<KER>& S, int c0, int c1, const float4* __restrict__ s
       if (jj[u] >= 0) {
         x[u] = spos[jj[u]];
         q[u] = qs[jj[u]];
-        if (KER == FMMB_LAPLACE_GNJ) n[u] = snrm[jj[u]];
+        if (base(KER) == FMMB_LAPLACE_GNJ) n[u] = snrm[jj[u]];
       }
     }
 #pragma unroll
@@ -192,7 +211,7 @@ __device__ void stage(Smem<KER>& S, int c0, int c1, const float4* __restrict__ s
         const float q0 = q[2 * h], q1 = q[2 * h + 1];
         S.A[pi] = make_float4(-x0.x, -x1.x, -x0.y, -x1.y);
         S.B[pi] = make_float2(-x0.z, -x1.z);
-        if (KER == FMMB_LAPLACE_GNJ) {
+        if (base(KER) == FMMB_LAPLACE_GNJ) {
           const float4 n0 = n[2 * h], n1 = n[2 * h + 1];
           S.M[pi] = make_float4(q0 * n0.x, q1 * n1.x, q0 * n0.y, q1 * n1.y);
           S.MZ[pi] = make_float2(q0 * n0.z, q1 * n1.z);
@@ -308,7 +327,7 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ w
       const int it = (ga + t) * kG + g;
       const bool on = t < ntl && it < li.y;
       const float4 x = on ? tpos[li.x + it] : z4;
-      const float4 n = (KER == FMMB_LAPLACE_GNI && on) ? tnrm[li.x + it] : z4;
+      const float4 n = (base(KER) == FMMB_LAPLACE_GNI && on) ? tnrm[li.x + it] : z4;
       tg[t] = Tgt{dup(x.x), dup(x.y), dup(x.z), dup(n.x), dup(n.y), dup(n.z)};
 #pragma unroll
       for (int c = 0; c < NC; c++) P[t][c] = 0.0;
@@ -355,10 +374,14 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ w
         if (t < ntl && it < li.y) {
           const int i = li.x + it;
           pot[i] = coef * P[t][0];
-          if (KER == FMMB_LAPLACE_G && grad) {
+          if (KER == FMMB_LAPLACE_G && grad) {  // grad(1/r) = -d / r^3
             grad[i] = -coef * P[t][1];
             grad[ni + i] = -coef * P[t][2];
             grad[2 * (size_t)ni + i] = -coef * P[t][3];
+          } else if (with_grad(KER)) {
+            grad[i] = coef * P[t][1];
+            grad[ni + i] = coef * P[t][2];
+            grad[2 * (size_t)ni + i] = coef * P[t][3];
           }
         }
       }
@@ -389,6 +412,12 @@ void launch_p2p_mixed(int kernel, int nwork, const int2* work, const int2* leaf_
   if (kernel == FMMB_LAPLACE_G)
     launch_k<FMMB_LAPLACE_G>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot,
                              grad, ni, st);
+  else if (kernel == FMMB_LAPLACE_GNI && grad)
+    launch_k<FMMB_LAPLACE_GNI | kWithGrad>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2,
+                                           s.coef, pot, grad, ni, st);
+  else if (kernel == FMMB_LAPLACE_GNJ && grad)
+    launch_k<FMMB_LAPLACE_GNJ | kWithGrad>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2,
+                                           s.coef, pot, grad, ni, st);
   else if (kernel == FMMB_LAPLACE_GNI)
     launch_k<FMMB_LAPLACE_GNI>(nwork, excl, work, leaf_i, leaf_j, list, tpos, tnrm, spos, snrm, qs, eps2, s.coef, pot,
                                grad, ni, st);

@@ -34,6 +34,9 @@ def test_solvation_energy_matches_dense(precision, tmp_path):
     cen, nrm, area = bem.panels(v, f)
     Ed, xd, _ = bem_oracle.solvation_energy_dense(cen, nrm, area, xa, qa)
     tol_e, tol_x = (1e-6, 1e-4) if precision == 0 else (1e-5, 1e-4)
-    assert info["iterations"] < 100 and info["rel_resid"] <= 1e-9
+    # rel_resid is the residual of the returned density through the FMM itself:
+    # at the iteration's own level in FP64, at the mixed matvec's rounding level
+    # (relative ~1e-7 of A x) in the mixed form
+    assert info["iterations"] < 100 and info["rel_resid"] <= (1e-9 if precision == 0 else 1e-5)
     assert abs(E - Ed) <= tol_e * abs(Ed)
     assert np.linalg.norm(info["density"] - xd) <= tol_x * np.linalg.norm(xd)
