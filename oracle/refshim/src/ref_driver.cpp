@@ -15,6 +15,13 @@
 // so the stale near-field list is reused for the level-2 M2L and the result is
 // inf.  Here mode 3 is mapped to mode 1 (every non-adjacent box at level 2),
 // which is what the level-2 step needs.
+//
+// A second link-time replacement: multipoleh() instead of
+// kernel/multipoleh.cxx, whose Bessel buffer (kernel/multipoleh.cxx:10,
+// double inr[mpcmp], mp entries) is one entry short of what in() writes
+// (nb + 1 = mp + 1, kernel/in.cxx:34) -- a stack overflow that crashes the
+// reference's Yukawa FMM (neq 10).  The replacement below has the longer
+// buffer and otherwise the same recurrences in the same order.
 #define MAIN
 #include "../include/constants.h"
 #include <arrays.h>
@@ -57,6 +64,40 @@ void ifbox(int mi, int mj, int nmp, int lbi, int lbj, int& lbjr, int lev, int ne
     for (int k = 0; k < nij[ii]; k++) g_lists.push_back(neij[ii][k]);
 }
 
+extern void in(double, double, const int, double*, int);
+
+// Replacement for kernel/multipoleh.cxx:8-33 (see the header comment): the
+// scaled modified spherical Bessel values i_n(lambda rh) (n = 0..mp, one entry
+// more than the reference's buffer holds) times (2n + 1) fac(n,m)^2
+// P_n^m(cos al) into bnm[n n + n + m], with the associated Legendre functions
+// by the upward recurrence in n from P_m^m = (-1)^m (2m-1)!! sin^m(al) --
+// operation for operation as the reference, so that the outputs are bit
+// identical; `be` is unused there too.
+void multipoleh(double rh, double al, double be, int mpx) {
+  (void)be;
+  double inr[mpcmp + 1];
+  in(scale, rh * lambda, mpx, inr, 0);
+  const double c = cos(al);
+  const double s = sqrt((1 - c) * (1 + c));
+  double pmm = 1, odd = 1;
+  for (int m = 0; m < mpx; m++) {
+    double pcur = pmm;  // P_m^m
+    int k = m * m + 2 * m;
+    bnm[k] = inr[m] * (2 * m + 1) * fac[k] * fac[k] * pcur;
+    double pprev = pcur;
+    pcur = c * (2 * m + 1) * pcur;  // P_{m+1}^m
+    for (int n = m + 1; n < mpx; n++) {
+      k = n * n + n + m;
+      bnm[k] = inr[n] * (2 * n + 1) * fac[k] * fac[k] * pcur;
+      const double pp = pprev;
+      pprev = pcur;
+      pcur = (c * (2 * n + 1) * pprev - (n + m) * pp) / (n - m + 1);
+    }
+    pmm = -pmm * odd * s;
+    odd += 2;
+  }
+}
+
 static void alloc_points(int n, int nbox) {
   int m = n > 0 ? n : 1;
   int mc = m > nbox ? m : nbox;
@@ -96,7 +137,13 @@ int ref_fmm(int ni, int nj, int neq, int lmax_in,
             const float* snx, const float* sny, const float* snz, const float* sq,
             float* v_out, float* gx_out, float* gy_out, float* gz_out, double* timings) {
   nprocs = 1; myrank = 0; umem = 0; ncheck = 0;
-  if (lmax_in > 0) lmax = lmax_in; else nlevel(nj);
+  static double tfmm_nlevel[100];  // nlevel() adds its time to tfmm[0] before the arrays exist
+  if (lmax_in > 0) {
+    lmax = lmax_in;
+  } else {
+    tfmm = tfmm_nlevel;
+    nlevel(nj);
+  }
   nbmax = 1 << 3 * lmax;
   xmin = xmin_in; ymin = ymin_in; zmin = zmin_in; rd = rd_in;
   lambda = lambda_in;

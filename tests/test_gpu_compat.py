@@ -3,6 +3,7 @@ fmm(mi, mj, neq), G_dir, Gni_dir, Gnj_dir over the reference's global arrays)
 driven from a C++ program shaped like the reference's test/test.cxx, against
 the reference's own outputs (golden fixtures made from the reference built
 from source)."""
+import ctypes
 import glob
 import os
 import subprocess
@@ -103,3 +104,50 @@ def test_yukawa_entry_points(driver, tmp_path, oracle):
     ref, _ = oracle.ref_direct(t, t, q, neq=10, lam=lam)
     assert rel(d10, ref.astype(np.float64)) < 1e-6
     assert rel(v10, ref.astype(np.float64)) < 1e-5
+
+
+def _testh_inputs():
+    """The inputs of the reference's Yukawa test driver (test/testh.cxx): 1000
+    points from C rand() (seed 1) uniform in [-pi, pi]^3 in single precision
+    (ten draws per point: x, y, z, three target normals, three source
+    normals, the charge in [0, 1]), the root cube around them, lambda = 0.1."""
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(1)
+    n = 1000
+    a = np.array([libc.rand() for _ in range(10 * n)], np.float64).reshape(n, 10).astype(np.float32)
+    u = a / np.float32(2147483647)
+    pi = np.float32(np.pi)
+    x = np.ascontiguousarray((u[:, 0:3] * np.float32(2) * pi - pi).T)
+    q = np.ascontiguousarray(u[:, 9])
+    lo, hi = x.min(axis=1), x.max(axis=1)
+    rd = np.float32((hi - lo).max())
+    xmin = (lo + hi) / np.float32(2) - rd / np.float32(2)
+    return x, q, (float(xmin[0]), float(xmin[1]), float(xmin[2]), float(rd)), 0.1
+
+
+@pytest.mark.gpu
+def test_yukawa_fmm_vs_reference_fmm(oracle):
+    """The Yukawa FMM against the reference's own Yukawa FMM (fmm(n, n, 10),
+    built from source with its kernel/multipoleh.cxx:10 buffer overflow fixed
+    at link time) on test/testh.cxx's inputs, at its order (mp = 9, p = 8;
+    its other plane-wave table, mp = 18, returns a relative error of 9 on
+    these inputs), the same depth (the reference's nlevel: 2) and root cube, softening 1e-6 and self pairs
+    included like the reference: the two agree to the reference's own error
+    against its direct sum (kernel/Helmholtz_G_dir.cxx), and this FMM is at
+    least as accurate as the reference's."""
+    import old_fmm_bem_b200 as ob
+    p = 8
+    if not oracle.ref_available(p):
+        pytest.skip("reference library not built")
+    x, q, bb, lam = _testh_inputs()
+    vr, _ = oracle.ref_fmm(x, x, q, neq=10, p=p, lmax=0, bbox=bb, lam=lam)
+    vd, _ = oracle.ref_direct(x, x, q, neq=10, p=p, lam=lam)
+    pl = ob.Plan(kernel=ob.YUKAWA, p=p, lmax=2, precision=ob.FP64, semantics=ob.SEM_ACCURATE, eps2=float(np.float32(1e-6)),
+                 exclude_self=False, wavenumber=lam)
+    pl.set_geometry(x, x, bbox=bb)
+    v, _ = pl.evaluate(q, f64=True)
+    pl.close()
+    vr, vd = vr.astype(np.float64), vd.astype(np.float64)
+    e_ref, e_ours = rel(vr, vd), rel(v, vd)
+    assert e_ours <= e_ref
+    assert rel(v, vr) <= 2 * e_ref

@@ -290,3 +290,53 @@ def test_many_rhs_near_field_vs_direct(neq, ob, oracle):
     for r in (0, 7, 8):
         ref, _ = oracle.direct(t, s, qs[r], neq=neq, eps2=0.0, exclude_self=True, tn=tn, sn=sn, targets=(0, 1000))
         assert rel(v[r * 8000:r * 8000 + 1000], ref) < 5e-6
+
+
+def _bench_sphere():
+    from old_fmm_bem_b200 import geometry
+    x, n, q = geometry.bem_double_layer_problem(6, seed=0)
+    return x, q
+
+
+def _bench_clusters(n):
+    rng = np.random.default_rng(13)
+    c = rng.uniform(0.1, 0.9, (3, 32))
+    lab = rng.integers(0, 32, 1 << 20)
+    x = np.clip(c[:, lab] + 0.02 * rng.standard_normal((3, 1 << 20)), 0.0, 1.0).astype(np.float32)
+    q = rng.standard_normal(1 << 20).astype(np.float32)
+    return np.ascontiguousarray(x[:, :n]), q[:n].copy()
+
+
+@pytest.mark.parametrize("case", ["sphere245760_lmax5", "clustered262144_lmax6"])
+def test_tree_bit_exact_vs_reference_at_benchmark_sizes(case, ob, oracle):
+    """Permutations, leaf ranges and every interaction list bit-exact against
+    the reference library itself (its boxn / csort / boxdata / boxm2m / ijbox
+    compiled from source, oracle/_ref) on the geometries the benchmarks run:
+    the 245,760-point icosphere at depth 5 (uneven leaves, most boxes empty)
+    and 262,144 points of the 32-cluster distribution at depth 6; potentials of
+    the FP64 form (reference semantics, p = 8) against the reference's float
+    outputs to 1e-6."""
+    if not oracle.ref_available(8):
+        pytest.skip("reference library not built (oracle/_ref)")
+    if case.startswith("sphere"):
+        x, q = _bench_sphere()
+        lmax = 5
+        lo = x.min(axis=1)
+        bb = (float(lo[0]), float(lo[1]), float(lo[2]), float((x.max(axis=1) - lo).max() * (1 + 1e-5)))
+    else:
+        x, q = _bench_clusters(262144)
+        lmax = 6
+        bb = (0.0, 0.0, 0.0, 1.0)
+    vr, gr = oracle.ref_fmm(x, x, q, neq=0, p=8, lmax=lmax, bbox=bb)
+    rr = oracle.ref_records(8)
+    pl = plan_for(ob, 0, 8, lmax, x, None, x, None, bbox=bb)
+    for k in (0, 1, 6, 7):
+        assert np.array_equal(pl.tree(k), rr[k]), k
+    la, lb = oracle.parse_lists(pl.tree(8)), oracle.parse_lists(rr[8])
+    assert len(la) == len(lb)
+    for a, b in zip(la, lb):
+        assert a[0] == b[0] and a[1] == b[1] and a[3] == b[3]
+    v, g = pl.evaluate(q, f64=True)
+    assert rel(v, vr.astype(np.float64)) < 1e-6
+    assert rel(g.reshape(3, -1), gr.astype(np.float64)) < 1e-6
+    pl.close()
