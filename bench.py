@@ -58,10 +58,13 @@ C3_METRIC = "FMM matvec Mpts/s at rel err <=1e-6 vs FP64 direct; mixed+adjoint v
 C3_REF_SLICES = 16
 C3_REF_LMAX = {C3_N // 16: 4, C3_N // 4: 5, C3_N // 2: 6}
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-# DRAM bytes (read + write) per evaluate of the two dominant kernels of the C2
-# workload, from one ncu capture of it: P2P runs as two launches (7.03 MB read
-# each, its outputs stay in L2), the M2L as one.
-NCU_TRAFFIC = {"p2p_mixed": 2 * 7.026e6, "translate_tc": 170.88e6}
+# DRAM bytes (read + write) per evaluate of the two dominant kernels, from
+# single-pass ncu captures of the timed steps of each workload (the near field
+# runs as two launches per evaluate; the M2L is translate_h16 + reduce_pairs)
+NCU_TRAFFIC = {
+    "adjoint1m": {"p2p_mixed": 2 * (31.84e6 + 0.07e6), "translate_tc": 118.2e6 + 1328.8e6 + 1497.1e6 + 5.3e6},
+    "bem": {"p2p_mixed": 2 * 10.0e6, "translate_tc": 25.6e6 + 88.2e6 + 148.3e6 + 3.2e6},
+}
 
 
 def measured_peaks():
@@ -380,16 +383,19 @@ def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, tra
                 "traffic": traffic.get("p2p_mixed"), "ms": float(phase_alone[0]),
                 "ms_in_overlapped_step": float(phase[0]),
                 "note": f"20 flops per algorithmic pair ({st['p2p_pairs']} pairs); ms = the kernel's own launches "
-                        f"(near field not overlapped), summed per step; peak = nominal FP32 at "
-                        f"{sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)"}
-    roof_m2l = {"kernel": "translate_tc+reduce_pairs (M2L)" if mixed else "translate_f64 (M2L)", "bound": "tensor",
+                        f"(near field not overlapped), summed per evaluate; peak = nominal FP32 at "
+                        f"{sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json); traffic per evaluate (two "
+                        f"launches)"}
+    roof_m2l = {"kernel": ("translate_h16+reduce_pairs (M2L)" if p <= 12 else "translate_tc+reduce_pairs (M2L)")
+                if mixed else "translate_f64 (M2L)", "bound": "tensor",
                 "achieved": m2l_ach, "peak": tf32_peak if mixed else None, "unit": "TFLOP/s",
                 "frac": (m2l_ach / tf32_peak) if mixed else None,
                 "traffic": traffic.get("translate_tc"), "ms": float(phase_alone[3]),
                 "ms_in_overlapped_step": float(phase[3]),
                 "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
-                        f"execute 3 TF32 MMAs per product on operators padded to 128-row blocks; peak = TF32 dense "
-                        f"= half of {peak_kind} bf16"}
+                        f"execute 3 FP16 MMAs per product (p <= 12; TF32 above) on operators padded to a multiple "
+                        f"of 16 rows; peak = TF32 dense = half of {peak_kind} bf16 (the FP16 one is twice that); "
+                        f"traffic per evaluate (translate + reduce_pairs)"}
     nb_i, nb_j = plan.tree(4), plan.tree(5)
     fp64_peak = 37.0
     ideal = {"p2p": 20.0 * st["p2p_pairs"] / fp32_peak,
@@ -500,7 +506,7 @@ def run_ours(args, rank, world, secondary=False):
     st = plan.stats()
     names = ["p2p", "p2m", "m2m", "m2l", "l2l", "l2p"]
     roof, roof2, matvec_roof = phase_rooflines(plan, P_ORDER, LMAX, npts, phase, phase_alone, ms_step,
-                                               args.precision == "mixed", NCU_TRAFFIC)
+                                               args.precision == "mixed", NCU_TRAFFIC["bem"])
     # CPU baseline: the reference's own fmm() on a bounded sample, one core
     cpu = None
     if not args.no_cpu and not secondary:
@@ -732,7 +738,8 @@ def run_headline(args, rank, world):
                       "dq": rel(dq[sel], psid), "dx": rel(dx, dxd), "targets": 1024}
     fd = c3_finite_differences(ob, x, q, w, lmax, ob.MIXED, args.fd)
     st = op.plan.stats()
-    roof, roof2, matvec_roof = phase_rooflines(op.plan, C3_P, lmax, n, ph, ph_alone, t_f, True)
+    roof, roof2, matvec_roof = phase_rooflines(op.plan, C3_P, lmax, n, ph, ph_alone, t_f, True,
+                                               NCU_TRAFFIC["adjoint1m"] if lmax == 6 else None)
     # CPU baseline: the reference's own forward + adjoint on one 65,536-point
     # slice of this point set, one core
     cpu = None

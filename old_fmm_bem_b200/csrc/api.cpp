@@ -328,11 +328,19 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
       upload(pl->d_m2l, pl->ops.m2l, s);
     }
     // FP64 translation tiles (M2L, M2M, L2L) per level
-    std::vector<int> keys(pl->tot_i), keys_j(pl->tot_j), par_j(pl->tot_j), lst((size_t)pl->tot_i * kM2LSlots);
+    std::vector<int> keys(pl->tot_i), keys_j(pl->tot_j), par_j(pl->tot_j), lst;
     FMMB_CUDA(cudaMemcpy(keys.data(), pl->key_i.get(), pl->tot_i * sizeof(int), cudaMemcpyDeviceToHost));
     FMMB_CUDA(cudaMemcpy(keys_j.data(), pl->key_j.get(), pl->tot_j * sizeof(int), cudaMemcpyDeviceToHost));
     FMMB_CUDA(cudaMemcpy(par_j.data(), pl->parent_j.get(), pl->tot_j * sizeof(int), cudaMemcpyDeviceToHost));
-    FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    // the M2L lists on the host only for the work lists built there: the FP64
+    // M2L's box tiles and the TF32 form's tiles (the FP16 form's are built on
+    // the device, setup.cu)
+    const bool tc_m2l = pl->cfg.precision == FMMB_MIXED && pl->K <= tc_max_k();
+    const bool h16_m2l = pl->cfg.precision == FMMB_MIXED && pl->K <= h16_max_k();
+    if (!h16_m2l) {
+      lst.resize((size_t)pl->tot_i * kM2LSlots);
+      FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    }
     const int XT = translate_tile_size();
     auto make_tiles = [&](const std::vector<std::vector<int>>& groups, int nslots, auto op_of) {
       std::unique_ptr<fmmb_plan::TileSet> ts(new fmmb_plan::TileSet());
@@ -374,9 +382,11 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     pl->m2m_list.alloc(m2m_list.size());
     FMMB_CUDA(cudaMemcpy(pl->m2m_list.get(), m2m_list.data(), m2m_list.size() * sizeof(int), cudaMemcpyHostToDevice));
     pl->m2l_tiles.clear();
+    // the FP64 M2L's box tiles (the tensor-core forms use the pair tiles below)
+    const bool fp64_m2l = !tc_m2l;
     for (int lev = 0; lev <= pl->lmax; lev++) {
       std::vector<std::vector<int>> by_oct(8);
-      if (lev >= 2)
+      if (lev >= 2 && fp64_m2l)
         for (int b = 0; b < pl->nbox_i[lev]; b++) by_oct[keys[pl->off_i[lev] + b] & 7].push_back(pl->off_i[lev] + b);
       pl->m2l_tiles.push_back(make_tiles(by_oct, kM2LSlots, [&](int box, int sl) {
         if (lst[(size_t)box * kM2LSlots + sl] < 0) return -1;
@@ -533,7 +543,11 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
         pl->tc_y.alloc((size_t)ntile * TT * job.ys);
       };
       // M2L, all levels in one job: operator = set(level)*316 + relative position
-      {
+      if (!(pl->use_h16 && build_m2l_job_dev(pl, pl->tc_m2l, (K + 3) / 4 * 4, s))) {
+        if (lst.empty()) {
+          lst.resize((size_t)pl->tot_i * kM2LSlots);
+          FMMB_CUDA(cudaMemcpy(lst.data(), pl->m2l_list.get(), lst.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        }
         std::vector<Pair> pairs;
         for (int lev = 2; lev <= pl->lmax; lev++) {
           const int set = pl->ops.m2l_sets > 1 ? lev - 2 : 0;
@@ -550,56 +564,15 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
         build_job(pl->tc_m2l, pairs);
       }
     }
-    // inverse target permutation (caller -> sorted) for the direct sum
-    {
-      std::vector<int> perm(ni), inv(ni);
-      FMMB_CUDA(cudaMemcpy(perm.data(), pl->perm_i.get(), ni * sizeof(int), cudaMemcpyDeviceToHost));
-      for (int i = 0; i < ni; i++) inv[perm[i]] = i;
-      pl->inv_i.alloc(ni);
-      FMMB_CUDA(cudaMemcpy(pl->inv_i.get(), inv.data(), ni * sizeof(int), cudaMemcpyHostToDevice));
-    }
-    // near-field work items: pieces of up to 128 targets of a leaf.  The
+    // inverse target permutation (caller -> sorted) for the direct sum, and the
+    // near-field work items: pieces of up to 128 targets of a leaf (the
     // many-right-hand-side pass takes them in leaf order; the one-right-hand-
-    // side kernels heaviest first (targets x sources of the 27 neighbour
-    // leaves), dealt alternately to the two near-field launches of an
-    // evaluate, so that each launch starts with its longest blocks
-    {
-      const int nleaf = pl->nbox_i[pl->lmax];
-      std::vector<int2> leaf(nleaf), leafj(pl->nbox_j[pl->lmax]), work;
-      std::vector<int> plist((size_t)nleaf * kP2PSlots);
-      FMMB_CUDA(cudaMemcpy(leaf.data(), pl->leaf_i.get(), nleaf * sizeof(int2), cudaMemcpyDeviceToHost));
-      FMMB_CUDA(cudaMemcpy(leafj.data(), pl->leaf_j.get(), leafj.size() * sizeof(int2), cudaMemcpyDeviceToHost));
-      FMMB_CUDA(cudaMemcpy(plist.data(), pl->p2p_list.get(), plist.size() * sizeof(int), cudaMemcpyDeviceToHost));
-      std::vector<std::pair<long long, int2>> items;
-      for (int b = 0; b < nleaf; b++) {
-        long long nsrc = 0;
-        for (int sl = 0; sl < kP2PSlots; sl++) {
-          const int jl = plist[(size_t)b * kP2PSlots + sl];
-          if (jl >= 0) nsrc += leafj[jl].y;
-        }
-        for (int t = 0; t < leaf[b].y; t += 128) {
-          work.push_back(make_int2(b, t));
-          items.push_back({(long long)std::min(128, leaf[b].y - t) * std::max(nsrc, 1LL), make_int2(b, t)});
-        }
-      }
-      pl->m_p2p_work.alloc(work.size());
-      if (!work.empty())
-        FMMB_CUDA(cudaMemcpy(pl->m_p2p_work.get(), work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice));
-      pl->m_p2p_nwork = (int)work.size();
-      std::stable_sort(items.begin(), items.end(),
-                       [](const std::pair<long long, int2>& x, const std::pair<long long, int2>& y) {
-                         return x.first > y.first;
-                       });
-      std::vector<int2> sorted;
-      sorted.reserve(items.size());
-      for (size_t k = 0; k < items.size(); k += 2) sorted.push_back(items[k].second);
-      pl->p2p_nwork0 = (int)sorted.size();
-      for (size_t k = 1; k < items.size(); k += 2) sorted.push_back(items[k].second);
-      pl->p2p_work.alloc(sorted.size());
-      if (!sorted.empty())
-        FMMB_CUDA(cudaMemcpy(pl->p2p_work.get(), sorted.data(), sorted.size() * sizeof(int2), cudaMemcpyHostToDevice));
-      pl->p2p_nwork = (int)sorted.size();
-    }
+    // side kernels heaviest first -- targets x sources of the 27 neighbour
+    // leaves -- dealt alternately to the two near-field launches of an
+    // evaluate, so that each launch starts with its longest blocks), on the
+    // device (setup.cu)
+    build_inverse_perm_dev(pl, s);
+    build_p2p_work_dev(pl, s);
     // evaluation buffers
     const int nr = pl->cfg.nrhs;
     pl->qs.alloc((size_t)nj * nr);

@@ -258,6 +258,12 @@ struct fmmb_plan {
 };
 
 namespace fmmb {
+// work lists built on the device from the tree (setup.cu): the FP16 M2L's pair
+// tiles and reduction CSR (false: too large for the int enumeration, build on
+// the host), the near-field work items, the inverse target permutation
+bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_t s);
+void build_p2p_work_dev(fmmb_plan* pl, cudaStream_t s);
+void build_inverse_perm_dev(fmmb_plan* pl, cudaStream_t s);
 // complex Helmholtz and Yukawa operators, pair jobs and buffers (helmholtz_host.cpp)
 void helm_setup(fmmb_plan* pl);
 // the kernels of the Helmholtz machinery (complex expansions, dense operators)

@@ -18,6 +18,10 @@ struct Sem {
 
 __host__ __device__ __forceinline__ int ifull_d(int n, int m) { return n * n + n + m; }
 
+// device primitives of the tree build (tree.cu), also used by the set-up of
+// the evaluation work lists (setup.cu); both synchronise the stream on return
+void exclusive_scan(int* data, int n, cudaStream_t s);  // in place
+void radix_sort(int* keys, int* vals, int n, int bits, cudaStream_t s);  // stable, keys >= 0 below 2^bits
 void launch_gather_charges(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
 // Near field of one right-hand side over work items (target leaf, first
 // target) of up to 128 targets of a leaf against its 27 neighbour slots

@@ -73,6 +73,8 @@ __global__ void scan_add(int* data, int n, const int* offs) {
   }
 }
 
+}  // namespace
+
 // In-place exclusive scan (multi-level).
 void exclusive_scan(int* data, int n, cudaStream_t s) {
   if (n <= 0) return;
@@ -91,6 +93,8 @@ void exclusive_scan(int* data, int n, cudaStream_t s) {
   FMMB_CHECK_LAUNCH();
   FMMB_CUDA(cudaStreamSynchronize(s));  // `sums` is freed on return
 }
+
+namespace {
 
 // ---- stable LSD radix sort of (key, index) ----
 constexpr int kRsWarps = 8;
@@ -158,6 +162,8 @@ __global__ void rs_scatter(const int* kin, const int* vin, int* kout, int* vout,
   }
 }
 
+}  // namespace
+
 void radix_sort(int* keys, int* vals, int n, int bits, cudaStream_t s) {
   if (n <= 1 || bits <= 0) return;
   const int nb = (n + kRsTile - 1) / kRsTile;
@@ -182,6 +188,8 @@ void radix_sort(int* keys, int* vals, int n, int bits, cudaStream_t s) {
   }
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
+
+namespace {
 
 // ---- keys (fmm/boxn.cxx:5-31) ----
 __device__ __forceinline__ int morton(int cx, int cy, int cz, int lev) {
