@@ -109,6 +109,27 @@ void upload_static_ops(fmmb_plan* pl) {
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
+// The tensor-core M2L's operator images (mixed form), rebuilt when the
+// operator set changed: FP16 (hi, lo) for K <= h16_max_k(), TF32 above.
+void m2l_images(fmmb_plan* pl) {
+  const int K = pl->K;
+  if (pl->cfg.precision != FMMB_MIXED || K > tc_max_k() || helm_family(pl->cfg.kernel) || pl->ops.m2l.empty()) return;
+  const bool stale = pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd;
+  if (K > h16_max_k() && (stale || pl->d_img_m2l.get() == nullptr)) {
+    std::vector<float> img;
+    build_tc_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, tc_kpad(K), img);
+    pl->d_img_m2l.alloc(img.size());
+    FMMB_CUDA(cudaMemcpy(pl->d_img_m2l.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
+  } else if (K <= h16_max_k() && (stale || pl->d_img_h16.get() == nullptr)) {
+    std::vector<unsigned char> img;
+    build_h16_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, h16_n(K), h16_kpad(K), h16_img_bytes(K), img);
+    pl->d_img_h16.alloc(img.size());
+    FMMB_CUDA(cudaMemcpy(pl->d_img_h16.get(), img.data(), img.size(), cudaMemcpyHostToDevice));
+  }
+  pl->opimg_sets = pl->ops.m2l_sets;
+  pl->opimg_rd = pl->ops.m2l_rd;
+}
+
 }  // namespace
 }  // namespace fmmb
 
@@ -187,6 +208,7 @@ int fmmb_plan_create(const fmmb_config* cfg, fmmb_plan** out) {
       if (!pl->ref && !helm_family(cfg->kernel)) {  // geometry-independent M2L set
         build_m2l_operators(pl->ops, 2, 1.0f);
         upload(pl->d_m2l, pl->ops.m2l, pl->st.main);
+        m2l_images(pl);
       }
     } catch (...) {
       fmmb_plan_destroy(pl);
@@ -465,23 +487,7 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     if (pl->use_h16) prepare_translate_h16();
     if (pl->use_tc || pl->use_h16) {
       const int K = pl->K, kpad = tc_kpad(K), nrb = pl->use_h16 ? 1 : (K + 127) / 128;
-      const bool stale = pl->opimg_sets != pl->ops.m2l_sets || pl->opimg_rd != pl->ops.m2l_rd;
-      if (pl->use_tc && (stale || pl->d_img_m2l.get() == nullptr)) {
-        std::vector<float> img;
-        build_tc_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, kpad, img);
-        pl->d_img_m2l.alloc(img.size());
-        FMMB_CUDA(cudaMemcpy(pl->d_img_m2l.get(), img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice));
-        pl->opimg_sets = pl->ops.m2l_sets;
-        pl->opimg_rd = pl->ops.m2l_rd;
-      }
-      if (pl->use_h16 && (stale || pl->d_img_h16.get() == nullptr)) {
-        std::vector<unsigned char> img;
-        build_h16_images(pl->ops.m2l, pl->ops.m2l_sets * 316, K, h16_n(K), h16_kpad(K), h16_img_bytes(K), img);
-        pl->d_img_h16.alloc(img.size());
-        FMMB_CUDA(cudaMemcpy(pl->d_img_h16.get(), img.data(), img.size(), cudaMemcpyHostToDevice));
-        pl->opimg_sets = pl->ops.m2l_sets;
-        pl->opimg_rd = pl->ops.m2l_rd;
-      }
+      m2l_images(pl);  // built once at plan creation in accurate semantics
       if (pl->use_tc) pl->Mtf.alloc((size_t)pl->tot_j * 2 * kpad);
       if (pl->use_h16) {
         pl->Xh.alloc((size_t)pl->tot_j * 2 * h16_kpad(K));
