@@ -7,7 +7,7 @@ Laplace G FMM as a torch.autograd operator):
   charges N(0,1), targets = sources (zero-distance pairs excluded), order
   p = 12 -- the lowest order whose potential meets rel. err <= 1e-6 against
   the FP64 direct sum on this point set -- mixed precision (FP32 near field,
-  TF32x3 tensor-core M2L, FP64 expansions).  The backward gives the
+  FP16x3 tensor-core M2L, FP64 expansions).  The backward gives the
   gradients of L = sum(w * pot) w.r.t. the charges (the transposed FMM) and
   the positions (the forward's field and the transposed FMM's field).
 Metric: FMM matvec Mpts/s at rel err <= 1e-6 vs FP64 direct (points per
@@ -347,7 +347,7 @@ def setup_line(plan, npts, ms_step):
     return {"tree_build_ms": tree_ms, "set_geometry_ms": setup_ms, "tree_algorithmic_bytes": nbytes,
             "tree_gbs": gbs, "tree_frac_of_hbm": gbs / peaks.get("hbm_gbs", 6650.0),
             "mpts_s_with_setup_per_matvec": npts / ((ms_step + setup_ms) * 1e-3) / 1e6,
-            "note": f"tree build = keys, radix sort, levels, lists, with host synchronisations between levels; "
+            "note": f"tree build = keys, radix sort, levels, lists (scratch from a stream-ordered pool, one host synchronisation for all level sizes); "
                     f"HBM peak {kind}"}
 
 
@@ -360,12 +360,13 @@ def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, tra
         r^2 6, rsqrt 1, r^-3 2, q r^-1 and q r^-3 2, potential 1, gradient 6;
         Gni/Gnj: the normal dot in place of the gradient); bound by the FP32
         pipes (peak 148 SMs x 128 lanes x 2 flops at the maximum SM clock);
-      * M2L (translate_tc + its pair-row reduction): 2 K^2 algorithmic flops
-        per box pair on the tensor cores; TF32 peak = half the measured dense
-        bf16;
+      * M2L (translate_h16 / translate_tc + its pair-row reduction): 2 K^2
+        algorithmic flops per box pair on the tensor cores; peak = the
+        measured dense bf16 for the FP16 kernel (p <= 12: FP16 and BF16 run at
+        the same rate), half of it (TF32) above;
     and the whole matvec against the sum of its phases' roofline times
     (algorithmic work of each phase over the peak of the unit it runs on: P2P,
-    P2M, L2P FP32; M2L TF32; M2M, L2L FP64 at the nominal 37 TFLOP/s).
+    P2M, L2P FP32; M2L FP16 or TF32; M2M, L2L FP64 at the nominal 37 TFLOP/s).
     traffic: DRAM bytes of one launch from an ncu capture, or None.
     Returns (dominant, other, matvec)."""
     st = plan.stats()
@@ -376,7 +377,7 @@ def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, tra
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
     p2p_ach = 20.0 * st["p2p_pairs"] / (phase_alone[0] * 1e-3) / 1e12
-    tf32_peak = peaks["bf16_tflops"] / 2
+    tc_peak = peaks["bf16_tflops"] if p <= 12 else peaks["bf16_tflops"] / 2  # FP16 / TF32 dense
     m2l_ach = 2.0 * K * K * st["m2l_pairs"] / (phase_alone[3] * 1e-3) / 1e12
     roof_p2p = {"kernel": "p2p_mixed" if mixed else "p2p_f64", "bound": "fp32", "achieved": p2p_ach,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": p2p_ach / fp32_peak,
@@ -388,20 +389,20 @@ def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, tra
                         f"launches)"}
     roof_m2l = {"kernel": ("translate_h16+reduce_pairs (M2L)" if p <= 12 else "translate_tc+reduce_pairs (M2L)")
                 if mixed else "translate_f64 (M2L)", "bound": "tensor",
-                "achieved": m2l_ach, "peak": tf32_peak if mixed else None, "unit": "TFLOP/s",
-                "frac": (m2l_ach / tf32_peak) if mixed else None,
+                "achieved": m2l_ach, "peak": tc_peak if mixed else None, "unit": "TFLOP/s",
+                "frac": (m2l_ach / tc_peak) if mixed else None,
                 "traffic": traffic.get("translate_tc"), "ms": float(phase_alone[3]),
                 "ms_in_overlapped_step": float(phase[3]),
                 "note": f"algorithmic 2*K^2 flops per box pair (K={K}, {st['m2l_pairs']} pairs); the tensor cores "
                         f"execute 3 FP16 MMAs per product (p <= 12; TF32 above) on operators padded to a multiple "
-                        f"of 16 rows; peak = TF32 dense = half of {peak_kind} bf16 (the FP16 one is twice that); "
+                        f"of 16 rows; peak = {peak_kind} dense bf16 (= FP16) for p <= 12, half of it (TF32) above; "
                         f"traffic per evaluate (translate + reduce_pairs)"}
     nb_i, nb_j = plan.tree(4), plan.tree(5)
     fp64_peak = 37.0
     ideal = {"p2p": 20.0 * st["p2p_pairs"] / fp32_peak,
              "p2m": 2.0 * npts * K / fp32_peak,
              "m2m": 2.0 * K * K * float(nb_j[3:lmax + 1].sum()) / fp64_peak,
-             "m2l": 2.0 * K * K * st["m2l_pairs"] / tf32_peak,
+             "m2l": 2.0 * K * K * st["m2l_pairs"] / tc_peak,
              "l2l": 2.0 * K * K * float(nb_i[3:lmax + 1].sum()) / fp64_peak,
              "l2p": 2.0 * npts * K / fp32_peak}
     ideal = {k: v / 1e9 for k, v in ideal.items()}  # flops / (TFLOP/s) -> ms
@@ -409,8 +410,8 @@ def phase_rooflines(plan, p, lmax, npts, phase, phase_alone, ms_step, mixed, tra
                    "frac_of_step": sum(ideal.values()) / ms_step,
                    "frac_per_phase_alone": {k: ideal[k] / float(phase_alone[i]) for i, k in enumerate(names)},
                    "note": "algorithmic flops per phase (P2P 20 per pair, P2M/L2P 2(p+1)^2 per point, M2L/M2M/L2L "
-                           "2(p+1)^4 per box pair) over FP32 (nominal), TF32 (half the measured bf16) and FP64 "
-                           "(nominal 37) peaks"}
+                           "2(p+1)^4 per box pair) over FP32 (nominal), FP16 (the measured bf16; TF32 = half of it "
+                           "above p = 12) and FP64 (nominal 37) peaks"}
     dom = int(np.argmax(phase_alone[:6]))
     if names[dom] == "m2l":
         return roof_m2l, roof_p2p, matvec_roof
@@ -523,7 +524,7 @@ def run_ours(args, rank, world, secondary=False):
     line = {
         "metric": METRIC, "value": value, "unit": "Mpts/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+tf32x3+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32+fp16x3+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": "Laplace Gnj double-layer BEM matvec, icosphere r=1, 81,920 triangles x 3 Gauss "
                                "points = 245,760 points, p=10, lmax=5, self pairs excluded",
                    "precision": args.precision, "points": npts, "p": P_ORDER, "lmax": LMAX,
@@ -759,7 +760,7 @@ def run_headline(args, rank, world):
     line = {
         "metric": C3_METRIC, "value": job_mpts_s(world, n, t_fb_job), "unit": "Mpts/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_fb_job, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+tf32x3+f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+fp16x3+f64", "data": "synthetic",
         "config": {"workload": "Laplace G FMM forward + backward (torch.autograd: gradients w.r.t. charges and "
                                "positions of sum(w*pot)), 1,048,576 points from 32 Gaussian clusters (sigma 0.02) in "
                                "[0,1]^3, q N(0,1), w N(0,1), p=12, mixed precision, self pairs excluded",
@@ -917,7 +918,7 @@ def run_c4(args):
     pts = 2 * n * nrhs * (iters + 1)
     print(json.dumps({"metric": "batched BEM GMRES: FMM matvec Mpts/s (64 unit-sphere problems, 8 RHS, Gni + Gnj)",
                       "value": pts / (total_ms * 1e-3) / 1e6, "unit": "Mpts/s", "n_gpus": 1,
-                      "steps": max(1, min(args.steps, 3)), "ms_per_step": total_ms, "dtype": "f32+tf32x3+f64",
+                      "steps": max(1, min(args.steps, 3)), "ms_per_step": total_ms, "dtype": "f32+fp16x3+f64",
                       "data": "synthetic",
                       "config": {"workload": f"64 geodesic unit spheres, {n} centroid points in all "
                                              f"({int(np.diff(off).min())}..{int(np.diff(off).max())} per problem), "
@@ -958,7 +959,7 @@ def run_c4_matvec(args):
         plan.close()
     print(json.dumps({"metric": "batched BEM matvec Mpts/s (64 unit-sphere problems, Gni, p=10, 1 and 8 RHS)",
                       "value": res["rhs8"]["mpts_s"], "unit": "Mpts/s", "n_gpus": 1, "steps": 5,
-                      "dtype": "f32+tf32x3+f64", "data": "synthetic",
+                      "dtype": "f32+fp16x3+f64", "data": "synthetic",
                       "config": {"workload": f"64 geodesic unit spheres, {n} centroids, Gni, depth {lmax}",
                                  "l2": "flushed between steps"}, "results": res}))
 

@@ -579,6 +579,7 @@ int geometry_impl(fmmb_plan* pl, int nprob, const int* toff, const int* soff, in
     // device (setup.cu)
     build_inverse_perm_dev(pl, s);
     build_p2p_work_dev(pl, s);
+    build_p2m_work_dev(pl, s);
     // evaluation buffers
     const int nr = pl->cfg.nrhs;
     pl->qs.alloc((size_t)nj * nr);
@@ -786,11 +787,19 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     if (pl->ref)  // the reference's spherical formulation, quirks included
       launch_p2m(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(),
                  qs, pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
-    else if (!(pl->cfg.precision == FMMB_MIXED &&
-               launch_p2m_f32(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(),
-                              pl->snrm.get(), qs, pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m)))
-      launch_p2m_cart(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(),
-                      pl->snrm.get(), qs, pl->d_fac.get(), pl->bbox, rb_leaf, pl->M.get() + (size_t)pl->off_j[lmax] * K, m);
+    else {
+      double* Mleaf = pl->M.get() + (size_t)pl->off_j[lmax] * K;
+      bool done = false;
+      if (pl->cfg.precision == FMMB_MIXED) {
+        if (pl->p2m_nwork > nleaf_j)  // some leaf is summed by several items: its rows start at zero
+          FMMB_CUDA(cudaMemsetAsync(Mleaf, 0, (size_t)nleaf_j * K * sizeof(double), m));
+        done = launch_p2m_f32(ker, pl->p2m_nwork, pl->p2m_work.get(), p, K, pl->leafkey_j.get(), pl->leaf_j.get(),
+                              pl->spos.get(), pl->snrm.get(), qs, pl->bbox, rb_leaf, Mleaf, m);
+      }
+      if (!done)
+        launch_p2m_cart(ker, nleaf_j, p, K, pl->leafkey_j.get(), pl->leaf_j.get(), pl->spos.get(), pl->snrm.get(), qs,
+                        pl->d_fac.get(), pl->bbox, rb_leaf, Mleaf, m);
+    }
   }
   FMMB_CUDA(time_mark(pl, pl->ev[3], m));
   // upward pass: parents accumulate their children (levels below lmax start at zero)
@@ -891,7 +900,7 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
       launch_l2p(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(), pl->tnrm.get(),
                  pl->d_fac.get(), s, pl->bbox, rb_leaf, pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m);
     else if (!(pl->cfg.precision == FMMB_MIXED && (ker == FMMB_LAPLACE_G || !want_grad) &&
-               launch_l2p_f32(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
+               launch_l2p_f32(ker, pl->m_p2p_nwork, pl->m_p2p_work.get(), p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),
                               pl->tnrm.get(), pl->d_fac.get(), pl->bbox, rb_leaf, s.coef,
                               pl->L.get() + (size_t)pl->off_i[lmax] * K, pot_far, g_far, pl->ni, m)))
       launch_l2p_cart(ker, nleaf_i, p, K, pl->leafkey_i.get(), pl->leaf_i.get(), pl->tpos.get(),

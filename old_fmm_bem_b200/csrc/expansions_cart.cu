@@ -169,22 +169,29 @@ __global__ void __launch_bounds__(128) p2m_cart(int p, int K, const int* __restr
 // compile time, runtime order p <= P), writes its contributions to shared
 // memory, and the block reduces the columns in FP64.  The multipole of a leaf
 // carries FP32 rounding of each point's terms (relative 1e-7) -- below the
-// TF32x3 error of the translations that consume it.
+// tensor-core error of the translations that consume it.  A block is one work
+// item of up to kP2MItem sources of a leaf, so that the dense leaves of
+// clustered points (a thousand points and more) spread over many SMs; a leaf
+// of several items is summed with FP64 atomics into zeroed rows.
 __constant__ float c_fac32[21 * 21 + 21];  // fac(n, m) at n*n+n+m, n <= 20
 
-constexpr int kP2MThreads = 64;
+constexpr int kP2MThreads = kP2MItem;
 
 template <int KER, int P>
-__global__ void __launch_bounds__(kP2MThreads) p2m_f32(int p, int K, const int* __restrict__ keys,
+__global__ void __launch_bounds__(kP2MThreads) p2m_f32(int p, int K, const int2* __restrict__ work,
+                                                       const int* __restrict__ keys,
                                                        const int2* __restrict__ leaf, const float4* __restrict__ spos,
                                                        const float4* __restrict__ snrm, const float* __restrict__ qs,
                                                        float xmin, float ymin, float zmin, double rb,
                                                        double* __restrict__ M) {
   extern __shared__ float contrib[];  // [kP2MThreads][K]
-  const int b = blockIdx.x;
+  const int2 wk = work[blockIdx.x];
+  const int b = wk.x;
   double xc, yc, zc;
   box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
-  const int2 lf = leaf[b];
+  const int2 leaf_b = leaf[b];
+  const bool shared_leaf = leaf_b.y > kP2MThreads;  // summed by several items
+  const int2 lf = make_int2(leaf_b.x + wk.y, min(kP2MThreads, leaf_b.y - wk.y));
   const double inv_rb = 1.0 / rb;
   double acc0 = 0.0, acc1 = 0.0;  // columns threadIdx.x and threadIdx.x + 64 (K <= 128 per pass)
   double acc[(P + 1) * (P + 1) / kP2MThreads + 1];
@@ -299,7 +306,10 @@ __global__ void __launch_bounds__(kP2MThreads) p2m_f32(int p, int K, const int* 
 #pragma unroll
   for (int i = 0; i < (P + 1) * (P + 1) / kP2MThreads + 1; i++) {
     const int k = threadIdx.x + i * kP2MThreads;
-    if (k < K) M[(size_t)b * K + k] = acc[i];
+    if (k < K) {
+      if (shared_leaf) atomicAdd(M + (size_t)b * K + k, acc[i]);
+      else M[(size_t)b * K + k] = acc[i];
+    }
   }
 }
 
@@ -555,25 +565,17 @@ __global__ void __launch_bounds__(kL2PHThreads) l2p_hess_gni(int p, int K, const
 // (computed in FP64, stored as FP32 pairs), the solid harmonics S_n^m of a
 // point by the P2M recurrence in FP32 registers (fully unrolled to order P),
 // each degree's partial sums in FP32 and promoted to FP64 accumulators.
-constexpr int kL2PF32Threads = 64;
+constexpr int kL2PF32Threads = 128;  // one work item of up to 128 targets per block
 
-// Shared-memory coefficient read that the compiler may not hoist out of the
-// point loop (hoisting all of them would need hundreds of registers).
-__device__ __forceinline__ float2 lds2(const float2* p) {
-  float2 v;
-  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
-               : "=f"(v.x), "=f"(v.y)
-               : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
-  return v;
-}
-__device__ __forceinline__ float lds1(const float* p) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))));
-  return v;
-}
+// Shared-memory coefficient reads.  A thread evaluates one point (a block is
+// one work item of up to 128 targets), so the compiler is free to schedule
+// these loads ahead of their use in the unrolled degree / order loops.
+__device__ __forceinline__ float2 lds2(const float2* p) { return *p; }
+__device__ __forceinline__ float lds1(const float* p) { return *p; }
 
 template <int KER, int P>
-__global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const int* __restrict__ keys,
+__global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const int2* __restrict__ work,
+                                                          const int* __restrict__ keys,
                                                           const int2* __restrict__ leaf, const float4* __restrict__ tpos,
                                                           const float4* __restrict__ tnrm, const double* __restrict__ fac,
                                                           float xmin, float ymin, float zmin, double rb, double coef,
@@ -583,7 +585,8 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
   constexpr bool DER = KER != FMMB_LAPLACE_GNJ;  // derivative sums needed
   __shared__ float2 Cphi[NT], Cz[DER ? NT : 1], Cp[DER ? NT : 1], Cm[DER ? NT : 1];
   __shared__ float Cs[P + 1];
-  const int b = blockIdx.x;
+  const int2 wk = work[blockIdx.x];
+  const int b = wk.x;
   const double* Lb = L + (size_t)b * K;
   auto Lnm = [&](int n, int m) -> cplx {
     if (m == 0) return {Lb[n * n], 0.0};
@@ -611,10 +614,11 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
   __syncthreads();
   double xc, yc, zc;
   box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
-  const int2 lf = leaf[b];
+  const int2 leaf_b = leaf[b];
+  const int2 lf = make_int2(leaf_b.x + wk.y, min(kL2PF32Threads, leaf_b.y - wk.y));  // this item's targets
   const double inv_rb = 1.0 / rb;
-  for (int ii = threadIdx.x; ii < lf.y; ii += blockDim.x) {
-    const int i = lf.x + ii;
+  if ((int)threadIdx.x < lf.y) {  // one target per thread
+    const int i = lf.x + threadIdx.x;
     const float4 xt = tpos[i];
     const float x = (float)(((double)xt.x - xc) * inv_rb), y = (float)(((double)xt.y - yc) * inv_rb),
                 z = (float)(((double)xt.z - zc) * inv_rb);
@@ -697,15 +701,15 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
 }
 
 template <int P>
-void l2p_f32_launch(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
-                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
-                    double* pot, double* grad, int ni, cudaStream_t st) {
+void l2p_f32_launch(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* tpos, const float4* tnrm, const double* fac, const float* bbox, double rb,
+                    double coef, const double* L, double* pot, double* grad, int ni, cudaStream_t st) {
   if (kernel == FMMB_LAPLACE_G)
-    l2p_f32<FMMB_LAPLACE_G, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+    l2p_f32<FMMB_LAPLACE_G, P><<<nwork, kL2PF32Threads, 0, st>>>(p, K, work, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
   else if (kernel == FMMB_LAPLACE_GNI)
-    l2p_f32<FMMB_LAPLACE_GNI, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+    l2p_f32<FMMB_LAPLACE_GNI, P><<<nwork, kL2PF32Threads, 0, st>>>(p, K, work, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
   else
-    l2p_f32<FMMB_LAPLACE_GNJ, P><<<nleaf, kL2PF32Threads, 0, st>>>(p, K, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
+    l2p_f32<FMMB_LAPLACE_GNJ, P><<<nwork, kL2PF32Threads, 0, st>>>(p, K, work, keys, leaf, tpos, tnrm, fac, bbox[0], bbox[1], bbox[2], rb, coef, L, pot, grad, ni);
 }
 
 }  // namespace
@@ -732,13 +736,14 @@ void launch_p2m_cart(int kernel, int nleaf, int p, int K, const int* keys, const
 
 namespace {
 template <int P>
-void p2m_f32_launch(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
-                    const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
+void p2m_f32_launch(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* spos, const float4* snrm, const float* qs, const float* bbox, double rb, double* M,
+                    cudaStream_t st) {
   const size_t sm = (size_t)kP2MThreads * K * sizeof(float);
   if (kernel == FMMB_LAPLACE_GNJ)
-    p2m_f32<FMMB_LAPLACE_GNJ, P><<<nleaf, kP2MThreads, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
+    p2m_f32<FMMB_LAPLACE_GNJ, P><<<nwork, kP2MThreads, sm, st>>>(p, K, work, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
   else
-    p2m_f32<FMMB_LAPLACE_G, P><<<nleaf, kP2MThreads, sm, st>>>(p, K, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
+    p2m_f32<FMMB_LAPLACE_G, P><<<nwork, kP2MThreads, sm, st>>>(p, K, work, keys, leaf, spos, snrm, qs, bbox[0], bbox[1], bbox[2], rb, M);
 }
 }  // namespace
 
@@ -758,15 +763,16 @@ void init_fac32() {
   if (dev < 64) done[dev] = true;
 }
 
-bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
-                    const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st) {
-  if (nleaf <= 0) return true;
+bool launch_p2m_f32(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* spos, const float4* snrm, const float* qs, const float* bbox, double rb, double* M,
+                    cudaStream_t st) {
   if ((size_t)kP2MThreads * K * sizeof(float) > 48 * 1024) return false;  // per-point rows staged in shared memory
-  if (p <= 8) p2m_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
-  else if (p <= 10) p2m_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
-  else if (p <= 12) p2m_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
-  else if (p <= 16) p2m_f32_launch<16>(kernel, nleaf, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
-  else return false;
+  if (p > 16) return false;
+  if (nwork <= 0) return true;
+  if (p <= 8) p2m_f32_launch<8>(kernel, nwork, work, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else if (p <= 10) p2m_f32_launch<10>(kernel, nwork, work, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else if (p <= 12) p2m_f32_launch<12>(kernel, nwork, work, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
+  else p2m_f32_launch<16>(kernel, nwork, work, p, K, keys, leaf, spos, snrm, qs, bbox, rb, M, st);
   FMMB_CHECK_LAUNCH();
   return true;
 }
@@ -797,15 +803,15 @@ void launch_l2p_hess_gni(int nleaf, int p, int K, const int* keys, const int2* l
   FMMB_CHECK_LAUNCH();
 }
 
-bool launch_l2p_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
-                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
-                    double* pot, double* grad, int ni, cudaStream_t st) {
-  if (nleaf <= 0) return true;
-  if (p <= 8) l2p_f32_launch<8>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
-  else if (p <= 10) l2p_f32_launch<10>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
-  else if (p <= 12) l2p_f32_launch<12>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
-  else if (p <= 16) l2p_f32_launch<16>(kernel, nleaf, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
-  else return false;
+bool launch_l2p_f32(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* tpos, const float4* tnrm, const double* fac, const float* bbox, double rb,
+                    double coef, const double* L, double* pot, double* grad, int ni, cudaStream_t st) {
+  if (p > 16) return false;
+  if (nwork <= 0) return true;
+  if (p <= 8) l2p_f32_launch<8>(kernel, nwork, work, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else if (p <= 10) l2p_f32_launch<10>(kernel, nwork, work, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else if (p <= 12) l2p_f32_launch<12>(kernel, nwork, work, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
+  else l2p_f32_launch<16>(kernel, nwork, work, p, K, keys, leaf, tpos, tnrm, fac, bbox, rb, coef, L, pot, grad, ni, st);
   FMMB_CHECK_LAUNCH();
   return true;
 }

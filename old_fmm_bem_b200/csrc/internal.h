@@ -59,6 +59,48 @@ struct DevBuf {
   T* get() const { return ptr; }
 };
 
+// Per-device memory pool of the set-up scratch (tree build, work lists):
+// stream-ordered, keeping up to kScratchPoolKeep bytes between calls so that
+// repeated geometries of similar size reuse its memory.
+constexpr uint64_t kScratchPoolKeep = 512ull << 20;
+cudaMemPool_t scratch_pool();
+
+// Scratch buffer of one set-up call: allocated from scratch_pool() in the
+// order of stream `s` and freed in that order on destruction, so freeing it
+// waits for nothing (cudaFree synchronises the device).
+template <typename T>
+struct TmpBuf {
+  T* ptr = nullptr;
+  size_t n = 0;
+  cudaStream_t s = nullptr;
+  explicit TmpBuf(cudaStream_t st) : s(st) {}
+  TmpBuf(const TmpBuf&) = delete;
+  TmpBuf& operator=(const TmpBuf&) = delete;
+  TmpBuf(TmpBuf&& o) noexcept : ptr(o.ptr), n(o.n), s(o.s) {
+    o.ptr = nullptr;
+    o.n = 0;
+  }
+  ~TmpBuf() { release(); }
+  void release() {
+    if (ptr) cudaFreeAsync(ptr, s);
+    ptr = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count <= n && ptr) return;
+    release();
+    const size_t bytes = (count ? count : 1) * sizeof(T);
+    cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), bytes, scratch_pool(), s);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      throw Error{FMMB_ERR_NOMEM, std::string("cudaMallocFromPoolAsync ") + std::to_string(bytes) + " B: " +
+                                      cudaGetErrorString(e)};
+    }
+    n = count;
+  }
+  T* get() const { return ptr; }
+};
+
 inline int isym(int n, int m) { return n * (n + 1) / 2 + m; }
 inline int ifull(int n, int m) { return n * n + n + m; }
 
@@ -208,6 +250,10 @@ struct fmmb_plan {
   fmmb::DevBuf<float> qs_far;
   fmmb::DevBuf<int2> m_p2p_work;  // (target leaf, first target), up to 128 targets each
   int m_p2p_nwork = 0;
+  // P2M work items of the mixed form: (source leaf, first source), up to
+  // kP2MItem sources each, in leaf order
+  fmmb::DevBuf<int2> p2m_work;
+  int p2m_nwork = 0;
   // the same items for the one-right-hand-side near field, heaviest first in
   // each of its two launches: [0, p2p_nwork0) and [p2p_nwork0, p2p_nwork)
   fmmb::DevBuf<int2> p2p_work;
@@ -263,6 +309,7 @@ namespace fmmb {
 // the host), the near-field work items, the inverse target permutation
 bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_t s);
 void build_p2p_work_dev(fmmb_plan* pl, cudaStream_t s);
+void build_p2m_work_dev(fmmb_plan* pl, cudaStream_t s);
 void build_inverse_perm_dev(fmmb_plan* pl, cudaStream_t s);
 // complex Helmholtz and Yukawa operators, pair jobs and buffers (helmholtz_host.cpp)
 void helm_setup(fmmb_plan* pl);

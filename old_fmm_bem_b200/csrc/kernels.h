@@ -53,15 +53,20 @@ void launch_l2p_hess_gni(int nleaf, int p, int K, const int* keys, const int2* l
 int launch_p2p_multi(int kernel, int nrhs, int nwork, const int2* work, const int2* leaf_i, const int2* leaf_j,
                      const int* list, const float4* tpos, const float4* tnrm, const float4* spos, const float4* snrm,
                      const float* qs, int nj, const Sem& s, double* pot, double* grad, int ni, cudaStream_t st);
-// FP32 point-per-thread P2M for the mixed form (accurate semantics, p <= 11:
-// its 64 x K staging must fit 48 KB of shared memory); returns false outside
-// that range
-bool launch_p2m_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* spos,
-                    const float4* snrm, const float* qs, const float* bbox, double rb, double* M, cudaStream_t st);
-// FP32 L2P for the mixed form (accurate semantics, p <= 16); false outside its range
-bool launch_l2p_f32(int kernel, int nleaf, int p, int K, const int* keys, const int2* leaf, const float4* tpos,
-                    const float4* tnrm, const double* fac, const float* bbox, double rb, double coef, const double* L,
-                    double* pot, double* grad, int ni, cudaStream_t st);
+// FP32 point-per-thread P2M for the mixed form (accurate semantics, p <= 12:
+// its kP2MItem x K staging must fit 48 KB of shared memory); returns false
+// outside that range.  work: (source leaf, first source) items of up to
+// kP2MItem sources (build_p2m_work_dev); a leaf of more sources is summed by
+// several items with FP64 atomics, so its rows of M must be zero beforehand.
+constexpr int kP2MItem = 64;
+bool launch_p2m_f32(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* spos, const float4* snrm, const float* qs, const float* bbox, double rb, double* M,
+                    cudaStream_t st);
+// FP32 L2P for the mixed form (accurate semantics, p <= 16); false outside its
+// range.  work: (target leaf, first target) items of up to 128 targets.
+bool launch_l2p_f32(int kernel, int nwork, const int2* work, int p, int K, const int* keys, const int2* leaf,
+                    const float4* tpos, const float4* tnrm, const double* fac, const float* bbox, double rb,
+                    double coef, const double* L, double* pot, double* grad, int ni, cudaStream_t st);
 int translate_tile_size();
 // batched FP64 translation (M2L / M2M / L2L), see kernels_fp64.cu
 void launch_translate_f64(int ntile, int nsplit, int K, int nslots, const int* tile_boxes, const int* tile_ops,

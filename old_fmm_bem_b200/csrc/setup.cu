@@ -167,6 +167,20 @@ __global__ void leaf_items(int nleaf, const int2* __restrict__ leaf_i, const lon
   }
 }
 
+// ---- P2M work items: pieces of up to `per` sources of a source leaf ----
+__global__ void src_item_counts(int nleaf, int per, const int2* __restrict__ leaf_j, int* __restrict__ cnt) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nleaf) cnt[b] = (leaf_j[b].y + per - 1) / per;
+}
+
+__global__ void src_items(int nleaf, int per, const int2* __restrict__ leaf_j, const int* __restrict__ base,
+                          int2* __restrict__ work) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nleaf) return;
+  const int n = leaf_j[b].y;
+  for (int t = 0, k = base[b]; t < n; t += per, k++) work[k] = make_int2(b, t);
+}
+
 // sorted item j -> launch (j & 1), position j >> 1 within it
 __global__ void deal_items(int n, int n0, const int* __restrict__ sorted, const int2* __restrict__ work,
                            int2* __restrict__ out) {
@@ -207,14 +221,14 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
   T.vstart[T.nlev] = (int)V;
   const int nv = (int)V;
   const int nops = pl->ops.m2l_sets * 316;
-  DevBuf<int> pos;
+  TmpBuf<int> pos(s);
   pos.alloc((size_t)nv + 1);
   m2l_pair_flags<<<nblk(nv, kT), kT, 0, s>>>(nv, T, pl->m2l_list.get(), pos.get());
   FMMB_CHECK_LAUNCH();
   FMMB_CUDA(cudaMemsetAsync(pos.get() + nv, 0, sizeof(int), s));
   exclusive_scan(pos.get(), nv + 1, s);
   const int npair = d2h_int(pos.get() + nv, s);
-  DevBuf<int> opk, ord, src, dst;
+  TmpBuf<int> opk(s), ord(s), src(s), dst(s);
   opk.alloc(npair);
   ord.alloc(npair);
   src.alloc(npair);
@@ -225,7 +239,7 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
   FMMB_CHECK_LAUNCH();
   radix_sort(opk.get(), ord.get(), npair, bits_for(nops), s);  // stable: enumeration order within an operator
   // tiles of 128 pairs per operator
-  DevBuf<int> cnt, op_start, tile_base;
+  TmpBuf<int> cnt(s), op_start(s), tile_base(s);
   cnt.alloc(nops + 1);
   op_start.alloc(nops + 1);
   tile_base.alloc(nops + 1);
@@ -244,7 +258,7 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
   job.tile_op.alloc(std::max(ntile, 1));
   job.tile_src.alloc((size_t)std::max(ntile, 1) * 128);
   job.tile_y.alloc((size_t)std::max(ntile, 1) * 2);
-  DevBuf<int> tdst;
+  TmpBuf<int> tdst(s);
   tdst.alloc((size_t)std::max(ntile, 1) * 128);
   FMMB_CUDA(cudaMemsetAsync(job.tile_src.get(), 0xff, (size_t)ntile * 128 * sizeof(int), s));
   FMMB_CUDA(cudaMemsetAsync(tdst.get(), 0xff, (size_t)ntile * 128 * sizeof(int), s));
@@ -259,7 +273,7 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
   }
   // per output box, its pair rows (tile * 128 + column) in increasing order
   const int ncol = ntile * 128;
-  DevBuf<int> cpos;
+  TmpBuf<int> cpos(s);
   cpos.alloc((size_t)ncol + 1);
   if (ncol > 0) {
     nonneg_flags<<<nblk(ncol, kT), kT, 0, s>>>(ncol, tdst.get(), cpos.get());
@@ -267,7 +281,7 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
   }
   FMMB_CUDA(cudaMemsetAsync(cpos.get() + ncol, 0, sizeof(int), s));
   exclusive_scan(cpos.get(), ncol + 1, s);
-  DevBuf<int> rowk, colk;
+  TmpBuf<int> rowk(s), colk(s);
   rowk.alloc(std::max(npair, 1));
   colk.alloc(std::max(npair, 1));
   if (ncol > 0) {
@@ -275,7 +289,7 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
     FMMB_CHECK_LAUNCH();
   }
   radix_sort(rowk.get(), colk.get(), npair, bits_for(pl->tot_i), s);
-  DevBuf<int> rpos;
+  TmpBuf<int> rpos(s);
   rpos.alloc((size_t)npair + 1);
   if (npair > 0) {
     run_starts<<<nblk(npair, kT), kT, 0, s>>>(npair, rowk.get(), rpos.get());
@@ -304,8 +318,8 @@ bool build_m2l_job_dev(fmmb_plan* pl, fmmb_plan::TcJob& job, int ys, cudaStream_
 
 void build_p2p_work_dev(fmmb_plan* pl, cudaStream_t s) {
   const int nleaf = pl->nbox_i[pl->lmax];
-  DevBuf<int> cnt;
-  DevBuf<long long> nsrc;
+  TmpBuf<int> cnt(s);
+  TmpBuf<long long> nsrc(s);
   cnt.alloc((size_t)nleaf + 1);
   nsrc.alloc(std::max(nleaf, 1));
   FMMB_CUDA(cudaMemsetAsync(cnt.get() + nleaf, 0, sizeof(int), s));
@@ -318,7 +332,7 @@ void build_p2p_work_dev(fmmb_plan* pl, cudaStream_t s) {
   const int n = d2h_int(cnt.get() + nleaf, s);
   pl->m_p2p_work.alloc(std::max(n, 1));
   pl->m_p2p_nwork = n;
-  DevBuf<int> skey, sval;
+  TmpBuf<int> skey(s), sval(s);
   skey.alloc(std::max(n, 1));
   sval.alloc(std::max(n, 1));
   if (nleaf > 0) {
@@ -335,6 +349,26 @@ void build_p2p_work_dev(fmmb_plan* pl, cudaStream_t s) {
   }
   pl->p2p_nwork = n;
   pl->p2p_nwork0 = n0;
+  FMMB_CUDA(cudaStreamSynchronize(s));
+}
+
+void build_p2m_work_dev(fmmb_plan* pl, cudaStream_t s) {
+  const int nleaf = pl->nbox_j[pl->lmax], per = kP2MItem;
+  TmpBuf<int> cnt(s);
+  cnt.alloc((size_t)nleaf + 1);
+  FMMB_CUDA(cudaMemsetAsync(cnt.get() + nleaf, 0, sizeof(int), s));
+  if (nleaf > 0) {
+    src_item_counts<<<nblk(nleaf, kT), kT, 0, s>>>(nleaf, per, pl->leaf_j.get(), cnt.get());
+    FMMB_CHECK_LAUNCH();
+  }
+  exclusive_scan(cnt.get(), nleaf + 1, s);
+  const int n = d2h_int(cnt.get() + nleaf, s);
+  pl->p2m_work.alloc(std::max(n, 1));
+  pl->p2m_nwork = n;
+  if (nleaf > 0) {
+    src_items<<<nblk(nleaf, kT), kT, 0, s>>>(nleaf, per, pl->leaf_j.get(), cnt.get(), pl->p2m_work.get());
+    FMMB_CHECK_LAUNCH();
+  }
   FMMB_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cstring>
+#include <mutex>
 
 #include "internal.h"
 
@@ -84,14 +85,34 @@ void exclusive_scan(int* data, int n, cudaStream_t s) {
     FMMB_CHECK_LAUNCH();
     return;
   }
-  DevBuf<int> sums;
+  TmpBuf<int> sums(s);  // freed in stream order
   sums.alloc(nb);
   scan_tiles<<<nb, kScanThreads, 0, s>>>(data, n, sums.get());
   FMMB_CHECK_LAUNCH();
   exclusive_scan(sums.get(), nb, s);
   scan_add<<<nb, kScanThreads, 0, s>>>(data, n, sums.get());
   FMMB_CHECK_LAUNCH();
-  FMMB_CUDA(cudaStreamSynchronize(s));  // `sums` is freed on return
+}
+
+cudaMemPool_t scratch_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  FMMB_CUDA(cudaGetDevice(&dev));
+  FMMB_REQUIRE(dev >= 0 && dev < 64, FMMB_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    FMMB_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = kScratchPoolKeep;
+    FMMB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pools[dev] = pool;
+  }
+  return pools[dev];
 }
 
 namespace {
@@ -167,7 +188,7 @@ __global__ void rs_scatter(const int* kin, const int* vin, int* kout, int* vout,
 void radix_sort(int* keys, int* vals, int n, int bits, cudaStream_t s) {
   if (n <= 1 || bits <= 0) return;
   const int nb = (n + kRsTile - 1) / kRsTile;
-  DevBuf<int> k2, v2, counts;
+  TmpBuf<int> k2(s), v2(s), counts(s);
   k2.alloc(n);
   v2.alloc(n);
   counts.alloc((size_t)256 * nb);
@@ -186,7 +207,6 @@ void radix_sort(int* keys, int* vals, int n, int bits, cudaStream_t s) {
     FMMB_CUDA(cudaMemcpyAsync(keys, ka, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
     FMMB_CUDA(cudaMemcpyAsync(vals, va, n * sizeof(int), cudaMemcpyDeviceToDevice, s));
   }
-  FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
 namespace {
@@ -256,10 +276,17 @@ __global__ void gather_points(int n, const int* perm, const float* x, const floa
 }
 
 // flag[i] = 1 where a new run of (key >> shift) starts
-__global__ void run_flags(int n, const int* key, int shift, int* flag) {
+__global__ void run_flags(int n, const int* key, int shift, int* flag, int* flag_copy) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  flag[i] = (i == 0 || (key[i] >> shift) != (key[i - 1] >> shift)) ? 1 : 0;
+  const int f = (i == 0 || (key[i] >> shift) != (key[i - 1] >> shift)) ? 1 : 0;
+  flag[i] = f;
+  flag_copy[i] = f;
+}
+
+// runs of a level = last scanned flag + last flag
+__global__ void run_count(int n, const int* scanned, const int* flag_copy, int* count) {
+  *count = n > 0 ? scanned[n - 1] + flag_copy[n - 1] : 0;
 }
 
 // After the exclusive scan of the flags: write compact keys, run starts and
@@ -410,7 +437,7 @@ int prob_bits(int nprob) {
 // Builds keys, order, sorted points and all levels of one point set.
 void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
   const int n = sd.n, lmax = pl->lmax;
-  DevBuf<int> key, idx, flag, flag2;
+  TmpBuf<int> key(s), idx(s), flag(s), flag2(s), nbd(s);
   key.alloc(n);
   idx.alloc(n);
   const double rb = (double)((float)(1 << lmax) / pl->bbox[3]);  // kl/rd: float division, as the reference
@@ -433,28 +460,38 @@ void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
   // first point of each child.
   std::vector<int>& nbox = is_target ? pl->nbox_i : pl->nbox_j;
   nbox.assign(lmax + 1, 0);
-  std::vector<DevBuf<int>> kstore(lmax + 1), fstore(lmax + 1), rstore(lmax + 1);
+  // every level's runs at once (arrays of n, the bound), the counts read
+  // back with one synchronisation
+  std::vector<TmpBuf<int>> kstore, fstore, rstore;
+  for (int lev = 0; lev <= lmax; lev++) {
+    kstore.emplace_back(s);
+    fstore.emplace_back(s);
+    rstore.emplace_back(s);
+  }
   flag.alloc(n);
   flag2.alloc(n);
+  nbd.alloc(lmax + 1);
   for (int lev = lmax; lev >= 2; lev--) {
     const int shift = 3 * (lmax - lev);
-    run_flags<<<blocks(n, 256), 256, 0, s>>>(n, key.get(), shift, flag.get());
-    FMMB_CHECK_LAUNCH();
-    FMMB_CUDA(cudaMemcpyAsync(flag2.get(), flag.get(), n * sizeof(int), cudaMemcpyDeviceToDevice, s));
-    int last_flag = 0, last_scan = 0;
+    if (n > 0) {
+      run_flags<<<blocks(n, 256), 256, 0, s>>>(n, key.get(), shift, flag.get(), flag2.get());
+      FMMB_CHECK_LAUNCH();
+    }
     exclusive_scan(flag.get(), n, s);
-    FMMB_CUDA(cudaMemcpyAsync(&last_flag, flag2.get() + n - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaMemcpyAsync(&last_scan, flag.get() + n - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaStreamSynchronize(s));
-    const int nb = last_flag + last_scan;
-    nbox[lev] = nb;
-    kstore[lev].alloc(nb);
-    fstore[lev].alloc(nb);
-    rstore[lev].alloc(n);
-    run_compact<<<blocks(n, 256), 256, 0, s>>>(n, key.get(), shift, flag.get(), flag2.get(), kstore[lev].get(),
-                                               fstore[lev].get(), rstore[lev].get());
+    run_count<<<1, 1, 0, s>>>(n, flag.get(), flag2.get(), nbd.get() + lev);
     FMMB_CHECK_LAUNCH();
+    kstore[lev].alloc(n);
+    fstore[lev].alloc(n);
+    rstore[lev].alloc(n);
+    if (n > 0) {
+      run_compact<<<blocks(n, 256), 256, 0, s>>>(n, key.get(), shift, flag.get(), flag2.get(), kstore[lev].get(),
+                                                 fstore[lev].get(), rstore[lev].get());
+      FMMB_CHECK_LAUNCH();
+    }
   }
+  FMMB_CUDA(cudaMemcpyAsync(nbox.data(), nbd.get(), (lmax + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+  FMMB_CUDA(cudaStreamSynchronize(s));
+  nbox[0] = nbox[1] = 0;
   // concatenated per-level arrays, lmax first (the reference's nlbi/nlbj layout)
   std::vector<int>& off = is_target ? pl->off_i : pl->off_j;
   off.assign(lmax + 1, 0);
@@ -504,28 +541,29 @@ void build_side(fmmb_plan* pl, const Side& sd, bool is_target, cudaStream_t s) {
                                                              pl->child_count_j.get() + off[lev - 1]);
       FMMB_CHECK_LAUNCH();
     }
-    // every parent must own 1..8 children: a cheap host check that keeps a
-    // broken tree from reaching the expansion kernels
-    std::vector<int> cc(tot);
-    FMMB_CUDA(cudaMemcpyAsync(cc.data(), pl->child_count_j.get(), tot * sizeof(int), cudaMemcpyDeviceToHost, s));
-    FMMB_CUDA(cudaStreamSynchronize(s));
-    for (int lev = lmax - 1; lev >= 2; lev--)
-      for (int b = 0; b < nbox[lev]; b++) {
-        const int c = cc[off[lev] + b];
-        FMMB_REQUIRE(c >= 1 && c <= 8, FMMB_ERR_STATE, "tree build: inconsistent child count");
-      }
   }
   {
-    std::vector<int> pa(tot);
+    // cheap host checks that keep a broken tree from reaching the expansion
+    // kernels: every parent owns 1..8 children, every parent index is in range
+    std::vector<int> pa(tot), cc;
     FMMB_CUDA(cudaMemcpyAsync(pa.data(), parent_all.get(), tot * sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (!is_target) {
+      cc.resize(tot);
+      FMMB_CUDA(cudaMemcpyAsync(cc.data(), pl->child_count_j.get(), tot * sizeof(int), cudaMemcpyDeviceToHost, s));
+    }
     FMMB_CUDA(cudaStreamSynchronize(s));
+    if (!is_target)
+      for (int lev = lmax - 1; lev >= 2; lev--)
+        for (int b = 0; b < nbox[lev]; b++) {
+          const int c = cc[off[lev] + b];
+          FMMB_REQUIRE(c >= 1 && c <= 8, FMMB_ERR_STATE, "tree build: inconsistent child count");
+        }
     for (int lev = lmax; lev >= 3; lev--)
       for (int b = 0; b < nbox[lev]; b++) {
         const int q = pa[off[lev] + b];
         FMMB_REQUIRE(q >= 0 && q < nbox[lev - 1], FMMB_ERR_STATE, "tree build: parent index out of range");
       }
   }
-  FMMB_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace
@@ -545,7 +583,7 @@ void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const f
     // root cube from the extent of all points, as the BEM drivers do
     // (biobem/fmm_matmult.h:29-114): corner at the minimum, side = largest
     // extent * (1 + 1e-5).
-    DevBuf<float> mm;
+    TmpBuf<float> mm(s);
     mm.alloc(6 * 2);
     float init[12];
     for (int k = 0; k < 6; k++) {
@@ -605,7 +643,7 @@ void build_tree(fmmb_plan* pl, int ni, const float* tx, const float* ty, const f
         pl->d_slot_rel.get(), pl->m2l_list.get() + (size_t)pl->off_i[lev] * kM2LSlots);
     FMMB_CHECK_LAUNCH();
   }
-  DevBuf<unsigned long long> cnt;
+  TmpBuf<unsigned long long> cnt(s);
   cnt.alloc(2);
   FMMB_CUDA(cudaMemsetAsync(cnt.get(), 0, 2 * sizeof(unsigned long long), s));
   count_p2p_pairs<<<blocks(nleaf_i, 128), 128, 0, s>>>(nleaf_i, pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(),
