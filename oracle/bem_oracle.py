@@ -109,3 +109,81 @@ def solvation_energy_dense(cen, nrm, area, x_atoms, q_atoms, e1=4.0, e2=20.0):
     kg = kernel_matrix(x_atoms, 0, xs=cen)
     phi = kg @ (x * np.asarray(area) / e1)
     return float(0.5 * 332.112 * np.dot(np.asarray(q_atoms, np.float64), phi)), x, phi
+
+
+def biobem_matvec(geom, x, e1=4.0, e2=20.0):
+    """The reference's 6-node double-layer operator (biobem/fmm_matmult.h:9-196,
+    mymatmult) with dense FP64 direct sums, restated in its own order: stage
+    1 puts, for every node m, an impulse on m and one source at each
+    quadrature point of every element around m (charge 0.5 hsg phi_m x_m / e1,
+    position and normal interpolated from the element's nodes, :53-109);
+    stage 2 every quadrature point with charge -0.5 hsg (:112-160), the result
+    times x / e1 (:171-173); then the (e1 + e2) / (e1 - e2) x / e1 term
+    (:176-178).  Targets: the nodes.  geom: old_fmm_bem_b200.mesh6 arrays."""
+    ptr = geom["ptr"].astype(np.float64)
+    vna = geom["vna"].astype(np.float64)
+    ntr, hsg, phi = geom["ntr"], geom["hsg"].astype(np.float64), geom["phi"].astype(np.float64)
+    nne_ptr, nne_elm = geom["nne_ptr"], geom["nne_elm"]
+    nwn, ngl = len(ptr), hsg.shape[1]
+    x = np.asarray(x, np.float64)
+
+    def point(k, j):
+        xs = np.zeros(3)
+        ns = np.zeros(3)
+        for i in range(6):
+            xs = xs + ptr[ntr[k, i]] * phi[k, j, i]
+            ns = ns + vna[ntr[k, i]] * phi[k, j, i]
+        return xs.astype(np.float32), ns.astype(np.float32)
+
+    pts = {}
+    pos1, nrm1, q1 = [], [], []
+    for m in range(nwn):
+        for k in nne_elm[nne_ptr[m]:nne_ptr[m + 1]]:
+            for j in range(ngl):
+                if (k, j) not in pts:
+                    pts[(k, j)] = point(k, j)
+                xs, ns = pts[(k, j)]
+                qint = sum(phi[k, j, i] for i in range(6) if ntr[k, i] == m)
+                pos1.append(xs)
+                nrm1.append(ns)
+                q1.append(0.5 * hsg[k, j] * qint * x[m] / e1)
+    y = kernel_matrix(ptr.T, 2, ns=np.array(nrm1).T, xs=np.array(pos1).T) @ np.array(q1)
+    pos2 = np.array([pts[(k, j)][0] for k in range(len(ntr)) for j in range(ngl)])
+    nrm2 = np.array([pts[(k, j)][1] for k in range(len(ntr)) for j in range(ngl)])
+    s2 = kernel_matrix(ptr.T, 2, ns=nrm2.T, xs=pos2.T) @ (-0.5 * hsg.reshape(-1))
+    return y + s2 * x / e1 + (e1 + e2) / (e1 - e2) * x / e1
+
+
+def biobem_energy_dense(geom, e1=4.0, e2=20.0):
+    """The reference's biobem pipeline (biobem/main.cxx:101-195) with dense
+    FP64 matrices and a direct solve: right-hand side -4 pi Gni(charges ->
+    nodes, target normals -vna) / e1, the operator of biobem_matvec as a dense
+    matrix, reaction potential G(quadrature charges -> atoms), energy
+    0.5 * 332.112 * sum q phi.  The operator is assembled from the quadrature
+    points once (interpolation matrix times the kernel matrix), the same sums
+    as biobem_matvec's node-by-node order.  Returns (energy, node densities,
+    the dense operator)."""
+    ptr = geom["ptr"].astype(np.float64)
+    vna = geom["vna"].astype(np.float64)
+    nwn = len(ptr)
+    xq, vq = geom["xq"].astype(np.float64), geom["vq"].astype(np.float64)
+    b = -4 * np.pi * (kernel_matrix(ptr.T, 1, nt=-vna.T, xs=xq) @ vq) / e1
+    ntr, hsg, phi = geom["ntr"], geom["hsg"].astype(np.float64), geom["phi"].astype(np.float64)
+    ne, ngl = hsg.shape
+    pos = np.zeros((ne, ngl, 3))
+    nrm = np.zeros((ne, ngl, 3))
+    W = np.zeros((ne * ngl, nwn))  # node values -> quadrature charges / (0.5 hsg / e1)
+    rows = np.arange(ne * ngl).reshape(ne, ngl)
+    for i in range(6):
+        pos += ptr[ntr[:, i]][:, None, :] * phi[:, :, i:i + 1]
+        nrm += vna[ntr[:, i]][:, None, :] * phi[:, :, i:i + 1]
+        np.add.at(W, (rows, np.repeat(ntr[:, i:i + 1], ngl, 1)), phi[:, :, i])
+    pos = pos.reshape(-1, 3).astype(np.float32).astype(np.float64)
+    nrm = nrm.reshape(-1, 3).astype(np.float32).astype(np.float64)
+    w = 0.5 * hsg.reshape(-1) / e1
+    K = kernel_matrix(ptr.T, 2, ns=nrm.T, xs=pos.T)
+    s2 = K @ (-0.5 * hsg.reshape(-1))
+    A = K @ (w[:, None] * W) + np.diag(s2 / e1 + (e1 + e2) / (e1 - e2) / e1)
+    si = np.linalg.solve(A, b)
+    pot = kernel_matrix(xq, 0, xs=pos.T) @ (w * (W @ si))
+    return float(0.5 * 332.112 * np.dot(vq, pot)), si, A

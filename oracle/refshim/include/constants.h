@@ -52,7 +52,11 @@ const int nblok0  = 128;
 const int nblok1  = 64;
 const int nblok2  = 4;
 const int ins     = 50;
+#ifdef REF_NGL
+const int ngl     = REF_NGL;     // Gauss points per triangle (the biobem geometry build sets it)
+#else
 const int ngl     = 3;
+#endif
 const float eps   = 1e-6;        // softening / angle guard, single precision like the reference
 const float pi    = M_PI;        // single-precision pi, as the reference uses it
 
