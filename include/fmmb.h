@@ -295,6 +295,25 @@ FMMB_API int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx,
                                 const float* snz, const float* bbox, int lmin, int lmax_hi, int reps, int* best,
                                 float* ms_out);
 
+/* Chooses the expansion order and octree depth for an accuracy target.  For
+ * p = p_lo, p_lo + 1, ... p_hi: the depth from fmmb_autotune_lmax (reps timed
+ * evaluates per candidate depth), then one FP64-output evaluate at that
+ * (p, depth) of fixed pseudo-random charges, compared with the FP64 direct
+ * sum (fmmb_direct_f64) on nsample targets (0: 1024) taken as 16 runs of
+ * consecutive targets spread over the set.  Stops at the first order whose
+ * relative error (2-norm over the sample) is at most tol: *p_out, *lmax_out,
+ * *err_out (may be NULL) and *ms_out (may be NULL, ms per evaluate at that
+ * depth) describe it; when no order in the range reaches tol they describe
+ * p_hi and *err_out > tol tells.  Laplace kernels; the other cfg fields
+ * (precision, semantics, ...) as given.  The reference fixes the order at
+ * compile time (include/constants.h:15, mp); this chooses it per geometry and
+ * tolerance, the depth as fmmb_autotune_lmax (fmm/nlevel.cxx:5-31). */
+FMMB_API int fmmb_autotune_order(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                                 const float* tnx, const float* tny, const float* tnz, int nj, const float* sx,
+                                 const float* sy, const float* sz, const float* snx, const float* sny,
+                                 const float* snz, const float* bbox, double tol, int p_lo, int p_hi, int nsample,
+                                 int reps, int* p_out, int* lmax_out, double* err_out, float* ms_out);
+
 /* fmmb_autotune_lmax for a batch of independent problems
  * (fmmb_set_geometry_batch's arguments): the one depth of the forest. */
 FMMB_API int fmmb_autotune_lmax_batch(const fmmb_config* cfg, int nprob, const int* t_off, const float* tx,

@@ -36,7 +36,8 @@ EXPORTS = ["fmmb_config_init", "fmmb_plan_create", "fmmb_plan_destroy", "fmmb_se
            "fmmb_last_error", "fmmb_direct_static", "fmmb_autotune_lmax", "fmmb_evaluate_transpose",
            "fmmb_evaluate_transpose_f64", "fmmb_position_grad", "fmmb_set_geometry_batch", "fmmb_gmres_config_init",
            "fmmb_gmres", "fmmb_autotune_lmax_batch", "fmmb_gpu_p2p",
-           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times", "fmmb_set_overlap", "fmmb_adjoint_f64"]
+           "fmmb_gpu_p2m", "fmmb_gpu_l2p", "fmmb_gpu_m2l", "fmmb_get_setup_times", "fmmb_set_overlap", "fmmb_adjoint_f64",
+           "fmmb_autotune_order"]
 
 
 def lib_path() -> str:
@@ -88,6 +89,8 @@ def load():
     lib.fmmb_adjoint_f64.argtypes = [_vp] * 7
     lib.fmmb_autotune_lmax.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
         [_vp] * 6 + [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp]
+    lib.fmmb_autotune_order.argtypes = [ctypes.POINTER(_Config), ctypes.c_int] + [_vp] * 6 + [ctypes.c_int] + \
+        [_vp] * 6 + [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, _vp]
     lib.fmmb_gpu_p2p.argtypes = [_vp] * 15
     lib.fmmb_gpu_p2m.argtypes = [_vp] * 14
     lib.fmmb_gpu_l2p.argtypes = [_vp] * 14
@@ -446,6 +449,27 @@ def autotune_lmax(targets, sources, *, kernel=LAPLACE_G, target_normals=None, so
                      lambda lib, cfg, best, ms: lib.fmmb_autotune_lmax(
                          ctypes.byref(cfg), ni, *t, *tn, nj, *s, *sn, bb, lmin, lmax, reps, ctypes.byref(best),
                          ms.ctypes.data))
+
+
+def autotune_order(targets, sources, tol, *, kernel=LAPLACE_G, target_normals=None, source_normals=None, p_lo=4,
+                   p_hi=16, precision=FP64, semantics=SEM_ACCURATE, eps2=0.0, exclude_self=False, bbox=None,
+                   nsample=1024, reps=2):
+    """Lowest expansion order in [p_lo, p_hi] whose FMM meets the relative
+    error tol against the FP64 direct sum on a sample of targets, with its
+    autotuned depth (fmmb_autotune_order).  Returns (p, lmax, rel_err,
+    ms_per_evaluate); rel_err > tol when no order in the range meets tol."""
+    lib = load()
+    t, tn, s, sn, bb, keep = _sets(targets, sources, target_normals, source_normals, bbox)
+    ni, nj = len(targets[0]), len(sources[0])
+    cfg = _Config()
+    lib.fmmb_config_init(ctypes.byref(cfg))
+    cfg.kernel, cfg.p, cfg.precision, cfg.semantics = kernel, p_lo, precision, semantics
+    cfg.eps2, cfg.exclude_self = eps2, int(exclude_self)
+    p, lm, err, ms = ctypes.c_int(-1), ctypes.c_int(-1), ctypes.c_double(0.0), ctypes.c_float(0.0)
+    _check(lib.fmmb_autotune_order(ctypes.byref(cfg), ni, *t, *tn, nj, *s, *sn, bb, ctypes.c_double(tol), p_lo, p_hi,
+                                   nsample, reps, ctypes.byref(p), ctypes.byref(lm), ctypes.byref(err),
+                                   ctypes.byref(ms)))
+    return p.value, lm.value, err.value, ms.value
 
 
 def autotune_lmax_batch(t_off, targets, s_off, sources, *, kernel=LAPLACE_G, target_normals=None,

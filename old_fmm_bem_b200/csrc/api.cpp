@@ -1209,6 +1209,95 @@ int fmmb_autotune_lmax(const fmmb_config* cfg, int ni, const float* tx, const fl
   });
 }
 
+int fmmb_autotune_order(const fmmb_config* cfg, int ni, const float* tx, const float* ty, const float* tz,
+                        const float* tnx, const float* tny, const float* tnz, int nj, const float* sx, const float* sy,
+                        const float* sz, const float* snx, const float* sny, const float* snz, const float* bbox,
+                        double tol, int p_lo, int p_hi, int nsample, int reps, int* p_out, int* lmax_out,
+                        double* err_out, float* ms_out) {
+  return guarded([&] {
+    FMMB_REQUIRE(cfg && p_out && lmax_out, FMMB_ERR_ARG, "null argument");
+    FMMB_REQUIRE(!helm_family(cfg->kernel), FMMB_ERR_ARG, "order autotuning takes the Laplace kernels");
+    FMMB_REQUIRE(tol > 0.0 && 1 <= p_lo && p_lo <= p_hi && p_hi <= 20, FMMB_ERR_ARG,
+                 "need tol > 0 and 1 <= p_lo <= p_hi <= 20");
+    FMMB_REQUIRE(ni >= 1 && nj >= 1, FMMB_ERR_ARG, "need at least one target and one source");
+    nsample = std::max(1, std::min(nsample > 0 ? nsample : 1024, ni));
+    // pseudo-random charges (caller order) and the FP64 direct sums on the
+    // sample: 16 runs of consecutive targets spread over [0, ni)
+    std::vector<float> hq(nj);
+    uint64_t st = 0x2545F4914F6CDD1Dull;
+    for (auto& v : hq) {
+      st = st * 6364136223846793005ull + 1442695040888963407ull;
+      v = (float)((st >> 40) * (2.0 / 16777216.0) - 1.0);
+    }
+    DevBuf<float> dq;
+    dq.alloc(nj);
+    FMMB_CUDA(cudaMemcpy(dq.get(), hq.data(), nj * sizeof(float), cudaMemcpyHostToDevice));
+    const int nrun = std::min(16, nsample), per = nsample / nrun;
+    std::vector<std::pair<int, int>> runs;
+    for (int r = 0; r < nrun; r++) {
+      const int a = (int)((long long)ni * r / nrun);
+      runs.push_back({a, std::min(ni, a + per)});
+    }
+    std::vector<double> ref;
+    {
+      fmmb_config c = *cfg;
+      c.nrhs = 1;
+      c.lmax = 2;
+      fmmb_plan* pl = nullptr;
+      int rc = fmmb_plan_create(&c, &pl);
+      if (rc == FMMB_OK) rc = fmmb_set_geometry(pl, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+      for (const auto& r : runs) {
+        std::vector<double> h(r.second - r.first);
+        if (rc == FMMB_OK) rc = fmmb_direct_f64(pl, dq.get(), r.first, r.second, h.data(), nullptr);
+        ref.insert(ref.end(), h.begin(), h.end());
+      }
+      const std::string err = rc == FMMB_OK ? std::string() : std::string(fmmb_last_error());
+      if (pl) fmmb_plan_destroy(pl);
+      if (rc != FMMB_OK) throw Error{rc, "order autotune, direct sum: " + err};
+    }
+    double rn = 0.0;
+    for (double v : ref) rn += v * v;
+    DevBuf<double> dpot;
+    dpot.alloc(ni);
+    std::vector<double> pot(ni);
+    *p_out = -1;
+    for (int p = p_lo; p <= p_hi; p++) {
+      fmmb_config c = *cfg;
+      c.p = p;
+      c.nrhs = 1;
+      int best = -1;
+      std::vector<float> ms(16, -1.f);
+      int rc = fmmb_autotune_lmax(&c, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox, 0, 0, reps,
+                                  &best, ms.data());
+      if (rc != FMMB_OK) throw Error{rc, "order autotune at p " + std::to_string(p) + ": " + fmmb_last_error()};
+      c.lmax = best;
+      fmmb_plan* pl = nullptr;
+      rc = fmmb_plan_create(&c, &pl);
+      if (rc == FMMB_OK) rc = fmmb_set_geometry(pl, ni, tx, ty, tz, tnx, tny, tnz, nj, sx, sy, sz, snx, sny, snz, bbox);
+      if (rc == FMMB_OK) rc = fmmb_evaluate_f64(pl, dq.get(), dpot.get(), nullptr);
+      const std::string err = rc == FMMB_OK ? std::string() : std::string(fmmb_last_error());
+      if (pl) fmmb_plan_destroy(pl);
+      if (rc != FMMB_OK) throw Error{rc, "order autotune at p " + std::to_string(p) + ": " + err};
+      FMMB_CUDA(cudaMemcpy(pot.data(), dpot.get(), ni * sizeof(double), cudaMemcpyDeviceToHost));
+      double dn = 0.0;
+      size_t k = 0;
+      for (const auto& r : runs)
+        for (int i = r.first; i < r.second; i++, k++) dn += (pot[i] - ref[k]) * (pot[i] - ref[k]);
+      const double e = rn > 0.0 ? std::sqrt(dn / rn) : std::sqrt(dn);
+      *p_out = p;
+      *lmax_out = best;
+      if (err_out) *err_out = e;
+      if (ms_out) {
+        // the chosen depth's time: autotune_lmax's range starts at its own estimate
+        int l = 2;
+        while (l < 10 && (double)std::max(ni, nj) / std::pow(8.0, l) > 64.0) l++;
+        *ms_out = ms[best - std::max(2, l - 1)];
+      }
+      if (e <= tol) break;
+    }
+  });
+}
+
 int fmmb_autotune_lmax_batch(const fmmb_config* cfg, int nprob, const int* t_off, const float* tx, const float* ty,
                              const float* tz, const float* tnx, const float* tny, const float* tnz, const int* s_off,
                              const float* sx, const float* sy, const float* sz, const float* snx, const float* sny,

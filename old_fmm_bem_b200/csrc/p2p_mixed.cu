@@ -374,10 +374,12 @@ __global__ void __launch_bounds__(kThreads) p2p_mixed(const int2* __restrict__ w
         if (t < ntl && it < li.y) {
           const int i = li.x + it;
           pot[i] = coef * P[t][0];
-          if (KER == FMMB_LAPLACE_G && grad) {  // grad(1/r) = -d / r^3
-            grad[i] = -coef * P[t][1];
-            grad[ni + i] = -coef * P[t][2];
-            grad[2 * (size_t)ni + i] = -coef * P[t][3];
+          if (KER == FMMB_LAPLACE_G) {  // grad(1/r) = -d / r^3; G's gradient is optional
+            if (grad) {
+              grad[i] = -coef * P[t][1];
+              grad[ni + i] = -coef * P[t][2];
+              grad[2 * (size_t)ni + i] = -coef * P[t][3];
+            }
           } else if (with_grad(KER)) {
             grad[i] = coef * P[t][1];
             grad[ni + i] = coef * P[t][2];

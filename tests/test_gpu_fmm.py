@@ -255,6 +255,41 @@ def test_autotune_lmax_picks_a_measured_depth(ob):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_laplace_g_without_gradient(precision, ob):
+    """An evaluate of the G kernel with no gradient output (a NULL grad
+    through the C ABI) gives the potential of the evaluate with gradient."""
+    import ctypes
+    t, tn, s, sn, q = make_points(20000, 92, "clustered")
+    pl = plan_for(ob, 0, 10, 4, t, tn, s, sn, semantics=1, precision=precision, exclude_self=True)
+    v, g = pl.evaluate(q, f64=True)
+    pot = np.zeros(t.shape[1])
+    for _ in range(2):  # the first call captures the no-gradient graph, the second replays it
+        rc = ob.load().fmmb_evaluate_f64(pl._h, q.ctypes.data, pot.ctypes.data, None)
+        assert rc == 0, ob.load().fmmb_last_error()
+        assert rel(pot, v) < 1e-13  # the same sums (FP64 atomics in the M2M: rounding order only)
+    pl.close()
+
+
+def test_autotune_order_meets_the_tolerance(ob):
+    """fmmb_autotune_order: the lowest order in the range whose FMM meets the
+    tolerance against the FP64 direct sum on its sample of targets, at the
+    depth fmmb_autotune_lmax picks for it; the order below misses it, and the
+    chosen plan meets it on targets outside the sample too."""
+    t, _, _, _, q = make_points(30000, 91, "clustered")
+    kw = dict(kernel=0, precision=ob.MIXED, semantics=ob.SEM_ACCURATE, exclude_self=True, bbox=(0, 0, 0, 1))
+    p, lmax, err, ms = ob.autotune_order(t, t, 1e-6, p_lo=6, p_hi=14, **kw)
+    assert 6 < p <= 14 and err <= 1e-6 and 2 <= lmax <= 10 and ms > 0
+    _, _, err_below, _ = ob.autotune_order(t, t, 1e-6, p_lo=p - 1, p_hi=p - 1, **kw)
+    assert err_below > 1e-6
+    pl = ob.Plan(kernel=0, p=p, lmax=lmax, precision=ob.MIXED, semantics=ob.SEM_ACCURATE, exclude_self=True)
+    pl.set_geometry(t, t, bbox=(0, 0, 0, 1))
+    v, _ = pl.evaluate(q, f64=True)
+    vd, _ = pl.direct(q, 20000, 21000)
+    pl.close()
+    assert rel(v[20000:21000], vd) < 2e-6
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 def test_many_right_hand_sides_equal_single_evaluates(precision, ob):
     """nrhs = 3 in one evaluate gives the three single evaluates, gradients
     included: FP64 form (each right-hand side replayed through the plan's CUDA
