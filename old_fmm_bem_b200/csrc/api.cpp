@@ -682,7 +682,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   {
     PhaseTimer tm(pl, 0, side);
     launch_helm_p2p(pl->cfg.precision == FMMB_MIXED, yuk, (float)k, (float)pl->cfg.eps2, pl->cfg.exclude_self != 0,
-                    pl->h_p2p_nwork, pl->h_p2p_work.get(),
+                    (float)wleaf, pl->h_p2p_nwork, pl->h_p2p_work.get(),
                     pl->leaf_i.get(), pl->leaf_j.get(), pl->p2p_list.get(), pl->tpos.get(), pl->spos.get(), qs,
                     pot_near, side);
   }

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(128) helm_l2p(int p, int K, double k, int yuk,
 // phase reduced to [-pi, pi]), summed over 32 sources, then added in FP64;
 // FP64 form: everything in FP64.  Zero-distance pairs
 // contribute nothing (their inverse distance is taken as 0).
-template <bool YUK>
+template <bool YUK, bool REDUCE>
 __device__ __forceinline__ void helm_pair(float k, float eps2, bool excl, const float4 x, const float4 s,
                                           const float2 q, float& fr, float& fi) {
   const float dx = x.x - s.x, dy = x.y - s.y, dz = x.z - s.z;
@@ -365,10 +365,11 @@ __device__ __forceinline__ void helm_pair(float k, float eps2, bool excl, const 
     fi = fmaf(q.y, e, fi);
     return;
   }
-  // phase k r reduced to [-pi, pi] (exact for k r < pi, the usual near-field
-  // range), then the hardware sine / cosine (absolute error ~4e-7 there)
+  // phase k r reduced to [-pi, pi] (the identity for k r < pi, the usual
+  // near-field range), then the hardware sine / cosine (absolute error ~4e-7
+  // there)
   const float ph = k * (r2 * rinv);
-  const float red = fmaf(-6.28318530717958647f, rintf(ph * 0.159154943091895336f), ph);
+  const float red = REDUCE ? fmaf(-6.28318530717958647f, rintf(ph * 0.159154943091895336f), ph) : ph;
   float sn, cs;
   __sincosf(red, &sn, &cs);
   fr += (q.x * cs - q.y * sn) * rinv;
@@ -393,14 +394,29 @@ __device__ __forceinline__ void helm_pair64(double k, double eps2, bool excl, co
   ai += (q.x * sn + q.y * cs) / r;
 }
 
-template <bool F32, bool YUK>
+// Near field.  A block of 128 threads takes a work item of up to 256 targets
+// of one leaf (2 per thread).  The sources of its (up to 27) neighbour leaves
+// are staged into shared memory as one list in chunks of kHC (warp 0 lays the
+// leaves end to end with one lane per neighbour slot: ballot + scan), so a
+// chunk costs two barriers whatever the leaf sizes -- the former per-leaf
+// staging paid two barriers per 128 sources of every leaf.  Each thread sums
+// runs of 32 sources in FP32 (mixed form) and promotes each run's partial sum
+// to FP64.  REDUCE: reduce the phase k r to [-pi, pi] before the hardware sine
+// and cosine; the launcher leaves it out when every near-field distance is
+// below pi / k (then the reduction is the identity: same values).
+constexpr int kHC = 1024;
+
+template <bool F32, bool YUK, bool REDUCE>
 __global__ void __launch_bounds__(128) helm_p2p(float k, float eps2, int excl, const int2* __restrict__ work,
                                                 const int2* __restrict__ leaf_i,
                                                 const int2* __restrict__ leaf_j, const int* __restrict__ list,
                                                 const float4* __restrict__ tpos, const float4* __restrict__ spos,
                                                 const float2* __restrict__ q, double2* __restrict__ pot) {
-  __shared__ float4 sp[128];
-  __shared__ float2 sq[128];
+  __shared__ float4 sp[kHC];
+  __shared__ float2 sq[kHC];
+  __shared__ int2 seg[32];  // (first source, count) of each non-empty neighbour leaf
+  __shared__ int vst[33];   // start of each leaf in the staged list, then the total
+  __shared__ int nseg_s;
   const int2 wk = work[blockIdx.x];
   const int b = wk.x;
   const int2 li = leaf_i[b];
@@ -408,45 +424,71 @@ __global__ void __launch_bounds__(128) helm_p2p(float k, float eps2, int excl, c
   const bool on0 = i0 < li.y, on1 = i1 < li.y;
   const float4 x0 = on0 ? tpos[li.x + i0] : make_float4(0.f, 0.f, 0.f, 0.f);
   const float4 x1 = on1 ? tpos[li.x + i1] : make_float4(0.f, 0.f, 0.f, 0.f);
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    int2 sg = make_int2(0, 0);
+    if (lane < kP2PSlots) {
+      const int jl = list[(size_t)b * kP2PSlots + lane];
+      if (jl >= 0) sg = leaf_j[jl];
+    }
+    const bool has = sg.y > 0;
+    const unsigned mask = __ballot_sync(0xffffffffu, has);
+    const int pos = __popc(mask & ((1u << lane) - 1u));
+    int incl = has ? sg.y : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (has) {
+      seg[pos] = sg;
+      vst[pos] = incl - sg.y;
+    }
+    if (lane == 31) {
+      vst[__popc(mask)] = incl;  // the total
+      nseg_s = __popc(mask);
+    }
+  }
+  __syncthreads();
+  const int nseg = nseg_s, ntot = vst[nseg];
   double ar0 = 0, ai0 = 0, ar1 = 0, ai1 = 0;
-  for (int sl = 0; sl < kP2PSlots; sl++) {
-    const int jl = list[(size_t)b * kP2PSlots + sl];
-    if (jl < 0) continue;
-    const int2 lj = leaf_j[jl];
-    for (int c0 = 0; c0 < lj.y; c0 += 128) {
-      __syncthreads();
-      if (c0 + threadIdx.x < lj.y) {
-        sp[threadIdx.x] = spos[lj.x + c0 + threadIdx.x];
-        sq[threadIdx.x] = q[lj.x + c0 + threadIdx.x];
-      }
-      __syncthreads();
-      const int nc = min(128, lj.y - c0);
-      if (!on0) continue;
-      for (int r0 = 0; r0 < nc; r0 += 32) {
-        const int re = min(nc, r0 + 32);
-        if (F32) {
-          float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
-          if (on1) {
-            for (int jj = r0; jj < re; jj++) {
-              const float4 sv = sp[jj];
-              const float2 qq = sq[jj];
-              helm_pair<YUK>(k, eps2, excl, x0, sv, qq, fr0, fi0);
-              helm_pair<YUK>(k, eps2, excl, x1, sv, qq, fr1, fi1);
-            }
-          } else {
-            for (int jj = r0; jj < re; jj++) helm_pair<YUK>(k, eps2, excl, x0, sp[jj], sq[jj], fr0, fi0);
-          }
-          ar0 += fr0;
-          ai0 += fi0;
-          ar1 += fr1;
-          ai1 += fi1;
-        } else {
+  for (int c0 = 0; c0 < ntot; c0 += kHC) {
+    const int nc = min(kHC, ntot - c0);
+    __syncthreads();  // the previous chunk's readers are done
+    for (int u = threadIdx.x; u < nc; u += 128) {
+      const int v = c0 + u;
+      int sgi = 0;
+      while (sgi + 1 < nseg && vst[sgi + 1] <= v) sgi++;
+      const int j = seg[sgi].x + (v - vst[sgi]);
+      sp[u] = spos[j];
+      sq[u] = q[j];
+    }
+    __syncthreads();
+    if (!on0) continue;
+    for (int r0 = 0; r0 < nc; r0 += 32) {
+      const int re = min(nc, r0 + 32);
+      if (F32) {
+        float fr0 = 0.f, fi0 = 0.f, fr1 = 0.f, fi1 = 0.f;
+        if (on1) {
           for (int jj = r0; jj < re; jj++) {
             const float4 sv = sp[jj];
             const float2 qq = sq[jj];
-            helm_pair64<YUK>((double)k, (double)eps2, excl, x0, sv, qq, ar0, ai0);
-            if (on1) helm_pair64<YUK>((double)k, (double)eps2, excl, x1, sv, qq, ar1, ai1);
+            helm_pair<YUK, REDUCE>(k, eps2, excl, x0, sv, qq, fr0, fi0);
+            helm_pair<YUK, REDUCE>(k, eps2, excl, x1, sv, qq, fr1, fi1);
           }
+        } else {
+          for (int jj = r0; jj < re; jj++) helm_pair<YUK, REDUCE>(k, eps2, excl, x0, sp[jj], sq[jj], fr0, fi0);
+        }
+        ar0 += fr0;
+        ai0 += fi0;
+        ar1 += fr1;
+        ai1 += fi1;
+      } else {
+        for (int jj = r0; jj < re; jj++) {
+          const float4 sv = sp[jj];
+          const float2 qq = sq[jj];
+          helm_pair64<YUK>((double)k, (double)eps2, excl, x0, sv, qq, ar0, ai0);
+          if (on1) helm_pair64<YUK>((double)k, (double)eps2, excl, x1, sv, qq, ar1, ai1);
         }
       }
     }
@@ -650,21 +692,27 @@ void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float*
   FMMB_CHECK_LAUNCH();
 }
 
-void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, int nwork, const int2* work,
-                     const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos, const float4* spos,
-                     const float* qs, double* pot, cudaStream_t st) {
+void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, float leaf_side, int nwork,
+                     const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
+                     const float4* spos, const float* qs, double* pot, cudaStream_t st) {
   if (nwork <= 0) return;
   const float2* q2 = (const float2*)qs;
   double2* p2 = (double2*)pot;
   const int ex = excl ? 1 : 0;
-  if (f32 && !yuk)
-    helm_p2p<true, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+  // points of neighbouring leaves lie at most 2 sqrt(3) leaf sides apart:
+  // below pi / k (with a margin for the float phase) no reduction is needed
+  const double rmax = std::sqrt(12.0 * (double)leaf_side * leaf_side + (double)eps2);
+  const bool reduce = !((double)k * rmax < 0.999 * M_PI);
+  if (f32 && !yuk && reduce)
+    helm_p2p<true, false, true><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+  else if (f32 && !yuk)
+    helm_p2p<true, false, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   else if (f32)
-    helm_p2p<true, true><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+    helm_p2p<true, true, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   else if (!yuk)
-    helm_p2p<false, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+    helm_p2p<false, false, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   else
-    helm_p2p<false, true><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
+    helm_p2p<false, true, false><<<nwork, 128, 0, st>>>(k, eps2, ex, work, leaf_i, leaf_j, list, tpos, spos, q2, p2);
   FMMB_CHECK_LAUNCH();
 }
 

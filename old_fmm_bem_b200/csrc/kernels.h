@@ -162,9 +162,11 @@ struct HelmOp {          // one translation operator to build
 void launch_helm_gather(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
 // work: (target leaf, first target) per item of up to 256 targets; yuk: the
 // Yukawa kernel (real e^{-k r}/(4 pi r), complex charges with zero imaginary parts)
-void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, int nwork, const int2* work,
-                     const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos, const float4* spos,
-                     const float* qs, double* pot, cudaStream_t st);
+// leaf_side: side of a leaf box (decides whether the FP32 phase needs its
+// range reduction)
+void launch_helm_p2p(bool f32, bool yuk, float k, float eps2, bool excl, float leaf_side, int nwork,
+                     const int2* work, const int2* leaf_i, const int2* leaf_j, const int* list, const float4* tpos,
+                     const float4* spos, const float* qs, double* pot, cudaStream_t st);
 void launch_helm_gather_real(int n, int nrhs, const int* perm, const float* q, float* qs, cudaStream_t st);
 template <typename T>
 void launch_helm_finalize_real(int n, const int* perm, const double* near, const double* far, double scale, T* out,
