@@ -257,8 +257,10 @@ FMMB_API int fmmb_gmres(fmmb_plan* plan, const fmmb_gmres_config* cfg, const flo
 
 /* Direct sum without a plan that allocates nothing (no cudaMalloc/cudaFree,
  * no allocating library routine).  It has no counterpart in the reference:
- * it serves callers that must not allocate, such as a stream about to be
- * captured into a CUDA graph.  Same arithmetic as fmmb_direct_f64 (FP64, the
+ * it serves callers that must not allocate device memory -- a host framework
+ * that reserves the whole device memory up front for its own allocator, or a
+ * loop that cannot take the implicit device synchronisation and the possible
+ * failure of an allocation.  Same arithmetic as fmmb_direct_f64 (FP64, the
  * kernel, semantics, eps2 and exclude_self of cfg; the other fields are
  * ignored), float outputs pot[ni] and, for FMMB_LAPLACE_G, grad[3*ni] (may be
  * NULL).  Every pointer must be device memory of the current device (or
