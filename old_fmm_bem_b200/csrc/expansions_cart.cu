@@ -585,6 +585,12 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
   constexpr bool DER = KER != FMMB_LAPLACE_GNJ;  // derivative sums needed
   __shared__ float2 Cphi[NT], Cz[DER ? NT : 1], Cp[DER ? NT : 1], Cm[DER ? NT : 1];
   __shared__ float Cs[P + 1];
+  // the derivative sums in pairs for the two-lane FP32 FMAs: (fn, zn) from
+  // CA = (Cphi.re, Cz.re, -Cphi.im, -Cz.im), (pr, mr) and (pi, mi) from
+  // CB = (Cp.re, Cm.re, -Cp.im, -Cm.im) and CC = (Cp.im, Cm.im); the same
+  // per-lane operations, in the same order, as the scalar sums
+  __shared__ float4 CA[DER ? NT : 1], CB[DER ? NT : 1];
+  __shared__ float2 CC[DER ? NT : 1];
   const int2 wk = work[blockIdx.x];
   const int b = wk.x;
   const double* Lb = L + (size_t)b * K;
@@ -611,6 +617,15 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
     }
   }
   for (int n = threadIdx.x; n <= P; n += blockDim.x) Cs[n] = (n < p) ? (float)(fac[ifull_d(n + 1, 0)] * Lb[(n + 1) * (n + 1)]) : 0.f;
+  if (DER) {
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NT; idx += blockDim.x) {
+      const float2 f = Cphi[idx], zz = Cz[idx], pp = Cp[idx], mm = Cm[idx];
+      CA[idx] = make_float4(f.x, zz.x, -f.y, -zz.y);
+      CB[idx] = make_float4(pp.x, mm.x, -pp.y, -mm.y);
+      CC[idx] = make_float2(pp.y, mm.y);
+    }
+  }
   __syncthreads();
   double xc, yc, zc;
   box_center(keys[b], xmin, ymin, zmin, rb, xc, yc, zc);
@@ -630,7 +645,8 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
 #pragma unroll
     for (int n = 0; n <= P; n++) {
       float cre[P + 1], cim[P + 1];
-      float fn = 0.f, zn = 0.f, pr = 0.f, pi = 0.f, mr = 0.f, mi = 0.f;
+      float fn = 0.f;
+      float2 fz = make_float2(0.f, 0.f), pmr = fz, pmi = fz;  // (fn, zn), (pr, mr), (pi, mi)
 #pragma unroll
       for (int m = 0; m <= P; m++) {
         cre[m] = cim[m] = 0.f;
@@ -652,29 +668,32 @@ __global__ void __launch_bounds__(kL2PF32Threads) l2p_f32(int p, int K, const in
           cim[m] = a * r1im[m] - c * r2im[m];
         }
         const int idx = n * (n + 1) / 2 + m;
-        const float2 cf = lds2(Cphi + idx);
-        fn = fmaf(cf.x, cre[m], fmaf(-cf.y, cim[m], fn));
         if (DER) {
-          const float2 cz = lds2(Cz + idx), cp = lds2(Cp + idx), cmm = lds2(Cm + idx);
-          zn = fmaf(cz.x, cre[m], fmaf(-cz.y, cim[m], zn));
-          pr = fmaf(cp.x, cre[m], fmaf(-cp.y, cim[m], pr));
-          pi = fmaf(cp.x, cim[m], fmaf(cp.y, cre[m], pi));
-          mr = fmaf(cmm.x, cre[m], fmaf(-cmm.y, cim[m], mr));
-          mi = fmaf(cmm.x, cim[m], fmaf(cmm.y, cre[m], mi));
+          const float4 a = CA[idx], bq = CB[idx];
+          const float2 cc = CC[idx];
+          const float2 re2 = make_float2(cre[m], cre[m]), im2 = make_float2(cim[m], cim[m]);
+          fz = __ffma2_rn(make_float2(a.x, a.y), re2, __ffma2_rn(make_float2(a.z, a.w), im2, fz));
+          pmr = __ffma2_rn(make_float2(bq.x, bq.y), re2, __ffma2_rn(make_float2(bq.z, bq.w), im2, pmr));
+          pmi = __ffma2_rn(make_float2(bq.x, bq.y), im2, __ffma2_rn(cc, re2, pmi));
           if (m == 1) {  // Cs[n] * conj(S_n^1)
             const float cs = lds1(Cs + n);
-            mr = fmaf(cs, cre[m], mr);
-            mi = fmaf(-cs, cim[m], mi);
+            pmr.y = fmaf(cs, cre[m], pmr.y);
+            pmi.y = fmaf(-cs, cim[m], pmi.y);
           }
+        } else {
+          const float2 cf = lds2(Cphi + idx);
+          fn = fmaf(cf.x, cre[m], fmaf(-cf.y, cim[m], fn));
         }
       }
-      F += (double)fn;
       if (DER) {
-        dzr += (double)zn;
-        dpr += (double)pr;
-        dpi += (double)pi;
-        dmr += (double)mr;
-        dmi += (double)mi;
+        F += (double)fz.x;
+        dzr += (double)fz.y;
+        dpr += (double)pmr.x;
+        dpi += (double)pmi.x;
+        dmr += (double)pmr.y;
+        dmi += (double)pmi.y;
+      } else {
+        F += (double)fn;
       }
 #pragma unroll
       for (int m = 0; m <= P; m++) {

@@ -287,6 +287,11 @@ def test_autotune_order_meets_the_tolerance(ob):
     vd, _ = pl.direct(q, 20000, 21000)
     pl.close()
     assert rel(v[20000:21000], vd) < 2e-6
+    # a tolerance no order in the range reaches: the last order, its error reported
+    p2, _, err2, _ = ob.autotune_order(t, t, 1e-14, p_lo=4, p_hi=5, **kw)
+    assert p2 == 5 and err2 > 1e-14
+    with pytest.raises(ob.FMMError):
+        ob.autotune_order(t, t, 1e-6, p_lo=8, p_hi=4, **kw)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
