@@ -56,7 +56,12 @@ constexpr int kStageBytes = 2 * kAHalf;     // hi and lo (32 KB)
 constexpr int kBarBytes = 256;
 constexpr int kTmemCols = 512;
 constexpr int kAccStride = 256;             // accumulator b starts at tensor-memory column 256 b
-constexpr unsigned kSpinLimit = 1u << 22;   // bounded waits
+// Bounded waits: each try_wait may suspend the thread for up to kSuspendNs
+// (it resumes as soon as the phase completes), so a waiting warp polls the
+// barrier rarely instead of keeping the load/store pipe busy; kSpinLimit
+// tries bound a wait to a few seconds.
+constexpr unsigned kSpinLimit = 1u << 18;
+constexpr unsigned kSuspendNs = 16384;
 
 // NKB K-blocks of 64 inputs (K <= 64 NKB); operators of up to kNMax output
 // rows; the input ring takes what the resident operator leaves.
@@ -105,10 +110,10 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(a), "r"(parity)
+        : "r"(a), "r"(parity), "n"(kSuspendNs)
         : "memory");
     if (done) return true;
   }
