@@ -720,7 +720,7 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
   FMMB_CUDA(time_mark(pl, pl->ev[4], m));
   FMMB_CUDA(cudaMemsetAsync(pl->L.get(), 0, (size_t)pl->tot_i * 2 * K * sizeof(double), m));
   pairs_run(*pl->h_m2l, pl->M.get(), pl->L.get(), 1, 3);
-  for (int lev = 3; lev <= lmax; lev++) pairs_run(*pl->l2l_pairs[lev], pl->L.get(), pl->L.get(), 0, 4);
+  for (int lev = 3; lev <= lmax; lev++) pairs_run(*pl->l2l_pairs[lev], pl->L.get(), pl->L.get(), 1, 4);
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);
@@ -891,8 +891,8 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     }
   }
   near_field(p2p_split, pl->p2p_nwork, true);
-  for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each)
-    pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 0, 4);
+  for (int lev = 3; lev <= lmax; lev++)  // children at lev from their parent (one pair each, added by one atomic)
+    pairs_run(*pl->l2l_pairs[lev], pl->d_l2l_t.get(), pl->L.get(), pl->L.get(), 1, 4);
   FMMB_CUDA(time_mark(pl, pl->ev[5], m));
   {
     PhaseTimer tm(pl, 5, m);

@@ -594,9 +594,12 @@ namespace {
 // Box-pair translations (M2M, L2L, and every dense translation of the
 // Helmholtz-family kernels) in FP64: a tile holds up to 32 pairs sharing one
 // operator T, and  out[dst[p]][r] (+)= sum_c T[r][c] in[src[p]][c]  (added
-// atomically when an output row receives several pairs: M2M, M2L).  Two
-// kernels: operators that fit in shared memory are staged whole (one bulk
-// copy per block); larger ones run as grouped GEMMs on the FP64 tensor cores.
+// atomically when an output row receives several pairs: M2M, M2L; L2L adds
+// atomically too, although each of its output rows receives one pair: the
+// single atomic addition gives the value of a read-modify-write without the
+// warp waiting for the read).  Two kernels: operators that fit in shared
+// memory are staged whole (one bulk copy per block); larger ones run as
+// grouped GEMMs on the FP64 tensor cores.
 constexpr int kGN = 32;  // pairs per tile (at most)
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -621,8 +624,8 @@ __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int byt
 // Thread t takes row pair t % 64 and pair group t / 64.  The transposed operator
 // (opT[op][c][r], row stride KP = K rounded up to even) is first brought into
 // shared memory with one bulk copy (STAGED; the launcher takes this kernel
-// only when the operator fits).  Outputs are added (atomically when an output
-// row receives several pairs, M2M).
+// only when the operator fits).  Outputs are added, atomically when the
+// launch asks for it.
 template <int TP, bool STAGED>
 __global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
   extern __shared__ __align__(16) double dsm[];
@@ -780,9 +783,9 @@ __global__ void __launch_bounds__(kDT) pairs_dmma_f64(PairArgs P) {
       cp_async16(smem_addr(As + (st * kDK + c) * kDAs + rr), ok ? T + (size_t)col * KP + row : T, ok ? 16 : 0);
     }
 #pragma unroll
-    for (int i = 0; i < kDK * kDN / kDT; i++) {  // inputs: 8 bytes each
+    for (int i = 0; i < kDK * kDN / kDT; i++) {  // inputs: 8 bytes each, a pair's kDK columns from adjacent lanes
       const int e = (int)threadIdx.x + i * kDT;
-      const int pi = e % kDN, c = e / kDN;
+      const int pi = e / kDK, c = e % kDK;
       const int sj = ssrc[pi], col = k0 + c;
       const bool ok = sj >= 0 && col < K;
       cp_async8(smem_addr(Xs + (st * kDK + c) * kDXs + pi), ok ? P.xin + (size_t)sj * K + col : P.xin, ok ? 8 : 0);
