@@ -71,9 +71,9 @@ class FMMFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, q, x_t, x_s, op):
         qd = q.detach().to(torch.float32).contiguous()
-        pot = torch.zeros(op.ni, dtype=torch.float64, device=q.device)
+        pot = torch.empty(op.ni, dtype=torch.float64, device=q.device)  # every entry is written
         want_field = x_t.requires_grad
-        grad = torch.zeros(3 * op.ni, dtype=torch.float64, device=q.device) if want_field else None
+        grad = torch.empty(3 * op.ni, dtype=torch.float64, device=q.device) if want_field else None
         op.plan.evaluate(qd, pot, grad, f64=True)
         ctx.op = op
         ctx.save_for_backward(qd)

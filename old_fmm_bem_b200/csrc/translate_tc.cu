@@ -528,13 +528,15 @@ __global__ void reduce_pairs(int nrow, const int* __restrict__ rows, const int* 
       a[c][3] += v.w;
     }
   }
+  // each output row has one warp: its single atomic addition is the value of
+  // a read-modify-write, without the warp waiting for the read
   double* o = out + (size_t)rows[w] * K;
 #pragma unroll
   for (int c = 0; c < 2; c++)
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const int k = 128 * c + 4 * lane + u;
-      if (k < K) o[k] += a[c][u];
+      if (k < K) atomicAdd(o + k, a[c][u]);
     }
 }
 
