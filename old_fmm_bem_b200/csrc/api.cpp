@@ -230,6 +230,9 @@ int fmmb_plan_destroy(fmmb_plan* pl) {
   if (pl->st.fork) cudaEventDestroy(pl->st.fork);
   if (pl->st.join) cudaEventDestroy(pl->st.join);
   if (pl->st.near_done) cudaEventDestroy(pl->st.near_done);
+  if (pl->st.copy) cudaStreamDestroy(pl->st.copy);
+  for (auto& e : pl->st.copy_ev)
+    if (e) cudaEventDestroy(e);
   for (auto& e : pl->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : pl->evp)
@@ -1453,34 +1456,59 @@ int fmmb_adjoint_f64(fmmb_plan* pl, const float* q, const float* w, const double
     double* os = fs + 3 * (size_t)nj;
     double* ft = os + 3 * (size_t)nj;
     double* ot = ft + 3 * (size_t)ni;
+    // host copies that need not wait for the transposed matvec go on a copy
+    // stream beside it: dL/dx_t (it needs only w and the forward field) to the
+    // host, and q to the device
+    const bool host_q = dxs && !is_device_ptr(q), host_dxt = dxt && !is_device_ptr(dxt);
+    cudaStream_t cs = m;
+    if (host_q || host_dxt) {
+      if (!pl->st.copy) {
+        FMMB_CUDA(cudaStreamCreateWithFlags(&pl->st.copy, cudaStreamNonBlocking));
+        for (auto& e : pl->st.copy_ev) FMMB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      }
+      cs = pl->st.copy;
+      FMMB_CUDA(cudaEventRecord(pl->st.copy_ev[0], m));  // the plan's earlier work on its buffers is done
+      FMMB_CUDA(cudaStreamWaitEvent(cs, pl->st.copy_ev[0], 0));
+    }
     // w (ni nrhs) and q (nj) staged once when they are host arrays
     const float* wd = to_device(w, (size_t)ni * pl->cfg.nrhs, pl->adj_ws, m);
-    if (dq || dxs) {
-      if (is_device_ptr(dq)) adj = dq;
-      const int rc = fmmb_evaluate_transpose_f64(pl, wd, adj, dxs ? fs : nullptr);
-      if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
-      if (dq && adj != dq) FMMB_CUDA(cudaMemcpyAsync(dq, adj, nadj * sizeof(double), cudaMemcpyDeviceToHost, m));
-      if (dxs) {  // dL/dx_s = q * grad(psi)(x_s)
-        const float* qd = to_device(q, nj, pl->adj_qs, m);
-        if (is_device_ptr(dxs)) os = dxs;
-        launch_weight_field(nj, qd, fs, os, m);
-        if (os != dxs) FMMB_CUDA(cudaMemcpyAsync(dxs, os, 3 * (size_t)nj * sizeof(double), cudaMemcpyDeviceToHost, m));
-      }
-    }
+    const float* qd = dxs ? to_device(q, nj, pl->adj_qs, cs) : nullptr;
     if (dxt) {  // dL/dx_t = w * grad(pot)(x_t)
       const double* fd = field_t;
       if (!is_device_ptr(field_t)) {
         FMMB_CUDA(cudaMemcpyAsync(ft, field_t, 3 * (size_t)ni * sizeof(double), cudaMemcpyHostToDevice, m));
         fd = ft;
       }
-      if (is_device_ptr(dxt)) ot = dxt;
+      if (!host_dxt) ot = dxt;
       launch_weight_field(ni, wd, fd, ot, m);
-      if (ot != dxt) FMMB_CUDA(cudaMemcpyAsync(dxt, ot, 3 * (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, m));
+      if (host_dxt) {
+        FMMB_CUDA(cudaEventRecord(pl->st.copy_ev[0], m));
+        FMMB_CUDA(cudaStreamWaitEvent(cs, pl->st.copy_ev[0], 0));
+        FMMB_CUDA(cudaMemcpyAsync(dxt, ot, 3 * (size_t)ni * sizeof(double), cudaMemcpyDeviceToHost, cs));
+      }
     }
-    // host outputs are complete on return; device outputs are ordered on the plan's stream
+    if (dq || dxs) {
+      if (is_device_ptr(dq)) adj = dq;
+      const int rc = fmmb_evaluate_transpose_f64(pl, wd, adj, dxs ? fs : nullptr);
+      if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+      if (dq && adj != dq) FMMB_CUDA(cudaMemcpyAsync(dq, adj, nadj * sizeof(double), cudaMemcpyDeviceToHost, m));
+      if (dxs) {  // dL/dx_s = q * grad(psi)(x_s)
+        if (host_q) {
+          FMMB_CUDA(cudaEventRecord(pl->st.copy_ev[1], cs));
+          FMMB_CUDA(cudaStreamWaitEvent(m, pl->st.copy_ev[1], 0));
+        }
+        if (is_device_ptr(dxs)) os = dxs;
+        launch_weight_field(nj, qd, fs, os, m);
+        if (os != dxs) FMMB_CUDA(cudaMemcpyAsync(dxs, os, 3 * (size_t)nj * sizeof(double), cudaMemcpyDeviceToHost, m));
+      }
+    }
+    // host outputs are complete on return; device outputs are ordered on the
+    // plan's stream (the copy stream carries host-side work only)
     if (!is_device_ptr(w) || (q && !is_device_ptr(q)) || (dq && !is_device_ptr(dq)) || (dxt && !is_device_ptr(dxt)) ||
-        (dxs && !is_device_ptr(dxs)) || (field_t && !is_device_ptr(field_t)))
+        (dxs && !is_device_ptr(dxs)) || (field_t && !is_device_ptr(field_t))) {
       FMMB_CUDA(cudaStreamSynchronize(m));
+      if (cs != m) FMMB_CUDA(cudaStreamSynchronize(cs));
+    }
   });
 }
 

@@ -144,6 +144,10 @@ struct Stream2 {
   cudaStream_t cap = nullptr;  // private stream the evaluate graphs are captured on
   cudaEvent_t fork = nullptr, join = nullptr;
   cudaEvent_t near_done = nullptr;  // the all-right-hand-side near field finished
+  // host copies that overlap the main stream's work (fmmb_adjoint_f64):
+  // a stream made on first use, and its two ordering events
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copy_ev[2] = {nullptr, nullptr};
 };
 
 }  // namespace fmmb

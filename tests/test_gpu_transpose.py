@@ -123,3 +123,41 @@ def test_position_grad_rejects_normal_kernels(ob):
     with pytest.raises(ob.FMMError):
         pl.position_grad(q, w)
     pl.close()
+
+
+@pytest.mark.parametrize("shared", [False, True])
+def test_adjoint_host_buffers(shared, ob, oracle):
+    """fmmb_adjoint_f64 with host charges, weights and outputs (its copies of
+    q to the device and of dL/dx_t to the host overlap the transposed matvec
+    on a second stream) gives the numbers of the device-buffer call, and both
+    match the direct sums; the forward field is given on the device (as the
+    forward leaves it) and on the host."""
+    xt, xs, nt, ns, q, w = _sets(60, 3200, 3200 if shared else 4100)
+    if shared:
+        xs = xt
+    ni, nj = xt.shape[1], xs.shape[1]
+    pl = ob.Plan(kernel=0, p=12, lmax=3, precision=1, semantics=1, exclude_self=True)
+    pl.set_geometry(xt, xs, bbox=(0, 0, 0, 1))
+    pot, field = pl.evaluate(q, f64=True)
+    field = np.ascontiguousarray(field, np.float64).reshape(-1)
+    _, gt = oracle.direct(xt, xs, q, neq=0, eps2=0.0, exclude_self=True)
+    aw, gs = oracle.direct(xs, xt, w, neq=0, eps2=0.0, exclude_self=True)
+    for fld in (field, torch.from_numpy(field).cuda()):
+        for _ in range(2):  # a second call reuses the copy stream and the staged buffers
+            dq, dxt, dxs = pl.adjoint(q, w, fld, want_dxs=True)
+            assert rel(dq, aw) < 2e-5
+            assert rel(dxt.reshape(3, -1), w.astype(np.float64) * gt) < 2e-5
+            assert rel(dxs.reshape(3, -1), q.astype(np.float64) * gs) < 2e-5
+    Dq = torch.zeros(nj, dtype=torch.float64, device="cuda")
+    Dt = torch.zeros(3 * ni, dtype=torch.float64, device="cuda")
+    Ds = torch.zeros(3 * nj, dtype=torch.float64, device="cuda")
+    pl.adjoint(torch.from_numpy(q).cuda(), torch.from_numpy(w).cuda(), torch.from_numpy(field).cuda(), Dq, Dt, Ds,
+               want_dxs=True)
+    torch.cuda.synchronize()
+    # (the upward pass adds children into parents with FP64 atomics in no fixed
+    # order, and an ulp of a multipole can move a rounding of the FP32 tensor-core
+    # M2L: runs agree to ~1e-10, as the position-gradient test allows)
+    assert rel(Dq.cpu().numpy(), dq) < 1e-9
+    assert rel(Dt.cpu().numpy(), dxt) < 1e-9
+    assert rel(Ds.cpu().numpy(), dxs) < 1e-9
+    pl.close()
