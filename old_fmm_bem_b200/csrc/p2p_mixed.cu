@@ -3,10 +3,10 @@
 // Same sums as the reference's P2P kernels (kernel/G_p2p.cxx:12-37,
 // kernel/Gni_p2p.cxx:12-28, kernel/Gnj_p2p.cxx:12-28) over the 27-slot
 // neighbour lists of the GPU tree.  Pair arithmetic is FP32 (hardware rsqrt);
-// each lane sums up to 64 sources at a time in FP32 (two lanes of 32, added
+// each lane sums up to 128 sources at a time in FP32 (two lanes of 64, added
 // before the conversion) and promotes every partial sum into FP64
 // accumulators, so the accumulated rounding stays at the FP32 level of one
-// 64-term sum whatever the number of sources.
+// 128-term sum whatever the number of sources.
 //
 // Layout: one block of 4 warps per work item, up to 128 targets of one
 // target leaf (a leaf of more targets is several items, so that the dense
@@ -240,7 +240,7 @@ __device__ __forceinline__ void tile_runs(const Smem<KER>& S, int c0, int c1, in
     for (int t = 0; t < NT; t++)
 #pragma unroll
       for (int c = 0; c < NC; c++) acc[t][c] = make_float2(0.f, 0.f);
-    for (int i = 0; i < 8 && r < rend; i++, r += m) {
+    for (int i = 0; i < 16 && r < rend; i++, r += m) {  // 16 runs: 64 sources in each lane's two sums
       const int pb = ((r * 32 - c0) >> 1) + s;
       if (EXCL && r * 32 < self_end)
         run16<KER, true, NT>(S, pb, tg, e2, acc);
