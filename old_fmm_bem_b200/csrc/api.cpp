@@ -713,7 +713,6 @@ void run_one_helm(fmmb_plan* pl, const float* qs) {
     a.ostride = (size_t)4 * K * K;
     a.xin = xin;
     a.out = out;
-    a.err = pl->d_err.get();
     launch_translate_pairs_f64(a, m);
   };
   // parents are accumulated from their children, level by level
@@ -847,7 +846,6 @@ void run_one(fmmb_plan* pl, const float* qs, bool want_grad) {
     a.ostride = pair_op_stride(K);
     a.xin = xin;
     a.out = out;
-    a.err = pl->d_err.get();
     launch_translate_pairs_f64(a, m);
   };
   for (int lev = lmax - 1; lev >= 2; lev--)  // parents at lev from their children (several per parent)

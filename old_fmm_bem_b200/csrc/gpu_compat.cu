@@ -393,7 +393,6 @@ int morton3_decode(int code, int* c) {  // (x, y, z) of a 3-level key, bit order
 
 DevBuf<int> g_top, g_tsrc, g_tdst;
 DevBuf<double> g_in, g_tout;
-DevBuf<int> g_err;
 
 }  // namespace
 }  // namespace fmmb
@@ -486,8 +485,6 @@ extern "C" int fmmb_gpu_m2l(const int* nvecd, const double* rb, float* arex, flo
     if (!in.empty()) FMMB_CUDA(cudaMemcpy(g_in.get(), in.data(), in.size() * sizeof(double), cudaMemcpyHostToDevice));
     g_tout.alloc((size_t)nblock * K);
     FMMB_CUDA(cudaMemset(g_tout.get(), 0, (size_t)nblock * K * sizeof(double)));
-    g_err.alloc(1);
-    FMMB_CUDA(cudaMemset(g_err.get(), 0, sizeof(int)));
     prepare_translate_pairs_f64();
     PairArgs a{};
     a.ntile = (int)top.size();
@@ -501,13 +498,9 @@ extern "C" int fmmb_gpu_m2l(const int* nvecd, const double* rb, float* arex, flo
     a.ostride = (size_t)K * ((K + 1) & ~1);
     a.xin = g_in.get();
     a.out = g_tout.get();
-    a.err = g_err.get();
     launch_translate_pairs_f64(a, cudaStreamLegacy);
     std::vector<double> out((size_t)nblock * K);
     FMMB_CUDA(cudaMemcpy(out.data(), g_tout.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost));
-    int err = 0;
-    FMMB_CUDA(cudaMemcpy(&err, g_err.get(), sizeof(int), cudaMemcpyDeviceToHost));
-    FMMB_REQUIRE(err == 0, FMMB_ERR_CUDA, "translation operator copy timed out");
     // scaled outputs -> the reference's complex coefficients of each block
     const double r_out = *rb;  // side of the output boxes: parents (M2M), the level (M2L), children (L2L)
     for (int b = 0; b < nblock; b++) {

@@ -205,7 +205,7 @@ struct fmmb_plan {
 
   // operators on the device
   fmmb::DevBuf<double> d_fac, d_m2l;
-  fmmb::DevBuf<double> d_m2m_t, d_l2l_t;    // [8][column][row] (transposed for translate_pairs_f64)
+  fmmb::DevBuf<double> d_m2m_t, d_l2l_t;    // [8][column][row] (transposed for the FP64 pair kernel)
   fmmb::DevBuf<int> d_slot_rel, d_rel_to_op;
   fmmb::DevBuf<float> d_img_m2l;             // [sets*316][4 K-blocks][2][128*32] TF32 images (mixed)
 

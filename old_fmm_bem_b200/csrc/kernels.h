@@ -99,9 +99,8 @@ struct PairArgs {
   size_t ostride;                            // doubles per operator: K * (K rounded up to even)
   const double* xin;                         // input expansions [rows][K]
   double* out;                               // output expansions [rows][K]
-  int* err;                                  // set to 4 on a timed-out operator copy
 };
-// pairs per tile for npair pairs: enough tiles for the SMs, shared memory <= 48 KB
+// pairs per tile (the FP64 tensor-core kernel's 32)
 int pairs_f64_tile(int K, int npair, int nsm);
 // once per device, before any launch (and outside stream capture)
 void prepare_translate_pairs_f64();

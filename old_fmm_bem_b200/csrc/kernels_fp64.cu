@@ -592,14 +592,13 @@ void launch_finalize_f64(int n, const int* perm, const double* pn, const double*
 namespace {
 
 // Box-pair translations (M2M, L2L, and every dense translation of the
-// Helmholtz-family kernels) in FP64: a tile holds up to 32 pairs sharing one
-// operator T, and  out[dst[p]][r] (+)= sum_c T[r][c] in[src[p]][c]  (added
-// atomically when an output row receives several pairs: M2M, M2L; L2L adds
-// atomically too, although each of its output rows receives one pair: the
+// Helmholtz-family kernels) in FP64 on the FP64 tensor cores: a tile holds up
+// to 32 pairs sharing one operator T, and
+//   out[dst[p]][r] (+)= sum_c T[r][c] in[src[p]][c]
+// added atomically when an output row receives several pairs (M2M, M2L) and
+// also for L2L, although each of its output rows receives one pair: the
 // single atomic addition gives the value of a read-modify-write without the
-// warp waiting for the read).  Two kernels: operators that fit in shared
-// memory are staged whole (one bulk copy per block); larger ones run as
-// grouped GEMMs on the FP64 tensor cores.
+// warp waiting for the read.
 constexpr int kGN = 32;  // pairs per tile (at most)
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -613,132 +612,6 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int by
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
-
-// Operators that fit in shared memory (K <= 160: the Laplace M2M / L2L up to
-// p = 11): a block takes a tile of TP pairs sharing one operator, stages their
-// input expansions in
-// shared memory (transposed, [coefficient][pair], row stride TP + 2) and forms
-// the outputs with a register tile per thread of 2 consecutive output rows x
-// J = TP / 4 pairs: per operator column c one 16-byte read of
-// T[c][2rp..2rp+1] and J/2 broadcast reads of the inputs feed 2J FMAs.
-// Thread t takes row pair t % 64 and pair group t / 64.  The transposed operator
-// (opT[op][c][r], row stride KP = K rounded up to even) is first brought into
-// shared memory with one bulk copy (STAGED; the launcher takes this kernel
-// only when the operator fits).  Outputs are added, atomically when the
-// launch asks for it.
-template <int TP, bool STAGED>
-__global__ void __launch_bounds__(256) translate_pairs_f64(PairArgs P) {
-  extern __shared__ __align__(16) double dsm[];
-  __shared__ __align__(8) uint64_t bar;
-  __shared__ int ssrc[TP];
-  constexpr int S = TP + 2;
-  constexpr int J = TP / 4 < 2 ? 2 : TP / 4;  // pairs per thread
-  constexpr int G = TP / J;                    // pair groups (4: all 256 threads busy)
-  const int g = blockIdx.x, K = P.K, KP = (K + 1) & ~1;
-  const int op = P.tile_op[g];
-  const int* src = P.tile_src + (size_t)g * TP;
-  const int* dst = P.tile_dst + (size_t)g * TP;
-  double* xs = STAGED ? dsm + P.ostride : dsm;
-  const double* T = P.opT + (size_t)op * P.ostride;
-  if (STAGED && threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bar)));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
-                 "r"((uint32_t)(P.ostride * sizeof(double)))
-                 : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dsm)),
-                 "l"(T), "r"((uint32_t)(P.ostride * sizeof(double))), "r"(smem_addr(&bar))
-                 : "memory");
-  }
-  // input expansions of the tile: warp w copies pairs w, w+8, ..., its lanes
-  // consecutive coefficients (coalesced), all loads of a warp issued before
-  // its stores
-  if (threadIdx.x < TP) ssrc[threadIdx.x] = src[threadIdx.x];
-  __syncthreads();
-  {
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    constexpr int kPW = (TP + 7) / 8;  // pairs per warp
-    for (int c0 = 0; c0 < K; c0 += 128) {
-      double v[kPW][4];
-#pragma unroll
-      for (int q = 0; q < kPW; q++) {
-        const int j = w + 8 * q;
-        const int sj = j < TP ? ssrc[j] : -1;
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int c = c0 + l + 32 * u;
-          v[q][u] = (sj >= 0 && c < K) ? __ldg(P.xin + (size_t)sj * K + c) : 0.0;
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < kPW; q++) {
-        const int j = w + 8 * q;
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          const int c = c0 + l + 32 * u;
-          if (j < TP && c < K) xs[c * S + j] = v[q][u];
-        }
-      }
-    }
-  }
-  __syncthreads();
-  if (STAGED) {  // bounded wait for the operator
-    bool done = false;
-    for (unsigned it = 0; it < (1u << 22) && !done; it++) {
-      uint32_t ok;
-      asm volatile(
-          "{\n\t.reg .pred p;\n\t"
-          "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-          "selp.u32 %0, 1, 0, p;\n\t}"
-          : "=r"(ok)
-          : "r"(smem_addr(&bar))
-          : "memory");
-      done = ok != 0;
-    }
-    if (!done) {
-      if (threadIdx.x == 0) atomicExch(P.err, 4);
-      return;  // the copy may still be landing: nothing below reads it
-    }
-    T = dsm;
-  }
-  const int grp = threadIdx.x >> 6, rp = threadIdx.x & 63;
-  if (grp >= G) return;
-  const double* xg = xs + grp * J;
-  for (int r0 = 2 * rp; r0 < K; r0 += 128) {
-    double a0[J], a1[J];
-#pragma unroll
-    for (int j = 0; j < J; j++) a0[j] = a1[j] = 0.0;
-#pragma unroll 4
-    for (int c = 0; c < K; c++) {
-      const double2 t = STAGED ? *reinterpret_cast<const double2*>(T + (size_t)c * KP + r0)
-                               : __ldg(reinterpret_cast<const double2*>(T + (size_t)c * KP + r0));
-      const double2* xc = reinterpret_cast<const double2*>(xg + c * S);
-#pragma unroll
-      for (int j2 = 0; j2 < J / 2; j2++) {
-        const double2 v = xc[j2];
-        a0[2 * j2] = fma(t.x, v.x, a0[2 * j2]);
-        a0[2 * j2 + 1] = fma(t.x, v.y, a0[2 * j2 + 1]);
-        a1[2 * j2] = fma(t.y, v.x, a1[2 * j2]);
-        a1[2 * j2 + 1] = fma(t.y, v.y, a1[2 * j2 + 1]);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < J; j++) {
-      const int d = dst[grp * J + j];
-      if (d < 0) continue;
-      double* o = P.out + (size_t)d * K + r0;
-      if (P.atomic) {
-        atomicAdd(o, a0[j]);
-        if (r0 + 1 < K) atomicAdd(o + 1, a1[j]);
-      } else {
-        o[0] += a0[j];
-        if (r0 + 1 < K) o[1] += a1[j];
-      }
-    }
-  }
-}
-
 
 // Grouped GEMM on the FP64 tensor cores (mma.sync m8n8k4 .f64, 256 FMA per
 // warp instruction): a block of 8 warps computes 128 output rows x the
@@ -800,23 +673,27 @@ __global__ void __launch_bounds__(kDT) pairs_dmma_f64(PairArgs P) {
   for (int i = 0; i < 4; i++)
 #pragma unroll
     for (int j = 0; j < 2; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+  // this block's column chunks [kc0, kc1): blockIdx.z of gridDim.z parts of
+  // the columns (the parts' sums are added atomically)
   const int nk = (K + kDK - 1) / kDK;
+  const int kc0 = (int)(blockIdx.z * (unsigned)nk / gridDim.z), kc1 = (int)((blockIdx.z + 1) * (unsigned)nk / gridDim.z);
+  const int nkb = kc1 - kc0;
 #pragma unroll
   for (int st = 0; st < kDS - 1; st++) {
-    if (st < nk)
-      issue(st, st);
+    if (st < nkb)
+      issue(kc0 + st, st);
     else
       asm volatile("cp.async.commit_group;" ::: "memory");
   }
-  for (int kc = 0; kc < nk; kc++) {
-    if (kc + kDS - 1 < nk)
-      issue(kc + kDS - 1, (kc + kDS - 1) % kDS);
+  for (int kb = 0; kb < nkb; kb++) {
+    if (kb + kDS - 1 < nkb)
+      issue(kc0 + kb + kDS - 1, (kb + kDS - 1) % kDS);
     else
       asm volatile("cp.async.commit_group;" ::: "memory");
     asm volatile("cp.async.wait_group %0;" ::"n"(kDS - 1) : "memory");
     __syncthreads();
-    const double* a = As + (kc % kDS) * kDK * kDAs + wr + gq;
-    const double* x = Xs + (kc % kDS) * kDK * kDXs + wp + gq;
+    const double* a = As + (kb % kDS) * kDK * kDAs + wr + gq;
+    const double* x = Xs + (kb % kDS) * kDK * kDXs + wp + gq;
 #pragma unroll
     for (int k4 = 0; k4 < kDK; k4 += 4) {
       const int kr = k4 + tq;  // the k-row of this lane's A column / B row
@@ -844,7 +721,7 @@ __global__ void __launch_bounds__(kDT) pairs_dmma_f64(PairArgs P) {
         const int r = r0 + wr + 8 * i + gq;
         if (r >= K) continue;
         double* o = P.out + (size_t)d * K + r;
-        if (P.atomic)
+        if (P.atomic || gridDim.z > 1)
           atomicAdd(o, acc[i][j][h]);
         else
           *o += acc[i][j][h];
@@ -853,53 +730,31 @@ __global__ void __launch_bounds__(kDT) pairs_dmma_f64(PairArgs P) {
 }
 }  // namespace
 
-namespace {
-size_t pairs_smem(int K, int tp, size_t ostride) { return ostride * sizeof(double) + (size_t)K * (tp + 2) * sizeof(double); }
-constexpr size_t kPairsSmemMax = 224 * 1024;  // below the 227 KB opt-in limit, which includes static shared memory
-bool staged_fits(int K) { return pairs_smem(K, 8, (size_t)K * ((K + 1) & ~1)) <= kPairsSmemMax && K <= 160; }
-
-template <int TP>
-void launch_tp(const PairArgs& a, cudaStream_t st) {
-  translate_pairs_f64<TP, true><<<a.ntile, 256, pairs_smem(a.K, TP, a.ostride), st>>>(a);
-}
-
-template <int TP>
-void prepare_tp() {
-  FMMB_CUDA(cudaFuncSetAttribute(translate_pairs_f64<TP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kPairsSmemMax));
-}
-}  // namespace
-
-// Staged kernel (small K): tiles of 8-32 pairs, enough tiles for the SMs and
-// the inputs within 48 KB; tensor-core GEMM (larger K): 32 pairs.
-int pairs_f64_tile(int K, int npair, int nsm) {
-  if (!staged_fits(K)) return kGN;
-  int tp = 32;
-  while (tp > 8 && ((long long)npair + tp - 1) / tp < nsm) tp /= 2;
-  while (tp > 8 && (size_t)K * (tp + 2) * sizeof(double) > 48 * 1024) tp /= 2;
-  return tp;
-}
+// One operator's tiles of up to 32 pairs (the tensor-core kernel's block
+// width); a tile of fewer pairs leaves the rest of the block's columns idle.
+int pairs_f64_tile(int, int, int) { return kGN; }
 
 void prepare_translate_pairs_f64() {
   FMMB_CUDA(cudaFuncSetAttribute(pairs_dmma_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDSmem));
-  prepare_tp<32>();
-  prepare_tp<16>();
-  prepare_tp<8>();
 }
 
 void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
   if (a.ntile <= 0) return;
   FMMB_REQUIRE(a.tp >= 1 && a.tp <= kGN, FMMB_ERR_ARG, "pair tile larger than 32");
-  if (staged_fits(a.K) && (a.tp == 8 || a.tp == 16 || a.tp == 32)) {
-    switch (a.tp) {
-      case 32: launch_tp<32>(a, st); break;
-      case 16: launch_tp<16>(a, st); break;
-      default: launch_tp<8>(a, st); break;
-    }
-  } else {
-    const dim3 grid((unsigned)a.ntile, (unsigned)((a.K + kDM - 1) / kDM));
-    pairs_dmma_f64<<<grid, kDT, kDSmem, st>>>(a);
+  // the columns split into parts (added atomically) when the tiles alone give
+  // fewer than two blocks per SM: the small levels' launches are one block's
+  // chain of column chunks long, so a part of the chain per block shortens them
+  const int nrb = (a.K + kDM - 1) / kDM, nk = (a.K + kDK - 1) / kDK;
+  int kz = 1;
+  if (a.atomic) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long blocks = (long long)a.ntile * nrb;
+    while (kz < 8 && 2 * kz <= nk && blocks * kz < 2LL * nsm) kz *= 2;
   }
+  const dim3 grid((unsigned)a.ntile, (unsigned)nrb, (unsigned)kz);
+  pairs_dmma_f64<<<grid, kDT, kDSmem, st>>>(a);
   FMMB_CHECK_LAUNCH();
 }
 
