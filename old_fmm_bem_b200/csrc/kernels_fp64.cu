@@ -742,8 +742,9 @@ void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
   if (a.ntile <= 0) return;
   FMMB_REQUIRE(a.tp >= 1 && a.tp <= kGN, FMMB_ERR_ARG, "pair tile larger than 32");
   // the columns split into parts (added atomically) when the tiles alone give
-  // fewer than two blocks per SM: the small levels' launches are one block's
+  // fewer than four blocks per SM: the small levels' launches are one block's
   // chain of column chunks long, so a part of the chain per block shortens them
+  // (a target of 2 or 8 blocks per SM ran the surface matvec 2 % / 1 % slower)
   const int nrb = (a.K + kDM - 1) / kDM, nk = (a.K + kDK - 1) / kDK;
   int kz = 1;
   if (a.atomic) {
@@ -751,7 +752,7 @@ void launch_translate_pairs_f64(const PairArgs& a, cudaStream_t st) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const long long blocks = (long long)a.ntile * nrb;
-    while (kz < 8 && 2 * kz <= nk && blocks * kz < 2LL * nsm) kz *= 2;
+    while (kz < 8 && 2 * kz <= nk && blocks * kz < 4LL * nsm) kz *= 2;
   }
   const dim3 grid((unsigned)a.ntile, (unsigned)nrb, (unsigned)kz);
   pairs_dmma_f64<<<grid, kDT, kDSmem, st>>>(a);
