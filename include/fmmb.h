@@ -159,9 +159,12 @@ FMMB_API int fmmb_position_grad(fmmb_plan* plan, const float* q, const float* w,
  * output of the forward fmmb_evaluate_f64 with the same q.  Any of dq, dxs,
  * dxt may be NULL (dxt needs field_t); position gradients of Gni / Gnj need
  * accurate semantics.  Costs one transposed matvec (with gradient when dxs is
- * asked for); host or device pointers.  When the targets and sources were
- * given as the same arrays the transposed matvec runs on this plan.  No
- * reference counterpart (the reference has no adjoint). */
+ * asked for); host or device pointers.  With host pointers, q's copy to the
+ * device and dxt's copy to the host run on a second stream of the plan (made
+ * on first use) while the transposed matvec runs; host outputs are complete
+ * on return.  When the targets and sources were given as the same arrays the
+ * transposed matvec runs on this plan.  No reference counterpart (the
+ * reference has no adjoint). */
 FMMB_API int fmmb_adjoint_f64(fmmb_plan* plan, const float* q, const float* w, const double* field_t, double* dq,
                               double* dxt, double* dxs);
 
