@@ -83,7 +83,9 @@ constexpr int ncomp() {
 
 // Negated positions of sources j, j + 1 (even j) of the staged list, packed
 // for the two-lane FP32 instructions: (-x_j, -x_j+1, -y_j, -y_j+1) and
-// (-z_j, -z_j+1); charges (q_j, q_j+1) (G, Gni) or q n (Gnj).  Pair values
+// (-z_j, -z_j+1, q_j, q_j+1) (G, Gni; for Gnj the charge slots hold
+// q_j n_z, q_j+1 n_z and M the x, y components of q n): one 16-byte read per
+// quantity pair.  Pair values
 // are bit-identical to the scalar forms (x_i + (-x_j) = x_i - x_j, the same
 // operation order after it); each lane keeps two FP32 partial sums, over the
 // even and the odd sources.
@@ -92,10 +94,8 @@ struct Smem {
   static constexpr int NC = ncomp<KER>();
   static constexpr int NP = kCap / 2;
   float4 A[NP];
-  float2 B[NP];
-  float2 Q[base(KER) == FMMB_LAPLACE_GNJ ? 1 : NP];
+  float4 BQ[NP];                                      // (-z j, j+1, q j, j+1) or (-z j, j+1, qn_z j, j+1)
   float4 M[base(KER) == FMMB_LAPLACE_GNJ ? NP : 1];   // (qn_x j, j+1, qn_y j, j+1)
-  float2 MZ[base(KER) == FMMB_LAPLACE_GNJ ? NP : 1];  // (qn_z j, j+1)
   double red[kWarps][kMaxNT][NC][kG];           // team partial sums
   int2 seg[32];                                 // (first source, count), own leaf first
   int vst[32];                                  // virtual start of each segment, then INT_MAX
@@ -116,16 +116,16 @@ __device__ __forceinline__ void run16(const Smem<KER>& S, int pb, const Tgt (&tg
 #pragma unroll (EXCL ? 1 : 4)
   for (int u = 0; u < 4; u++) {
     const int pi = pb + 4 * u;
-    const float4 a = S.A[pi];
-    const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w), sz = S.B[pi];
+    const float4 a = S.A[pi], bq = S.BQ[pi];
+    const float2 sx = make_float2(a.x, a.y), sy = make_float2(a.z, a.w), sz = make_float2(bq.x, bq.y);
     float2 q2 = make_float2(0.f, 0.f), mx = q2, my = q2, mz = q2;
     if (base(KER) == FMMB_LAPLACE_GNJ) {
       const float4 m = S.M[pi];
       mx = make_float2(m.x, m.y);
       my = make_float2(m.z, m.w);
-      mz = S.MZ[pi];
+      mz = make_float2(bq.z, bq.w);
     } else {
-      q2 = S.Q[pi];
+      q2 = make_float2(bq.z, bq.w);
     }
 #pragma unroll
     for (int t = 0; t < NT; t++) {
@@ -211,13 +211,12 @@ __device__ void stage(Smem<KER>& S, int c0, int c1, const float4* __restrict__ s
         const float4 x0 = x[2 * h], x1 = x[2 * h + 1];
         const float q0 = q[2 * h], q1 = q[2 * h + 1];
         S.A[pi] = make_float4(-x0.x, -x1.x, -x0.y, -x1.y);
-        S.B[pi] = make_float2(-x0.z, -x1.z);
         if (base(KER) == FMMB_LAPLACE_GNJ) {
           const float4 n0 = n[2 * h], n1 = n[2 * h + 1];
           S.M[pi] = make_float4(q0 * n0.x, q1 * n1.x, q0 * n0.y, q1 * n1.y);
-          S.MZ[pi] = make_float2(q0 * n0.z, q1 * n1.z);
+          S.BQ[pi] = make_float4(-x0.z, -x1.z, q0 * n0.z, q1 * n1.z);
         } else {
-          S.Q[pi] = make_float2(q0, q1);
+          S.BQ[pi] = make_float4(-x0.z, -x1.z, q0, q1);
         }
       }
     }
