@@ -184,8 +184,11 @@ def test_serial_phases_give_the_same_results(ob):
         pl.set_overlap(True)
         c = pl.evaluate(q, f64=True)[0]
         pl.close()
-        # the same sums (FP64 atomics in some translations: rounding order only)
-        assert rel(b, a) < 1e-13 and rel(c, a) < 1e-13
+        # the same sums (FP64 atomics in some translations: rounding order only;
+        # in the mixed form an ulp of a multipole can move a rounding of its
+        # FP16 split for the M2L, ~1e-10 at most)
+        tol = 1e-13 if prec == 0 else 1e-9
+        assert rel(b, a) < tol and rel(c, a) < tol
         assert ph["p2p"] > 0 and ph["m2l"] > 0
 
 
@@ -266,7 +269,9 @@ def test_laplace_g_without_gradient(precision, ob):
     for _ in range(2):  # the first call captures the no-gradient graph, the second replays it
         rc = ob.load().fmmb_evaluate_f64(pl._h, q.ctypes.data, pot.ctypes.data, None)
         assert rc == 0, ob.load().fmmb_last_error()
-        assert rel(pot, v) < 1e-13  # the same sums (FP64 atomics in the M2M: rounding order only)
+        # the same sums (FP64 atomics in the M2M: rounding order only; in the
+        # mixed form an ulp of a multipole can move a rounding of its FP16 split)
+        assert rel(pot, v) < (1e-13 if precision == 0 else 1e-9)
     pl.close()
 
 
