@@ -1488,7 +1488,11 @@ int fmmb_adjoint_f64(fmmb_plan* pl, const float* q, const float* w, const double
     if (dq || dxs) {
       if (is_device_ptr(dq)) adj = dq;
       const int rc = fmmb_evaluate_transpose_f64(pl, wd, adj, dxs ? fs : nullptr);
-      if (rc != FMMB_OK) throw Error{rc, std::string(fmmb_last_error())};
+      if (rc != FMMB_OK) {
+        const std::string msg(fmmb_last_error());
+        if (cs != m) cudaStreamSynchronize(cs);  // no copy into the caller's memory after the error returns
+        throw Error{rc, msg};
+      }
       if (dq && adj != dq) FMMB_CUDA(cudaMemcpyAsync(dq, adj, nadj * sizeof(double), cudaMemcpyDeviceToHost, m));
       if (dxs) {  // dL/dx_s = q * grad(psi)(x_s)
         if (host_q) {
